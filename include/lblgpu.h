@@ -1,0 +1,241 @@
+/*
+ * lblgpu.h -- C ABI of the B200 line-by-line layer optical-depth and
+ * radiance-merge library.
+ *
+ * The entry points replace the per-layer calls that LBLRTM's layer loop
+ * makes (src/lblrtm.f90 XLAYER, standard loop :3640-3657):
+ *
+ *   CALL OPDPTH (MPTS)                      -> lbl_layer_od
+ *   CALL XMERGE (NPTS,LFILE,MFILE,JPATHL)   -> lbl_merge_layer
+ *
+ * plus whole-profile and many-profile forms of the same loop
+ * (lbl_forward, lbl_forward_batch) and the radiance Jacobians
+ * (lbl_jacobian), which the reference obtains from its IMRG=40-43
+ * analytic-derivative workflow (src/lblrtm.f90:2855-3067).
+ *
+ * The reference passes everything through COMMON blocks (/FILHDR/,
+ * /MANE/, /CNTSCL/) and disk files (TAPE3 lines, TAPE10 layer optical
+ * depth, TAPE11/12 accumulated radiance).  Here the same quantities are
+ * passed as plain structs and caller-owned buffers; every function returns
+ * an lbl_status and never exits the process (the reference STOPs).
+ *
+ * Pointers marked "host or device" may point to either memory; the library
+ * inspects them and copies as needed.  All functions are thread-safe on
+ * distinct contexts; one context must not be used from two threads at once.
+ */
+#ifndef LBLGPU_H
+#define LBLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBL_WKDIM 60      /* /FILHDR/ WK(60), src/oprop.f90:107 */
+#define LBL_MXMOL 47      /* MXMOL, src/lblparams.f90:28 */
+
+typedef enum lbl_status {
+  LBL_OK = 0,
+  LBL_E_ARG = 1,          /* bad argument (NULL pointer, size, flag value) */
+  LBL_E_UNSORTED = 2,     /* line centres not ascending (RDLIN assumes it) */
+  LBL_E_NREC = 3,         /* a TAPE3 panel holds more than 250 lines
+                             ('RDLIN; NREC GT LIMIN', src/oprop.f90:763) */
+  LBL_E_ITYPE = 4,        /* layer DV ratio not allowed by the merge
+                             (' RADMRG; ITYPE LT 0 ', src/xmerge.f90:2741) */
+  LBL_E_CUDA = 5,         /* a CUDA runtime call failed */
+  LBL_E_NOMEM = 6,        /* device or host allocation failed */
+  LBL_E_RANGE = 7,        /* input outside the supported range (e.g. TIPS
+                             temperature outside 70-3000 K, DV rule TYPE>2.5,
+                             'PATH; ISTOP EQ 1' src/lblrtm.f90:5557) */
+  LBL_E_NOTREADY = 8,     /* lines or tables not uploaded yet */
+  LBL_E_CONVERGE = 9,     /* far-wing rejection fixpoint did not settle */
+  LBL_E_FORMAT = 10,      /* malformed TAPE3 file */
+  LBL_E_NODEVICE = 11     /* no CUDA device / library built without one */
+} lbl_status;
+
+/* Arithmetic of the line-shape, far-wing and merge kernels. */
+typedef enum lbl_precision {
+  LBL_PREC_FP64 = 0,      /* plain FP64 throughout: the drop-in form */
+  LBL_PREC_SPLIT = 1      /* FP32 line shapes, far wing and merge; FP64 grid
+                             positions, line-centre offsets and compensated
+                             optical-depth sums */
+} lbl_precision;
+
+/* Run-level control: TAPE5 records 1.2, 1.2a, 1.3, 1.4 (subset on the hot
+ * path).  Field names follow the reference variables. */
+typedef struct lbl_run {
+  int32_t ihirac;   /* 1: Voigt line shape (HIRAC1); the only value supported */
+  int32_t ilblf4;   /* 0: no far wing; 1: F4 far wing with BOUND4=25 cm-1;
+                       2: as 1 but BOUND4=5 cm-1 when PAVE<=0.5 mb
+                       (src/lblrtm.f90:6246-6247) */
+  int32_t icntnm;   /* 0: no continuum; 1: MT_CKD-style H2O self+foreign
+                       (table from lbl_mtckd_upload) */
+  int32_t iemit;    /* 0: optical depth only (ABINIT/ABSMRG);
+                       1: radiance and transmittance (EMINIT/RADMRG) */
+  int32_t ipathl;   /* 1: upwelling (looking down, surface first); only 1 */
+  int32_t jrad;     /* initial JRAD: 1 (IRAD=0) or -1 (no radiation term),
+                       src/lblrtm.f90:828-833 */
+  double v1, v2;    /* spectral range, cm-1 (V2-V1 <= 2020 as in TAPE5 1.3) */
+  double sample;    /* SAMPLE   (default 4)    */
+  double dvset;     /* DVSET    (default 0)    */
+  double alfal0;    /* ALFAL0   (default 0.04) */
+  double avmass;    /* AVMASS   (default 36)   */
+  double dptmin;    /* DPTMIN   (default 2e-4) */
+  double dptfac;    /* DPTFAC   (default 1e-3) */
+  double xself;     /* continuum scale factors, /CNTSCL/ (default 1) */
+  double xfrgn;
+  double tmpbnd;    /* boundary temperature TMPBND, K (record 1.4) */
+  double bndemi;    /* boundary emissivity BNDEMI(1); BNDEMI(2:3)=0 */
+} lbl_run;
+
+/* One layer: the /FILHDR/ quantities OPDPTH and XMERGE read
+ * (src/lblrtm.f90:4374-4412). */
+typedef struct lbl_layer {
+  double pave, tave;       /* layer pressure (mb) and temperature (K) */
+  double pzl, pzu;         /* lower / upper level pressure (mb) */
+  double tzl, tzu;         /* lower / upper level temperature (K) */
+  double wk[LBL_WKDIM];    /* column amounts, molec/cm2; wk[m-1] is HITRAN
+                              molecule m */
+  double wbroad;           /* broadening-gas column, molec/cm2 */
+  int32_t nmol;            /* molecules in use (<= LBL_MXMOL) */
+  int32_t itype;           /* ITYL from the DV rule (output of lbl_dv_rule) */
+  double dv;               /* layer DV, cm-1 (output of lbl_dv_rule) */
+} lbl_layer;
+
+/* TAPE3 line records in structure-of-arrays form, in file order
+ * (struct_types.f90:106-125: VNU is REAL*8, the rest REAL*4/INTEGER*4).
+ * Lines are grouped into TAPE3 panels of at most 250 records; the panel
+ * boundaries matter to the far-wing line shrinking (LINF4) and to when
+ * lines are read, so they are part of the input. */
+typedef struct lbl_lines {
+  int64_t n;
+  const double*  vnu;      /* line centre, cm-1, ascending */
+  const float*   sp;       /* strength, cm-1/(molec cm-2) at 296 K */
+  const float*   alfa;     /* air-broadened HWHM at 296 K, 1013 mb */
+  const float*   epp;      /* lower-state energy, cm-1 */
+  const int32_t* mol;      /* ISO*100 + MOL */
+  const float*   hwhms;    /* self-broadened HWHM */
+  const float*   tmpalf;   /* temperature exponent of the width */
+  const float*   pshift;   /* pressure shift, cm-1/atm */
+  const int32_t* iflg;     /* line flag; <0 records are coupling data */
+  int64_t nblock;          /* number of TAPE3 panels, 0 = consecutive 250 */
+  const int64_t* block_start; /* nblock+1 offsets into the arrays, or NULL */
+} lbl_lines;
+
+/* MT_CKD-style H2O continuum coefficient table on a uniform grid, the
+ * layout of absco-ref_wv-mt-ckd.nc read by mt_ckd_h2o_module.f90:68-174. */
+typedef struct lbl_mtckd {
+  int64_t n;
+  double v0, dv;                 /* wavenumber of entry 0 and spacing */
+  const double* self_absco_ref;  /* cm2/molec/cm-1 at ref_press/ref_temp */
+  const double* for_absco_ref;
+  const double* self_texp;
+  double ref_press, ref_temp;    /* 1013 mb, 296 K in the reference file */
+} lbl_mtckd;
+
+typedef struct lbl_ctx lbl_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Create a context on CUDA device `device`; builds the line-shape tables
+ * (SHAPEL/SHAPEG/VERFN, src/oprop.f90:1822-1991) on the device. */
+int lbl_ctx_create(int device, lbl_ctx** out);
+int lbl_ctx_destroy(lbl_ctx* ctx);
+/* Last error message of this context (empty if none). */
+const char* lbl_last_error(const lbl_ctx* ctx);
+/* Set the CUDA stream (cudaStream_t) used by later calls; NULL = default. */
+int lbl_set_stream(lbl_ctx* ctx, void* stream);
+
+/* ---- inputs ----------------------------------------------------------- */
+
+/* Copy the TAPE3 line records (host arrays) to the device, where they stay
+ * resident.  Replaces opening TAPE3 on unit LINFIL (src/lblrtm.f90:801-808)
+ * and the per-layer re-reads of RDLIN (src/oprop.f90:678).  Fails with
+ * LBL_E_UNSORTED / LBL_E_NREC on the conditions RDLIN assumes or STOPs on. */
+int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* lines);
+
+/* Read a TAPE3 file (Fortran unformatted, 4-byte record markers, the
+ * INPUT_HEADER/INPUT_BLOCK records of struct_types.f90:106-125) and upload
+ * it.  Returns the number of line records through *nlines (may be NULL). */
+int lbl_lines_load_tape3(lbl_ctx* ctx, const char* path, int64_t* nlines);
+
+/* Upload the H2O continuum coefficient table (CONTNM, contnm.f90:279-324). */
+int lbl_mtckd_upload(lbl_ctx* ctx, const lbl_mtckd* table);
+
+/* ---- host-side planning (no device work) ------------------------------ */
+
+/* The per-layer DV rule of PATH (src/lblrtm.f90:5407-5510): fills
+ * layers[l].dv and layers[l].itype for l = 0..nlay-1 in path order. */
+int lbl_dv_rule(const lbl_run* run, lbl_layer* layers, int32_t nlay);
+
+/* Number of points OPDPTH writes for a layer of spacing dv: the panels of
+ * PANEL (src/oprop.f90:1435-1451) end at the first grid point >= V2. */
+int64_t lbl_layer_npts(const lbl_run* run, double dv);
+
+/* ---- one layer: OPDPTH ------------------------------------------------ */
+
+/* Monochromatic optical depth of one layer on its own grid
+ * v_i = V1 + i*dv, i = 0..npts-1 (TAPE10 content, src/lblrtm.f90:6135).
+ * *jrad is the sticky JRAD flag (FSCDID(9)); it is read and updated as
+ * OPDPTH does (src/lblrtm.f90:6211).  od: host or device, npts doubles. */
+int lbl_layer_od(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
+                 int32_t* jrad, double* od, int64_t npts, int32_t precision);
+
+/* ---- one merge step: XMERGE ------------------------------------------ */
+
+/* Merge one layer's optical depth into the accumulated radiance and
+ * transmittance (XMERGE IEMIT=1: EMINIT for the first layer, RADMRG/RADNN
+ * after, src/xmerge.f90:25-167; IEMIT=0: ABINIT/ABSMRG).
+ *   od            layer optical depth, n_new points (host or device)
+ *   rad_in/tr_in  accumulated radiance/transmittance on the previous
+ *                 layer's grid, n_old points (ignored when first != 0)
+ *   rad_out/tr_out results on the layer grid, n_new points
+ * For IEMIT=0 rad_* carry accumulated optical depth and tr_* is unused. */
+int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
+                    int32_t first, double dv_old, const double* rad_in,
+                    const double* tr_in, int64_t n_old, const double* od,
+                    double* rad_out, double* tr_out, int64_t n_new);
+
+/* ---- whole path ------------------------------------------------------- */
+
+/* The standard layer loop (XLAYER :3640-3657) for one profile: DV rule,
+ * OPDPTH per layer, XMERGE per layer.  Outputs on the last layer's grid
+ * (lbl_layer_npts of layers[nlay-1].dv points, host or device):
+ *   rad: upwelling radiance at the top (W/(cm2 sr cm-1)), IEMIT=1, or total
+ *        optical depth, IEMIT=0;  tr: total transmittance (may be NULL).
+ * layers[].dv/itype are computed here (lbl_dv_rule) and written back. */
+int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
+                int32_t nlay, double* rad, double* tr, int64_t npts,
+                int32_t precision);
+
+/* Many independent profiles (uneven layer counts) in one call.  layers is
+ * the concatenation of all profiles' layers; nlay[p] is profile p's count.
+ * rad/tr are concatenated per profile; offsets[p] (output, nprof+1 entries)
+ * gives where profile p starts; npts_total bounds the buffers. */
+int lbl_forward_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
+                      const int32_t* nlay, int32_t nprof, double* rad,
+                      double* tr, int64_t* offsets, int64_t npts_total,
+                      int32_t precision);
+
+/* Jacobians of the top-of-atmosphere radiance of one profile with respect
+ * to each layer's temperature (K) and the log column amount of the listed
+ * molecules, computed by one forward sweep plus one reverse (adjoint) sweep
+ * through the merge and the line shapes.  Output layout:
+ *   jac[(k*nlay + l)*npts + i]  k=0: d rad_i / d T_l,
+ *                               k=1..nq: d rad_i / d ln W_{mols[k-1]},l
+ * on the last layer's grid.  rad (optional) receives the forward result. */
+int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
+                 int32_t nlay, const int32_t* mols, int32_t nq, double* rad,
+                 double* jac, int64_t npts, int32_t precision);
+
+/* Brightness temperature of a radiance spectrum (TEM, src/pltlbl.f90:1568):
+ * bt_i = RADCN2*v_i / ln(RADCN1*v_i^3/rad_i + 1).  Host arrays. */
+int lbl_brightness_temperature(const double* rad, int64_t n, double v1,
+                               double dv, double* bt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBLGPU_H */
