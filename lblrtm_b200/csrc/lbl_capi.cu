@@ -1,0 +1,763 @@
+// lbl_capi.cu -- the C ABI of include/lblgpu.h.
+//
+// A context owns the resident TAPE3 lines, the line-shape tables, the
+// continuum table and a grow-only device arena for the per-call work
+// buffers.  lbl_forward plans every layer on the host (exact FP64 panel and
+// window schedule), lays all layers' buffers out in the arena, runs the
+// optical-depth pipeline for all layers in a handful of batched launches,
+// then merges the layers bottom-up on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lblgpu.h"
+#include "lbl_kernels.cuh"
+#include "lbl_plan.h"
+
+using namespace lbl;
+
+namespace {
+
+// Grow-only device arena; sub-allocations are 256-byte aligned.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+  cudaError_t reserve(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    size_t want = std::max(bytes, cap * 3 / 2);
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&base, want);
+    if (e != cudaSuccess) return e;
+    cap = want;
+    return cudaSuccess;
+  }
+  void reset() { used = 0; }
+  template <typename T>
+  T* take(size_t n) {
+    size_t off = (used + 255) & ~size_t(255);
+    used = off + n * sizeof(T);
+    return reinterpret_cast<T*>(base + off);
+  }
+};
+
+// Pass 1 of a layout computes the size, pass 2 hands out pointers.
+struct Layout {
+  size_t bytes = 0;
+  template <typename T>
+  void add(size_t n) {
+    bytes = ((bytes + 255) & ~size_t(255)) + n * sizeof(T);
+  }
+};
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+struct lbl_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  // lines: host copies for planning, device copies for the kernels
+  std::vector<double> h_vnu;
+  std::vector<float> h_sp, h_pshift;
+  std::vector<int32_t> h_mol, h_iflg;
+  std::vector<int64_t> h_bs;
+  DevLines dl{};
+  void* line_mem = nullptr;
+  bool have_lines = false;
+  // tables
+  DevShapes sh{};
+  void* shape_mem = nullptr;
+  DevMtckd ck{};
+  void* ck_mem = nullptr;
+  bool have_ck = false;
+  Arena arena;
+  // merge buffers (ping-pong)
+  double* mbuf[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t mcap = 0;
+  // pinned staging for plans
+  std::vector<char> hstage;
+};
+
+namespace {
+
+int fail(lbl_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(ctx, LBL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// Device view of one batch of planned layers.
+struct Batch {
+  std::vector<LayerPlan> plans;
+  std::vector<LayerDev> ld;
+  Work w{};
+  LayerDev* d_ld = nullptr;
+  int32_t* d_win_layer = nullptr;
+  int32_t* d_panel_layer = nullptr;
+  int64_t* d_panel_base = nullptr;
+  int64_t* d_tile_prefix = nullptr;
+  int64_t* d_blk_base = nullptr;
+  int64_t nblk_total = 0;
+  int32_t nwin_total = 0;
+  int64_t npanel_total = 0, ntiles = 0, max_far = 0, max_r3 = 0, max_r2 = 0;
+  int64_t od_total = 0;
+};
+
+// Plan layers [0,n), lay their buffers out in the arena, upload the plans.
+int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n, int jrad_in,
+                  int* jrad_out, Batch& B) {
+  HostLines H{ctx->h_vnu.data(), ctx->h_sp.data(), ctx->h_pshift.data(), ctx->h_mol.data(),
+              ctx->h_iflg.data(), (int64_t)ctx->h_vnu.size(), ctx->h_bs.data(),
+              (int64_t)ctx->h_bs.size() - 1};
+  B.plans.resize(n);
+  int jrad = jrad_in;
+  for (int l = 0; l < n; l++) {
+    std::string e;
+    int rc = plan_layer(R, layers[l], jrad, H, &B.plans[l], &e);
+    if (rc != LBL_OK) return fail(ctx, rc, "layer " + std::to_string(l) + ": " + e);
+    jrad = B.plans[l].d.jrad;
+  }
+  if (jrad_out) *jrad_out = jrad;
+  // offsets
+  int64_t o_r1 = 0, o_r2 = 0, o_r3 = 0, o_od = 0, o_pan = 0, o_win = 0, o_far = 0, o_near = 0,
+          o_b9 = 0, o_abs = 0;
+  B.ld.resize(n);
+  std::vector<int64_t> tile_prefix(3 * n + 1, 0);
+  std::vector<int64_t> blk_base(n + 1, 0);
+  for (int l = 0; l < n; l++) {
+    LayerDev& d = B.plans[l].d;
+    d.off_r1 = o_r1;
+    d.off_r2 = o_r2;
+    d.off_r3 = o_r3;
+    d.off_od = o_od;
+    d.off_panel = o_pan;
+    d.off_win = o_win;
+    d.off_r4 = o_win * kR4Stride;
+    d.off_far = o_far;
+    d.off_shr = o_far;
+    d.off_near = o_near;
+    d.off_blk9 = o_b9;
+    d.off_abs = o_abs;
+    d.off_seg = blk_base[l];
+    blk_base[l + 1] = blk_base[l] + (d.fblk_hi - d.fblk_lo);
+    o_r1 += d.n_r1 + 1;
+    o_r2 += d.n_r2 + 1;
+    o_r3 += d.n_r3 + 1;
+    o_od += d.npts;
+    o_pan += d.npanel;
+    o_win += d.nwin;
+    const int64_t nfar = d.far_hi - d.far_lo;
+    o_far += nfar;
+    o_near += d.near_hi - d.near_lo;
+    o_b9 += nfar / 1000 + 2;
+    o_abs += (d.icntnm ? d.nptabs : 0) + 8;
+    B.max_far = std::max(B.max_far, nfar);
+    B.max_r3 = std::max(B.max_r3, d.n_r3);
+    B.max_r2 = std::max(B.max_r2, d.n_r2);
+    const int64_t ng[3] = {d.n_r1, d.n_r2, d.n_r3};
+    for (int k = 0; k < 3; k++)
+      tile_prefix[3 * l + k + 1] = tile_prefix[3 * l + k] + (ng[k] + 1023) / 1024;
+    B.ld[l] = d;
+  }
+  B.nwin_total = (int32_t)o_win;
+  B.npanel_total = o_pan;
+  B.ntiles = tile_prefix[3 * n];
+  B.od_total = o_od;
+  B.nblk_total = blk_base[n];
+  const int64_t nbt = B.nblk_total + 1;
+  // arena layout
+  Layout lay;
+  lay.add<LayerDev>(n);
+  lay.add<double>(o_pan);
+  lay.add<int32_t>(o_pan);
+  lay.add<int32_t>(o_pan);
+  lay.add<int64_t>(n + 1);
+  lay.add<WinDev>(std::max<int64_t>(o_win, 1));
+  lay.add<int32_t>(std::max<int64_t>(o_win, 1));
+  lay.add<double>(std::max<int64_t>(o_win, 1) * kR4Stride);
+  for (int k = 0; k < 5; k++) lay.add<double>(o_far + 1);
+  lay.add<int8_t>(o_far + 1);
+  lay.add<int8_t>(o_far + 1);
+  for (int k = 0; k < 5; k++) lay.add<double>(o_far + 1);
+  lay.add<int8_t>(o_far + 1);
+  lay.add<int64_t>(n);
+  lay.add<int64_t>(o_b9 + 1);
+  lay.add<double>(o_b9 + 1);
+  lay.add<int64_t>(n);
+  lay.add<double>(o_near + 1);
+  lay.add<double>(o_near + 1);
+  lay.add<double>(5 * (o_near + 1));
+  lay.add<double>(o_near + 1);
+  for (int k = 0; k < 4; k++) lay.add<int32_t>(o_near + 1);
+  lay.add<int8_t>(o_near + 1);
+  lay.add<double>(o_r1);
+  lay.add<double>(o_r2);
+  lay.add<double>(o_r3);
+  lay.add<double>(o_abs);
+  lay.add<double>(o_od);
+  lay.add<int64_t>(3 * n + 1);
+  lay.add<int32_t>(4);
+  lay.add<int32_t>(nbt * kSegMaxBlk);
+  lay.add<int32_t>(nbt * kSegMaxBlk);
+  lay.add<int32_t>(nbt);
+  lay.add<int32_t>(nbt);
+  lay.add<int64_t>(nbt);
+  lay.add<int64_t>(n);
+  lay.add<int64_t>(n + 1);
+  CK(ctx->arena.reserve(lay.bytes + 4096));
+  Arena& A = ctx->arena;
+  A.reset();
+  Work& w = B.w;
+  B.d_ld = A.take<LayerDev>(n);
+  double* d_vft = A.take<double>(o_pan);
+  int32_t* d_win_of = A.take<int32_t>(o_pan);
+  B.d_panel_layer = A.take<int32_t>(o_pan);
+  B.d_panel_base = A.take<int64_t>(n + 1);
+  WinDev* d_win = A.take<WinDev>(std::max<int64_t>(o_win, 1));
+  B.d_win_layer = A.take<int32_t>(std::max<int64_t>(o_win, 1));
+  w.r4 = A.take<double>(std::max<int64_t>(o_win, 1) * kR4Stride);
+  w.f_vnu = A.take<double>(o_far + 1);
+  w.f_sp = A.take<double>(o_far + 1);
+  w.f_alfa = A.take<double>(o_far + 1);
+  w.f_epp = A.take<double>(o_far + 1);
+  w.f_spp = A.take<double>(o_far + 1);
+  w.f_ok = A.take<int8_t>(o_far + 1);
+  w.f_co2 = A.take<int8_t>(o_far + 1);
+  w.s_vnu = A.take<double>(o_far + 1);
+  w.s_sp = A.take<double>(o_far + 1);
+  w.s_alfa = A.take<double>(o_far + 1);
+  w.s_epp = A.take<double>(o_far + 1);
+  w.s_spp = A.take<double>(o_far + 1);
+  w.s_co2 = A.take<int8_t>(o_far + 1);
+  w.s_count = A.take<int64_t>(n);
+  w.b9_start = A.take<int64_t>(o_b9 + 1);
+  w.b9_vnuhi = A.take<double>(o_b9 + 1);
+  w.b9_count = A.take<int64_t>(n);
+  w.n_zint = A.take<double>(o_near + 1);
+  w.n_zslope = A.take<double>(o_near + 1);
+  w.n_str = A.take<double>(5 * (o_near + 1));
+  w.n_sppsp = A.take<double>(o_near + 1);
+  w.n_jmin1 = A.take<int32_t>(o_near + 1);
+  w.n_jmax1 = A.take<int32_t>(o_near + 1);
+  w.n_j2 = A.take<int32_t>(o_near + 1);
+  w.n_j3 = A.take<int32_t>(o_near + 1);
+  w.n_ok = A.take<int8_t>(o_near + 1);
+  w.r1 = A.take<double>(o_r1);
+  w.r2 = A.take<double>(o_r2);
+  w.r3 = A.take<double>(o_r3);
+  w.absrb = A.take<double>(o_abs);
+  w.od = A.take<double>(o_od);
+  B.d_tile_prefix = A.take<int64_t>(3 * n + 1);
+  w.status = A.take<int32_t>(4);
+  w.c_raw = A.take<int32_t>(nbt * kSegMaxBlk);
+  w.c_out = A.take<int32_t>(nbt * kSegMaxBlk);
+  w.seg_blk = A.take<int32_t>(nbt);
+  w.seg_nblk = A.take<int32_t>(nbt);
+  w.seg_out = A.take<int64_t>(nbt);
+  w.seg_count = A.take<int64_t>(n);
+  B.d_blk_base = A.take<int64_t>(n + 1);
+  w.L = B.d_ld;
+  w.nlay = n;
+  w.vft = d_vft;
+  w.win_of = d_win_of;
+  w.win = d_win;
+  // host-side staging of the plan tables
+  std::vector<double> h_vft(o_pan);
+  std::vector<int32_t> h_wof(o_pan), h_play(o_pan), h_wlay(std::max<int64_t>(o_win, 1));
+  std::vector<int64_t> h_pbase(n + 1);
+  std::vector<WinDev> h_win(std::max<int64_t>(o_win, 1));
+  for (int l = 0; l < n; l++) {
+    const LayerPlan& P = B.plans[l];
+    const LayerDev& d = B.ld[l];
+    h_pbase[l] = d.off_panel;
+    for (int64_t p = 0; p < d.npanel; p++) {
+      h_vft[d.off_panel + p] = P.vft[p];
+      h_wof[d.off_panel + p] = P.win_of[p];
+      h_play[d.off_panel + p] = l;
+    }
+    for (int k = 0; k < d.nwin; k++) {
+      h_win[d.off_win + k] = P.win[k];
+      h_wlay[d.off_win + k] = l;
+    }
+  }
+  h_pbase[n] = o_pan;
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(B.d_ld, B.ld.data(), sizeof(LayerDev) * n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_vft, h_vft.data(), sizeof(double) * o_pan, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_win_of, h_wof.data(), sizeof(int32_t) * o_pan, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(B.d_panel_layer, h_play.data(), sizeof(int32_t) * o_pan,
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(B.d_panel_base, h_pbase.data(), sizeof(int64_t) * (n + 1),
+                     cudaMemcpyHostToDevice, s));
+  if (o_win > 0) {
+    CK(cudaMemcpyAsync(d_win, h_win.data(), sizeof(WinDev) * o_win, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.d_win_layer, h_wlay.data(), sizeof(int32_t) * o_win,
+                       cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemcpyAsync(B.d_tile_prefix, tile_prefix.data(), sizeof(int64_t) * (3 * n + 1),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(B.d_blk_base, blk_base.data(), sizeof(int64_t) * (n + 1),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(w.status, 0, 4 * sizeof(int32_t), s));
+  // the host vectors must live until the copies finish
+  CK(cudaStreamSynchronize(s));
+  return LBL_OK;
+}
+
+// Optical depth of every layer of the batch into B.w.od.
+int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
+  cudaStream_t s = ctx->stream;
+  const Work& w = B.w;
+  CK(launch_far_scale(w, ctx->dl, B.max_far, s));
+  CK(launch_shrink(w, ctx->dl.bs, B.d_blk_base, B.nblk_total, s));
+  CK(launch_far_wing(w, B.nwin_total, B.d_win_layer, s));
+  CK(launch_near_scale(w, ctx->dl, s));
+  if (R.icntnm) {
+    if (!ctx->have_ck) return fail(ctx, LBL_E_NOTREADY, "continuum table not uploaded");
+    CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, s));
+  }
+  CK(launch_grids(w, ctx->dl, ctx->sh, B.d_tile_prefix, B.ntiles, precision, s));
+  CK(launch_combine(w, B.max_r3, B.max_r2, B.npanel_total, B.d_panel_layer, B.d_panel_base, s));
+  int32_t st[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (st[0] == 2)
+    return fail(ctx, LBL_E_RANGE,
+                "far-wing line file too sparse: a LINF4 segment spans more than 48 TAPE3 panels");
+  if (st[0] != 0) return fail(ctx, LBL_E_CUDA, "device status " + std::to_string(st[0]));
+  return LBL_OK;
+}
+
+int copy_out(lbl_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (is_device_ptr(dst)) {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  } else {
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  return LBL_OK;
+}
+
+int check_run(lbl_ctx* ctx, const lbl_run* R) {
+  if (!R) return fail(ctx, LBL_E_ARG, "run is NULL");
+  if (R->ihirac != 1) return fail(ctx, LBL_E_ARG, "only IHIRAC=1 (Voigt) is supported");
+  if (R->ilblf4 < 0 || R->ilblf4 > 2) return fail(ctx, LBL_E_ARG, "ILBLF4 must be 0, 1 or 2");
+  if (!(R->v2 > R->v1)) return fail(ctx, LBL_E_ARG, "V2 must exceed V1");
+  if (R->v2 - R->v1 > 2020.) return fail(ctx, LBL_E_RANGE, "V2-V1 above 2020 cm-1");
+  if (R->v1 - 32. * 1e-9 <= 0.) return fail(ctx, LBL_E_RANGE, "V1 must be positive");
+  if (!(R->sample > 0.) || !(R->alfal0 > 0.)) return fail(ctx, LBL_E_ARG, "SAMPLE/ALFAL0");
+  if (R->iemit != 0 && R->iemit != 1) return fail(ctx, LBL_E_ARG, "IEMIT must be 0 or 1");
+  if (R->iemit == 1 && R->ipathl != 1) return fail(ctx, LBL_E_ARG, "only IPATHL=1 is supported");
+  if (!ctx->have_lines) return fail(ctx, LBL_E_NOTREADY, "lines not uploaded");
+  return LBL_OK;
+}
+
+int ensure_merge_buffers(lbl_ctx* ctx, size_t n) {
+  if (n <= ctx->mcap) return LBL_OK;
+  for (int k = 0; k < 4; k++) {
+    if (ctx->mbuf[k]) cudaFree(ctx->mbuf[k]);
+    ctx->mbuf[k] = nullptr;
+  }
+  for (int k = 0; k < 4; k++) CK(cudaMalloc(&ctx->mbuf[k], n * sizeof(double)));
+  ctx->mcap = n;
+  return LBL_OK;
+}
+
+// Merge every layer of the batch bottom-up; result in mbuf[res], mbuf[res+1].
+int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B, int n,
+              int* res) {
+  size_t mx = 0;
+  for (auto& d : B.ld) mx = std::max<size_t>(mx, d.npts);
+  int rc = ensure_merge_buffers(ctx, mx + 8);
+  if (rc) return rc;
+  int cur = 0;
+  double dv_old = 0.;
+  int64_t n_old = 0;
+  for (int l = 0; l < n; l++) {
+    const LayerDev& d = B.ld[l];
+    const int nxt = cur ^ 2;
+    const double tbnd = (l == 0 && R.ipathl == 1) ? R.tmpbnd : 0.;
+    CK(launch_merge(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
+                    dv_old, n_old, ctx->mbuf[cur], ctx->mbuf[cur + 1], ctx->mbuf[nxt],
+                    ctx->mbuf[nxt + 1], tbnd, R.bndemi, R.iemit, layers[l].tzu, ctx->stream));
+    if (l > 0 && d.dv > dv_old) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
+    cur = nxt;
+    dv_old = d.dv;
+    n_old = d.npts;
+  }
+  *res = cur;
+  return LBL_OK;
+}
+
+}  // namespace
+
+// ==========================================================================
+extern "C" {
+
+int lbl_ctx_create(int device, lbl_ctx** out) {
+  if (!out) return LBL_E_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LBL_E_NODEVICE;
+  }
+  if (device < 0 || device >= ndev) return LBL_E_ARG;
+  lbl_ctx* ctx = new lbl_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete ctx;
+    return LBL_E_CUDA;
+  }
+  upload_voicon();
+  init_kernel_attributes();
+  ShapeTables* t = new ShapeTables;
+  build_shape_tables(t);
+  const size_t nd = kNfmx + 1;
+  char* mem = nullptr;
+  if (cudaMalloc(&mem, 5 * nd * (sizeof(double) + sizeof(float)) + 1024) != cudaSuccess) {
+    delete t;
+    delete ctx;
+    return LBL_E_NOMEM;
+  }
+  ctx->shape_mem = mem;
+  const double* src[5] = {t->f1, t->f2, t->f3, t->fg, t->xver};
+  double* dd = reinterpret_cast<double*>(mem);
+  float* ff = reinterpret_cast<float*>(mem + 5 * nd * sizeof(double));
+  std::vector<float> tmp(nd);
+  for (int k = 0; k < 5; k++) {
+    cudaMemcpy(dd + k * nd, src[k], nd * sizeof(double), cudaMemcpyHostToDevice);
+    for (size_t i = 0; i < nd; i++) tmp[i] = (float)src[k][i];
+    cudaMemcpy(ff + k * nd, tmp.data(), nd * sizeof(float), cudaMemcpyHostToDevice);
+  }
+  delete t;
+  ctx->sh = DevShapes{dd, dd + nd, dd + 2 * nd, dd + 3 * nd, dd + 4 * nd,
+                      ff, ff + nd, ff + 2 * nd, ff + 3 * nd, ff + 4 * nd};
+  if (cudaGetLastError() != cudaSuccess) {
+    lbl_ctx_destroy(ctx);
+    return LBL_E_CUDA;
+  }
+  *out = ctx;
+  return LBL_OK;
+}
+
+int lbl_ctx_destroy(lbl_ctx* ctx) {
+  if (!ctx) return LBL_E_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->line_mem) cudaFree(ctx->line_mem);
+  if (ctx->shape_mem) cudaFree(ctx->shape_mem);
+  if (ctx->ck_mem) cudaFree(ctx->ck_mem);
+  if (ctx->arena.base) cudaFree(ctx->arena.base);
+  for (int k = 0; k < 4; k++)
+    if (ctx->mbuf[k]) cudaFree(ctx->mbuf[k]);
+  delete ctx;
+  return LBL_OK;
+}
+
+const char* lbl_last_error(const lbl_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int lbl_set_stream(lbl_ctx* ctx, void* stream) {
+  if (!ctx) return LBL_E_ARG;
+  ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+  return LBL_OK;
+}
+
+int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
+  if (!ctx || !L || L->n < 0) return fail(ctx, LBL_E_ARG, "bad lines");
+  const int64_t n = L->n;
+  if (n > 0 && (!L->vnu || !L->sp || !L->alfa || !L->epp || !L->mol || !L->hwhms ||
+                !L->tmpalf || !L->pshift || !L->iflg))
+    return fail(ctx, LBL_E_ARG, "NULL line array");
+  for (int64_t i = 1; i < n; i++)
+    if (!(L->vnu[i] >= L->vnu[i - 1]))
+      return fail(ctx, LBL_E_UNSORTED, "line centres not ascending at record " + std::to_string(i));
+  std::vector<int64_t> bs;
+  if (L->nblock > 0 && L->block_start) {
+    bs.assign(L->block_start, L->block_start + L->nblock + 1);
+    if (bs.front() != 0 || bs.back() != n) return fail(ctx, LBL_E_ARG, "block_start must span 0..n");
+  } else {
+    for (int64_t s = 0; s < n; s += 250) bs.push_back(s);
+    bs.push_back(n);
+  }
+  for (size_t b = 0; b + 1 < bs.size(); b++) {
+    if (bs[b + 1] < bs[b]) return fail(ctx, LBL_E_ARG, "block_start not increasing");
+    if (bs[b + 1] - bs[b] > 250) return fail(ctx, LBL_E_NREC, "RDLIN; NREC GT LIMIN");
+  }
+  ctx->h_vnu.assign(L->vnu, L->vnu + n);
+  ctx->h_sp.assign(L->sp, L->sp + n);
+  ctx->h_pshift.assign(L->pshift, L->pshift + n);
+  ctx->h_mol.assign(L->mol, L->mol + n);
+  ctx->h_iflg.assign(L->iflg, L->iflg + n);
+  ctx->h_bs = bs;
+  cudaSetDevice(ctx->device);
+  if (ctx->line_mem) cudaFree(ctx->line_mem);
+  ctx->line_mem = nullptr;
+  const size_t nn = (size_t)std::max<int64_t>(n, 1) + 2;  // +2: coupling record reads
+  size_t bytes = nn * (8 + 6 * 4 + 2 * 4) + bs.size() * 8 + 16 * 256;  // 10 aligned arrays
+  char* m = nullptr;
+  CK(cudaMalloc(&m, bytes));
+  ctx->line_mem = m;
+  CK(cudaMemset(m, 0, bytes));
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    off = (off + 255) & ~size_t(255);
+    char* p = m + off;
+    off += b;
+    return p;
+  };
+  DevLines d;
+  d.vnu = reinterpret_cast<double*>(take(nn * 8));
+  d.sp = reinterpret_cast<float*>(take(nn * 4));
+  d.alfa = reinterpret_cast<float*>(take(nn * 4));
+  d.epp = reinterpret_cast<float*>(take(nn * 4));
+  d.hwhms = reinterpret_cast<float*>(take(nn * 4));
+  d.tmpalf = reinterpret_cast<float*>(take(nn * 4));
+  d.pshift = reinterpret_cast<float*>(take(nn * 4));
+  d.mol = reinterpret_cast<int32_t*>(take(nn * 4));
+  d.iflg = reinterpret_cast<int32_t*>(take(nn * 4));
+  d.bs = reinterpret_cast<int64_t*>(take(bs.size() * 8));
+  d.n = n;
+  d.nblk = (int64_t)bs.size() - 1;
+  if (n > 0) {
+    CK(cudaMemcpy((void*)d.vnu, L->vnu, n * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.sp, L->sp, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.alfa, L->alfa, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.epp, L->epp, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.hwhms, L->hwhms, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.tmpalf, L->tmpalf, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.pshift, L->pshift, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.mol, L->mol, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((void*)d.iflg, L->iflg, n * 4, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy((void*)d.bs, bs.data(), bs.size() * 8, cudaMemcpyHostToDevice));
+  ctx->dl = d;
+  ctx->have_lines = true;
+  return LBL_OK;
+}
+
+int lbl_mtckd_upload(lbl_ctx* ctx, const lbl_mtckd* T) {
+  if (!ctx || !T || T->n < 4 || !T->self_absco_ref || !T->for_absco_ref || !T->self_texp ||
+      !(T->dv > 0.))
+    return fail(ctx, LBL_E_ARG, "bad continuum table");
+  cudaSetDevice(ctx->device);
+  if (ctx->ck_mem) cudaFree(ctx->ck_mem);
+  ctx->ck_mem = nullptr;
+  double* m = nullptr;
+  CK(cudaMalloc(&m, 3 * T->n * sizeof(double)));
+  ctx->ck_mem = m;
+  CK(cudaMemcpy(m, T->self_absco_ref, T->n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m + T->n, T->for_absco_ref, T->n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m + 2 * T->n, T->self_texp, T->n * 8, cudaMemcpyHostToDevice));
+  ctx->ck = DevMtckd{m, m + T->n, m + 2 * T->n, T->v0, T->dv, T->ref_press, T->ref_temp, T->n};
+  ctx->have_ck = true;
+  return LBL_OK;
+}
+
+int lbl_dv_rule(const lbl_run* run, lbl_layer* layers, int32_t nlay) {
+  if (!run || !layers || nlay < 1) return LBL_E_ARG;
+  std::string e;
+  return dv_rule(*run, layers, nlay, &e);
+}
+
+int64_t lbl_layer_npts(const lbl_run* run, double dv) {
+  if (!run || !(dv > 0.) || !(run->v2 > run->v1)) return -1;
+  return layer_npts(*run, dv);
+}
+
+int lbl_layer_od(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, int32_t* jrad,
+                 double* od, int64_t npts, int32_t precision) {
+  if (!ctx) return LBL_E_ARG;
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  if (!layer || !jrad || !od) return fail(ctx, LBL_E_ARG, "NULL argument");
+  cudaSetDevice(ctx->device);
+  if (layer_npts(*run, layer->dv) != npts) return fail(ctx, LBL_E_ARG, "npts does not match the layer grid");
+  Batch B;
+  int jout = 0;
+  rc = prepare_batch(ctx, *run, layer, 1, *jrad, &jout, B);
+  if (rc) return rc;
+  rc = run_od(ctx, *run, B, precision);
+  if (rc) return rc;
+  rc = copy_out(ctx, od, B.w.od, sizeof(double) * npts);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  *jrad = jout;
+  return LBL_OK;
+}
+
+int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, int32_t first,
+                    double dv_old, const double* rad_in, const double* tr_in, int64_t n_old,
+                    const double* od, double* rad_out, double* tr_out, int64_t n_new) {
+  if (!ctx) return LBL_E_ARG;
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  if (!layer || !od || !rad_out || (run->iemit == 1 && !tr_out)) return fail(ctx, LBL_E_ARG, "NULL argument");
+  if (!first && (!rad_in || (run->iemit == 1 && !tr_in) || n_old < 1))
+    return fail(ctx, LBL_E_ARG, "accumulated input missing");
+  if (!first && layer->dv > dv_old) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
+  cudaSetDevice(ctx->device);
+  if (layer_npts(*run, layer->dv) != n_new) return fail(ctx, LBL_E_ARG, "n_new does not match the layer grid");
+  HostLines H{ctx->h_vnu.data(), ctx->h_sp.data(), ctx->h_pshift.data(), ctx->h_mol.data(),
+              ctx->h_iflg.data(), (int64_t)ctx->h_vnu.size(), ctx->h_bs.data(),
+              (int64_t)ctx->h_bs.size() - 1};
+  LayerPlan P;
+  std::string e;
+  rc = plan_layer(*run, *layer, run->jrad, H, &P, &e);
+  if (rc) return fail(ctx, rc, e);
+  const size_t nn = (size_t)std::max(n_new, n_old) + 8;
+  rc = ensure_merge_buffers(ctx, nn);
+  if (rc) return rc;
+  CK(ctx->arena.reserve(sizeof(LayerDev) + P.vft.size() * 8 + n_new * 8 + 4096));
+  ctx->arena.reset();
+  LayerDev* dL = ctx->arena.take<LayerDev>(1);
+  double* dv = ctx->arena.take<double>(P.vft.size());
+  double* dod = ctx->arena.take<double>(n_new);
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(dL, &P.d, sizeof(LayerDev), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dv, P.vft.data(), P.vft.size() * 8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dod, od, n_new * 8, cudaMemcpyDefault, s));
+  if (!first) {
+    CK(cudaMemcpyAsync(ctx->mbuf[0], rad_in, n_old * 8, cudaMemcpyDefault, s));
+    if (run->iemit == 1) CK(cudaMemcpyAsync(ctx->mbuf[1], tr_in, n_old * 8, cudaMemcpyDefault, s));
+  }
+  const double tbnd = (first && run->ipathl == 1) ? run->tmpbnd : 0.;
+  CK(launch_merge(dL, dv, dod, n_new, first, dv_old, n_old, ctx->mbuf[0], ctx->mbuf[1],
+                  ctx->mbuf[2], ctx->mbuf[3], tbnd, run->bndemi, run->iemit, layer->tzu, s));
+  CK(cudaMemcpyAsync(rad_out, ctx->mbuf[2], n_new * 8, cudaMemcpyDefault, s));
+  if (tr_out) CK(cudaMemcpyAsync(tr_out, ctx->mbuf[3], n_new * 8, cudaMemcpyDefault, s));
+  CK(cudaStreamSynchronize(s));
+  return LBL_OK;
+}
+
+int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nlay, double* rad,
+                double* tr, int64_t npts, int32_t precision) {
+  if (!ctx) return LBL_E_ARG;
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  if (!layers || nlay < 1 || !rad) return fail(ctx, LBL_E_ARG, "NULL argument");
+  cudaSetDevice(ctx->device);
+  std::string e;
+  rc = dv_rule(*run, layers, nlay, &e);
+  if (rc) return fail(ctx, rc, e);
+  if (layer_npts(*run, layers[nlay - 1].dv) != npts)
+    return fail(ctx, LBL_E_ARG, "npts does not match the last layer's grid");
+  Batch B;
+  rc = prepare_batch(ctx, *run, layers, nlay, run->jrad, nullptr, B);
+  if (rc) return rc;
+  rc = run_od(ctx, *run, B, precision);
+  if (rc) return rc;
+  int res = 0;
+  rc = run_merge(ctx, *run, layers, B, nlay, &res);
+  if (rc) return rc;
+  rc = copy_out(ctx, rad, ctx->mbuf[res], sizeof(double) * npts);
+  if (rc) return rc;
+  if (tr) {
+    rc = copy_out(ctx, tr, ctx->mbuf[res + 1], sizeof(double) * npts);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LBL_OK;
+}
+
+int lbl_forward_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, const int32_t* nlay,
+                      int32_t nprof, double* rad, double* tr, int64_t* offsets,
+                      int64_t npts_total, int32_t precision) {
+  if (!ctx) return LBL_E_ARG;
+  if (!layers || !nlay || nprof < 1 || !rad || !offsets) return fail(ctx, LBL_E_ARG, "NULL argument");
+  int64_t lay0 = 0, off = 0;
+  offsets[0] = 0;
+  for (int p = 0; p < nprof; p++) {
+    std::string e;
+    int rc = dv_rule(*run, layers + lay0, nlay[p], &e);
+    if (rc) return fail(ctx, rc, e);
+    off += layer_npts(*run, layers[lay0 + nlay[p] - 1].dv);
+    offsets[p + 1] = off;
+    lay0 += nlay[p];
+  }
+  if (off > npts_total) return fail(ctx, LBL_E_ARG, "output buffer too small");
+  lay0 = 0;
+  for (int p = 0; p < nprof; p++) {
+    const int64_t n = offsets[p + 1] - offsets[p];
+    int rc = lbl_forward(ctx, run, layers + lay0, nlay[p], rad + offsets[p],
+                         tr ? tr + offsets[p] : nullptr, n, precision);
+    if (rc) return rc;
+    lay0 += nlay[p];
+  }
+  return LBL_OK;
+}
+
+int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nlay,
+                 const int32_t* mols, int32_t nq, double* rad, double* jac, int64_t npts,
+                 int32_t precision) {
+  (void)run; (void)layers; (void)nlay; (void)mols; (void)nq; (void)rad; (void)jac; (void)npts;
+  (void)precision;
+  return fail(ctx, LBL_E_ARG, "lbl_jacobian: not available in this build");
+}
+
+int lbl_brightness_temperature(const double* rad, int64_t n, double v1, double dv, double* bt) {
+  if (!rad || !bt || n < 0) return LBL_E_ARG;
+  const double c1 = 1.191042722E-12, c2 = 1.4387752;
+  for (int64_t i = 0; i < n; i++) {
+    const double v = v1 + double(i) * dv;
+    bt[i] = c2 * v / std::log(c1 * v * v * v / rad[i] + 1.);
+  }
+  return LBL_OK;
+}
+
+}  // extern "C"
+
+// ---- TAPE3 file input ------------------------------------------------------
+extern "C" int lbl_tape3_parse(const char* path, std::vector<double>* vnu, std::vector<float>* sp,
+                               std::vector<float>* alfa, std::vector<float>* epp,
+                               std::vector<int32_t>* mol, std::vector<float>* hw,
+                               std::vector<float>* tmp, std::vector<float>* psh,
+                               std::vector<int32_t>* iflg, std::vector<int64_t>* bs,
+                               std::string* err);
+
+extern "C" int lbl_lines_load_tape3(lbl_ctx* ctx, const char* path, int64_t* nlines) {
+  if (!ctx || !path) return LBL_E_ARG;
+  std::vector<double> vnu;
+  std::vector<float> sp, alfa, epp, hw, tmp, psh;
+  std::vector<int32_t> mol, iflg;
+  std::vector<int64_t> bs;
+  std::string e;
+  int rc = lbl_tape3_parse(path, &vnu, &sp, &alfa, &epp, &mol, &hw, &tmp, &psh, &iflg, &bs, &e);
+  if (rc) return fail(ctx, rc, e);
+  lbl_lines L;
+  L.n = (int64_t)vnu.size();
+  L.vnu = vnu.data();
+  L.sp = sp.data();
+  L.alfa = alfa.data();
+  L.epp = epp.data();
+  L.mol = mol.data();
+  L.hwhms = hw.data();
+  L.tmpalf = tmp.data();
+  L.pshift = psh.data();
+  L.iflg = iflg.data();
+  L.nblock = (int64_t)bs.size() - 1;
+  L.block_start = bs.data();
+  rc = lbl_lines_upload(ctx, &L);
+  if (rc == LBL_OK && nlines) *nlines = L.n;
+  return rc;
+}

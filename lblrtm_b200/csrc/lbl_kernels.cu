@@ -1,0 +1,1257 @@
+// lbl_kernels.cu -- sm_100a kernels of the layer optical-depth and merge path.
+//
+// Work is laid out on three global grids per layer instead of the
+// reference's streamed 2400-point panels: R1 (spacing DV), R2 (4*DV) and R3
+// (16*DV), all indexed from the panel-0 origin VFT0 = V1 - 32*DV with the
+// reference's 1-based convention (grid point g sits at VFT0 + (g-1)*dv_k).
+// A line's window limits are computed in panel-0 coordinates with Fortran
+// truncation, which reproduces the reference for every panel (later panels
+// only shift indices by multiples of 2400/600/150).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+
+#include "../data/ref_tables.h"
+#include "lbl_kernels.cuh"
+
+namespace lbl {
+
+namespace {
+
+constexpr double kRADCN1 = 1.191042722E-12;  // src/phys_consts.f90:73
+constexpr double kRADCN2 = 1.4387752;        // src/phys_consts.f90:74
+constexpr double kONEPL = 1.001, kONEMI = 0.999;
+constexpr double kHWDXF = 4. / 0.002;        // HWF1/DXF1
+constexpr double kODLO = 0.06;               // od_lo, src/lblparams.f90:47
+constexpr int kChunk = 32;                   // far-wing lines decided per step
+
+__constant__ double c_avrat[102], c_cf1[102], c_cf2[102], c_cf3[102], c_cgauss[102],
+    c_cer[102];
+__constant__ int c_isomax[48];
+
+__device__ __forceinline__ long fint(double x) { return (long)x; }
+
+// Radiation term (RADFN, src/oprop.f90:2235-2296)
+__device__ double radfn(double vi, double xkt) {
+  if (xkt > 0.0) {
+    double x = vi / xkt;
+    if (x <= 0.01) return 0.5 * x * vi;
+    if (x <= 10.0) {
+      double e = exp(-x);
+      return vi * (1. - e) / (1. + e);
+    }
+  }
+  return vi;
+}
+
+// Piecewise-linear radiation term over [VI, VINEW] (RADFNI, src/oprop.f90:2297-2475)
+__device__ double radfni(double vi, double dvi, double xkt, double& vinew, double& rdel,
+                         double& rdlast) {
+  const double fact1 = 3.0E-03;
+  const double xvi = vi;
+  if (rdlast < 0.) rdlast = radfn(xvi, xkt);
+  const double out = rdlast;
+  long intvls = 1;
+  double rdnext;
+  double xviokt = xkt > 0.0 ? xvi / xkt : 0.;
+  auto step = [&](double width) {
+    if (vinew >= 0.0) {
+      vinew = vi + width;
+      intvls = fint((vinew - vi) / dvi);
+      if (intvls < 1) intvls = 1;
+      vinew = vi + dvi * double(intvls);
+    } else {
+      vinew = fabs(vinew);
+      intvls = fint((vinew - vi) / dvi);
+      if (intvls < 1) intvls = 1;
+    }
+  };
+  if (xkt > 0.0 && xviokt <= 0.01) {
+    step(fact1 * 0.5 * xvi);
+    double xn = vinew / xkt;
+    rdnext = 0.5 * xn * vinew;
+  } else if (xkt > 0.0 && xviokt <= 10.0) {
+    double e = exp(-xviokt);
+    double xm = 1. - e, xp = 1. + e;
+    double c = xviokt * e;
+    step(fact1 * xvi / (1. + (c / xm + c / xp)));
+    double en = exp(-(vinew / xkt));
+    rdnext = vinew * (1. - en) / (1. + en);
+  } else {
+    step(fact1 * xvi);
+    rdnext = vinew;
+  }
+  rdel = (rdnext - out) / double(intvls);
+  rdlast = rdnext;
+  return out;
+}
+
+// Planck function (PLANCK, src/xmerge.f90:968-1017)
+__device__ __forceinline__ double planck(double vi, double xkt) {
+  double v = 0.;
+  if (xkt > 0.0) {
+    double x = vi / xkt;
+    if (x < 1e-2) {
+      v = (vi * vi) * xkt / (1. + 0.5 * x);
+    } else if (x <= 80.) {
+      double e = exp(-x);
+      v = (vi * vi * vi) * e / (1. - e);
+    }
+  }
+  return v * kRADCN1;
+}
+
+__device__ __forceinline__ float bits_float(int32_t v) { return __int_as_float(v); }
+
+// Y/G line-coupling coefficients carried by record i+1 (LNCOR1 :1039-1061,
+// LINF4 :3163-3190).  upper=true selects LINF4's bracket convention.
+__device__ void coupling(const DevLines& ln, int64_t i, int iflag, int ilc, double rectlc,
+                         double tmpdif, bool linf4, double& yi, double& gi, double& g1,
+                         double& g2) {
+  double A[5], B[5];
+  A[1] = ln.vnu[i + 1];
+  B[1] = (double)ln.sp[i + 1];
+  A[2] = (double)ln.alfa[i + 1];
+  B[2] = (double)ln.epp[i + 1];
+  A[3] = (double)bits_float(ln.mol[i + 1]);
+  B[3] = (double)ln.hwhms[i + 1];
+  A[4] = (double)ln.tmpalf[i + 1];
+  B[4] = (double)ln.pshift[i + 1];
+  double a, b;
+  if (linf4) {
+    double sa = (A[ilc] - A[ilc - 1]) * rectlc, sb = (B[ilc] - B[ilc - 1]) * rectlc;
+    a = A[ilc] + sa * tmpdif;
+    b = B[ilc] + sb * tmpdif;
+  } else {
+    double sa = (A[ilc + 1] - A[ilc]) * rectlc, sb = (B[ilc + 1] - B[ilc]) * rectlc;
+    a = A[ilc] + sa * tmpdif;
+    b = B[ilc] + sb * tmpdif;
+  }
+  if (iflag == 1) {
+    yi = a;
+    gi = b;
+  } else {
+    g1 = a;
+    g2 = b;
+  }
+}
+
+// air width with the O2/N2 foreign-width conversion of RDLIN/RDLNFL
+__device__ __forceinline__ double air_width(const DevLines& ln, int64_t i, int m) {
+  double a = (double)ln.alfa[i];
+  if (m == 7) a = (a - 0.21 * (double)ln.hwhms[i]) / (1.0 - 0.21);
+  if (m == 22) a = (a - 0.79 * (double)ln.hwhms[i]) / (1.0 - 0.79);
+  return a;
+}
+
+// =========================================================================
+// LINF4 line scaling (src/oprop.f90:3136-3220)
+// =========================================================================
+__global__ void k_far_scale(Work w, DevLines ln) {
+  const int l = blockIdx.y;
+  const LayerDev& L = w.L[l];
+  const int64_t i = L.far_lo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.far_hi) return;
+  const int64_t slot = L.off_far + (i - L.far_lo);
+  int8_t ok = 0;
+  if (ln.iflg[i] >= 0) {
+    const int mcode = ln.mol[i];
+    const int m = mcode % 100, iso = (mcode % 1000) / 100;
+    if (m >= 1 && m <= 47 && iso >= 1 && iso <= c_isomax[m]) {
+      const double wkm = (m <= L.nmol) ? L.wk[m] : 0.;
+      double sui = (double)ln.sp[i] * wkm;
+      const double vnu = ln.vnu[i];
+      if (sui != 0. && vnu >= L.v1l4) {
+        ok = 1;
+        const int iflag = ln.iflg[i];
+        double yi = 0., gi = 0., g1 = 0., g2 = 0.;
+        if (iflag == 1 || iflag == 3)
+          coupling(ln, i, iflag, L.ilc_f, L.rectlc_f, L.tmpdif_f, true, yi, gi, g1, g2);
+        const double vs = vnu + L.rhorat * (double)ln.pshift[i];
+        if (vs == 0.) sui = 2. * sui;
+        double epp = (double)ln.epp[i];
+        if (epp <= -1.001) epp = fabs(epp);
+        if (epp > -0.999)
+          sui = sui * L.scor[m][iso] * exp(-epp * L.betacr_f) * (1. + exp(-vs * L.beta_f));
+        const double tmpcor = pow(L.tratio, (double)ln.tmpalf[i]);
+        const double a0 = air_width(ln, i, m) * tmpcor;
+        const double hs = (double)ln.hwhms[i] * tmpcor;
+        double alfl = a0 * (L.rhorat - L.rhoslf[m]) + hs * L.rhoslf[m];
+        if (iflag == 3) alfl = alfl * (1.0 - g1 * L.pavp0 - g2 * L.pavp2);
+        w.f_vnu[slot] = vs;
+        w.f_alfa[slot] = alfl;
+        w.f_epp[slot] = vs * L.alfd1[m][iso];
+        w.f_sp[slot] = sui * (1. + gi * L.pavp2);
+        w.f_spp[slot] = sui * yi * L.pavp0;
+        w.f_co2[slot] = (m == 2);
+      }
+    }
+  }
+  w.f_ok[slot] = ok;
+}
+
+// =========================================================================
+// LINF4 segmenting + SHRINK (src/oprop.f90:3221-3292, 3508-3640): one thread
+// per layer walks the TAPE3 panels in order.  Raw lines accumulate until at
+// least LIMIN=1000 (shrunk-so-far + raw) are held, then the held raw lines
+// are merged in groups of width DVR4/2 (non-CO2 and CO2 separately); a
+// shrunk block is written once it holds >= 1000 lines or at the end.
+// =========================================================================
+__device__ void shrink_segment(const Work& w, const LayerDev& L, int64_t lo, int64_t hi,
+                               int64_t& out) {
+  const double dvh = L.dvr4 / 2.;
+  int64_t first = lo;
+  while (first < hi && !w.f_ok[L.off_far + first]) first++;
+  if (first >= hi) return;
+  double vlmt = w.f_vnu[L.off_far + first] + dvh;
+  double sal = 0., sad = 0., ss = 0., sv = 0., sc = 0.;
+  double sal2 = 0., sad2 = 0., ss2 = 0., sv2 = 0., sc2 = 0.;
+  const int64_t S = L.off_shr;
+  int64_t cur = first;
+  while (cur < hi) {
+    const int64_t c = L.off_far + cur;
+    int64_t nxt = cur + 1;
+    while (nxt < hi && !w.f_ok[L.off_far + nxt]) nxt++;
+    double sp = w.f_sp[c], spp = w.f_spp[c];
+    if (sp < 1.0e-35) {
+      sp = 0.0;
+      spp = 0.0;
+    }
+    const double vnu = w.f_vnu[c];
+    if (spp != 0.0) {
+      w.s_vnu[S + out] = vnu;
+      w.s_sp[S + out] = sp;
+      w.s_alfa[S + out] = w.f_alfa[c];
+      w.s_epp[S + out] = w.f_epp[c];
+      w.s_spp[S + out] = spp;
+      w.s_co2[S + out] = w.f_co2[c];
+      out++;
+    } else if (!w.f_co2[c]) {
+      sv = sv + vnu * sp;
+      ss = ss + sp;
+      sal = sal + sp * w.f_alfa[c];
+      sad = sad + sp * w.f_epp[c];
+      sc = sc + spp;
+    } else {
+      sv2 = sv2 + vnu * sp;
+      ss2 = ss2 + sp;
+      sal2 = sal2 + sp * w.f_alfa[c];
+      sad2 = sad2 + sp * w.f_epp[c];
+      sc2 = sc2 + spp;
+    }
+    bool close = true;
+    if (nxt < hi && w.f_vnu[L.off_far + nxt] <= vlmt) close = false;
+    if (close) {
+      vlmt = vnu + dvh;
+      if (ss > 0.) {
+        w.s_sp[S + out] = ss;
+        w.s_alfa[S + out] = sal / ss;
+        w.s_epp[S + out] = sad / ss;
+        w.s_vnu[S + out] = sv / ss;
+        w.s_spp[S + out] = sc;
+        w.s_co2[S + out] = 0;
+        out++;
+        sal = sad = ss = sv = sc = 0.;
+      }
+      if (ss2 > 0.) {
+        w.s_sp[S + out] = ss2;
+        w.s_alfa[S + out] = sal2 / ss2;
+        w.s_epp[S + out] = sad2 / ss2;
+        w.s_vnu[S + out] = sv2 / ss2;
+        w.s_spp[S + out] = sc2;
+        w.s_co2[S + out] = 1;
+        out++;
+        sal2 = sad2 = ss2 = sv2 = sc2 = 0.;
+      }
+    }
+    cur = nxt;
+  }
+}
+
+// Parallel form of the LINF4 panel loop.  A segment (the raw lines held
+// between two SHRINK calls) always starts at a TAPE3 panel boundary and ends
+// at the first panel end where held-shrunk + raw >= LIMIN, so:
+//   k_shr_count  for every start panel b, walks forward and records the raw
+//                count and the shrunk-output count a segment b..e would have;
+//   k_shr_plan   per layer, replays the LINF4 state machine on those counts
+//                (segments, their output offsets, shrunk-block starts);
+//   k_shr_write  per segment, performs SHRINK and writes the shrunk lines.
+__device__ __forceinline__ int64_t far_slot_begin(const LayerDev& L, const int64_t* bs, int64_t b) {
+  return bs[b] > L.far_lo ? bs[b] - L.far_lo : 0;
+}
+__device__ __forceinline__ int64_t far_slot_end(const LayerDev& L, const int64_t* bs, int64_t b) {
+  const int64_t e = bs[b + 1] - L.far_lo;
+  const int64_t n = L.far_hi - L.far_lo;
+  return e > n ? n : e;
+}
+
+__global__ void k_shr_count(Work w, const int64_t* bs, const int64_t* blk_base, int nlay) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // thread -> (layer, local start block) through the per-layer block base
+  int lo = 0, hi = nlay;
+  while (lo < hi) {
+    int m = (lo + hi) >> 1;
+    if (blk_base[m + 1] <= t) lo = m + 1;
+    else hi = m;
+  }
+  if (lo >= nlay) return;
+  const int l = lo;
+  const LayerDev& L = w.L[l];
+  const int64_t bl = t - blk_base[l];
+  const int64_t nb = L.fblk_hi - L.fblk_lo;
+  if (bl >= nb) return;
+  int32_t* craw = w.c_raw + (blk_base[l] + bl) * kSegMaxBlk;
+  int32_t* cout = w.c_out + (blk_base[l] + bl) * kSegMaxBlk;
+  const double dvh = L.dvr4 / 2.;
+  const int64_t F = L.off_far;
+  int32_t raw = 0, out = 0;
+  double ss = 0., ss2 = 0.;
+  bool open = false;  // a group is pending
+  double vlmt = 0.;
+  int k = 0;
+  for (int64_t b = L.fblk_lo + bl; b < L.fblk_hi && k < kSegMaxBlk; b++, k++) {
+    const int64_t a = far_slot_begin(L, bs, b), e = far_slot_end(L, bs, b);
+    int64_t last_valid = -1;
+    for (int64_t s = a; s < e; s++)
+      if (w.f_ok[F + s]) last_valid = s;
+    for (int64_t s = a; s < e; s++) {
+      if (!w.f_ok[F + s]) continue;
+      double sp = w.f_sp[F + s], spp = w.f_spp[F + s];
+      if (sp < 1.0e-35) {
+        sp = 0.;
+        spp = 0.;
+      }
+      const double v = w.f_vnu[F + s];
+      if (!open) {
+        vlmt = (raw == 0) ? v + dvh : vlmt;
+        open = true;
+      }
+      raw++;
+      if (spp != 0.) out++;
+      else if (!w.f_co2[F + s]) ss = ss + sp;
+      else ss2 = ss2 + sp;
+      if (s == last_valid) {
+        // outputs if the segment were closed at the end of this panel
+        craw[k] = raw;
+        cout[k] = out + (ss > 0.) + (ss2 > 0.);
+      }
+      // real close decision, looking at the next valid line (any panel)
+      int64_t nx = s + 1;
+      const int64_t nfar = L.far_hi - L.far_lo;
+      while (nx < nfar && !w.f_ok[F + nx]) nx++;
+      const bool close = !(nx < nfar && w.f_vnu[F + nx] <= vlmt);
+      if (close) {
+        out += (ss > 0.) + (ss2 > 0.);
+        ss = ss2 = 0.;
+        vlmt = v + dvh;
+      }
+    }
+    if (last_valid < 0) {
+      craw[k] = raw;
+      cout[k] = out + (ss > 0.) + (ss2 > 0.);
+    }
+    if (raw >= 1000) {
+      k++;
+      break;
+    }
+  }
+  for (; k < kSegMaxBlk; k++) craw[k] = -1;  // not reached
+}
+
+__global__ void k_shr_plan(Work w, const int64_t* blk_base) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= w.nlay) return;
+  const LayerDev& L = w.L[l];
+  int64_t nseg = 0, total = 0, nb9 = 0, blk_start = 0, J = 0;
+  if (L.ilblf4 >= 1 && L.far_hi > L.far_lo) {
+    const int64_t nb = L.fblk_hi - L.fblk_lo;
+    int64_t b = 0;
+    while (b < nb) {
+      const int32_t* craw = w.c_raw + (blk_base[l] + b) * kSegMaxBlk;
+      const int32_t* cout = w.c_out + (blk_base[l] + b) * kSegMaxBlk;
+      int k = 0;
+      for (;; k++) {
+        if (k >= kSegMaxBlk || craw[k] < 0) {
+          w.status[0] = 2;  // segment longer than the count table: fall back
+          w.s_count[l] = -1;
+          return;
+        }
+        if (b + k == nb - 1 || J + craw[k] >= 1000) break;
+      }
+      const int64_t n = cout[k];
+      w.seg_blk[L.off_seg + nseg] = (int32_t)b;
+      w.seg_nblk[L.off_seg + nseg] = (int32_t)(k + 1);
+      w.seg_out[L.off_seg + nseg] = total;
+      nseg++;
+      total += n;
+      J += n;
+      b += k + 1;
+      if (J >= 1000 || b >= nb) {
+        if (J > 0) {
+          w.b9_start[L.off_blk9 + nb9] = blk_start;
+          nb9++;
+        }
+        blk_start = total;
+        J = 0;
+      }
+    }
+  }
+  w.seg_count[l] = nseg;
+  w.s_count[l] = total;
+  w.b9_count[l] = nb9;
+}
+
+__global__ void k_shr_write(Work w, const int64_t* bs, const int64_t* seg_base, int nlay) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int lo = 0, hi = nlay;
+  while (lo < hi) {
+    int m = (lo + hi) >> 1;
+    if (seg_base[m + 1] <= t) lo = m + 1;
+    else hi = m;
+  }
+  if (lo >= nlay) return;
+  const int l = lo;
+  const LayerDev& L = w.L[l];
+  const int64_t sgi = t - seg_base[l];
+  if (w.s_count[l] < 0 || sgi >= w.seg_count[l]) return;
+  const int64_t b0 = L.fblk_lo + w.seg_blk[L.off_seg + sgi];
+  const int64_t b1 = b0 + w.seg_nblk[L.off_seg + sgi];
+  int64_t out = w.seg_out[L.off_seg + sgi];
+  shrink_segment(w, L, far_slot_begin(L, bs, b0), far_slot_end(L, bs, b1 - 1), out);
+}
+
+// =========================================================================
+// LBLF4/CONVF4 far wing (src/oprop.f90:3641-4039), one CTA per window.
+// Lines are taken in file order 32 at a time: warp 0 decides acceptance in
+// order against the running R4 (held in shared memory) plus the earlier
+// accepted lines of the same chunk -- exactly the reference's test against
+// the partially accumulated R4 -- then every thread adds the accepted
+// lines to the window points it owns.
+// =========================================================================
+struct F4Line {
+  double xnui, sil, siv_a3, siv_b3, alfl2, rvi2, f4bnd, dptrat, spp, vnu;
+  int32_t jmin, jmax, co2, has;  // has: 1 main, 2 mirror
+  double mxnui, mdptrat, mspp;
+  int32_t mjmin, mjmax;
+};
+
+__device__ __forceinline__ double f4_eval(const F4Line& p, bool mirror, int j, double dvr4,
+                                          double bndsq) {
+  const double xnui = mirror ? p.mxnui : p.xnui;
+  const double xm = double(j - 1) * dvr4 - xnui;
+  const double xmsq = xm * xm;
+  const double zvsq = xmsq * p.rvi2;
+  const double sub = p.co2 ? (2. - xmsq / bndsq) * p.f4bnd : p.f4bnd;
+  double f;
+  if (zvsq <= 4096.)
+    f = (p.siv_a3 + zvsq * p.siv_b3) - sub;
+  else
+    f = p.sil / (p.alfl2 + xmsq) - sub;
+  const double spp = mirror ? p.mspp : p.spp;
+  if (spp != 0.) f = f + xm * (mirror ? p.mdptrat : p.dptrat) * f;
+  return f;
+}
+
+__global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_layer) {
+  const int gw = blockIdx.x;
+  const int l = win_layer[gw];
+  const LayerDev& L = w.L[l];
+  const WinDev W = w.win[gw];
+  __shared__ double R4s[kR4Stride];
+  __shared__ F4Line cl[kChunk];
+  __shared__ int s_nacc, s_term;
+  __shared__ int s_acc[kChunk];
+  for (int j = threadIdx.x; j < kR4Stride; j += blockDim.x) R4s[j] = 0.;
+  if (threadIdx.x == 0) s_term = 0;
+  __syncthreads();
+  const double dvr4 = L.dvr4, bnd = L.bound4, bndsq = bnd * bnd;
+  const double recpi = 1. / (2. * asin(1.));
+  const double zsq = 64. * 64.;
+  const double A3 = (1. + 2. * zsq) / ((1. + zsq) * (1. + zsq));
+  const double B3 = -1. / ((1. + zsq) * (1. + zsq));
+  const int npt = W.nptr4;
+  const int64_t S = L.off_shr;
+  const int64_t ns = w.s_count[l];
+  const int64_t nb9 = w.b9_count[l];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int term = 0;
+  for (int64_t b = 0; b < nb9 && !term; b++) {
+    const int64_t b0 = w.b9_start[L.off_blk9 + b];
+    const int64_t b1 = (b + 1 < nb9) ? w.b9_start[L.off_blk9 + b + 1] : ns;
+    if (w.s_vnu[S + b1 - 1] < W.vlo) continue;  // RDLIN4 skips blocks with VMAX < VLO (:3815)
+    for (int64_t c0 = b0; c0 < b1; c0 += kChunk) {
+      // every thread has finished with the previous chunk's shared state
+      // before warp 0 rewrites it
+      __syncthreads();
+      if (warp == 0) {
+        const int64_t i = c0 + lane;
+        bool cand = false;
+        double speak = 0., base = 0.;
+        int jj = 1;
+        F4Line p;
+        p.has = 0;
+        if (i < b1) {
+          const double sp = w.s_sp[S + i], spp = w.s_spp[S + i];
+          cand = !(sp == 0. && spp == 0.);
+          const double ad = w.s_epp[S + i], al = w.s_alfa[S + i], v = w.s_vnu[S + i];
+          const double zeta = al / (al + ad);
+          long iz = fint(100. * zeta + kONEPL);
+          iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);  // zeta in [0,1]; guards bad input
+          const double zd = 100. * zeta - double(iz - 1);
+          const double alfav = (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (al + ad);
+          const double ralfv = 1. / alfav;
+          const double sil = sp * recpi * al;
+          const double siv = (al * ralfv) * sp * recpi * ralfv;
+          speak = A3 * fabs(siv);
+          long jjl = fint((v - W.v1r4) / dvr4 + 1.);
+          jjl = jjl < 1 ? 1 : (jjl > npt ? npt : jjl);
+          jj = (int)jjl;
+          p.vnu = v;
+          p.xnui = v - W.v1r4;
+          p.sil = sil;
+          p.siv_a3 = siv * A3;
+          p.siv_b3 = siv * B3;
+          p.alfl2 = al * al;
+          p.rvi2 = 1. / (alfav * alfav);
+          p.f4bnd = sil / (al * al + bndsq);
+          p.spp = spp;
+          p.dptrat = spp / (sp * alfav);
+          p.co2 = w.s_co2[S + i];
+          const long jmin = fint((p.xnui - bnd) / dvr4 + 2.);
+          const long jmax = fint((p.xnui + bnd) / dvr4 + 1.);
+          p.jmin = (int)(jmin < 1 ? 1 : (jmin > npt + 1 ? npt + 1 : jmin));
+          p.jmax = (int)(jmax > npt ? npt : (jmax < 0 ? 0 : jmax));
+          const bool beyond = jmin > npt;  // GO TO 60: no wing, no image
+          if (!beyond && p.jmax >= p.jmin) p.has |= 1;
+          if (!beyond && v > 0. && v <= 25.) {  // Van Vleck-Weisskopf image (:4014-4024)
+            p.mxnui = -v - W.v1r4;
+            p.mspp = -spp;
+            p.mdptrat = -spp / (sp * alfav);
+            const long mjmin = fint((p.mxnui - bnd) / dvr4 + 2.);
+            const long mjmax = fint((p.mxnui + bnd) / dvr4 + 1.);
+            p.mjmin = (int)(mjmin < 1 ? 1 : mjmin);
+            p.mjmax = (int)(mjmax > npt ? npt : mjmax);
+            if (mjmin <= npt && p.mjmax >= p.mjmin) p.has |= 2;
+          }
+          base = R4s[jj];
+        }
+        cl[lane] = p;
+        __syncwarp();
+        double partial = 0.;
+        int term_at = kChunk;
+        for (int k = 0; k < kChunk; k++) {
+          if (c0 + k >= b1) break;
+          const bool ck = __shfl_sync(0xffffffffu, cand, k);
+          if (!ck) {
+            if (lane == k) s_acc[k] = 0;
+            continue;
+          }
+          int acc = 0;
+          if (lane == k) {
+            const double r = base + partial;
+            acc = !(speak <= (W.dptmn + L.dptfc * r) && p.spp == 0.);
+          }
+          acc = __shfl_sync(0xffffffffu, acc, k);
+          if (lane == k) s_acc[k] = acc;
+          if (!acc) continue;
+          const F4Line& q = cl[k];
+          if (q.vnu >= W.vnulst) {  // end of convolution (:3928, IHI=-1)
+            term_at = k;
+            if (lane == k) s_acc[k] = 0;
+            break;
+          }
+          if (lane > k && (c0 + lane) < b1 && cand) {
+            if ((q.has & 1) && jj >= q.jmin && jj <= q.jmax) partial += f4_eval(q, false, jj, dvr4, bndsq);
+            if ((q.has & 2) && jj >= q.mjmin && jj <= q.mjmax) partial += f4_eval(q, true, jj, dvr4, bndsq);
+          }
+        }
+        if (lane == 0) {
+          int n = 0;
+          const int lim = (int)((b1 - c0) < kChunk ? (b1 - c0) : kChunk);
+          for (int k = 0; k < lim && k < term_at; k++)
+            if (s_acc[k] && cl[k].has) s_acc[n++] = k;
+          s_nacc = n;
+          if (term_at < kChunk) s_term = 1;
+        }
+      }
+      __syncthreads();
+      const int nacc = s_nacc;
+      for (int j = 1 + threadIdx.x; j <= npt; j += blockDim.x) {
+        double add = 0.;
+        for (int a = 0; a < nacc; a++) {
+          const F4Line& q = cl[s_acc[a]];
+          if ((q.has & 1) && j >= q.jmin && j <= q.jmax) add += f4_eval(q, false, j, dvr4, bndsq);
+          if ((q.has & 2) && j >= q.mjmin && j <= q.mjmax) add += f4_eval(q, true, j, dvr4, bndsq);
+        }
+        R4s[j] += add;
+      }
+      __syncthreads();
+      term = s_term;
+      if (term) break;
+    }
+  }
+  __syncthreads();
+  double* out = w.r4 + (int64_t)gw * kR4Stride;
+  if (L.jrad == 1) {
+    // radiation field applied to R4 (LBLF4 :3726-3758)
+    if (threadIdx.x == 0) {
+      const double xkt = 1. / L.beta_f;
+      double vitst = W.v1r4 - dvr4, rdlast = -1.;
+      long n1 = 0, n2 = 0;
+      do {
+        n1 = n2 + 1;
+        double vi = W.v1r4 + dvr4 * double(n1 - 1), rdel;
+        double rv = radfni(vi, dvr4, xkt, vitst, rdel, rdlast);
+        n2 = fint((vitst - W.v1r4) / dvr4 + 0.001);
+        if (n2 > npt) n2 = npt;
+        for (long i = n1; i <= n2; i++) {
+          R4s[i] = R4s[i] * rv;
+          rv = rv + rdel;
+        }
+      } while (n2 < npt);
+    }
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < kR4Stride; j += blockDim.x) out[j] = (j >= 1 && j <= npt) ? R4s[j] : 0.;
+}
+
+// =========================================================================
+// RDLIN/LNCOR1 near-wing line scaling and rejection (src/oprop.f90:678-1197),
+// one CTA per layer walking the TAPE3 panels in order: each panel's lines are
+// scaled with the far-wing window and panel origin current when HIRAC1 reads
+// that panel, which is the first panel able to hold all earlier accepted lines.
+// =========================================================================
+__device__ __forceinline__ long jmax1_at(double vnu, double vft, double dv, double bhw) {
+  return fint((vnu - vft) / dv + bhw + 1.5);
+}
+
+__global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
+  const int l = blockIdx.x;
+  const LayerDev& L = w.L[l];
+  __shared__ int s_pmax, s_stop_at;
+  __shared__ int s_pread;
+  if (threadIdx.x == 0) {
+    s_pread = 0;
+  }
+  __syncthreads();
+  const double DV = L.dv;
+  const int npanel = (int)L.npanel;
+  bool stopped = false;
+  for (int64_t b = L.blk_lo; b < L.blk_hi; b++) {
+    int64_t a = ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo;
+    int64_t e = ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi;
+    const int pread = s_pread;
+    const double VFT = w.vft[L.off_panel + pread];
+    const int wi = L.nwin > 0 ? w.win_of[L.off_panel + pread] : -1;
+    if (threadIdx.x == 0) {
+      s_pmax = pread;
+      s_stop_at = 1 << 30;
+    }
+    __syncthreads();
+    const int64_t i = a + threadIdx.x;
+    int pfit = -1;
+    bool ok = false;
+    int64_t slot = i - L.near_lo + L.off_near;
+    if (i < e && !stopped && ln.iflg[i] >= 0) {
+      const int mcode = ln.mol[i];
+      const int m = mcode % 100, iso = (mcode % 1000) / 100;
+      double sui = 0.;
+      bool rej = !(m >= 1 && m <= 47 && iso >= 1 && iso <= c_isomax[m]);
+      if (!rej) {
+        const double wkm = (m <= L.nmol) ? L.wk[m] : 0.;
+        sui = (double)ln.sp[i] * wkm;
+        if (L.jrad == 1) sui = sui * radfn(ln.vnu[i], L.xkt);
+        if (sui == 0.) rej = true;
+      }
+      if (!rej) {
+        const int iflag = ln.iflg[i];
+        double yi = 0., gi = 0., g1 = 0., g2 = 0.;
+        if (iflag == 1 || iflag == 3)
+          coupling(ln, i, iflag, L.ilc_n, L.rectlc_n, L.tmpdif_n, false, yi, gi, g1, g2);
+        const double vnu = ln.vnu[i] + L.rhorat * (double)ln.pshift[i];
+        const double tmpcor = pow(L.tratio, (double)ln.tmpalf[i]);
+        const double a0 = air_width(ln, i, m) * tmpcor;
+        const double hs = (double)ln.hwhms[i] * tmpcor;
+        double alfl = a0 * (L.rhorat - L.rhoslf[m]) + hs * L.rhoslf[m];
+        if (iflag == 3) alfl = alfl * (1.0 - g1 * L.pavp0 - g2 * L.pavp2);
+        const double alfad = vnu * L.alfd1[m][iso];
+        const double zeta = alfl / (alfl + alfad);
+        const double fz = 100. * zeta;
+        long iz = fint(fz + kONEPL);
+        iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);
+        const double zd = fz - double(iz - 1);
+        double alfv = (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (alfl + alfad);
+        if (alfv < DV) alfv = DV;
+        if (alfv > L.alfmax) alfv = L.alfmax;
+        if (64. * alfv + vnu < VFT) rej = true;  // HWF3*ALFV+VNU < VFT (:1120)
+        double recalf = 0.;
+        if (!rej) {
+          recalf = 1. / alfv;
+          double epp = (double)ln.epp[i];
+          if (epp <= -1.001) epp = fabs(epp);
+          if (epp > -0.999)
+            sui = sui * L.scor[m][iso] * exp(-epp * L.betacr_n) * (1. + exp(-vnu / L.xkt));
+          const double sp = sui * (1. + gi * L.pavp2);
+          const double sppsp = (sui * yi * L.pavp0) / sp;
+          if (iflag == 0) {
+            const double speak = sui * recalf;
+            if (L.dvr4 <= 0.) {
+              if (speak <= L.dptmn) rej = true;
+            } else {
+              const WinDev& W = w.win[L.off_win + wi];
+              long jj = fint((vnu - W.v1r4) / L.dvr4 + 1.);
+              jj = jj < 1 ? 1 : (jj > W.nptr4 ? W.nptr4 : jj);
+              const double r4 = w.r4[(L.off_win + wi) * kR4Stride + jj];
+              if (speak <= (L.dptmn + L.dptfc * r4) && sppsp == 0.) rej = true;
+            }
+          }
+          if (!rej) {
+            // CNVFNV constants in panel-0 coordinates (:1283-1305)
+            const double depth = sp * recalf;
+            const double zslope = recalf * L.wavdxf;
+            const double zint = (vnu - L.vft0) / DV;
+            const double bhw = kHWDXF / zslope;
+            const long jmax1 = fint(zint + bhw + 1.5);
+            const long jmin1 = fint(zint - bhw + 1.5);
+            const double rs = zint < 0.0 ? -0.5 : 0.5;
+            const long j2 = fint(zint * (1. - L.conf2) + rs);
+            const long j3 = fint(zint * (1. - L.conf3) + rs);
+            double* str = w.n_str + 5 * slot;
+            const double* cf[5] = {c_cf1, c_cf2, c_cf3, c_cgauss, c_cer};
+#pragma unroll
+            for (int k = 0; k < 5; k++) str[k] = depth * (cf[k][iz - 1] + zd * (cf[k][iz] - cf[k][iz - 1]));
+            w.n_zint[slot] = zint;
+            w.n_zslope[slot] = zslope;
+            w.n_sppsp[slot] = sppsp;
+            w.n_jmin1[slot] = (int32_t)jmin1;
+            w.n_jmax1[slot] = (int32_t)jmax1;
+            w.n_j2[slot] = (int32_t)j2;
+            w.n_j3[slot] = (int32_t)j3;
+            ok = true;
+            // first panel whose buffer holds the line's R1 window
+            int p = pread;
+            const long excess = jmax1_at(vnu, w.vft[L.off_panel + p], DV, bhw) - L.max1;
+            if (excess > 0) p += (int)((excess + 2399) / 2400);
+            if (p > npanel) p = npanel;
+            while (p > pread && jmax1_at(vnu, w.vft[L.off_panel + p - 1], DV, bhw) <= L.max1) p--;
+            while (p < npanel && jmax1_at(vnu, w.vft[L.off_panel + p], DV, bhw) > L.max1) p++;
+            pfit = p;
+          }
+        }
+      }
+    }
+    if (ok) {
+      if (pfit >= npanel) atomicMin(&s_stop_at, (int)threadIdx.x);
+    }
+    __syncthreads();
+    const int stop_at = s_stop_at;
+    if (ok && (int)threadIdx.x > stop_at) ok = false;   // never reached by CNVFNV
+    if (ok && (int)threadIdx.x == stop_at) ok = false;
+    if (ok) atomicMax(&s_pmax, pfit);
+    if (i < e) w.n_ok[slot] = ok ? 1 : 0;
+    __syncthreads();
+    if (threadIdx.x == 0) s_pread = s_pmax;
+    if (stop_at != (1 << 30)) stopped = true;
+    __syncthreads();
+  }
+  // lines of the range beyond the walked panels are not used
+}
+
+// =========================================================================
+// CNVFNV gather onto the three grids (src/oprop.f90:1283-1351).  Each CTA
+// owns 256 consecutive points of one grid of one layer; candidate lines are
+// found by binary search on the sorted TAPE3 centres and staged in shared
+// memory; every thread sums the lines whose window covers its point.
+// =========================================================================
+__device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double x) {
+  while (lo < hi) {
+    int64_t m = (lo + hi) >> 1;
+    if (v[m] < x) lo = m + 1;
+    else hi = m;
+  }
+  return lo;
+}
+
+struct NearStage {
+  double zint, zslope, s0, s1, s2, sppsp;
+  int32_t lo, hi;
+};
+
+constexpr int kGridTile = 1024;  // points per CTA (4 per thread)
+
+__global__ void __launch_bounds__(256) k_grids(Work w, DevLines ln, DevShapes sh,
+                                               const int64_t* tile_prefix, int ntp) {
+  // tile -> (layer, grid) by binary search of the prefix (3 entries per layer)
+  const int64_t t = blockIdx.x;
+  int lo = 0, hi = ntp;
+  while (lo < hi) {
+    int m = (lo + hi) >> 1;
+    if (tile_prefix[m + 1] <= t) lo = m + 1;
+    else hi = m;
+  }
+  const int idx = lo;
+  const int l = idx / 3, grid = idx % 3;
+  const LayerDev& L = w.L[l];
+  const int64_t g0 = 1 + (t - tile_prefix[idx]) * kGridTile;
+  const int64_t ng = grid == 0 ? L.n_r1 : (grid == 1 ? L.n_r2 : L.n_r3);
+  const double dvk = grid == 0 ? L.dv : (grid == 1 ? L.dvr2 : L.dvr3);
+  const double conf = grid == 0 ? 1. : (grid == 1 ? L.conf2 : L.conf3);
+  const double reach = (grid == 0 ? 4. : (grid == 1 ? 16. : 64.)) * L.alfmax +
+                       (grid == 0 ? 2. : (grid == 1 ? 8. : 32.)) * L.dv + fabs(L.rhorat) * 1.0;
+  const int64_t g1e = (g0 + kGridTile - 1 < ng) ? g0 + kGridTile - 1 : ng;
+  __shared__ int64_t s_lo, s_hi;
+  if (threadIdx.x == 0)
+    s_lo = lower_bound_d(ln.vnu, L.near_lo, L.near_hi, L.vft0 + double(g0 - 1) * dvk - reach);
+  if (threadIdx.x == 32)
+    s_hi = lower_bound_d(ln.vnu, L.near_lo, L.near_hi, L.vft0 + double(g1e - 1) * dvk + reach);
+  __syncthreads();
+  const int64_t clo = s_lo, chi = s_hi;
+  __shared__ NearStage st[256];
+  __shared__ int s_n;
+  constexpr int PT = kGridTile / 256;
+  double acc[PT];
+#pragma unroll
+  for (int q = 0; q < PT; q++) acc[q] = 0.;
+  for (int64_t c0 = clo; c0 < chi; c0 += 256) {
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const int64_t i = c0 + threadIdx.x;
+    if (i < chi) {
+      const int64_t slot = L.off_near + (i - L.near_lo);
+      if (w.n_ok[slot]) {
+        NearStage q;
+        q.zint = w.n_zint[slot];
+        q.zslope = w.n_zslope[slot];
+        const double* sv = w.n_str + 5 * slot;
+        const int32_t sh2 = grid == 0 ? 0 : (grid == 1 ? w.n_j2[slot] : w.n_j3[slot]);
+        q.lo = w.n_jmin1[slot] - sh2;
+        q.hi = w.n_jmax1[slot] - sh2;
+        if (grid == 0) {
+          q.s0 = sv[0];
+          q.s1 = sv[3];
+          q.s2 = sv[4];
+        } else {
+          q.s0 = sv[grid];
+          q.s1 = q.s2 = 0.;
+        }
+        q.sppsp = w.n_sppsp[slot];
+        if (q.hi >= g0 && q.lo <= g1e) {
+          const int k = atomicAdd(&s_n, 1);
+          st[k] = q;
+        }
+      }
+    }
+    __syncthreads();
+    const int n = s_n;
+    for (int k = 0; k < n; k++) {
+      const NearStage& q = st[k];
+#pragma unroll
+      for (int qq = 0; qq < PT; qq++) {
+        const int64_t g = g0 + threadIdx.x + 256 * qq;
+        if (g > g1e || g < q.lo || g > q.hi) continue;
+        const double zf = (double(g - 1) - q.zint * conf) * q.zslope;
+        long iz = fint(fabs(zf) + 1.5);
+        iz = iz > kNfmx ? kNfmx : iz;  // window limits keep iz <= 2501
+        double v;
+        if (grid == 0) v = q.s0 * sh.f1[iz] + q.s1 * sh.fg[iz] + q.s2 * sh.xver[iz];
+        else if (grid == 1) v = q.s0 * sh.f2[iz];
+        else v = q.s0 * sh.f3[iz];
+        if (q.sppsp != 0.) {
+          // line coupling (:1322-1351): strengths scaled by CLCk*DPTRAT, times ZF
+          const double clc = grid == 0 ? 4. / 2000. : (grid == 1 ? 16. / 2000. : 64. / 2000.);
+          v = v + v * clc * q.sppsp * zf;
+        }
+        acc[qq] += v;
+      }
+    }
+    __syncthreads();
+  }
+  double* out = grid == 0 ? w.r1 + L.off_r1 : (grid == 1 ? w.r2 + L.off_r2 : w.r3 + L.off_r3);
+#pragma unroll
+  for (int qq = 0; qq < PT; qq++) {
+    const int64_t g = g0 + threadIdx.x + 256 * qq;
+    if (g <= g1e) out[g] = acc[qq];
+  }
+}
+
+// =========================================================================
+// Continuum: mt_ckd_h2o_absco + CONTNM (mt_ckd_h2o_module.f90:68-174,
+// contnm.f90:279-311), one CTA per layer onto the 1 cm-1 ABSRB grid.
+// =========================================================================
+__global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn) {
+  const int l = blockIdx.x;
+  const LayerDev& L = w.L[l];
+  double* absrb = w.absrb + L.off_abs;  // 1-based, nptabs+4
+  for (int64_t j = threadIdx.x; j < L.nptabs + 8; j += blockDim.x) absrb[j] = 0.;
+  if (!L.icntnm) return;
+  __syncthreads();
+  double wtot = 0.;
+  const double h2o_fac = L.h2o_fac;  // WK(1)/WTOT of CONTNM (contnm.f90:261)
+  if (!((L.v2 > -20.0) && (L.v1 < 20000.) && ((xself > 0.) || (xfrgn > 0)))) return;
+  (void)wtot;
+  const double wv1 = L.v1abs, wv2 = L.v2abs, dva = L.dvabs;
+  auto wvn = [&](int64_t i) { return ck.v0 + ck.dv * double(i - 1); };
+  __shared__ int64_t s_i1, s_i2;
+  if (threadIdx.x == 0) {
+    const double dvc = wvn(2) - wvn(1);
+    int64_t i = 1;
+    while (i < ck.n && wvn(i) <= (wv1 - 2 * dvc)) i++;
+    int64_t i1 = i - 1;
+    if (i1 == 0) i1 = 1;
+    while (i < ck.n && wvn(i) < (wv2 + 2 * dvc)) i++;
+    s_i1 = i1;
+    s_i2 = i;
+  }
+  __syncthreads();
+  const int64_t i1 = s_i1, i2 = s_i2;
+  const int64_t ncoeff = i2 - i1 + 1;
+  const double xkt = L.tave / kRADCN2;
+  const double rho = (L.pave / ck.ref_press) * (ck.ref_temp / L.tave);
+  const bool radflag = (L.jrad != 0);
+  const double dvc = wvn(2) - wvn(1);
+  const int64_t nptabs = fint((wv2 - wv1) / dva + 1);
+  int64_t ist = fint(2 + (wvn(1) - wv1) / dva + 1.e-5);
+  if (ist < 1) ist = 1;
+  int64_t lst = fint(1 + (wvn(ck.n) - wv1) / dva + 1.e-5);
+  if (lst > nptabs) lst = nptabs;
+  const double v1a = wvn(i1), v2a = wvn(i2);
+  int64_t ilo = fint((v1a + dvc - wv1) / dva + 1. + kONEMI);
+  if (ilo < ist) ilo = ist;
+  int64_t ihi = fint((v2a - dvc - wv1) / dva + kONEMI);
+  if (ihi > lst) ihi = lst;
+  auto coef = [&](int64_t k, bool self) -> double {
+    if (k < 1 || k > ncoeff) return 0.;
+    const int64_t ii = i1 + k - 1;
+    const double vi = wvn(ii);
+    double c;
+    if (self)
+      c = ck.self[ii - 1] * pow(ck.ref_temp / L.tave, ck.texp[ii - 1]) * h2o_fac * rho;
+    else
+      c = ck.forn[ii - 1] * (1 - h2o_fac) * rho;
+    if (radflag) {
+      const double x = vi / xkt;
+      double r = vi;
+      if (x <= 0.01) r = 0.5 * x * vi;
+      else if (x <= 10.) {
+        const double e = exp(-x);
+        r = vi * (1 - e) / (1. + e);
+      }
+      c = c * r;
+    }
+    return c;
+  };
+  const double rec = 1. / dvc;
+  for (int64_t I = ilo + threadIdx.x; I <= ihi; I += blockDim.x) {
+    const double vi = wv1 + dva * double(I - 1);
+    const long J = fint((vi - v1a) * rec + kONEPL);
+    const double vj = v1a + dvc * double(J - 1);
+    const double p = rec * (vi - vj);
+    const double C = (3. - 2. * p) * p * p;
+    const double B = 0.5 * p * (1. - p);
+    const double b1 = B * (1. - p), b2 = B * p;
+    double cs = -coef(J - 1, true) * b1 + coef(J, true) * (1. - C + b2) +
+                coef(J + 1, true) * (C + b1) - coef(J + 2, true) * b2;
+    double cf = -coef(J - 1, false) * b1 + coef(J, false) * (1. - C + b2) +
+                coef(J + 1, false) * (C + b1) - coef(J + 2, false) * b2;
+    absrb[I] = L.wk[1] * cs * xself + L.wk[1] * cf * xfrgn;
+  }
+}
+
+// =========================================================================
+// PANEL combination (src/oprop.f90:1371-1561) on the global grids:
+//   R3 += XINT(R4 of the panel's window) + XINT(ABSRB)      (:515-519)
+//   R2 += 4-point interpolation of R3                        (:1459-1480)
+//   OD  = R1 + 4-point interpolation of R2, times RADFNI     (:1482-1519)
+// =========================================================================
+__device__ __forceinline__ double xint_at(double v1a, double v2a, double dva, const double* A,
+                                          double vft, double dvr3, long I, long n1, long n2) {
+  const double rec = 1. / dva;
+  long ilo = fint((v1a + dva - vft) / dvr3 + 1. + kONEMI);
+  if (ilo < n1) ilo = n1;
+  long ihi = fint((v2a - dva - vft) / dvr3 + kONEMI);
+  if (ihi > n2) ihi = n2;
+  if (I < ilo || I > ihi) return 0.;
+  const double vi = vft + dvr3 * double(I - 1);
+  const long J = fint((vi - v1a) * rec + kONEPL);
+  const double vj = v1a + dva * double(J - 1);
+  const double p = rec * (vi - vj);
+  const double C = (3. - 2. * p) * p * p;
+  const double B = 0.5 * p * (1. - p);
+  const double b1 = B * (1. - p), b2 = B * p;
+  return -A[J - 1] * b1 + A[J] * (1. - C + b2) + A[J + 1] * (C + b1) - A[J + 2] * b2;
+}
+
+__global__ void k_combine_r3(Work w) {
+  const int l = blockIdx.y;
+  const LayerDev& L = w.L[l];
+  const int64_t g = 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > L.n_r3) return;
+  // panel owning R3 point g: panel 0 covers 1..155, panel p>=1 covers
+  // 150p+6..150p+155 (N1R3/N2R3, src/oprop.f90:474-486)
+  int64_t p = (g <= 155) ? 0 : (g - 6) / 150;
+  if (p >= L.npanel) return;
+  const long I = (long)(g - 150 * p);
+  const long n1 = (p == 0) ? 1 : 6;
+  const double vft = w.vft[L.off_panel + p];
+  double add = 0.;
+  if (L.ilblf4 >= 1 && L.nwin > 0) {
+    const int wi = w.win_of[L.off_panel + p];
+    const WinDev& W = w.win[L.off_win + wi];
+    add += xint_at(W.v1r4, W.v2r4, L.dvr4, w.r4 + (L.off_win + wi) * kR4Stride, vft, L.dvr3, I,
+                   n1, 155);
+  }
+  if (L.icntnm >= 1)
+    add += xint_at(L.v1abs, L.v2abs, L.dvabs, w.absrb + L.off_abs, vft, L.dvr3, I, n1, 155);
+  w.r3[L.off_r3 + g] += add;
+}
+
+constexpr double X00 = -7. / 128., X01 = 105. / 128., X02 = 35. / 128., X03 = -5. / 128.,
+                 X10 = -1. / 16., X11 = 9. / 16.;
+
+__device__ __forceinline__ double interp4(const double* R, int64_t J, int r) {
+  // value added at fine point J*4-3+r from coarse points J-1..J+2
+  if (r == 0) return R[J];
+  if (r == 1) return X00 * R[J - 1] + X01 * R[J] + X02 * R[J + 1] + X03 * R[J + 2];
+  if (r == 2) return X10 * (R[J - 1] + R[J + 2]) + X11 * (R[J] + R[J + 1]);
+  return X03 * R[J - 1] + X02 * R[J] + X01 * R[J + 1] + X00 * R[J + 2];
+}
+
+__global__ void k_combine_r2(Work w) {
+  const int l = blockIdx.y;
+  const LayerDev& L = w.L[l];
+  const int64_t g = 5 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g > L.n_r2 - 3) return;
+  const int64_t J3 = (g - 1) / 4 + 1;
+  const int r = (int)((g - 1) % 4);
+  w.r2[L.off_r2 + g] += interp4(w.r3 + L.off_r3, J3, r);
+}
+
+// One CTA per (layer, panel): radiation segments (RADFNI restarted each
+// panel) built by thread 0 in shared memory, then the panel's points.
+__global__ void __launch_bounds__(256) k_combine_od(Work w, const int32_t* panel_layer,
+                                                    const int64_t* panel_base) {
+  const int64_t gp = blockIdx.x;
+  const int l = panel_layer[gp];
+  const LayerDev& L = w.L[l];
+  const int64_t p = gp - panel_base[l];
+  const double DV = L.dv;
+  const double vft = w.vft[L.off_panel + p];
+  const long nhi = (p == L.npanel - 1) ? (long)(L.npts - 2400 * (L.npanel - 1) + 32) : 2432;
+  extern __shared__ double segbuf[];  // [start, radvi, rdel] * nseg
+  __shared__ int s_nseg;
+  const int maxseg = 2400;
+  if (L.jrad == 0) {
+    if (threadIdx.x == 0) {
+      const double v1p = vft + double(33 - 1) * DV;
+      double vi = v1p - DV, vitst = vi, rdlast = -1.;
+      long n1 = 32, n2 = 32;
+      int ns = 0;
+      do {
+        n1 = n2 + 1;
+        vi = vft + double(n1 - 1) * DV;
+        double rdel;
+        double rv = radfni(vi, DV, L.xkt, vitst, rdel, rdlast);
+        n2 = fint((vitst - vft) / DV + 0.001);
+        if (n2 > nhi) n2 = nhi;
+        if (ns < maxseg) {
+          segbuf[3 * ns] = double(n1);
+          segbuf[3 * ns + 1] = rv;
+          segbuf[3 * ns + 2] = rdel;
+          ns++;
+        }
+      } while (n2 < nhi);
+      s_nseg = ns;
+    }
+    __syncthreads();
+  }
+  const double* r1 = w.r1 + L.off_r1;
+  const double* r2 = w.r2 + L.off_r2;
+  for (long I = 33 + threadIdx.x; I <= nhi; I += blockDim.x) {
+    const int64_t g = 2400 * p + I;
+    const int64_t J2 = (g - 1) / 4 + 1;
+    const int r = (int)((g - 1) % 4);
+    double od = r1[g] + interp4(r2, J2, r);
+    if (L.jrad == 0) {
+      int lo = 0, hi = s_nseg - 1;
+      while (lo < hi) {
+        int m = (lo + hi + 1) >> 1;
+        if (segbuf[3 * m] <= double(I)) lo = m;
+        else hi = m - 1;
+      }
+      const double rad = segbuf[3 * lo + 1] + double(I - (long)segbuf[3 * lo]) * segbuf[3 * lo + 2];
+      od = od * rad;
+    }
+    w.od[L.off_od + (g - 33)] = od;
+  }
+}
+
+// =========================================================================
+// XMERGE for one layer: EMIN (src/xmerge.f90:1795-1855) then EMINIT
+// (:2436-2484) for the first layer or RADNN IPATH=1 (:2985-3130) after.
+// =========================================================================
+__global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const double* od,
+                        int first, double dv_old, int64_t n_old, const double* rad_in,
+                        const double* tr_in, double* rad_out, double* tr_out, double tbnd,
+                        double emis, int iemit, double tzu) {
+  const LayerDev& L = *Lp;
+  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= L.npts) return;
+  const double DV = L.dv;
+  const int64_t p = f / 2400;
+  const double vi = (vft_panel[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
+  const double odv = od[f];
+  if (iemit == 0) {
+    // ABINIT / ABSMRG: optical depths add (regrid below)
+    double old = 0.;
+    if (!first) {
+      const double dvk = DV;
+      long itype = (dv_old == dvk) ? 0 : fint(dvk / (dv_old - dvk) + 0.5);
+      const int64_t LL = itype + 1;
+      const int64_t q = f / LL, r = f % LL;
+      auto O = [&](int64_t c) { return rad_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+      if (r == 0) {
+        old = O(q * itype);
+      } else {
+        const int64_t ipl = q * itype + r - 1;
+        const double P = 1.0 - double(r) / double(LL);
+        const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
+        const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
+        old = a1 * O(ipl - 1) + a2 * O(ipl) + a3 * O(ipl + 1) + a4 * O(ipl + 2);
+      }
+    }
+    rad_out[f] = odv + old;
+    if (tr_out) tr_out[f] = 0.;
+    return;
+  }
+  const double xkt = L.tave / kRADCN2;
+  const double xkta = tzu / kRADCN2;
+  double o = odv;
+  if (o < -kODLO) o = -kODLO;
+  const double tr = exp(-o);
+  const double fi = (o <= kODLO) ? o / 6. : 1. - 2. * (tr / (tr - 1.) + 1. / o);
+  const double bb = planck(vi, xkt);
+  const double bbd = (xkta > 0.) ? planck(vi, xkta) - bb : 0.;
+  double em = (1. - tr) * (bb + bbd * fi);
+  if (first) {
+    if (tbnd > 0.) em = em + tr * planck(vi, tbnd / kRADCN2) * emis;
+    rad_out[f] = em;
+    tr_out[f] = tr;
+    return;
+  }
+  const double dvk = DV;
+  const long itype = (dv_old == dvk) ? 0 : fint(dvk / (dv_old - dvk) + 0.5);
+  const int64_t LL = itype + 1;
+  const int64_t q = f / LL, r = f % LL;
+  auto R = [&](int64_t c) { return rad_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+  auto T = [&](int64_t c) { return tr_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+  double ro, to;
+  if (itype == 0) {
+    ro = R(f);
+    to = T(f);
+  } else if (r == 0) {
+    ro = R(q * itype);
+    to = T(q * itype);
+  } else {
+    const int64_t ipl = q * itype + r - 1;
+    const double P = 1.0 - double(r) / double(LL);
+    const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
+    const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
+    ro = a1 * R(ipl - 1) + a2 * R(ipl) + a3 * R(ipl + 1) + a4 * R(ipl + 2);
+    to = a1 * T(ipl - 1) + a2 * T(ipl) + a3 * T(ipl + 1) + a4 * T(ipl + 2);
+  }
+  rad_out[f] = tr * ro + em;
+  tr_out[f] = tr * to;
+}
+
+}  // namespace
+
+void init_kernel_attributes() {
+  cudaFuncSetAttribute(k_combine_od, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       3 * 2400 * (int)sizeof(double));
+}
+
+void upload_voicon() {
+  cudaMemcpyToSymbol(c_avrat, LBL_AVRAT, sizeof(LBL_AVRAT));
+  cudaMemcpyToSymbol(c_cf1, LBL_CF1, sizeof(LBL_CF1));
+  cudaMemcpyToSymbol(c_cf2, LBL_CF2, sizeof(LBL_CF2));
+  cudaMemcpyToSymbol(c_cf3, LBL_CF3, sizeof(LBL_CF3));
+  cudaMemcpyToSymbol(c_cgauss, LBL_CGAUSS, sizeof(LBL_CGAUSS));
+  cudaMemcpyToSymbol(c_cer, LBL_CER, sizeof(LBL_CER));
+  int iso[48] = {0};
+  for (int m = 1; m <= 47; m++) iso[m] = LBL_ISO_MAX[m - 1];
+  cudaMemcpyToSymbol(c_isomax, iso, sizeof(iso));
+}
+
+cudaError_t launch_far_scale(const Work& w, const DevLines& ln, int64_t max_far, cudaStream_t s) {
+  if (max_far <= 0) return cudaSuccess;
+  dim3 g((unsigned)((max_far + 255) / 256), (unsigned)w.nlay);
+  k_far_scale<<<g, 256, 0, s>>>(w, ln);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_base,
+                          int64_t nblk_total, cudaStream_t s) {
+  if (nblk_total > 0) {
+    k_shr_count<<<(unsigned)((nblk_total + 127) / 128), 128, 0, s>>>(w, bs, blk_base, w.nlay);
+    k_shr_plan<<<(w.nlay + 31) / 32, 32, 0, s>>>(w, blk_base);
+    k_shr_write<<<(unsigned)((nblk_total + 127) / 128), 128, 0, s>>>(w, bs, blk_base, w.nlay);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_layer,
+                            cudaStream_t s) {
+  if (nwin_total <= 0) return cudaSuccess;
+  k_far_wing<<<nwin_total, 256, 0, s>>>(w, win_layer);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s) {
+  k_near_scale<<<w.nlay, 256, 0, s>>>(w, ln);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
+                             cudaStream_t s) {
+  k_continuum<<<w.nlay, 256, 0, s>>>(w, ck, xself, xfrgn);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grids(const Work& w, const DevLines& ln, const DevShapes& sh,
+                         const int64_t* tile_prefix, int64_t ntiles, int precision,
+                         cudaStream_t s) {
+  (void)precision;
+  if (ntiles <= 0) return cudaSuccess;
+  k_grids<<<(unsigned)ntiles, 256, 0, s>>>(w, ln, sh, tile_prefix, 3 * w.nlay);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine(const Work& w, int64_t max_r3, int64_t max_r2, int64_t npanel_total,
+                           const int32_t* panel_layer, const int64_t* panel_base,
+                           cudaStream_t s) {
+  if (max_r3 > 0) {
+    dim3 g3((unsigned)((max_r3 + 255) / 256), (unsigned)w.nlay);
+    k_combine_r3<<<g3, 256, 0, s>>>(w);
+  }
+  if (max_r2 > 0) {
+    dim3 g2((unsigned)((max_r2 + 255) / 256), (unsigned)w.nlay);
+    k_combine_r2<<<g2, 256, 0, s>>>(w);
+  }
+  k_combine_od<<<(unsigned)npanel_total, 256, 3 * 2400 * sizeof(double), s>>>(w, panel_layer,
+                                                                             panel_base);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const double* od,
+                         int64_t npts, int first, double dv_old, int64_t n_old,
+                         const double* rad_in, const double* tr_in, double* rad_out,
+                         double* tr_out, double tbnd, double emis, int iemit, double tzu,
+                         cudaStream_t s) {
+  k_merge<<<(unsigned)((npts + 255) / 256), 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old,
+                                                        rad_in, tr_in, rad_out, tr_out, tbnd,
+                                                        emis, iemit, tzu);
+  return cudaGetLastError();
+}
+
+}  // namespace lbl

@@ -1,0 +1,99 @@
+// lbl_kernels.cuh -- device-side data structures and kernel launchers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "lbl_plan.h"
+
+namespace lbl {
+
+constexpr int kSegMaxBlk = 48;  // panels a LINF4 segment may span
+
+// Resident TAPE3 lines (device pointers).
+struct DevLines {
+  const double* vnu;
+  const float *sp, *alfa, *epp, *hwhms, *tmpalf, *pshift;
+  const int32_t *mol, *iflg;
+  const int64_t* bs;  // panel starts, nblk+1
+  int64_t n, nblk;
+};
+
+// Line-shape tables, 1-based, kNfmx+1 entries each (device pointers).
+struct DevShapes {
+  const double *f1, *f2, *f3, *fg, *xver;
+  const float *f1s, *f2s, *f3s, *fgs, *xvers;
+};
+
+// Continuum coefficient table (device pointers).
+struct DevMtckd {
+  const double *self, *forn, *texp;
+  double v0, dv, ref_press, ref_temp;
+  int64_t n;
+};
+
+// Work buffers of one batch of layers; offsets come from LayerDev.
+struct Work {
+  const LayerDev* L;     // nlay entries
+  int32_t nlay;
+  // per-panel
+  const double* vft;
+  const int32_t* win_of;
+  int32_t* nseg;         // radiation segments per panel
+  double* seg;           // [panel][kMaxSeg][3]: start, radvi, rdel
+  // windows
+  const WinDev* win;
+  double* r4;
+  // far-wing raw lines (slot = line index - far_lo)
+  double *f_vnu, *f_sp, *f_alfa, *f_epp, *f_spp;
+  int8_t *f_ok, *f_co2;
+  // shrunk lines
+  double *s_vnu, *s_sp, *s_alfa, *s_epp, *s_spp;
+  int8_t* s_co2;
+  int64_t* s_count;      // per layer
+  int64_t* b9_start;     // per layer TAPE9 block starts (local shrunk index)
+  double* b9_vnuhi;
+  int64_t* b9_count;     // per layer number of TAPE9 blocks
+  // LINF4 segmenting: per (layer, start panel) count tables and segments
+  int32_t *c_raw, *c_out;  // [far panel][kSegMaxBlk]
+  int32_t *seg_blk, *seg_nblk;
+  int64_t* seg_out;
+  int64_t* seg_count;    // per layer
+  // near-wing lines (slot = line index - near_lo)
+  double *n_zint, *n_zslope, *n_str;  // n_str: 5 per slot (F1,F2,F3,FG,VER)
+  double* n_sppsp;
+  int32_t *n_jmin1, *n_jmax1, *n_j2, *n_j3;
+  int8_t* n_ok;
+  // grids
+  double *r1, *r2, *r3;
+  double* absrb;
+  double* od;
+  // diagnostics
+  int32_t* status;       // device error flag (0 ok)
+};
+
+void upload_voicon();
+
+cudaError_t launch_far_scale(const Work& w, const DevLines& ln, int64_t max_far, cudaStream_t s);
+cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_base,
+                          int64_t nblk_total, cudaStream_t s);
+cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_layer,
+                            cudaStream_t s);
+cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s);
+cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
+                             cudaStream_t s);
+cudaError_t launch_grids(const Work& w, const DevLines& ln, const DevShapes& sh,
+                         const int64_t* tile_prefix, int64_t ntiles, int precision,
+                         cudaStream_t s);
+cudaError_t launch_combine(const Work& w, int64_t max_r3, int64_t max_r2, int64_t npanel_total,
+                           const int32_t* panel_layer, const int64_t* panel_base,
+                           cudaStream_t s);
+// One merge step (EMINIT when first) for the layer whose LayerDev is Ld.
+cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const double* od,
+                         int64_t npts, int first, double dv_old, int64_t n_old,
+                         const double* rad_in, const double* tr_in, double* rad_out,
+                         double* tr_out, double tbnd, double emis, int iemit, double tzu,
+                         cudaStream_t s);
+void init_kernel_attributes();
+
+}  // namespace lbl

@@ -1,0 +1,467 @@
+// lbl_plan.cpp -- host-side planning: DV rule, per-layer constants, panel
+// and far-wing window schedule, line-index ranges.  Compiled without FMA
+// contraction so the FP64 schedule arithmetic rounds exactly as the
+// reference's does (each product and sum rounded separately).
+#include "lbl_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "../data/ref_tables.h"
+
+namespace lbl {
+namespace {
+
+const double PI = 3.1415926535898;        // src/phys_consts.f90:66
+const double BOLTZ = 1.3806503E-16;
+const double CLIGHT = 2.99792458E+10;
+const double AVOGAD = 6.02214199E+23;
+const double RADCN2 = 1.4387752;
+const double ONEPL = 1.001;
+const double P0 = 1013.25, TEMP0 = 296.;   // src/lblrtm.f90:2115-2116
+const double HWF3 = 64.;
+const double DXF1 = 0.002, DXF2 = 0.008, DXF3 = 0.032;
+const double TEMPLC[5] = {0., 200., 250., 296., 340.};
+
+inline long fint(double x) { return (long)x; }
+
+// Radiation term (RADFN, src/oprop.f90:2235-2296).
+double radfn(double vi, double xkt) {
+  if (xkt > 0.0) {
+    double x = vi / xkt;
+    if (x <= 0.01) return 0.5 * x * vi;
+    if (x <= 10.0) {
+      double e = std::exp(-x);
+      return vi * (1. - e) / (1. + e);
+    }
+  }
+  return vi;
+}
+
+// Lagrange 3/4-point table recall of TIPS (AtoB, src/oprop.f90:11708).
+double lagrange_recall(double t, const double* T, const double* Q, int n) {
+  auto nz = [](double d) { return d == 0. ? 0.0001 : d; };
+  for (int i = 1; i < n; i++) {            // 0-based i <-> Fortran I = i+1
+    if (T[i] < t) continue;
+    int I = i + 1;
+    if (I < 3 || I == n) {
+      int J = (I < 3) ? 3 : n;
+      const double a0 = T[J - 3], a1 = T[J - 2], a2 = T[J - 1];
+      double w0 = (t - a1) * (t - a2) / (nz(a0 - a1) * nz(a0 - a2));
+      double w1 = (t - a0) * (t - a2) / (nz(a1 - a0) * nz(a1 - a2));
+      double w2 = (t - a0) * (t - a1) / (nz(a2 - a0) * nz(a2 - a1));
+      return w0 * Q[J - 3] + w1 * Q[J - 2] + w2 * Q[J - 1];
+    }
+    const double a0 = T[I - 3], a1 = T[I - 2], a2 = T[I - 1], a3 = T[I];
+    double w0 = (t - a1) * (t - a2) * (t - a3);
+    w0 = w0 / (nz(a0 - a1) * nz(a0 - a2) * nz(a0 - a3));
+    double w1 = (t - a0) * (t - a2) * (t - a3);
+    w1 = w1 / (nz(a1 - a0) * nz(a1 - a2) * nz(a1 - a3));
+    double w2 = (t - a0) * (t - a1) * (t - a3);
+    w2 = w2 / (nz(a2 - a0) * nz(a2 - a1) * nz(a2 - a3));
+    double w3 = (t - a0) * (t - a1) * (t - a2);
+    w3 = w3 / (nz(a3 - a0) * nz(a3 - a1) * nz(a3 - a2));
+    return w0 * Q[I - 3] + w1 * Q[I - 2] + w2 * Q[I - 1] + w3 * Q[I];
+  }
+  return 0.;
+}
+
+bool partition_q(int mol, int iso, double t, double* q) {
+  if (mol < 1 || mol > LBL_NQMOL || iso < 1 || iso > LBL_QNISO[mol - 1]) return false;
+  if (t < 70. || t > 3000.) return false;
+  *q = lagrange_recall(t, LBL_TDAT, LBL_QOFT[mol - 1][iso - 1], 119);
+  return true;
+}
+
+}  // namespace
+
+void build_shape_tables(ShapeTables* t) {
+  // Sub-functions of the approximate Voigt shape (SHAPEL/SHAPEG/VERFN,
+  // src/oprop.f90:1822-1991): F1 = L - Q1 on 0..4, F2 = Q1 - Q2 (then
+  // L - Q2) on 0..16, F3 = Q2 - Q3 (then L - Q3) on 0..64, with
+  // Q_k(x^2) = A(z_k) + B(z_k) x^2 matching the Lorentzian L at z_k.
+  std::memset(t, 0, sizeof(*t));
+  const double rpi = 1. / (2. * std::asin(1.));
+  auto A = [](double z) { return (1. + 2. * z * z) / std::pow(1. + z * z, 2); };
+  auto B = [](double z) { return -1. / std::pow(1. + z * z, 2); };
+  const double a1 = A(4.), b1 = B(4.), a2 = A(16.), b2 = B(16.), a3 = A(64.), b3 = B(64.);
+  auto lor = [](double x2) { return 1. / (1. + x2); };
+  t->f1[1] = rpi * (lor(0.) - a1);
+  for (int j = 2; j <= 2001; j++) {
+    double x = double(j - 1) * DXF1, x2 = x * x;
+    t->f1[j] = rpi * (lor(x2) - (a1 + b1 * x2));
+  }
+  t->f1[2001] = 0.;
+  t->f2[1] = rpi * (a1 - a2);
+  long j1 = fint(4. / DXF2 + 1.001);
+  for (long j = 2; j <= 2001; j++) {
+    double x = double(j - 1) * DXF2, x2 = x * x;
+    t->f2[j] = (j <= j1) ? rpi * ((a1 + b1 * x2) - (a2 + b2 * x2))
+                         : rpi * (lor(x2) - (a2 + b2 * x2));
+  }
+  t->f2[2001] = 0.;
+  t->f3[1] = rpi * (a2 - a3);
+  long j2 = fint(16. / DXF3 + 1.001);
+  for (long j = 2; j <= 2001; j++) {
+    double x = double(j - 1) * DXF3, x2 = x * x;
+    t->f3[j] = (j <= j2) ? rpi * ((a2 + b2 * x2) - (a3 + b3 * x2))
+                         : rpi * (lor(x2) - (a3 + b3 * x2));
+  }
+  const double ln2 = std::log(2.);
+  const double gnorm = std::sqrt(ln2 * rpi);
+  t->fg[1] = gnorm * std::exp(-ln2 * 0.);
+  for (int j = 2; j <= 2001; j++) {
+    double x = double(j - 1) * DXF1;
+    t->fg[j] = gnorm * std::exp(-ln2 * (x * x));
+  }
+  t->fg[2001] = 0.;
+  const double cexp = 0.45, ce0 = 1., ce2 = -.20737285249, ce4 = -.00872684335747;
+  const double se0 = std::sqrt(cexp / PI), ae2 = 2. * cexp, ae4 = ae2 * ae2 / 3.;
+  for (int i = 1; i <= kNfmx; i++) {
+    double z = DXF1 * double(i - 1), z2 = z * z;
+    double xe0 = se0 * std::exp(-cexp * z2);
+    t->xver[i] = (1. / (ce0 + ce2 + ce4)) * (ce0 + ce2 * ae2 * z2 + ce4 * ae4 * z2 * z2) * xe0;
+  }
+}
+
+int dv_rule(const lbl_run& R, lbl_layer* Ls, int nlay, std::string* err) {
+  double dv = 0.;
+  const bool iset = R.dvset > 0.;
+  for (int l = 0; l < nlay; l++) {
+    lbl_layer& L = Ls[l];
+    if (L.nmol < 1 || L.nmol > LBL_WKDIM || L.pave <= 0. || L.tave <= 0.) {
+      *err = "layer " + std::to_string(l) + ": bad nmol/pave/tave";
+      return LBL_E_ARG;
+    }
+    double sumwk = 0.;
+    for (int m = 0; m < L.nmol; m++) sumwk = sumwk + L.wk[m];
+    double wtotl = sumwk + L.wbroad;
+    double frh2o = L.wk[0] / wtotl;
+    double alfcor = (L.pave / P0) * std::sqrt(TEMP0 / L.tave);
+    double h2oslf = (1. - frh2o + 5. * frh2o);
+    double albar = R.alfal0 * alfcor * h2oslf;
+    double adbar = 3.58115E-07 * (0.5 * (R.v1 + R.v2)) * std::sqrt(L.tave / R.avmass);
+    double avbar = 0.5 * (albar + std::sqrt(albar * albar + 4. * adbar * adbar));
+    double olddv = dv;
+    dv = avbar / R.sample;
+    if (dv < R.dvset && iset) {
+      dv = olddv;
+      if (l == 0 && dv == 0.) dv = R.dvset;
+    }
+    long itype = 99;
+    if (l == 0) {
+      long iscal = fint(std::log10(dv) - 3.);
+      double scal = 1.;
+      for (long k = 0; k < std::labs(iscal); k++) scal *= 10.;
+      if (iscal < 0) scal = 1. / scal;
+      long idv = fint((dv / scal) + 0.5);
+      if (idv % 2 > 0) idv = idv + 1;
+      dv = scal * double(idv);
+    } else {
+      double type = olddv / dv;
+      if (type > 2.5) {
+        *err = "DV rule: OLDDV/DV above 2.5 at layer " + std::to_string(l) +
+               " ('PATH; ISTOP EQ 1')";
+        return LBL_E_RANGE;
+      } else if (type >= 1.2) {
+        itype = fint(1. / (type - 1.) + 0.5);
+        if (itype == 3) itype = 2;
+        dv = olddv * double(itype) / double(itype + 1);
+      } else if (type >= 0.8) {
+        dv = olddv;
+        itype = 0;
+      } else {
+        dv = olddv;
+        itype = 0;
+        if (R.iemit == 0) {
+          itype = fint(type / (1. - type) + 0.5);
+          dv = dv * double(itype + 1) / double(itype);
+          itype = -itype;
+        }
+      }
+    }
+    L.dv = dv;
+    L.itype = (int32_t)itype;
+  }
+  return LBL_OK;
+}
+
+int64_t layer_npts(const lbl_run& R, double dv) {
+  double vft = R.v1 - 32. * dv;
+  int64_t n = 0;
+  for (;;) {
+    long nhi = 2432;
+    if ((vft + double(nhi - 1) * dv) > R.v2) {
+      nhi = fint((R.v2 - vft) / dv + 1.);
+      double v2p = vft + double(nhi - 1) * dv;
+      if (v2p < R.v2) nhi = nhi + 1;
+      return n + (nhi - 33 + 1);
+    }
+    n += 2400;
+    vft = vft + double(kNlim1 - 1) * dv;
+  }
+}
+
+int next_jrad(const lbl_run& R, const lbl_layer& L, int jrad) {
+  double xkt = L.tave / RADCN2;
+  if (((R.v1 / xkt) < 5.) && (jrad != -1)) return 0;
+  return jrad;
+}
+
+int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad_in, const HostLines& H,
+               LayerPlan* P, std::string* err) {
+  const double* vnu = H.vnu;
+  const int64_t nlines = H.n;
+  const int64_t* bs = H.bs;
+  const int64_t nblk = H.nblk;
+  LayerDev& d = P->d;
+  std::memset(&d, 0, sizeof(d));
+  if (L.nmol < 1 || L.nmol > kNMolTab) {
+    *err = "nmol must be 1..7 (molecules with TIPS tables)";
+    return LBL_E_RANGE;
+  }
+  if (!(L.dv > 0.)) {
+    *err = "layer dv not set (run lbl_dv_rule)";
+    return LBL_E_ARG;
+  }
+  if (L.tave < 70. || L.tave > 3000.) {
+    *err = "layer temperature outside the TIPS range 70-3000 K";
+    return LBL_E_RANGE;
+  }
+  const double DV = L.dv;
+  d.pave = L.pave;
+  d.tave = L.tave;
+  d.dv = DV;
+  d.v1 = R.v1;
+  d.v2 = R.v2;
+  d.nmol = L.nmol;
+  d.jrad = next_jrad(R, L, jrad_in);
+  d.ilblf4 = R.ilblf4;
+  d.icntnm = R.icntnm;
+  d.xkt = L.tave / RADCN2;
+  const double xkt0 = TEMP0 / RADCN2;
+  d.betacr_n = (1. / d.xkt) - (1. / xkt0);
+  d.beta_f = RADCN2 / L.tave;
+  d.betacr_f = d.beta_f - RADCN2 / TEMP0;
+  d.tratio = L.tave / TEMP0;
+  d.rhorat = (L.pave / P0) * (TEMP0 / L.tave);
+  d.pavp0 = L.pave / P0;
+  d.pavp2 = d.pavp0 * d.pavp0;
+  // line-coupling temperature brackets: LNCOR1 (:989-997) and LINF4 (:3124-3130)
+  long ilc = 1;
+  for (long il = 1; il <= 3; il++) {
+    ilc = il;
+    if (L.tave < TEMPLC[ilc + 1]) break;
+  }
+  d.ilc_n = (int32_t)ilc;
+  d.rectlc_n = 1.0 / (TEMPLC[ilc + 1] - TEMPLC[ilc]);
+  d.tmpdif_n = L.tave - TEMPLC[ilc];
+  for (ilc = 1; ilc <= 4; ilc++)
+    if (L.tave <= TEMPLC[ilc]) break;
+  if (ilc == 1) ilc = 2;
+  if (ilc == 5) ilc = 4;
+  d.ilc_f = (int32_t)ilc;
+  d.rectlc_f = 1.0 / (TEMPLC[ilc] - TEMPLC[ilc - 1]);
+  d.tmpdif_f = L.tave - TEMPLC[ilc];
+
+  // MOLEC IND=2 (src/oprop.f90:2535-2552) with TIPS_2003 scor = Q(296)/Q(T)
+  double wtot = L.wbroad;
+  for (int m = 0; m < L.nmol; m++) wtot += L.wk[m];
+  d.h2o_fac = L.wk[0] / wtot;
+  const double fad = std::log(2.) * 2. * AVOGAD * BOLTZ / (CLIGHT * CLIGHT);
+  for (int m = 1; m <= L.nmol; m++) {
+    d.wk[m] = L.wk[m - 1];
+    d.rhoslf[m] = d.rhorat * L.wk[m - 1] / wtot;
+    d.isomax[m] = LBL_ISO_MAX[m - 1];
+    for (int iso = 1; iso <= LBL_ISO_MAX[m - 1]; iso++) {
+      double q296, qt;
+      if (!partition_q(m, iso, 296., &q296) || !partition_q(m, iso, L.tave, &qt)) {
+        *err = "TIPS table missing";
+        return LBL_E_RANGE;
+      }
+      d.scor[m][iso] = q296 / qt;
+      d.alfd1[m][iso] = std::sqrt(fad * L.tave / LBL_SMASS[m - 1][iso - 1]);
+    }
+  }
+
+  // HIRAC1 constants (src/oprop.f90:229-307)
+  d.dptmn = R.dptmin;
+  if (d.jrad != 1) d.dptmn = R.dptmin / radfn(R.v2, L.tave / RADCN2);
+  d.dptfc = R.dptfac;
+  d.alfmax = 4 * R.sample * DV * 0.04 / R.alfal0;
+  long nalfmax = fint(d.alfmax / DV);
+  long nbound = fint((2. * HWF3) * double(nalfmax) + 0.01);
+  long max1 = kNShift + kNlim1 + kNShift + nbound / 2;
+  max1 = max1 + 4 * nalfmax;
+  d.max1 = max1;
+  d.bound = double(nbound) * DV / 2.;
+  d.dvr2 = (DXF2 / DXF1) * DV;
+  d.dvr3 = (DXF3 / DXF1) * DV;
+  d.conf2 = DV / d.dvr2;
+  d.conf3 = DV / d.dvr3;
+  d.wavdxf = DV / DXF1;
+  d.vft0 = R.v1 - double(kNShift) * DV;
+  d.vbot = R.v1 - d.bound;
+  d.vtop = R.v2 + d.bound;
+
+  // continuum grid (OPDPTH, src/lblrtm.f90:6216-6228)
+  if (R.icntnm != 0) {
+    d.dvabs = 1.;
+    d.v1abs = (double)fint(R.v1);
+    if (R.v1 < 0.) d.v1abs = d.v1abs - 1.;
+    d.v1abs = d.v1abs - 3. * d.dvabs;
+    d.v2abs = (double)fint(R.v2 + 3. * d.dvabs + 0.5);
+    d.nptabs = fint((d.v2abs - d.v1abs) / d.dvabs + 1.5);
+  }
+
+  // far-wing grid (OPDPTH, src/lblrtm.f90:6232-6256)
+  double v1r4st = 0., v2r4st = 0.;
+  if (R.ilblf4 >= 1) {
+    double alfav = R.sample * DV;
+    double alfav4 = 64. * alfav;
+    d.dvr4 = alfav4 / R.sample;
+    d.bound4 = 25.;
+    if (R.ilblf4 == 2 && L.pave <= 0.5) d.bound4 = 5.;
+    v1r4st = R.v1 - 2. * d.dvr4;
+    v2r4st = R.v2 + 2. * d.dvr4;
+    d.v1l4 = v1r4st - d.bound4 - d.dvr4;
+    d.v2l4 = v2r4st + d.bound4 + 2 * d.dvr4;
+  }
+  const double dptmn4 = R.dptmin / radfn(v2r4st, L.tave / RADCN2);
+  P->win.clear();
+  auto add_window = [&](double v1w, int first_panel) {
+    WinDev w;
+    w.v1r4 = v1w;
+    long npt = fint((v2r4st - v1w) / d.dvr4 + ONEPL);
+    npt = std::min<long>(npt, kLimOut);
+    w.nptr4 = (int32_t)npt;
+    w.v2r4 = v1w + d.dvr4 * double(npt - 1);
+    w.vlo = w.v1r4 - d.bound4;
+    w.vhi = w.v2r4 + d.bound4;
+    w.vnulst = w.v2r4 + d.bound4;
+    w.dptmn = dptmn4;
+    w.first_panel = first_panel;
+    P->win.push_back(w);
+  };
+  if (R.ilblf4 >= 1) add_window(v1r4st, 0);
+
+  // panel loop: accumulated VFT_p, last-panel rule, window refreshes
+  P->vft.clear();
+  P->win_of.clear();
+  double vft = d.vft0;
+  const long n2r3 = 155;
+  long nhi_last = 0;
+  for (long p = 0;; p++) {
+    P->vft.push_back(vft);
+    P->win_of.push_back((int32_t)P->win.size() - 1);
+    long nhi = 2432;
+    bool stop = false;
+    if ((vft + double(nhi - 1) * DV) > R.v2) {
+      nhi = fint((R.v2 - vft) / DV + 1.);
+      double v2p = vft + double(nhi - 1) * DV;
+      if (v2p < R.v2) nhi = nhi + 1;
+      stop = true;
+    }
+    vft = vft + double(kNlim1 - 1) * DV;
+    if (stop) {
+      nhi_last = nhi;
+      break;
+    }
+    if (R.ilblf4 >= 1) {
+      const WinDev& cur = P->win.back();
+      double vf1 = vft - 2. * d.dvr4;
+      vf1 = R.v1 + std::floor((vf1 - R.v1) / d.dvr4) * d.dvr4;
+      double vf2 = vft + 2. * d.dvr4 + double(n2r3 + 4) * d.dvr3;
+      if (vf2 > cur.v2r4 && cur.v2r4 != v2r4st) add_window(vf1, (int)p + 1);
+    }
+  }
+  d.npanel = (int64_t)P->vft.size();
+  d.npts = 2400 * (d.npanel - 1) + (nhi_last - 33 + 1);
+  d.nwin = (int32_t)P->win.size();
+  if (d.npts != layer_npts(R, DV)) {
+    *err = "internal: panel count mismatch";
+    return LBL_E_ARG;
+  }
+  // global grid extents: R1 index g1 covers output points 33..32+npts plus
+  // the interpolation stencil; R2/R3 their 4- and 16-fold coarser images.
+  d.n_r1 = 32 + d.npts + 8;
+  d.n_r2 = d.n_r1 / 4 + 8;
+  d.n_r3 = d.n_r2 / 4 + 8;
+
+  // ---- line-index ranges ------------------------------------------------
+  auto lower = [&](double v) { return int64_t(std::lower_bound(vnu, vnu + nlines, v) - vnu); };
+  auto block_of = [&](int64_t i) {
+    return int64_t(std::upper_bound(bs, bs + nblk + 1, i) - bs) - 1;
+  };
+  // RDLIN (src/oprop.f90:741-875): panels with VMAX < VBOT are skipped; in
+  // the first panel read, lines below VBOT are skipped; in each panel the
+  // range ends at the first record (IFLG>=0, MOL>0) beyond VTOP, and when
+  // that record is the panel's last one the next panel is read as well.
+  d.near_lo = d.near_hi = 0;
+  d.blk_lo = d.blk_hi = 0;
+  {
+    int64_t b = 0;
+    while (b < nblk && vnu[bs[b + 1] - 1] < d.vbot) b++;
+    if (b < nblk) {
+      int64_t lo = bs[b];
+      if (vnu[bs[b]] < d.vbot) {
+        int64_t last_ok = -1;
+        lo = -1;
+        for (int64_t i = bs[b]; i < bs[b + 1]; i++) {
+          if (H.iflg[i] < 0) continue;
+          last_ok = i;
+          if (vnu[i] >= d.vbot) { lo = i; break; }
+        }
+        if (lo < 0) lo = last_ok >= 0 ? last_ok : bs[b];
+      }
+      d.near_lo = lo;
+      d.blk_lo = b;
+      int64_t hi = nlines;  // EOF unless a stop is found
+      int64_t bb = b;
+      int64_t from = lo;
+      while (bb < nblk) {
+        int64_t last_ok = -1, stop_at = -1;
+        for (int64_t i = from; i < bs[bb + 1]; i++) {
+          if (H.iflg[i] < 0) continue;
+          last_ok = i;
+          if (stop_at < 0 && H.mol[i] > 0 && vnu[i] > d.vtop) stop_at = i;
+        }
+        if (stop_at >= 0 && stop_at != last_ok) { hi = stop_at + 1; break; }
+        bb++;
+        if (bb < nblk) from = bs[bb];
+        if (stop_at >= 0 && bb >= nblk) { hi = stop_at + 1; break; }
+      }
+      d.near_hi = std::max(hi, lo);
+      d.blk_hi = d.near_hi > d.near_lo ? block_of(d.near_hi - 1) + 1 : d.blk_lo;
+    } else {
+      d.near_lo = d.near_hi = nlines;
+      d.blk_lo = d.blk_hi = nblk;
+    }
+  }
+  // LINF4 (src/oprop.f90:3136-3220): lines with VNU >= V1L4 whose strength
+  // times amount is non-zero, up to and including the first such line whose
+  // pressure-shifted centre lies beyond V2L4.
+  if (R.ilblf4 >= 1) {
+    d.far_lo = lower(d.v1l4);
+    int64_t hi = nlines;
+    for (int64_t i = d.far_lo; i < nlines; i++) {
+      if (H.iflg[i] < 0) continue;
+      int m = H.mol[i] % 100, iso = (H.mol[i] % 1000) / 100;
+      if (m < 1 || m > LBL_MXMOL || iso < 1 || iso > LBL_ISO_MAX[m - 1]) continue;
+      double wkm = (m <= L.nmol) ? L.wk[m - 1] : 0.;
+      if ((double)H.sp[i] * wkm == 0.) continue;
+      if (vnu[i] < d.v1l4) continue;
+      if (vnu[i] + d.rhorat * (double)H.pshift[i] > d.v2l4) { hi = i + 1; break; }
+    }
+    d.far_hi = hi;
+    d.fblk_lo = d.far_lo < nlines ? block_of(d.far_lo) : nblk;
+    d.fblk_hi = d.far_hi > d.far_lo ? block_of(d.far_hi - 1) + 1 : d.fblk_lo;
+  } else {
+    d.far_lo = d.far_hi = 0;
+    d.fblk_lo = d.fblk_hi = 0;
+  }
+  return LBL_OK;
+}
+
+}  // namespace lbl

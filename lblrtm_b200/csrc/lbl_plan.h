@@ -1,0 +1,123 @@
+// lbl_plan.h -- per-layer plan shared by the host planner and the kernels.
+//
+// The reference streams each layer through 2400-point panels (PANEL,
+// src/oprop.f90:1371) and 2500-point far-wing windows (LBLF4,
+// src/oprop.f90:3641).  Here the whole layer lives in device memory on
+// three global grids (spacing DV, 4*DV, 16*DV, indexed from the panel-0
+// origin VFT0 = V1 - 32*DV), so only the schedule quantities that decide
+// arithmetic -- the accumulated panel origins VFT_p, the far-wing window
+// boundaries and which window each panel uses -- are planned on the host,
+// in strict IEEE FP64 with the reference's operation order.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/lblgpu.h"
+
+namespace lbl {
+
+constexpr int kNMolTab = 7;     // HITRAN molecules with TIPS tables here
+constexpr int kNIsoTab = 12;    // isotopologue slots (1-based, 11 used)
+constexpr int kNfmx = 2601;     // NFMX, src/lblparams.f90:31
+constexpr int kNShift = 32;     // NSHIFT
+constexpr int kNlim1 = 2401;    // NLIM1
+constexpr int kLimOut = 2500;   // LIMOUT of LBLF4
+constexpr int kMaxSeg = 64;     // radiation segments per panel (RADFNI)
+
+// Per-layer scalars the kernels read.  Plain data, copied to the device.
+struct LayerDev {
+  // /FILHDR/ and derived
+  double pave, tave, dv, v1, v2, vft0;
+  double xkt;                 // TAVE/RADCN2
+  double betacr_n;            // LNCOR1: (1/XKT)-(1/XKT0)
+  double beta_f, betacr_f;    // LINF4: RADCN2/TAVE, BETA-BETA0
+  double tratio, rhorat, pavp0, pavp2;
+  double rectlc_n, tmpdif_n, rectlc_f, tmpdif_f;
+  int32_t ilc_n, ilc_f;       // line-coupling temperature brackets
+  int32_t jrad, ilblf4, icntnm, nmol;
+  // near wing (HIRAC1)
+  double dptmn, dptfc, alfmax, bound, vbot, vtop;
+  double dvr2, dvr3, conf2, conf3, wavdxf;
+  int64_t max1;
+  int64_t npts;               // output points
+  int64_t npanel;
+  // far wing (OPDPTH/LBLF4)
+  double dvr4, bound4, v1l4, v2l4;
+  int32_t nwin;
+  int32_t pad0;
+  // continuum grid (OPDPTH)
+  double v1abs, v2abs, dvabs, h2o_fac;
+  int64_t nptabs;
+  // molecular constants (MOLEC), 1-based molecule / isotopologue
+  double wk[kNMolTab + 1];
+  double scor[kNMolTab + 1][kNIsoTab];
+  double rhoslf[kNMolTab + 1];
+  double alfd1[kNMolTab + 1][kNIsoTab];
+  int32_t isomax[kNMolTab + 1];
+  // offsets of this layer's slices in the batch arrays
+  int64_t off_r1, n_r1;       // R1 global index g1 in [1, n_r1]
+  int64_t off_r2, n_r2;       // R2 g2 in [1, n_r2]
+  int64_t off_r3, n_r3;       // R3 g3 in [1, n_r3]
+  int64_t off_od;             // OD output (npts)
+  int64_t off_panel;          // per-panel arrays (npanel entries)
+  int64_t off_win;            // window table (nwin entries)
+  int64_t off_r4;             // R4 storage (nwin * kR4Stride)
+  int64_t off_far;            // raw far-wing line slots
+  int64_t off_shr;            // shrunk line slots
+  int64_t off_near;           // near-wing line slots
+  int64_t off_blk9;           // shrunk-line (TAPE9) block slots
+  int64_t off_abs;            // continuum (ABSRB) slots
+  int64_t off_seg;            // LINF4 segment slots (one per far-range panel)
+  // line index ranges into the TAPE3 arrays
+  int64_t far_lo, far_hi;     // [lo, hi) candidates for LINF4
+  int64_t near_lo, near_hi;   // [lo, hi) candidates for RDLIN/LNCOR1
+  int64_t blk_lo, blk_hi;     // TAPE3 panels spanned by the near range
+  int64_t fblk_lo, fblk_hi;   // TAPE3 panels spanned by the far range
+};
+
+constexpr int64_t kR4Stride = kLimOut + 8;
+
+// One LBLF4 call: window of NPTR4 points starting at V1R4.
+struct WinDev {
+  double v1r4, v2r4, vlo, vhi, vnulst, dptmn;
+  int32_t nptr4;
+  int32_t first_panel;        // first panel that uses this window
+};
+
+// Host-side plan of one layer.
+struct LayerPlan {
+  LayerDev d;
+  std::vector<double> vft;      // VFT_p, p = 0..npanel-1
+  std::vector<int32_t> win_of;  // window used by panel p
+  std::vector<WinDev> win;
+};
+
+// Tables built once per context (host copies; uploaded by the library).
+struct ShapeTables {
+  double f1[kNfmx + 1], f2[kNfmx + 1], f3[kNfmx + 1], fg[kNfmx + 1], xver[kNfmx + 1];
+};
+void build_shape_tables(ShapeTables* t);
+
+// PATH DV rule (src/lblrtm.f90:5355-5510).
+int dv_rule(const lbl_run& R, lbl_layer* L, int nlay, std::string* err);
+// Output points of a layer (PANEL last-panel rule).
+int64_t layer_npts(const lbl_run& R, double dv);
+// Host copy of the line fields the planner needs to find line ranges.
+struct HostLines {
+  const double* vnu;
+  const float* sp;
+  const float* pshift;
+  const int32_t* mol;
+  const int32_t* iflg;
+  int64_t n;
+  const int64_t* bs;   // TAPE3 panel starts, nblk+1 entries
+  int64_t nblk;
+};
+// Plan a layer; jrad is the sticky JRAD value entering OPDPTH.
+int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad,
+               const HostLines& H, LayerPlan* P, std::string* err);
+// JRAD after OPDPTH for this layer (src/lblrtm.f90:6211).
+int next_jrad(const lbl_run& R, const lbl_layer& L, int jrad);
+
+}  // namespace lbl

@@ -1,0 +1,177 @@
+"""Python binding of the CUDA library's C ABI (include/lblgpu.h).
+
+The product path: every call goes through lblrtm_b200/_lib/liblblgpu.so.
+There is no CPU fallback -- if the library or a CUDA device is missing the
+calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "liblblgpu.so")
+_LIB = None
+
+P_D = C.POINTER(C.c_double)
+P_I32 = C.POINTER(C.c_int32)
+P_I64 = C.POINTER(C.c_int64)
+
+# every entry point of include/lblgpu.h with its ctypes signature
+SIGNATURES = {
+    "lbl_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "lbl_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "lbl_last_error": (C.c_char_p, [C.c_void_p]),
+    "lbl_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "lbl_lines_upload": (C.c_int, [C.c_void_p, C.POINTER(abi.Lines)]),
+    "lbl_lines_load_tape3": (C.c_int, [C.c_void_p, C.c_char_p, P_I64]),
+    "lbl_mtckd_upload": (C.c_int, [C.c_void_p, C.POINTER(abi.Mtckd)]),
+    "lbl_dv_rule": (C.c_int, [C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32]),
+    "lbl_layer_npts": (C.c_int64, [C.POINTER(abi.Run), C.c_double]),
+    "lbl_layer_od": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), P_I32,
+                               C.c_void_p, C.c_int64, C.c_int32]),
+    "lbl_merge_layer": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer),
+                                  C.c_int32, C.c_double, C.c_void_p, C.c_void_p, C.c_int64,
+                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    "lbl_forward": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32,
+                              C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
+    "lbl_forward_batch": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), P_I32,
+                                    C.c_int32, C.c_void_p, C.c_void_p, P_I64, C.c_int64,
+                                    C.c_int32]),
+    "lbl_jacobian": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32,
+                               P_I32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
+    "lbl_brightness_temperature": (C.c_int, [P_D, C.c_int64, C.c_double, C.c_double, P_D]),
+}
+
+
+class LblError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{abi.STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load the library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} not built; run python -m lblrtm_b200.build")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def _ptr(a):
+    """Data pointer of a numpy array or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return C.c_void_p(a.ctypes.data)
+
+
+def dv_rule(run, layers):
+    rc = load().lbl_dv_rule(C.byref(run), layers, len(layers))
+    if rc:
+        raise LblError(rc, "DV rule")
+    return np.array([l.dv for l in layers]), np.array([l.itype for l in layers])
+
+
+def layer_npts(run, dv):
+    return int(load().lbl_layer_npts(C.byref(run), C.c_double(dv)))
+
+
+def brightness_temperature(rad, v1, dv):
+    rad = np.ascontiguousarray(rad, dtype=np.float64)
+    bt = np.empty_like(rad)
+    load().lbl_brightness_temperature(rad.ctypes.data_as(P_D), len(rad), v1, dv,
+                                      bt.ctypes.data_as(P_D))
+    return bt
+
+
+class Context:
+    """One device context: resident lines and tables, reusable buffers."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.lbl_ctx_create(device, C.byref(h))
+        if rc:
+            raise LblError(rc, "lbl_ctx_create")
+        self.h = h
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            self.lib.lbl_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            raise LblError(rc, f"{what}: {self.lib.lbl_last_error(self.h).decode()}")
+
+    def set_stream(self, stream_ptr):
+        self._check(self.lib.lbl_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
+
+    def upload_lines(self, lines):
+        lh = lines if isinstance(lines, abi.LinesHandle) else abi.LinesHandle(lines)
+        self._check(self.lib.lbl_lines_upload(self.h, C.byref(lh.struct)), "lines_upload")
+
+    def load_tape3(self, path):
+        n = C.c_int64()
+        self._check(self.lib.lbl_lines_load_tape3(self.h, path.encode(), C.byref(n)), "tape3")
+        return n.value
+
+    def upload_mtckd(self, table):
+        th = table if isinstance(table, abi.MtckdHandle) else abi.MtckdHandle(table)
+        self._check(self.lib.lbl_mtckd_upload(self.h, C.byref(th.struct)), "mtckd_upload")
+
+    def layer_od(self, run, layer, jrad=None, precision=abi.PREC_FP64, out=None):
+        n = layer_npts(run, layer.dv)
+        od = np.zeros(n) if out is None else out
+        j = C.c_int32(run.jrad if jrad is None else jrad)
+        self._check(self.lib.lbl_layer_od(self.h, C.byref(run), C.byref(layer), C.byref(j),
+                                          _ptr(od), n, precision), "layer_od")
+        return od, j.value
+
+    def merge_layer(self, run, layer, first, dv_old, rad_in, tr_in, od):
+        n = len(od)
+        rad = np.zeros(n)
+        tr = np.zeros(n)
+        self._check(self.lib.lbl_merge_layer(
+            self.h, C.byref(run), C.byref(layer), int(first), C.c_double(dv_old),
+            _ptr(rad_in), _ptr(tr_in), 0 if rad_in is None else len(rad_in), _ptr(od),
+            _ptr(rad), _ptr(tr), n), "merge_layer")
+        return rad, tr
+
+    def forward(self, run, layers, precision=abi.PREC_FP64, rad=None, tr=None):
+        dv, _ = dv_rule(run, layers)
+        n = layer_npts(run, dv[-1])
+        rad = np.zeros(n) if rad is None else rad
+        trb = np.zeros(n) if tr is None else tr
+        self._check(self.lib.lbl_forward(self.h, C.byref(run), layers, len(layers), _ptr(rad),
+                                         _ptr(trb), n, precision), "forward")
+        return rad, trb
+
+    def jacobian(self, run, layers, mols, precision=abi.PREC_SPLIT):
+        dv, _ = dv_rule(run, layers)
+        n = layer_npts(run, dv[-1])
+        nl = len(layers)
+        m = (C.c_int32 * len(mols))(*mols)
+        rad = np.zeros(n)
+        jac = np.zeros((1 + len(mols), nl, n))
+        self._check(self.lib.lbl_jacobian(self.h, C.byref(run), layers, nl, m, len(mols),
+                                          _ptr(rad), _ptr(jac), n, precision), "jacobian")
+        return rad, jac
