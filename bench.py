@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark: layer-points/s of the LBLRTM layer optical-depth + merge path.
+
+Workload (one "step"): the 60-layer upwelling forward of the config-1
+atmosphere -- 50,000 seeded synthetic lines of H2O/CO2/O3/CH4 over
+500-1500 cm-1, DV rule, per-layer optical depth (line shapes, far wing,
+panel combination, radiation term) and the bottom-up radiance merge to the
+top-of-atmosphere spectrum.  value = layer points processed per second
+(sum over layers of the points on each layer's own grid), whole job.
+
+Arms:
+  default           the CUDA library through its C ABI (lblrtm_b200.gpu)
+  --impl reference  the reference algorithm's CPU restatement (FP64 oracle,
+                    the Fortran reference cannot be built here), one forward
+                    per host core in parallel
+
+Multi-GPU (torchrun): each rank runs its own replica of the workload (the
+path shards by profile; there is no data-path collective); time is the max
+over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from lblrtm_b200 import abi, configs  # noqa: E402
+
+METRIC = "layer-pts/s fwd; Jacobians/s adjoint vs plain FD, 1 B200, <=0.01 K BT err"
+UNIT = "layer-points/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# nominal vector pipes of a B200 (148 SMs, 128 FP32 / 64 FP64 lanes per SM)
+N_SM, FP32_LANES, FP64_LANES = 148, 128, 64
+F4_FLOPS = 8      # algorithmic flops per far-wing line-point evaluation
+NEAR_FLOPS = 13   # per near-wing point triple (R1+R2+R3)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    p.add_argument("--nlines", type=int, default=50000)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-workers", type=int, default=0)
+    return p.parse_args()
+
+
+def workload(nlines):
+    cfg = configs.config1(nlines=nlines)
+    run = abi.make_run(**cfg["run"])
+    layers = abi.make_layers(cfg["profile"])
+    return cfg, run, layers
+
+
+def layer_points(run, layers, npts_fn):
+    return sum(npts_fn(run, layers[i].dv) for i in range(len(layers)))
+
+
+# ---------------------------------------------------------------------------
+# CPU arm: the oracle (restated reference), one forward per worker process
+# ---------------------------------------------------------------------------
+
+def _cpu_worker(args):
+    nlines, variant = args
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    cfg, run, layers = workload(nlines)
+    lh = abi.LinesHandle(cfg["lines"])
+    t = time.perf_counter()
+    O.forward(run, layers, lh, variant=variant)
+    dt = time.perf_counter() - t
+    pts = layer_points(run, layers, O.npts)
+    return pts, dt
+
+
+def cpu_run(nlines, workers, reps=1):
+    """Wall time of `workers` concurrent oracle forwards (spawned processes)."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    O.build()
+    ctx = mp.get_context("spawn")
+    out = []
+    with ctx.Pool(workers) as pool:
+        for _ in range(reps):
+            t = time.perf_counter()
+            res = pool.map(_cpu_worker, [(nlines, "_opt")] * workers)
+            wall = time.perf_counter() - t
+            pts = sum(r[0] for r in res)
+            out.append((pts, wall, max(r[1] for r in res)))
+    return out
+
+
+def default_workers():
+    n = os.cpu_count() or 1
+    return max(1, min(n, 32))
+
+
+def reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    workers = a.cpu_workers or default_workers()
+    # every step is one concurrent forward per worker: ~10 s of CPU time each
+    steps = max(1, min(a.steps, 6))
+    res = cpu_run(a.nlines, workers, reps=max(1, min(a.warmup, 1)) + steps)
+    timed = res[-steps:]
+    pts = timed[0][0]
+    wall = sum(r[1] for r in timed) / steps
+    value = pts / wall
+    cfgd = {"workload": "config1: 60 layers, 50,000 lines, 500-1500 cm-1, upwelling TOA radiance",
+            "nlines": a.nlines, "layers": 60, "precision": "fp64"}
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": steps, "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": cfgd,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                         "sample": f"{workers} concurrent config-1 forwards per step "
+                                   "(restated reference, C++ FP64 oracle)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while timing."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        for ln in out.strip().splitlines():
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def gpu_arm(a):
+    import torch
+    from lblrtm_b200 import gpu
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    prec = abi.PREC_FP64 if a.precision == "fp64" else abi.PREC_SPLIT
+    cfg, run, layers = workload(a.nlines)
+    ctx = gpu.Context(local)
+    lines_h = abi.LinesHandle(cfg["lines"])
+    ctx.upload_lines(lines_h)
+    dv, _ = gpu.dv_rule(run, layers)
+    npts_top = gpu.layer_npts(run, dv[-1])
+    pts = layer_points(run, layers, gpu.layer_npts)
+    rad_d = torch.empty(npts_top, dtype=torch.float64, device="cuda")
+    tr_d = torch.empty(npts_top, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(a.warmup):
+        ctx.forward(run, layers, precision=prec, rad=rad_d, tr=tr_d)
+    ctx.profile(True)
+    ctx.profile_read()
+    barrier()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            flush.fill_(1.0)  # evict L2 between steps (outside the timed events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.forward(run, layers, precision=prec, rad=rad_d, tr=tr_d)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        barrier()
+    stats = ctx.profile_read()
+    ctx.profile(False)
+    step_ms = sum(times) / len(times)
+    if dist is not None:
+        t = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * pts / (step_ms / 1e3)
+
+    # ---- end to end through the C ABI with host buffers ----
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in cfg["lines"].items()}
+    pin_np = {k: v.numpy() for k, v in pin.items()}
+    rad_h = torch.empty(npts_top, dtype=torch.float64).pin_memory()
+    tr_h = torch.empty(npts_top, dtype=torch.float64).pin_memory()
+    h2d = sum(v.nbytes for v in pin_np.values()) + C.sizeof(abi.Layer) * len(layers)
+    d2h = rad_h.numel() * 8 + tr_h.numel() * 8
+    e2e_times = []
+    barrier()
+    for k in range(a.steps + 1):
+        t0 = time.perf_counter()
+        ctx.upload_lines(abi.LinesHandle(pin_np))
+        ctx.forward(run, layers, precision=prec, rad=rad_h, tr=tr_h)
+        torch.cuda.synchronize()
+        if k > 0:
+            e2e_times.append(time.perf_counter() - t0)
+    barrier()
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * pts / e2e_s
+
+    # ---- roofline of the dominant kernel (far wing) ----
+    nstep = a.steps
+    fw = stats.get("far_wing", (0.0, 0, 0.0))
+    fw_ms = fw[0] / max(fw[1], 1)
+    evals = fw[2] / nstep
+    fw_flops = evals * F4_FLOPS
+    lanes = FP64_LANES if prec == abi.PREC_FP64 else FP32_LANES
+    peak_tf = N_SM * lanes * 2 * 1965e6 / 1e12
+    achieved_tf = fw_flops / (fw_ms / 1e3) / 1e12 if fw_ms > 0 else None
+    traffic = None
+    tf_path = os.path.join(ROOT, "profiles", "far_wing_traffic.json")
+    if os.path.exists(tf_path):
+        try:
+            traffic = json.load(open(tf_path)).get(a.precision)
+        except (OSError, ValueError):
+            traffic = None
+    roofline = {
+        "bound": "fp64" if prec == abi.PREC_FP64 else "fp32",
+        "kernel": "k_far_wing (LBLF4/CONVF4 far wing)",
+        "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+        "frac": (achieved_tf / peak_tf) if achieved_tf else None,
+        "traffic": traffic,
+        "peak_source": f"nominal {'FP64' if lanes == 64 else 'FP32'} vector rate: "
+                       f"{N_SM} SMs x {lanes} lanes x 2 x 1965 MHz (MEASURED_PEAKS.json "
+                       "holds HBM and bf16 only)",
+        "work": f"{evals:.4g} line-point evaluations x {F4_FLOPS} flops per launch",
+        "launch_ms": fw_ms,
+    }
+    # HBM roofline of the merge (bytes: FP64 OD read + R,T in/out per point)
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    mg = stats.get("merge", (0.0, 0, 0.0))
+    merge_bytes = mg[2] / nstep * (8 + 16 + 16)
+    merge_ms = mg[0] / nstep
+    roof_merge = {"bound": "hbm", "kernel": "k_merge (EMIN/RADNN)",
+                  "achieved": merge_bytes / (merge_ms / 1e3) / 1e9 if merge_ms > 0 else None,
+                  "peak": hbm_peak, "unit": "GB/s",
+                  "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650"}
+    if roof_merge["achieved"]:
+        roof_merge["frac"] = roof_merge["achieved"] / hbm_peak
+    launches = sum(v[1] for v in stats.values()) // max(nstep, 1)
+    stage_ms = {k: round(v[0] / nstep, 4) for k, v in stats.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        workers = a.cpu_workers or default_workers()
+        r = cpu_run(a.nlines, workers, reps=1)[0]
+        cpu = {"value": r[0] / r[1], "unit": UNIT, "cores": workers, "kind": "port",
+               "sample": f"{workers} concurrent config-1 forwards (restated reference, "
+                         f"C++ FP64 oracle), wall {r[1]:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == abi.PREC_FP64 else "f32/f64",
+            "data": "synthetic (seeded lines and atmosphere)",
+            "config": {"workload": "config1: 60 layers, 4 absorbers, 50,000 lines, "
+                                   "500-1500 cm-1, upwelling TOA radiance",
+                       "nlines": a.nlines, "layers": len(layers),
+                       "layer_points_per_step": pts, "precision": a.precision,
+                       "l2": "256 MB buffer written between timed steps",
+                       "parallelism": f"replica x{world}"},
+            "roofline": roofline, "roofline_merge": roof_merge,
+            "stage_ms": stage_ms,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        reference_arm(a)
+    else:
+        gpu_arm(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -230,6 +230,26 @@ int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
                  int32_t nlay, const int32_t* mols, int32_t nq, double* rad,
                  double* jac, int64_t npts, int32_t precision);
 
+/* ---- timing and work counters ------------------------------------------
+ * Per-stage device time, launch count and algorithmic work of the calls
+ * made since the last read -- the counterpart of the per-layer timing table
+ * HIRAC1 prints to TAPE6 (READ / CONVOLUTION / PANEL, src/oprop.f90:552-631).
+ * Stage times are taken with CUDA events on the context's stream only while
+ * profiling is enabled; launch counts and work are always recorded.
+ * work units: far_wing = line-point evaluations of F4 (CONVF4 loop 40/45);
+ * grids = near-wing point triples (CNVFNV loop 10); combine/merge = layer
+ * points. */
+typedef struct lbl_stage_stat {
+  char name[24];
+  double ms;           /* summed device time, 0 when profiling is off */
+  int64_t launches;    /* kernel launches */
+  double work;         /* algorithmic work units (see above) */
+} lbl_stage_stat;
+
+int lbl_profile(lbl_ctx* ctx, int32_t enable);
+/* Copy up to cap stage records into out, set *n, and reset the counters. */
+int lbl_profile_read(lbl_ctx* ctx, lbl_stage_stat* out, int32_t cap, int32_t* n);
+
 /* Brightness temperature of a radiance spectrum (TEM, src/pltlbl.f90:1568):
  * bt_i = RADCN2*v_i / ln(RADCN1*v_i^3/rad_i + 1).  Host arrays. */
 int lbl_brightness_temperature(const double* rad, int64_t n, double v1,

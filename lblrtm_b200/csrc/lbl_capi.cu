@@ -90,9 +90,72 @@ struct lbl_ctx {
   // merge buffers (ping-pong)
   double* mbuf[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t mcap = 0;
-  // pinned staging for plans
-  std::vector<char> hstage;
+  // stage timing / work counters
+  bool prof = false;
+  struct Stage {
+    std::string name;
+    double ms = 0., work = 0.;
+    int64_t launches = 0;
+  };
+  std::vector<Stage> stages;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  std::vector<cudaEvent_t> event_pool;
+  size_t event_next = 0;
+  Stage& stage(const char* nm) {
+    for (auto& s : stages)
+      if (s.name == nm) return s;
+    stages.push_back(Stage{nm});
+    return stages.back();
+  }
+  int stage_index(const char* nm) {
+    for (size_t i = 0; i < stages.size(); i++)
+      if (stages[i].name == nm) return (int)i;
+    stages.push_back(Stage{nm});
+    return (int)stages.size() - 1;
+  }
+  cudaEvent_t next_event() {
+    if (event_next >= event_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      event_pool.push_back(e);
+    }
+    return event_pool[event_next++];
+  }
 };
+
+namespace {
+// Brackets one stage's launches with events when profiling is on.
+struct StageTimer {
+  lbl_ctx* c;
+  int idx;
+  cudaEvent_t a = nullptr;
+  StageTimer(lbl_ctx* ctx, const char* nm, int64_t launches) : c(ctx) {
+    idx = c->stage_index(nm);
+    c->stages[idx].launches += launches;
+    if (c->prof) {
+      a = c->next_event();
+      cudaEventRecord(a, c->stream);
+    }
+  }
+  ~StageTimer() {
+    if (c->prof) {
+      cudaEvent_t b = c->next_event();
+      cudaEventRecord(b, c->stream);
+      c->pending.push_back({idx, {a, b}});
+    }
+  }
+};
+// Resolve recorded event pairs after the stream has been synchronised.
+void harvest(lbl_ctx* c) {
+  for (auto& p : c->pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess)
+      c->stages[p.first].ms += ms;
+  }
+  c->pending.clear();
+  c->event_next = 0;
+}
+}  // namespace
 
 namespace {
 
@@ -226,6 +289,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<int64_t>(nbt);
   lay.add<int64_t>(n);
   lay.add<int64_t>(n + 1);
+  lay.add<unsigned long long>(8);
   CK(ctx->arena.reserve(lay.bytes + 4096));
   Arena& A = ctx->arena;
   A.reset();
@@ -278,6 +342,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   w.seg_out = A.take<int64_t>(nbt);
   w.seg_count = A.take<int64_t>(n);
   B.d_blk_base = A.take<int64_t>(n + 1);
+  w.counters = A.take<unsigned long long>(8);
   w.L = B.d_ld;
   w.nlay = n;
   w.vft = d_vft;
@@ -321,6 +386,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   CK(cudaMemcpyAsync(B.d_blk_base, blk_base.data(), sizeof(int64_t) * (n + 1),
                      cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(w.status, 0, 4 * sizeof(int32_t), s));
+  CK(cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), s));
   // the host vectors must live until the copies finish
   CK(cudaStreamSynchronize(s));
   return LBL_OK;
@@ -330,19 +396,45 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
 int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   cudaStream_t s = ctx->stream;
   const Work& w = B.w;
-  CK(launch_far_scale(w, ctx->dl, B.max_far, s));
-  CK(launch_shrink(w, ctx->dl.bs, B.d_blk_base, B.nblk_total, s));
-  CK(launch_far_wing(w, B.nwin_total, B.d_win_layer, s));
-  CK(launch_near_scale(w, ctx->dl, s));
+  double npts = 0.;
+  for (auto& d : B.ld) npts += (double)d.npts;
+  {
+    StageTimer t(ctx, "far_scale", 1);
+    CK(launch_far_scale(w, ctx->dl, B.max_far, s));
+  }
+  {
+    StageTimer t(ctx, "shrink", 3);
+    CK(launch_shrink(w, ctx->dl.bs, B.d_blk_base, B.nblk_total, s));
+  }
+  {
+    StageTimer t(ctx, "far_wing", B.nwin_total > 0 ? 1 : 0);
+    CK(launch_far_wing(w, B.nwin_total, B.d_win_layer, s));
+  }
+  {
+    StageTimer t(ctx, "near_scale", 1);
+    CK(launch_near_scale(w, ctx->dl, s));
+  }
   if (R.icntnm) {
     if (!ctx->have_ck) return fail(ctx, LBL_E_NOTREADY, "continuum table not uploaded");
+    StageTimer t(ctx, "continuum", 1);
     CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, s));
   }
-  CK(launch_grids(w, ctx->dl, ctx->sh, B.d_tile_prefix, B.ntiles, precision, s));
-  CK(launch_combine(w, B.max_r3, B.max_r2, B.npanel_total, B.d_panel_layer, B.d_panel_base, s));
+  {
+    StageTimer t(ctx, "grids", 1);
+    CK(launch_grids(w, ctx->dl, ctx->sh, B.d_tile_prefix, B.ntiles, precision, s));
+  }
+  {
+    StageTimer t(ctx, "combine", 3);
+    CK(launch_combine(w, B.max_r3, B.max_r2, B.npanel_total, B.d_panel_layer, B.d_panel_base, s));
+  }
   int32_t st[4] = {0, 0, 0, 0};
+  unsigned long long cnt[8];
   CK(cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cnt, w.counters, sizeof(cnt), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  ctx->stage("far_wing").work += (double)cnt[0];
+  ctx->stage("grids").work += (double)cnt[1];
+  ctx->stage("combine").work += npts;
   if (st[0] == 2)
     return fail(ctx, LBL_E_RANGE,
                 "far-wing line file too sparse: a LINF4 segment spans more than 48 TAPE3 panels");
@@ -394,8 +486,10 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
   int cur = 0;
   double dv_old = 0.;
   int64_t n_old = 0;
+  StageTimer tm(ctx, "merge", n);
   for (int l = 0; l < n; l++) {
     const LayerDev& d = B.ld[l];
+    ctx->stage("merge").work += (double)d.npts;
     const int nxt = cur ^ 2;
     const double tbnd = (l == 0 && R.ipathl == 1) ? R.tmpbnd : 0.;
     CK(launch_merge(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
@@ -471,6 +565,7 @@ int lbl_ctx_destroy(lbl_ctx* ctx) {
   if (ctx->arena.base) cudaFree(ctx->arena.base);
   for (int k = 0; k < 4; k++)
     if (ctx->mbuf[k]) cudaFree(ctx->mbuf[k]);
+  for (auto e : ctx->event_pool) cudaEventDestroy(e);
   delete ctx;
   return LBL_OK;
 }
@@ -602,6 +697,7 @@ int lbl_layer_od(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, int32
   rc = copy_out(ctx, od, B.w.od, sizeof(double) * npts);
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
+  harvest(ctx);
   *jrad = jout;
   return LBL_OK;
 }
@@ -677,6 +773,7 @@ int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nla
     if (rc) return rc;
   }
   CK(cudaStreamSynchronize(ctx->stream));
+  harvest(ctx);
   return LBL_OK;
 }
 
@@ -713,6 +810,30 @@ int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nl
   (void)run; (void)layers; (void)nlay; (void)mols; (void)nq; (void)rad; (void)jac; (void)npts;
   (void)precision;
   return fail(ctx, LBL_E_ARG, "lbl_jacobian: not available in this build");
+}
+
+int lbl_profile(lbl_ctx* ctx, int32_t enable) {
+  if (!ctx) return LBL_E_ARG;
+  ctx->prof = enable != 0;
+  return LBL_OK;
+}
+
+int lbl_profile_read(lbl_ctx* ctx, lbl_stage_stat* out, int32_t cap, int32_t* n) {
+  if (!ctx || !n || (cap > 0 && !out)) return LBL_E_ARG;
+  int32_t k = 0;
+  for (auto& s : ctx->stages) {
+    if (k < cap) {
+      std::memset(&out[k], 0, sizeof(lbl_stage_stat));
+      std::strncpy(out[k].name, s.name.c_str(), sizeof(out[k].name) - 1);
+      out[k].ms = s.ms;
+      out[k].launches = s.launches;
+      out[k].work = s.work;
+    }
+    k++;
+  }
+  *n = std::min(k, cap);
+  ctx->stages.clear();
+  return LBL_OK;
 }
 
 int lbl_brightness_temperature(const double* rad, int64_t n, double v1, double dv, double* bt) {

@@ -476,6 +476,7 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
   const int64_t nb9 = w.b9_count[l];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int term = 0;
+  unsigned long long nevals = 0;
   for (int64_t b = 0; b < nb9 && !term; b++) {
     const int64_t b0 = w.b9_start[L.off_blk9 + b];
     const int64_t b1 = (b + 1 < nb9) ? w.b9_start[L.off_blk9 + b + 1] : ns;
@@ -581,8 +582,14 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
         double add = 0.;
         for (int a = 0; a < nacc; a++) {
           const F4Line& q = cl[s_acc[a]];
-          if ((q.has & 1) && j >= q.jmin && j <= q.jmax) add += f4_eval(q, false, j, dvr4, bndsq);
-          if ((q.has & 2) && j >= q.mjmin && j <= q.mjmax) add += f4_eval(q, true, j, dvr4, bndsq);
+          if ((q.has & 1) && j >= q.jmin && j <= q.jmax) {
+            add += f4_eval(q, false, j, dvr4, bndsq);
+            nevals++;
+          }
+          if ((q.has & 2) && j >= q.mjmin && j <= q.mjmax) {
+            add += f4_eval(q, true, j, dvr4, bndsq);
+            nevals++;
+          }
         }
         R4s[j] += add;
       }
@@ -591,6 +598,7 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
       if (term) break;
     }
   }
+  if (nevals) atomicAdd(&w.counters[0], nevals);
   __syncthreads();
   double* out = w.r4 + (int64_t)gw * kR4Stride;
   if (L.jrad == 1) {
@@ -652,6 +660,7 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
     const int64_t i = a + threadIdx.x;
     int pfit = -1;
     bool ok = false;
+    unsigned long long ntrip = 0;
     int64_t slot = i - L.near_lo + L.off_near;
     if (i < e && !stopped && ln.iflg[i] >= 0) {
       const int mcode = ln.mol[i];
@@ -729,6 +738,7 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
             w.n_j2[slot] = (int32_t)j2;
             w.n_j3[slot] = (int32_t)j3;
             ok = true;
+            ntrip = (unsigned long long)(jmax1 - jmin1 + 1);
             // first panel whose buffer holds the line's R1 window
             int p = pread;
             const long excess = jmax1_at(vnu, w.vft[L.off_panel + p], DV, bhw) - L.max1;
@@ -749,6 +759,7 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
     if (ok && (int)threadIdx.x > stop_at) ok = false;   // never reached by CNVFNV
     if (ok && (int)threadIdx.x == stop_at) ok = false;
     if (ok) atomicMax(&s_pmax, pfit);
+    if (ok && ntrip) atomicAdd(&w.counters[1], ntrip);
     if (i < e) w.n_ok[slot] = ok ? 1 : 0;
     __syncthreads();
     if (threadIdx.x == 0) s_pread = s_pmax;

@@ -70,6 +70,7 @@ struct Work {
   double* od;
   // diagnostics
   int32_t* status;       // device error flag (0 ok)
+  unsigned long long* counters;  // [0] F4 line-point evals, [1] near point triples
 };
 
 void upload_voicon();

@@ -43,7 +43,14 @@ SIGNATURES = {
     "lbl_jacobian": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32,
                                P_I32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
     "lbl_brightness_temperature": (C.c_int, [P_D, C.c_int64, C.c_double, C.c_double, P_D]),
+    "lbl_profile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "lbl_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, P_I32]),
 }
+
+
+class StageStat(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("ms", C.c_double), ("launches", C.c_int64),
+                ("work", C.c_double)]
 
 
 class LblError(RuntimeError):
@@ -121,6 +128,17 @@ class Context:
     def _check(self, rc, what):
         if rc:
             raise LblError(rc, f"{what}: {self.lib.lbl_last_error(self.h).decode()}")
+
+    def profile(self, enable=True):
+        self._check(self.lib.lbl_profile(self.h, int(enable)), "profile")
+
+    def profile_read(self):
+        """Per-stage {name: (ms, launches, work)} since the last read."""
+        buf = (StageStat * 32)()
+        n = C.c_int32()
+        self._check(self.lib.lbl_profile_read(self.h, buf, 32, C.byref(n)), "profile_read")
+        return {buf[i].name.decode(): (buf[i].ms, buf[i].launches, buf[i].work)
+                for i in range(n.value)}
 
     def set_stream(self, stream_ptr):
         self._check(self.lib.lbl_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
