@@ -198,6 +198,29 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
                     const double* tr_in, int64_t n_old, const double* od,
                     double* rad_out, double* tr_out, int64_t n_new);
 
+/* ---- one merge step without any allocation ------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- where a caching allocator owns the device, or the call sits in
+ * a region that must not grow the memory footprint, or a host framework
+ * only hands out buffers it already owns.  Runs the same merge kernel as
+ * lbl_merge_layer on device `device` and CUDA stream `stream` (NULL =
+ * default), with no context: od, rad_in, tr_in, rad_out and tr_out must all
+ * be caller-owned DEVICE memory (host pointers give LBL_E_ARG), and the call
+ * allocates nothing.  Its only scratch is a fixed device array inside the
+ * library, about 72 KB on every device that loads it, kept until the
+ * process exits; it bounds a layer to LBL_NOALLOC_MAX_PANELS panels of 2400
+ * points (19,660,800 points); longer layers return LBL_E_RANGE.  The first
+ * call on a device looks up that array's device address, so make it before
+ * any stream capture.  Every call rewrites all of the scratch it reads, but
+ * all calls share the one array: calls that overlap on the GPU (different
+ * host threads or streams) race.  The call returns after its stream has
+ * finished the merge. */
+#define LBL_NOALLOC_MAX_PANELS 8192
+int lbl_merge_layer_noalloc(int device, const lbl_run* run, const lbl_layer* layer,
+                            int32_t first, double dv_old, const double* rad_in,
+                            const double* tr_in, int64_t n_old, const double* od,
+                            double* rad_out, double* tr_out, int64_t n_new, void* stream);
+
 /* ---- whole path ------------------------------------------------------- */
 
 /* The standard layer loop (XLAYER :3640-3657) for one profile: DV rule,

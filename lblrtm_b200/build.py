@@ -14,7 +14,7 @@ OUT = os.path.join(HERE, "_lib")
 BUILD = os.path.join(HERE, "_lib", "obj")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SRCS = ["lbl_kernels.cu", "lbl_capi.cu"]
+CUDA_SRCS = ["lbl_kernels.cu", "lbl_capi.cu", "lbl_noalloc.cu"]
 CPP_SRCS = ["lbl_plan.cpp", "lbl_tape3.cpp"]
 HEADERS = ["lbl_kernels.cuh", "lbl_plan.h", "../../include/lblgpu.h", "../data/ref_tables.h"]
 

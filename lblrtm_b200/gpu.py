@@ -43,6 +43,10 @@ SIGNATURES = {
     "lbl_jacobian": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32,
                                P_I32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
     "lbl_brightness_temperature": (C.c_int, [P_D, C.c_int64, C.c_double, C.c_double, P_D]),
+    "lbl_merge_layer_noalloc": (C.c_int, [C.c_int, C.POINTER(abi.Run), C.POINTER(abi.Layer),
+                                          C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
+                                          C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_int64, C.c_void_p]),
     "lbl_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "lbl_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, P_I32]),
 }
