@@ -1,0 +1,189 @@
+"""Known-answer tests that pin the FP64 oracle to the reference's own
+arithmetic (no reference outputs exist to compare with)."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from lblrtm_b200 import abi, configs
+
+RADCN1, RADCN2 = 1.191042722E-12, 1.4387752
+
+
+def test_shapel_subfunctions_sum_to_lorentz_minus_q3():
+    # F1+F2+F3 = (1/pi)[1/(1+x^2) - Q3(x^2)] on the F1 grid (SHAPEL :1822-1911)
+    f1, f2, f3 = (O.shape_table(k) for k in range(3))
+    a3 = (1 + 2 * 64.0 ** 2) / (1 + 64.0 ** 2) ** 2
+    b3 = -1 / (1 + 64.0 ** 2) ** 2
+    for i in (0, 7, 250, 999, 1500):            # x = i*0.002 within HWF1
+        x = i * 0.002
+        j2, j3 = int(round(x / 0.008)), int(round(x / 0.032))
+        if abs(j2 * 0.008 - x) > 1e-12 or abs(j3 * 0.032 - x) > 1e-12:
+            continue
+        s = f1[i] + f2[j2] + f3[j3]
+        want = (1 / (1 + x * x) - (a3 + b3 * x * x)) / math.pi
+        assert abs(s - want) < 1e-12
+
+
+def test_shapel_normalisation_total():
+    # TOTAL of SHAPEL: integral of L - Q3 over [-64, 64] alpha_V
+    f1, f2, f3 = (O.shape_table(k) for k in range(3))
+    tot = 0.0
+    for f, dx in ((f1, 0.002), (f2, 0.008), (f3, 0.032)):
+        tot += (f[0] + 2 * f[1:2001].sum()) * dx
+    a3 = (1 + 2 * 64.0 ** 2) / (1 + 64.0 ** 2) ** 2
+    b3 = -1 / (1 + 64.0 ** 2) ** 2
+    exact = (2 * math.atan(64.0) - 2 * (a3 * 64.0 + b3 * 64.0 ** 3 / 3)) / math.pi
+    assert abs(tot - exact) < 2e-4
+
+
+def test_shapeg_norm():
+    fg = O.shape_table(3)
+    s = (fg[0] + 2 * fg[1:2001].sum()) * 0.002
+    assert abs(s - math.erf(4 * math.sqrt(math.log(2)))) < 1e-5
+
+
+def test_tips_identity_and_scaling():
+    for mol in (1, 2, 3, 6):
+        assert abs(O.tips_scor(mol, 1, 296.0) - 1.0) < 1e-12
+    # rotational partition sums grow ~T^1.5 (non-linear) / ~T (linear CO2)
+    assert 1.6 < O.tips_scor(1, 1, 200.0) < 2.0
+    assert 1.3 < O.tips_scor(2, 1, 200.0) < 1.9
+
+
+def test_planck_and_radfn():
+    for v, t in ((500.0, 290.0), (1500.0, 217.0), (10.0, 300.0)):
+        x = v * RADCN2 / t
+        b = RADCN1 * v ** 3 / math.expm1(x)
+        assert abs(lib_planck(v, t) - b) / b < 1e-12
+        assert abs(O.lib().orc_radfn(v, t) - v * math.tanh(x / 2)) / v < 1e-12
+
+
+def lib_planck(v, t):
+    return O.lib().orc_planck(v, t)
+
+
+def test_dv_rule_config0_and_config1():
+    cfg = configs.config0()
+    run = abi.make_run(**cfg["run"])
+    lays = abi.make_layers(cfg["profile"])
+    dv, it = O.dv_rule(run, lays)
+    assert dv[0] == pytest.approx(0.0102, abs=1e-15)
+    cfg = configs.config1()
+    run = abi.make_run(**cfg["run"])
+    lays = abi.make_layers(cfg["profile"])
+    dv, it = O.dv_rule(run, lays)
+    assert it[0] == 99 and set(it[1:]) <= {0, 1, 2, 4, 5}
+    ratio = dv[:-1] / dv[1:]
+    assert np.all((ratio > 0.999) & (ratio < 2.0001))
+
+
+def test_config0_matches_exact_voigt_sum():
+    """The approximate-Voigt decomposition follows an exact Voigt sum (with
+    the same 25 cm-1 bound subtraction) to its documented accuracy."""
+    from scipy.special import wofz
+    cfg = configs.config0()
+    run = abi.make_run(**cfg["run"], dptmin=0.0, dptfac=0.0)
+    lays = abi.make_layers(cfg["profile"])
+    O.dv_rule(run, lays)
+    lh = abi.LinesHandle(cfg["lines"])
+    od, _ = O.layer_od(run, lays[0], lh)
+    dv = lays[0].dv
+    v = 600.0 + dv * np.arange(len(od))
+    xkt = 296.0 / RADCN2
+    fad = math.log(2.0) * 2.0 * 6.02214199E+23 * 1.3806503E-16 / 2.99792458E+10 ** 2
+    alfd1 = math.sqrt(fad * 296.0 / 18.01)
+    L = cfg["lines"]
+    tot = np.zeros_like(v)
+    sel = np.arange(0, len(v), 7)
+    vs = v[sel]
+    for i in range(len(L["vnu"])):
+        nu, S, aL = L["vnu"][i], float(L["sp"][i]), float(L["alfa"][i])
+        sig = nu * alfd1 / math.sqrt(2 * math.log(2))
+        m = np.abs(vs - nu) < 25
+        V = lambda x: np.real(wofz((x + 1j * aL) / (sig * math.sqrt(2)))) / (sig * math.sqrt(2 * math.pi))  # noqa: E731
+        tot[sel[m]] += S * 1e22 * (1 + math.exp(-nu / xkt)) * (V(vs[m] - nu) - V(25.0))
+    rad = vs * np.tanh(vs / xkt / 2)
+    r = od[sel] / (tot[sel] * rad) - 1
+    assert np.median(np.abs(r)) < 1e-3
+    assert np.max(np.abs(r)) < 2e-2
+
+
+def _one_layer(amount, t=250.0):
+    prof = {"pave": np.array([500.0]), "tave": np.array([t]), "pzl": np.array([550.0]),
+            "pzu": np.array([450.0]), "tzl": np.array([t]), "tzu": np.array([t]),
+            "wk": np.zeros((1, 60)), "wbroad": np.array([1e24]), "nmol": 7}
+    prof["wk"][0, 0] = amount
+    return abi.make_layers(prof)
+
+
+def test_isothermal_opaque_layer_emits_planck():
+    lines = configs.gen_lines(400, 690.0, 710.0, seed=5)
+    lines["sp"][:] = 1e-17
+    t = 250.0
+    run = abi.make_run(v1=695.0, v2=705.0, iemit=1, tmpbnd=t, bndemi=1.0, dptmin=0., dptfac=0.)
+    lays = _one_layer(1e24, t)
+    lh = abi.LinesHandle(lines)
+    rad, tr = O.forward(run, lays, lh)
+    dv = lays[0].dv
+    v = 695.0 + dv * np.arange(len(rad))
+    bt = RADCN2 * v / np.log(RADCN1 * v ** 3 / rad + 1)
+    assert np.max(np.abs(bt - t)) < 1e-6
+
+
+def test_transparent_layer_keeps_radiance():
+    lines = configs.gen_lines(300, 690.0, 710.0, seed=6)
+    run = abi.make_run(v1=695.0, v2=705.0, iemit=1, tmpbnd=280.0, bndemi=0.9)
+    lays = _one_layer(1e20, 260.0)
+    O.dv_rule(run, lays)
+    lh = abi.LinesHandle(lines)
+    od, _ = O.layer_od(run, lays[0], lh)
+    rad0, tr0 = O.merge_layer(run, lays[0], True, 0.0, None, None, od)
+    # a second layer with zero optical depth on the same grid
+    rad1, tr1 = O.merge_layer(run, lays[0], False, lays[0].dv, rad0, tr0, np.zeros_like(od))
+    assert np.max(np.abs(rad1 - rad0) / rad0) < 1e-15
+    assert np.max(np.abs(tr1 - tr0)) < 1e-15
+
+
+def test_merge_regrid_exact_for_cubics():
+    """RADNN's 4-point Lagrange regrid reproduces a cubic in the interior."""
+    run = abi.make_run(v1=500.0, v2=540.0, iemit=1, tmpbnd=0.0)
+    lays = _one_layer(0.0)
+    lays[0].dv = 0.006
+    n_old = O.npts(run, 0.006)
+    v_old = 500.0 + 0.006 * np.arange(n_old)
+    cub = lambda x: 1.0 + 0.3 * (x - 520) + 0.01 * (x - 520) ** 2 - 1e-4 * (x - 520) ** 3  # noqa: E731
+    rad_in = cub(v_old)
+    tr_in = np.ones(n_old)
+    for itype in (1, 2, 4, 5):
+        dvn = 0.006 * itype / (itype + 1)
+        lays[0].dv = dvn
+        n_new = O.npts(run, dvn)
+        rad, tr = O.merge_layer(run, lays[0], False, 0.006, rad_in, tr_in, np.zeros(n_new))
+        v_new = 500.0 + dvn * np.arange(n_new)
+        inner = slice(10, n_new - 10)
+        assert np.max(np.abs(rad[inner] - cub(v_new[inner]))) < 1e-9
+
+
+def test_testmm_fixture_pins_tape3_format(tmp_path):
+    """The TESTMM line list of the reference (src/testmm.f90, 0-80 cm-1) as a
+    TAPE3: write, read back, and compute a layer with it."""
+    import os
+    from lblrtm_b200 import tape3
+    fx = os.path.join(os.path.dirname(__file__), "golden", "testmm_lines.npz")
+    L = dict(np.load(fx))
+    p = tmp_path / "TAPE3"
+    tape3.write(p, L)
+    R = tape3.read(p)
+    for k in ("vnu", "sp", "alfa", "epp", "mol", "hwhms", "tmpalf", "pshift", "iflg"):
+        assert np.array_equal(R[k], L[k])
+    assert R["block_start"][-1] == len(L["vnu"])
+    # a layer at 40-60 cm-1 through the oracle: finite, positive
+    run = abi.make_run(v1=40.0, v2=60.0, iemit=0)
+    lays = _one_layer(5e21, 250.0)
+    for m in (3, 4, 7):
+        lays[0].wk[m - 1] = 1e19
+    O.dv_rule(run, lays)
+    od, _ = O.layer_od(run, lays[0], abi.LinesHandle(R))
+    assert np.all(np.isfinite(od)) and od.min() > 0
