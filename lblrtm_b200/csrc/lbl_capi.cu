@@ -77,6 +77,7 @@ struct lbl_ctx {
   std::vector<float> h_sp, h_pshift;
   std::vector<int32_t> h_mol, h_iflg;
   std::vector<int64_t> h_bs;
+  double max_abs_pshift = 0.;
   DevLines dl{};
   void* line_mem = nullptr;
   bool have_lines = false;
@@ -193,7 +194,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
                   int* jrad_out, Batch& B) {
   HostLines H{ctx->h_vnu.data(), ctx->h_sp.data(), ctx->h_pshift.data(), ctx->h_mol.data(),
               ctx->h_iflg.data(), (int64_t)ctx->h_vnu.size(), ctx->h_bs.data(),
-              (int64_t)ctx->h_bs.size() - 1};
+              (int64_t)ctx->h_bs.size() - 1, ctx->max_abs_pshift};
   B.plans.resize(n);
   int jrad = jrad_in;
   for (int l = 0; l < n; l++) {
@@ -273,7 +274,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<double>(o_near + 1);
   lay.add<double>(5 * (o_near + 1));
   lay.add<double>(o_near + 1);
-  for (int k = 0; k < 4; k++) lay.add<int32_t>(o_near + 1);
+  for (int k = 0; k < 5; k++) lay.add<int32_t>(o_near + 1);
   lay.add<int8_t>(o_near + 1);
   lay.add<double>(o_r1);
   lay.add<double>(o_r2);
@@ -327,6 +328,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   w.n_jmax1 = A.take<int32_t>(o_near + 1);
   w.n_j2 = A.take<int32_t>(o_near + 1);
   w.n_j3 = A.take<int32_t>(o_near + 1);
+  w.n_pconv = A.take<int32_t>(o_near + 1);
   w.n_ok = A.take<int8_t>(o_near + 1);
   w.r1 = A.take<double>(o_r1);
   w.r2 = A.take<double>(o_r2);
@@ -408,7 +410,7 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   }
   {
     StageTimer t(ctx, "far_wing", B.nwin_total > 0 ? 1 : 0);
-    CK(launch_far_wing(w, B.nwin_total, B.d_win_layer, s));
+    CK(launch_far_wing(w, B.nwin_total, B.d_win_layer, precision, s));
   }
   {
     StageTimer t(ctx, "near_scale", 1);
@@ -478,7 +480,7 @@ int ensure_merge_buffers(lbl_ctx* ctx, size_t n) {
 
 // Merge every layer of the batch bottom-up; result in mbuf[res], mbuf[res+1].
 int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B, int n,
-              int* res) {
+              int* res, int precision) {
   size_t mx = 0;
   for (auto& d : B.ld) mx = std::max<size_t>(mx, d.npts);
   int rc = ensure_merge_buffers(ctx, mx + 8);
@@ -494,7 +496,8 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     const double tbnd = (l == 0 && R.ipathl == 1) ? R.tmpbnd : 0.;
     CK(launch_merge(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
                     dv_old, n_old, ctx->mbuf[cur], ctx->mbuf[cur + 1], ctx->mbuf[nxt],
-                    ctx->mbuf[nxt + 1], tbnd, R.bndemi, R.iemit, layers[l].tzu, ctx->stream));
+                    ctx->mbuf[nxt + 1], tbnd, R.bndemi, R.iemit, layers[l].tzu, ctx->stream,
+                    precision));
     if (l > 0 && d.dv > dv_old) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
     cur = nxt;
     dv_old = d.dv;
@@ -605,6 +608,9 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   ctx->h_mol.assign(L->mol, L->mol + n);
   ctx->h_iflg.assign(L->iflg, L->iflg + n);
   ctx->h_bs = bs;
+  ctx->max_abs_pshift = 0.;
+  for (int64_t i = 0; i < n; i++)
+    ctx->max_abs_pshift = std::max(ctx->max_abs_pshift, std::fabs((double)L->pshift[i]));
   cudaSetDevice(ctx->device);
   if (ctx->line_mem) cudaFree(ctx->line_mem);
   ctx->line_mem = nullptr;
@@ -716,7 +722,7 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, in
   if (layer_npts(*run, layer->dv) != n_new) return fail(ctx, LBL_E_ARG, "n_new does not match the layer grid");
   HostLines H{ctx->h_vnu.data(), ctx->h_sp.data(), ctx->h_pshift.data(), ctx->h_mol.data(),
               ctx->h_iflg.data(), (int64_t)ctx->h_vnu.size(), ctx->h_bs.data(),
-              (int64_t)ctx->h_bs.size() - 1};
+              (int64_t)ctx->h_bs.size() - 1, ctx->max_abs_pshift};
   LayerPlan P;
   std::string e;
   rc = plan_layer(*run, *layer, run->jrad, H, &P, &e);
@@ -764,7 +770,7 @@ int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nla
   rc = run_od(ctx, *run, B, precision);
   if (rc) return rc;
   int res = 0;
-  rc = run_merge(ctx, *run, layers, B, nlay, &res);
+  rc = run_merge(ctx, *run, layers, B, nlay, &res, precision);
   if (rc) return rc;
   rc = copy_out(ctx, rad, ctx->mbuf[res], sizeof(double) * npts);
   if (rc) return rc;

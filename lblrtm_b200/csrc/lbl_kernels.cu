@@ -442,7 +442,7 @@ __device__ __forceinline__ double f4_eval(const F4Line& p, bool mirror, int j, d
   const double xm = double(j - 1) * dvr4 - xnui;
   const double xmsq = xm * xm;
   const double zvsq = xmsq * p.rvi2;
-  const double sub = p.co2 ? (2. - xmsq / bndsq) * p.f4bnd : p.f4bnd;
+  const double sub = p.co2 ? (2. - xmsq * (1. / bndsq)) * p.f4bnd : p.f4bnd;
   double f;
   if (zvsq <= 4096.)
     f = (p.siv_a3 + zvsq * p.siv_b3) - sub;
@@ -453,6 +453,84 @@ __device__ __forceinline__ double f4_eval(const F4Line& p, bool mirror, int j, d
   return f;
 }
 
+// The line's F4 constants in the arithmetic of the evaluation.
+template <typename T>
+struct F4Reg {
+  T sil, sa3, sb3, alfl2, rvi2, f4bnd, dptrat, rbndsq, rdd;
+  double xnui, bnd;
+  int co2;
+  bool lc;
+};
+
+template <typename T>
+__device__ __forceinline__ F4Reg<T> f4_load(const F4Line& p, bool mirror, double bndsq) {
+  F4Reg<T> r;
+  r.sil = (T)p.sil;
+  r.sa3 = (T)p.siv_a3;
+  r.sb3 = (T)p.siv_b3;
+  r.alfl2 = (T)p.alfl2;
+  r.rvi2 = (T)p.rvi2;
+  r.f4bnd = (T)p.f4bnd;
+  r.dptrat = (T)(mirror ? p.mdptrat : p.dptrat);
+  r.rbndsq = (T)(1. / bndsq);
+  r.rdd = (T)(p.sil / (bndsq * (p.alfl2 + bndsq)));  // SIL/(B^2 (alpha_L^2+B^2))
+  r.bnd = sqrt(bndsq);
+  r.xnui = mirror ? p.mxnui : p.xnui;
+  r.co2 = p.co2;
+  r.lc = (mirror ? p.mspp : p.spp) != 0.;
+  return r;
+}
+
+// F4 at window point j: the offset to the line centre is formed in FP64
+// (grid position minus centre), the shape in T.
+template <typename T>
+__device__ __forceinline__ T f4_at(const F4Reg<T>& r, int j, double dvr4) {
+  const double xd = double(j - 1) * dvr4 - r.xnui;
+  const T xm = (T)xd;
+  const T xmsq = xm * xm;
+  const T zvsq = xmsq * r.rvi2;
+  T f;
+  if (zvsq <= (T)4096.) {
+    const T sub = r.co2 ? ((T)2. - xmsq * r.rbndsq) * r.f4bnd : r.f4bnd;
+    f = (r.sa3 + zvsq * r.sb3) - sub;
+  } else if constexpr (sizeof(T) == 8) {
+    // FP64: the reference's expression, L(x) - L(B) (CONVF4 :3990-4009)
+    const T sub = r.co2 ? ((T)2. - xmsq * r.rbndsq) * r.f4bnd : r.f4bnd;
+    f = r.sil / (r.alfl2 + xmsq) - sub;
+  } else {
+    // FP32: the same difference without cancellation near the bound B,
+    // with d = x^2 - B^2 = -(B-|x|)(B+|x|) formed in FP64:
+    //   non-CO2  L(x) - L(B)                = -SIL d / ((a^2+x^2)(a^2+B^2))
+    //   CO2      L(x) - (2 - x^2/B^2) L(B)  = SIL d (a^2+d) / (B^2 (a^2+B^2)(a^2+x^2))
+    const double ax = fabs(xd);
+    const T d = (T)(-((r.bnd - ax) * (r.bnd + ax)));
+    const T den = r.alfl2 + xmsq;
+    if (r.co2)
+      f = r.rdd * d * (r.alfl2 + d) / den;
+    else
+      f = -(r.rdd * (T)(r.bnd * r.bnd)) * d / den;
+  }
+  if (r.lc) f = f + xm * r.dptrat * f;
+  return f;
+}
+
+// compensated sum in FP32; FP64 sums need no compensation here
+template <typename T>
+__device__ __forceinline__ void kahan_add(T& sum, T& c, T x) {
+  if constexpr (sizeof(T) == 8) {
+    sum += x;
+  } else {
+    const T y = x - c;
+    const T t = sum + y;
+    c = (t - sum) - y;
+    sum = t;
+  }
+}
+
+constexpr int kFwThreads = 256;
+constexpr int kFwPts = (kLimOut + kFwThreads - 1) / kFwThreads;  // window points per thread
+
+template <typename T>
 __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_layer) {
   const int gw = blockIdx.x;
   const int l = win_layer[gw];
@@ -578,20 +656,34 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
       }
       __syncthreads();
       const int nacc = s_nacc;
-      for (int j = 1 + threadIdx.x; j <= npt; j += blockDim.x) {
-        double add = 0.;
+      if (nacc > 0) {
+        // each thread owns window points j = 1 + tid + 256 q; the line's
+        // constants are held in registers while it sweeps them
+        T acc[kFwPts], cmp[kFwPts];
+#pragma unroll
+        for (int q = 0; q < kFwPts; q++) acc[q] = cmp[q] = (T)0.;
         for (int a = 0; a < nacc; a++) {
-          const F4Line& q = cl[s_acc[a]];
-          if ((q.has & 1) && j >= q.jmin && j <= q.jmax) {
-            add += f4_eval(q, false, j, dvr4, bndsq);
-            nevals++;
-          }
-          if ((q.has & 2) && j >= q.mjmin && j <= q.mjmax) {
-            add += f4_eval(q, true, j, dvr4, bndsq);
-            nevals++;
+          const F4Line& pl = cl[s_acc[a]];
+#pragma unroll 1
+          for (int m = 0; m < 2; m++) {
+            if (!(pl.has & (1 << m))) continue;
+            const int lo = m ? pl.mjmin : pl.jmin, hi = m ? pl.mjmax : pl.jmax;
+            const F4Reg<T> r = f4_load<T>(pl, m == 1, bndsq);
+#pragma unroll
+            for (int q = 0; q < kFwPts; q++) {
+              const int j = 1 + (int)threadIdx.x + kFwThreads * q;
+              if (j >= lo && j <= hi) {
+                kahan_add(acc[q], cmp[q], f4_at<T>(r, j, dvr4));
+                nevals++;
+              }
+            }
           }
         }
-        R4s[j] += add;
+#pragma unroll
+        for (int q = 0; q < kFwPts; q++) {
+          const int j = 1 + (int)threadIdx.x + kFwThreads * q;
+          if (j <= npt) R4s[j] += (double)acc[q] - (double)cmp[q];
+        }
       }
       __syncthreads();
       term = s_term;
@@ -634,10 +726,36 @@ __device__ __forceinline__ long jmax1_at(double vnu, double vft, double dv, doub
   return fint((vnu - vft) / dv + bhw + 1.5);
 }
 
+// Inclusive max-scan over the CTA's threads in thread order.
+__device__ int block_max_scan(int v, int* sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, t);
+  }
+  if (lane == 31) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    int t = lane < (int)(blockDim.x >> 5) ? sh[lane] : -1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t = max(t, u);
+    }
+    sh[lane] = t;
+  }
+  __syncthreads();
+  const int r = (wid > 0) ? max(v, sh[wid - 1]) : v;
+  __syncthreads();
+  return r;
+}
+
 __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
   const int l = blockIdx.x;
   const LayerDev& L = w.L[l];
   __shared__ int s_pmax, s_stop_at;
+  __shared__ int s_scan[32];
   __shared__ int s_pread;
   if (threadIdx.x == 0) {
     s_pread = 0;
@@ -661,6 +779,7 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
     int pfit = -1;
     bool ok = false;
     unsigned long long ntrip = 0;
+    double zslope = 0., bhw = 0., vline = 0.;
     int64_t slot = i - L.near_lo + L.off_near;
     if (i < e && !stopped && ln.iflg[i] >= 0) {
       const int mcode = ln.mol[i];
@@ -716,30 +835,18 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
             }
           }
           if (!rej) {
-            // CNVFNV constants in panel-0 coordinates (:1283-1305)
+            // strengths of the sub-functions (CNVFNV :1270-1282)
             const double depth = sp * recalf;
-            const double zslope = recalf * L.wavdxf;
-            const double zint = (vnu - L.vft0) / DV;
-            const double bhw = kHWDXF / zslope;
-            const long jmax1 = fint(zint + bhw + 1.5);
-            const long jmin1 = fint(zint - bhw + 1.5);
-            const double rs = zint < 0.0 ? -0.5 : 0.5;
-            const long j2 = fint(zint * (1. - L.conf2) + rs);
-            const long j3 = fint(zint * (1. - L.conf3) + rs);
             double* str = w.n_str + 5 * slot;
             const double* cf[5] = {c_cf1, c_cf2, c_cf3, c_cgauss, c_cer};
 #pragma unroll
             for (int k = 0; k < 5; k++) str[k] = depth * (cf[k][iz - 1] + zd * (cf[k][iz] - cf[k][iz - 1]));
-            w.n_zint[slot] = zint;
-            w.n_zslope[slot] = zslope;
             w.n_sppsp[slot] = sppsp;
-            w.n_jmin1[slot] = (int32_t)jmin1;
-            w.n_jmax1[slot] = (int32_t)jmax1;
-            w.n_j2[slot] = (int32_t)j2;
-            w.n_j3[slot] = (int32_t)j3;
+            zslope = recalf * L.wavdxf;
+            bhw = kHWDXF / zslope;
+            vline = vnu;
             ok = true;
-            ntrip = (unsigned long long)(jmax1 - jmin1 + 1);
-            // first panel whose buffer holds the line's R1 window
+            // first panel whose buffer holds the line's R1 window (JMAX1 <= MAX1)
             int p = pread;
             const long excess = jmax1_at(vnu, w.vft[L.off_panel + p], DV, bhw) - L.max1;
             if (excess > 0) p += (int)((excess + 2399) / 2400);
@@ -756,10 +863,29 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
     }
     __syncthreads();
     const int stop_at = s_stop_at;
-    if (ok && (int)threadIdx.x > stop_at) ok = false;   // never reached by CNVFNV
-    if (ok && (int)threadIdx.x == stop_at) ok = false;
-    if (ok) atomicMax(&s_pmax, pfit);
-    if (ok && ntrip) atomicAdd(&w.counters[1], ntrip);
+    if (ok && (int)threadIdx.x >= stop_at) ok = false;   // never reached by CNVFNV
+    // CNVFNV convolves a line in the panel current when it reaches it: the
+    // read panel or later, as far as the earlier lines of the panel pushed it
+    const int pconv = max(pread, block_max_scan(ok ? pfit : -1, s_scan));
+    if (ok) {
+      atomicMax(&s_pmax, pfit);
+      // window limits and offsets in that panel's own coordinates (:1283-1305)
+      const double zint = (vline - w.vft[L.off_panel + pconv]) / DV;
+      const long jmax1 = fint(zint + bhw + 1.5);
+      const long jmin1 = fint(zint - bhw + 1.5);
+      const double rs = zint < 0.0 ? -0.5 : 0.5;
+      const long j2 = fint(zint * (1. - L.conf2) + rs);
+      const long j3 = fint(zint * (1. - L.conf3) + rs);
+      w.n_zint[slot] = zint;
+      w.n_zslope[slot] = zslope;
+      w.n_jmin1[slot] = (int32_t)jmin1;
+      w.n_jmax1[slot] = (int32_t)jmax1;
+      w.n_j2[slot] = (int32_t)j2;
+      w.n_j3[slot] = (int32_t)j3;
+      w.n_pconv[slot] = pconv;
+      ntrip = (unsigned long long)(jmax1 - jmin1 + 1);
+      if (ntrip) atomicAdd(&w.counters[1], ntrip);
+    }
     if (i < e) w.n_ok[slot] = ok ? 1 : 0;
     __syncthreads();
     if (threadIdx.x == 0) s_pread = s_pmax;
@@ -786,11 +912,20 @@ __device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double
 
 struct NearStage {
   double zint, zslope, s0, s1, s2, sppsp;
-  int32_t lo, hi;
+  int64_t lo, hi, pofs;  // global window; pofs = panel offset on this grid
 };
 
 constexpr int kGridTile = 1024;  // points per CTA (4 per thread)
 
+template <typename T>
+__device__ __forceinline__ const T* shape_table(const DevShapes& sh, int k) {
+  if constexpr (sizeof(T) == 8)
+    return k == 0 ? sh.f1 : k == 1 ? sh.f2 : k == 2 ? sh.f3 : k == 3 ? sh.fg : sh.xver;
+  else
+    return k == 0 ? sh.f1s : k == 1 ? sh.f2s : k == 2 ? sh.f3s : k == 3 ? sh.fgs : sh.xvers;
+}
+
+template <typename T>
 __global__ void __launch_bounds__(256) k_grids(Work w, DevLines ln, DevShapes sh,
                                                const int64_t* tile_prefix, int ntp) {
   // tile -> (layer, grid) by binary search of the prefix (3 entries per layer)
@@ -821,9 +956,15 @@ __global__ void __launch_bounds__(256) k_grids(Work w, DevLines ln, DevShapes sh
   __shared__ NearStage st[256];
   __shared__ int s_n;
   constexpr int PT = kGridTile / 256;
-  double acc[PT];
+  T acc[PT];
+  double acc64[PT];
 #pragma unroll
-  for (int q = 0; q < PT; q++) acc[q] = 0.;
+  for (int q = 0; q < PT; q++) {
+    acc[q] = (T)0.;
+    acc64[q] = 0.;
+  }
+  const T* tf2 = shape_table<T>(sh, 1);
+  const T* tf3 = shape_table<T>(sh, 2);
   for (int64_t c0 = clo; c0 < chi; c0 += 256) {
     if (threadIdx.x == 0) s_n = 0;
     __syncthreads();
@@ -835,9 +976,12 @@ __global__ void __launch_bounds__(256) k_grids(Work w, DevLines ln, DevShapes sh
         q.zint = w.n_zint[slot];
         q.zslope = w.n_zslope[slot];
         const double* sv = w.n_str + 5 * slot;
+        // panel-local window, shifted to the global grid by the line's panel
         const int32_t sh2 = grid == 0 ? 0 : (grid == 1 ? w.n_j2[slot] : w.n_j3[slot]);
-        q.lo = w.n_jmin1[slot] - sh2;
-        q.hi = w.n_jmax1[slot] - sh2;
+        const int64_t pofs = (int64_t)w.n_pconv[slot] * (grid == 0 ? 2400 : (grid == 1 ? 600 : 150));
+        q.pofs = pofs;
+        q.lo = w.n_jmin1[slot] - sh2 + pofs;
+        q.hi = w.n_jmax1[slot] - sh2 + pofs;
         if (grid == 0) {
           q.s0 = sv[0];
           q.s1 = sv[3];
@@ -855,25 +999,42 @@ __global__ void __launch_bounds__(256) k_grids(Work w, DevLines ln, DevShapes sh
     }
     __syncthreads();
     const int n = s_n;
-    for (int k = 0; k < n; k++) {
-      const NearStage& q = st[k];
+    if (grid == 0) {
+      // R1 (DV grid): F1 + FG + VERFN terms, whose negative VERFN part
+      // cancels the Doppler core in the wings -- evaluated in FP64 in every
+      // precision mode
+      for (int k = 0; k < n; k++) {
+        const NearStage& q = st[k];
 #pragma unroll
-      for (int qq = 0; qq < PT; qq++) {
-        const int64_t g = g0 + threadIdx.x + 256 * qq;
-        if (g > g1e || g < q.lo || g > q.hi) continue;
-        const double zf = (double(g - 1) - q.zint * conf) * q.zslope;
-        long iz = fint(fabs(zf) + 1.5);
-        iz = iz > kNfmx ? kNfmx : iz;  // window limits keep iz <= 2501
-        double v;
-        if (grid == 0) v = q.s0 * sh.f1[iz] + q.s1 * sh.fg[iz] + q.s2 * sh.xver[iz];
-        else if (grid == 1) v = q.s0 * sh.f2[iz];
-        else v = q.s0 * sh.f3[iz];
-        if (q.sppsp != 0.) {
-          // line coupling (:1322-1351): strengths scaled by CLCk*DPTRAT, times ZF
-          const double clc = grid == 0 ? 4. / 2000. : (grid == 1 ? 16. / 2000. : 64. / 2000.);
-          v = v + v * clc * q.sppsp * zf;
+        for (int qq = 0; qq < PT; qq++) {
+          const int64_t g = g0 + threadIdx.x + 256 * qq;
+          if (g > g1e || g < q.lo || g > q.hi) continue;
+          const double zf = (double(g - q.pofs - 1) - q.zint) * q.zslope;
+          long iz = fint(fabs(zf) + 1.5);
+          iz = iz > kNfmx ? kNfmx : iz;  // window limits keep iz <= 2501
+          double v = q.s0 * sh.f1[iz] + q.s1 * sh.fg[iz] + q.s2 * sh.xver[iz];
+          if (q.sppsp != 0.) v = v + v * (4. / 2000. * q.sppsp * zf);  // (:1322-1351)
+          acc64[qq] += v;
         }
-        acc[qq] += v;
+      }
+    } else {
+      const T* tf = grid == 1 ? tf2 : tf3;
+      const double clc = grid == 1 ? 16. / 2000. : 64. / 2000.;
+      for (int k = 0; k < n; k++) {
+        const NearStage& q = st[k];
+        const T s0 = (T)q.s0;
+#pragma unroll
+        for (int qq = 0; qq < PT; qq++) {
+          const int64_t g = g0 + threadIdx.x + 256 * qq;
+          if (g > g1e || g < q.lo || g > q.hi) continue;
+          // table position from the FP64 offset to the line centre
+          const double zf = (double(g - q.pofs - 1) - q.zint * conf) * q.zslope;
+          long iz = fint(fabs(zf) + 1.5);
+          iz = iz > kNfmx ? kNfmx : iz;
+          T v = s0 * tf[iz];
+          if (q.sppsp != 0.) v = v + v * (T)(clc * q.sppsp * zf);  // (:1322-1351)
+          acc[qq] += v;
+        }
       }
     }
     __syncthreads();
@@ -882,7 +1043,7 @@ __global__ void __launch_bounds__(256) k_grids(Work w, DevLines ln, DevShapes sh
 #pragma unroll
   for (int qq = 0; qq < PT; qq++) {
     const int64_t g = g0 + threadIdx.x + 256 * qq;
-    if (g <= g1e) out[g] = acc[qq];
+    if (g <= g1e) out[g] = grid == 0 ? acc64[qq] : (double)acc[qq];
   }
 }
 
@@ -1101,6 +1262,23 @@ __global__ void __launch_bounds__(256) k_combine_od(Work w, const int32_t* panel
 // XMERGE for one layer: EMIN (src/xmerge.f90:1795-1855) then EMINIT
 // (:2436-2484) for the first layer or RADNN IPATH=1 (:2985-3130) after.
 // =========================================================================
+// Planck function in the arithmetic T, from an FP64 wavenumber.
+template <typename T>
+__device__ __forceinline__ T planck_t(double vi, double xkt) {
+  if constexpr (sizeof(T) == 8) {
+    return planck(vi, xkt);
+  } else {
+    if (!(xkt > 0.0)) return 0.f;
+    const float x = (float)(vi / xkt);
+    const float v = (float)vi;
+    float b = 0.f;
+    if (x < 1e-2f) b = (v * v) * (float)xkt / (1.f + 0.5f * x);
+    else if (x <= 80.f) b = (v * v * v) / expm1f(x);
+    return b * (float)kRADCN1;
+  }
+}
+
+template <typename T>
 __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const double* od,
                         int first, double dv_old, int64_t n_old, const double* rad_in,
                         const double* tr_in, double* rad_out, double* tr_out, double tbnd,
@@ -1137,17 +1315,17 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
   }
   const double xkt = L.tave / kRADCN2;
   const double xkta = tzu / kRADCN2;
-  double o = odv;
-  if (o < -kODLO) o = -kODLO;
-  const double tr = exp(-o);
-  const double fi = (o <= kODLO) ? o / 6. : 1. - 2. * (tr / (tr - 1.) + 1. / o);
-  const double bb = planck(vi, xkt);
-  const double bbd = (xkta > 0.) ? planck(vi, xkta) - bb : 0.;
-  double em = (1. - tr) * (bb + bbd * fi);
+  T o = (T)odv;
+  if (o < (T)-kODLO) o = (T)-kODLO;
+  const T tr = exp(-o);
+  const T fi = (o <= (T)kODLO) ? o / (T)6. : (T)1. - (T)2. * (tr / (tr - (T)1.) + (T)1. / o);
+  const T bb = planck_t<T>(vi, xkt);
+  const T bbd = (xkta > 0.) ? planck_t<T>(vi, xkta) - bb : (T)0.;
+  T em = ((T)1. - tr) * (bb + bbd * fi);
   if (first) {
-    if (tbnd > 0.) em = em + tr * planck(vi, tbnd / kRADCN2) * emis;
-    rad_out[f] = em;
-    tr_out[f] = tr;
+    if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2) * (T)emis;
+    rad_out[f] = (double)em;
+    tr_out[f] = (double)tr;
     return;
   }
   const double dvk = DV;
@@ -1155,24 +1333,24 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
   const int64_t LL = itype + 1;
   const int64_t q = f / LL, r = f % LL;
   auto R = [&](int64_t c) { return rad_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
-  auto T = [&](int64_t c) { return tr_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+  auto TR = [&](int64_t c) { return tr_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
   double ro, to;
   if (itype == 0) {
     ro = R(f);
-    to = T(f);
+    to = TR(f);
   } else if (r == 0) {
     ro = R(q * itype);
-    to = T(q * itype);
+    to = TR(q * itype);
   } else {
     const int64_t ipl = q * itype + r - 1;
     const double P = 1.0 - double(r) / double(LL);
     const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
     const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
     ro = a1 * R(ipl - 1) + a2 * R(ipl) + a3 * R(ipl + 1) + a4 * R(ipl + 2);
-    to = a1 * T(ipl - 1) + a2 * T(ipl) + a3 * T(ipl + 1) + a4 * T(ipl + 2);
+    to = a1 * TR(ipl - 1) + a2 * TR(ipl) + a3 * TR(ipl + 1) + a4 * TR(ipl + 2);
   }
-  rad_out[f] = tr * ro + em;
-  tr_out[f] = tr * to;
+  rad_out[f] = (double)tr * ro + (double)em;
+  tr_out[f] = (double)tr * to;
 }
 
 }  // namespace
@@ -1212,9 +1390,12 @@ cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_b
 }
 
 cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_layer,
-                            cudaStream_t s) {
+                            int precision, cudaStream_t s) {
   if (nwin_total <= 0) return cudaSuccess;
-  k_far_wing<<<nwin_total, 256, 0, s>>>(w, win_layer);
+  if (precision == LBL_PREC_SPLIT)
+    k_far_wing<float><<<nwin_total, kFwThreads, 0, s>>>(w, win_layer);
+  else
+    k_far_wing<double><<<nwin_total, kFwThreads, 0, s>>>(w, win_layer);
   return cudaGetLastError();
 }
 
@@ -1232,9 +1413,13 @@ cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, do
 cudaError_t launch_grids(const Work& w, const DevLines& ln, const DevShapes& sh,
                          const int64_t* tile_prefix, int64_t ntiles, int precision,
                          cudaStream_t s) {
+  // The near-wing sums stay FP64 in every mode: the reference decomposition
+  // cancels in them (negative VERFN term; negative lobes of the 4-point
+  // PANEL interpolation where a line's R2/R3 window ends), which FP32 cannot
+  // resolve at a 1e-4 relative bar where the optical depth is small.
   (void)precision;
   if (ntiles <= 0) return cudaSuccess;
-  k_grids<<<(unsigned)ntiles, 256, 0, s>>>(w, ln, sh, tile_prefix, 3 * w.nlay);
+  k_grids<double><<<(unsigned)ntiles, 256, 0, s>>>(w, ln, sh, tile_prefix, 3 * w.nlay);
   return cudaGetLastError();
 }
 
@@ -1258,10 +1443,14 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          int64_t npts, int first, double dv_old, int64_t n_old,
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
-                         cudaStream_t s) {
-  k_merge<<<(unsigned)((npts + 255) / 256), 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old,
-                                                        rad_in, tr_in, rad_out, tr_out, tbnd,
-                                                        emis, iemit, tzu);
+                         cudaStream_t s, int precision) {
+  const unsigned nb = (unsigned)((npts + 255) / 256);
+  if (precision == LBL_PREC_SPLIT)
+    k_merge<float><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
+                                      rad_out, tr_out, tbnd, emis, iemit, tzu);
+  else
+    k_merge<double><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
+                                       rad_out, tr_out, tbnd, emis, iemit, tzu);
   return cudaGetLastError();
 }
 

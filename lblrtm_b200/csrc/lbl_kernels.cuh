@@ -62,7 +62,8 @@ struct Work {
   // near-wing lines (slot = line index - near_lo)
   double *n_zint, *n_zslope, *n_str;  // n_str: 5 per slot (F1,F2,F3,FG,VER)
   double* n_sppsp;
-  int32_t *n_jmin1, *n_jmax1, *n_j2, *n_j3;
+  int32_t *n_jmin1, *n_jmax1, *n_j2, *n_j3;  // in the convolution panel's coordinates
+  int32_t* n_pconv;      // panel in which CNVFNV convolves the line
   int8_t* n_ok;
   // grids
   double *r1, *r2, *r3;
@@ -79,7 +80,7 @@ cudaError_t launch_far_scale(const Work& w, const DevLines& ln, int64_t max_far,
 cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_base,
                           int64_t nblk_total, cudaStream_t s);
 cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_layer,
-                            cudaStream_t s);
+                            int precision, cudaStream_t s);
 cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
@@ -94,7 +95,7 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          int64_t npts, int first, double dv_old, int64_t n_old,
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
-                         cudaStream_t s);
+                         cudaStream_t s, int precision = LBL_PREC_FP64);
 void init_kernel_attributes();
 
 }  // namespace lbl

@@ -418,8 +418,15 @@ int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad_in, const HostLine
       d.near_lo = lo;
       d.blk_lo = b;
       int64_t hi = nlines;  // EOF unless a stop is found
+      // panels whose last line is <= VTOP hold no stop record: jump to the
+      // first panel reaching beyond VTOP
       int64_t bb = b;
-      int64_t from = lo;
+      {
+        const int64_t first_above = int64_t(std::upper_bound(vnu, vnu + nlines, d.vtop) - vnu);
+        if (first_above < nlines) bb = std::max(b, block_of(first_above));
+        else bb = nblk;
+      }
+      int64_t from = (bb == b) ? lo : (bb < nblk ? bs[bb] : nlines);
       while (bb < nblk) {
         int64_t last_ok = -1, stop_at = -1;
         for (int64_t i = from; i < bs[bb + 1]; i++) {
@@ -445,7 +452,11 @@ int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad_in, const HostLine
   if (R.ilblf4 >= 1) {
     d.far_lo = lower(d.v1l4);
     int64_t hi = nlines;
-    for (int64_t i = d.far_lo; i < nlines; i++) {
+    // a line can pass VHI only if its unshifted centre is within the largest
+    // pressure shift of it: start the search there
+    const double reach = std::fabs(d.rhorat) * H.max_abs_pshift;
+    const int64_t start = std::max(d.far_lo, lower(d.v2l4 - reach - 1e-9));
+    for (int64_t i = start; i < nlines; i++) {
       if (H.iflg[i] < 0) continue;
       int m = H.mol[i] % 100, iso = (H.mol[i] % 1000) / 100;
       if (m < 1 || m > LBL_MXMOL || iso < 1 || iso > LBL_ISO_MAX[m - 1]) continue;

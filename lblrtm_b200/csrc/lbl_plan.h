@@ -113,6 +113,7 @@ struct HostLines {
   int64_t n;
   const int64_t* bs;   // TAPE3 panel starts, nblk+1 entries
   int64_t nblk;
+  double max_abs_pshift;  // largest |PSHIFT| of the file
 };
 // Plan a layer; jrad is the sticky JRAD value entering OPDPTH.
 int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad,

@@ -15,6 +15,12 @@ pytestmark = pytest.mark.gpu
 
 RTOL_OD = 1e-4
 BT_TOL = 0.01
+# The FP32/FP64-split path is held to the same 1e-4 relative bar, but optical
+# depths below OD_FLOOR are compared in absolute terms: there the reference's
+# own decomposition cancels (negative lobes of the cubic/4-point
+# interpolations next to a line's window edge, the 25 cm-1 far-wing cut) and
+# the value is radiatively zero (transmittance within 1e-9 of 1).
+OD_FLOOR = 1e-9
 
 
 def rel_err(a, b):
@@ -73,14 +79,17 @@ def c1(gpu_ctx):
     return cfg, run, lays, lh
 
 
-@pytest.mark.parametrize("layer", [0, 7, 23, 41, 59])
-def test_config1_layers_fp64(gpu_ctx, c1, layer):
+def test_config1_every_layer_fp64(gpu_ctx, c1):
+    """Every layer of the 60-layer atmosphere (DV 9.6e-3 ... 2.5e-4)."""
     cfg, run, lays, lh = c1
-    jrad = 0  # every config-1 layer has V1/XKT < 5
-    od_ref, _ = O.layer_od(run, lays[layer], lh, jrad=jrad)
-    od, _ = gpu_ctx.layer_od(run, lays[layer], jrad=jrad)
-    e = rel_err(od, od_ref)
-    assert e.max() < RTOL_OD, (layer, e.max(), int(e.argmax()))
+    worst = []
+    for layer in range(len(lays)):
+        jrad = 0  # every config-1 layer has V1/XKT < 5
+        od_ref, _ = O.layer_od(run, lays[layer], lh, jrad=jrad)
+        od, _ = gpu_ctx.layer_od(run, lays[layer], jrad=jrad)
+        e = rel_err(od, od_ref)
+        worst.append((e.max(), layer, int(e.argmax())))
+    assert max(worst)[0] < RTOL_OD, max(worst)
 
 
 def test_config1_forward_fp64(gpu_ctx, c1):
@@ -92,3 +101,21 @@ def test_config1_forward_fp64(gpu_ctx, c1):
     assert np.abs(b - b_ref).max() < BT_TOL
     assert rel_err(rad, rad_ref).max() < RTOL_OD
     assert np.abs(tr - tr_ref).max() < 1e-6
+
+
+@pytest.mark.parametrize("layer", [0, 23, 50, 59])
+def test_config1_layers_split(gpu_ctx, c1, layer):
+    cfg, run, lays, lh = c1
+    od_ref, _ = O.layer_od(run, lays[layer], lh, jrad=0)
+    od, _ = gpu_ctx.layer_od(run, lays[layer], jrad=0, precision=abi.PREC_SPLIT)
+    e = np.abs(od - od_ref) / np.maximum(np.abs(od_ref), OD_FLOOR)
+    assert e.max() < RTOL_OD, (layer, e.max(), int(e.argmax()))
+
+
+def test_config1_forward_split(gpu_ctx, c1):
+    cfg, run, lays, lh = c1
+    rad_ref, tr_ref = O.forward(run, lays, lh)
+    rad, tr = gpu_ctx.forward(run, lays, precision=abi.PREC_SPLIT)
+    dv = lays[len(lays) - 1].dv
+    b_ref, b = bt(rad_ref, run.v1, dv), bt(rad, run.v1, dv)
+    assert np.abs(b - b_ref).max() < BT_TOL
