@@ -257,6 +257,7 @@ def gpu_arm(a):
         if k > 0:
             e2e_times.append(time.perf_counter() - t0)
     barrier()
+    print("e2e step ms:", [round(1e3 * t, 2) for t in e2e_times], file=sys.stderr)
     e2e_s = sum(e2e_times) / len(e2e_times)
     if dist is not None:
         t = torch.tensor([e2e_s], device="cuda")

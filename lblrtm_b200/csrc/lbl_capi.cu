@@ -80,6 +80,7 @@ struct lbl_ctx {
   double max_abs_pshift = 0.;
   DevLines dl{};
   void* line_mem = nullptr;
+  size_t line_cap = 0;  // bytes of line_mem (grow-only)
   bool have_lines = false;
   // tables
   DevShapes sh{};
@@ -179,6 +180,7 @@ struct Batch {
   Work w{};
   LayerDev* d_ld = nullptr;
   int32_t* d_win_layer = nullptr;
+  int32_t* d_win_order = nullptr;  // far-wing windows, most expensive first
   int32_t* d_panel_layer = nullptr;
   int64_t* d_panel_base = nullptr;
   int64_t* d_tile_prefix = nullptr;
@@ -260,6 +262,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<int64_t>(n + 1);
   lay.add<WinDev>(std::max<int64_t>(o_win, 1));
   lay.add<int32_t>(std::max<int64_t>(o_win, 1));
+  lay.add<int32_t>(std::max<int64_t>(o_win, 1));
   lay.add<double>(std::max<int64_t>(o_win, 1) * kR4Stride);
   for (int k = 0; k < 5; k++) lay.add<double>(o_far + 1);
   lay.add<int8_t>(o_far + 1);
@@ -302,6 +305,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   B.d_panel_base = A.take<int64_t>(n + 1);
   WinDev* d_win = A.take<WinDev>(std::max<int64_t>(o_win, 1));
   B.d_win_layer = A.take<int32_t>(std::max<int64_t>(o_win, 1));
+  B.d_win_order = A.take<int32_t>(std::max<int64_t>(o_win, 1));
   w.r4 = A.take<double>(std::max<int64_t>(o_win, 1) * kR4Stride);
   w.f_vnu = A.take<double>(o_far + 1);
   w.f_sp = A.take<double>(o_far + 1);
@@ -370,6 +374,25 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
     }
   }
   h_pbase[n] = o_pan;
+  // Far-wing windows are launched most expensive first so that the long
+  // ones do not start last.  Cost estimate: lines within the window's reach
+  // times the points one line covers.
+  std::vector<int32_t> h_word(std::max<int64_t>(o_win, 1), 0);
+  {
+    std::vector<double> cost(o_win);
+    const double* vb = ctx->h_vnu.data();
+    const double* ve = vb + ctx->h_vnu.size();
+    for (int64_t k = 0; k < o_win; k++) {
+      const WinDev& W = h_win[k];
+      const LayerDev& d = B.ld[h_wlay[k]];
+      const double nl = double(std::lower_bound(vb, ve, W.vnulst) - std::lower_bound(vb, ve, W.vlo));
+      const double span = std::min<double>(W.nptr4, 2. * d.bound4 / d.dvr4 + 1.);
+      cost[k] = nl * (span + 64.);
+      h_word[k] = (int32_t)k;
+    }
+    std::stable_sort(h_word.begin(), h_word.begin() + o_win,
+                     [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
+  }
   cudaStream_t s = ctx->stream;
   CK(cudaMemcpyAsync(B.d_ld, B.ld.data(), sizeof(LayerDev) * n, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_vft, h_vft.data(), sizeof(double) * o_pan, cudaMemcpyHostToDevice, s));
@@ -380,6 +403,8 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
                      cudaMemcpyHostToDevice, s));
   if (o_win > 0) {
     CK(cudaMemcpyAsync(d_win, h_win.data(), sizeof(WinDev) * o_win, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(B.d_win_order, h_word.data(), sizeof(int32_t) * o_win,
+                       cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(B.d_win_layer, h_wlay.data(), sizeof(int32_t) * o_win,
                        cudaMemcpyHostToDevice, s));
   }
@@ -410,7 +435,7 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   }
   {
     StageTimer t(ctx, "far_wing", B.nwin_total > 0 ? 1 : 0);
-    CK(launch_far_wing(w, B.nwin_total, B.d_win_layer, precision, s));
+    CK(launch_far_wing(w, B.nwin_total, B.d_win_order, B.d_win_layer, precision, s));
   }
   {
     StageTimer t(ctx, "near_scale", 1);
@@ -612,14 +637,24 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   for (int64_t i = 0; i < n; i++)
     ctx->max_abs_pshift = std::max(ctx->max_abs_pshift, std::fabs((double)L->pshift[i]));
   cudaSetDevice(ctx->device);
-  if (ctx->line_mem) cudaFree(ctx->line_mem);
-  ctx->line_mem = nullptr;
   const size_t nn = (size_t)std::max<int64_t>(n, 1) + 2;  // +2: coupling record reads
   size_t bytes = nn * (8 + 6 * 4 + 2 * 4) + bs.size() * 8 + 16 * 256;  // 10 aligned arrays
-  char* m = nullptr;
-  CK(cudaMalloc(&m, bytes));
-  ctx->line_mem = m;
-  CK(cudaMemset(m, 0, bytes));
+  // the line buffer grows only; work already queued on the stream that
+  // reads the old lines is ordered before the copies below
+  if (!ctx->line_mem || bytes > ctx->line_cap) {
+    if (ctx->line_mem) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      cudaFree(ctx->line_mem);
+    }
+    ctx->line_mem = nullptr;
+    ctx->line_cap = 0;
+    char* nm = nullptr;
+    CK(cudaMalloc(&nm, bytes));
+    ctx->line_mem = nm;
+    ctx->line_cap = bytes;
+  }
+  char* m = static_cast<char*>(ctx->line_mem);
+  CK(cudaMemsetAsync(m, 0, bytes, ctx->stream));
   size_t off = 0;
   auto take = [&](size_t b) {
     off = (off + 255) & ~size_t(255);
@@ -640,18 +675,21 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   d.bs = reinterpret_cast<int64_t*>(take(bs.size() * 8));
   d.n = n;
   d.nblk = (int64_t)bs.size() - 1;
+  cudaStream_t st = ctx->stream;
   if (n > 0) {
-    CK(cudaMemcpy((void*)d.vnu, L->vnu, n * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.sp, L->sp, n * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.alfa, L->alfa, n * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.epp, L->epp, n * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.hwhms, L->hwhms, n * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.tmpalf, L->tmpalf, n * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.pshift, L->pshift, n * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.mol, L->mol, n * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy((void*)d.iflg, L->iflg, n * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync((void*)d.vnu, L->vnu, n * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.sp, L->sp, n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.alfa, L->alfa, n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.epp, L->epp, n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.hwhms, L->hwhms, n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.tmpalf, L->tmpalf, n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.pshift, L->pshift, n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.mol, L->mol, n * 4, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.iflg, L->iflg, n * 4, cudaMemcpyHostToDevice, st));
   }
-  CK(cudaMemcpy((void*)d.bs, bs.data(), bs.size() * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync((void*)d.bs, bs.data(), bs.size() * 8, cudaMemcpyHostToDevice, st));
+  // the caller's arrays (and bs) must outlive the copies
+  CK(cudaStreamSynchronize(st));
   ctx->dl = d;
   ctx->have_lines = true;
   return LBL_OK;

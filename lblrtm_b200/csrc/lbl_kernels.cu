@@ -423,162 +423,292 @@ __global__ void k_shr_write(Work w, const int64_t* bs, const int64_t* seg_base, 
 
 // =========================================================================
 // LBLF4/CONVF4 far wing (src/oprop.f90:3641-4039), one CTA per window.
-// Lines are taken in file order 32 at a time: warp 0 decides acceptance in
-// order against the running R4 (held in shared memory) plus the earlier
-// accepted lines of the same chunk -- exactly the reference's test against
-// the partially accumulated R4 -- then every thread adds the accepted
-// lines to the window points it owns.
+// Lines are taken in file order 32 at a time; one warp decides acceptance
+// exactly as the reference's in-order test against the partially
+// accumulated R4 while the other threads add the previously accepted lines
+// to the window points they own (see k_far_wing).
 // =========================================================================
-struct F4Line {
-  double xnui, sil, siv_a3, siv_b3, alfl2, rvi2, f4bnd, dptrat, spp, vnu;
-  int32_t jmin, jmax, co2, has;  // has: 1 main, 2 mirror
-  double mxnui, mdptrat, mspp;
-  int32_t mjmin, mjmax;
+
+// FP32 evaluation constants of one side (line or image) of a line.  The
+// offset from the line centre and the distance to the bound B are taken
+// from integer point offsets plus fractions fixed per line in FP64:
+//     x_j     = (j - jc) dv - dlt
+//     B - x_j = ((mp - (j - jc)) + php) dv      (x_j >= 0)
+//     B + x_j = ((mm + (j - jc)) + phm) dv      (x_j <  0)
+// so u = B - |x_j| keeps its relative precision as x_j approaches B.
+struct F4Side32 {
+  float dlt, php, phm, mpf, mmf, dptrat;
+  int32_t jc;
 };
 
-__device__ __forceinline__ double f4_eval(const F4Line& p, bool mirror, int j, double dvr4,
-                                          double bndsq) {
-  const double xnui = mirror ? p.mxnui : p.xnui;
+struct F4Line {
+  // FP64 constants (CONVF4 :3965-3986); dptrat is 0 for an uncoupled line
+  double xnui, sil, siv_a3, siv_b3, alfl2, rvi2, f4bnd, dptrat, mxnui, mdptrat;
+  int32_t jmin, jmax, mjmin, mjmax, co2, has;  // has: 1 line, 2 image; empty range if absent
+  // FP32 copies for split-precision evaluation
+  float sil32, sa3_32, sb3_32, alfl2_32, rvi2_32, f4bnd32, rdd32;  // rdd = F4BND/B^2
+  F4Side32 s32[2];
+};
+
+// Reciprocal from the hardware estimate (rcp.approx) refined by
+// Newton-Raphson steps r <- r + r (1 - x r), each of which squares the
+// relative error: two steps take the FP64 estimate to full precision, one
+// step the FP32 estimate.  Used for the per-point divisions of the far wing,
+// whose denominators alpha^2 + x^2 are positive and normal.
+__device__ __forceinline__ double recip_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ float recip_nr(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return fmaf(r, fmaf(-x, r, 1.f), r);
+}
+
+// F4 of one side of line q at window point j in FP64 (CONVF4 :3990-4009);
+// 0 outside the side's point range.  Branch-free apart from the range, so
+// that several lines evaluate together.
+__device__ __forceinline__ double f4_side(const F4Line& q, bool image, int j, double dvr4,
+                                          double rbndsq) {
+  const double xnui = image ? q.mxnui : q.xnui;
+  const int lo = image ? q.mjmin : q.jmin, hi = image ? q.mjmax : q.jmax;
   const double xm = double(j - 1) * dvr4 - xnui;
   const double xmsq = xm * xm;
-  const double zvsq = xmsq * p.rvi2;
-  const double sub = p.co2 ? (2. - xmsq * (1. / bndsq)) * p.f4bnd : p.f4bnd;
-  double f;
-  if (zvsq <= 4096.)
-    f = (p.siv_a3 + zvsq * p.siv_b3) - sub;
-  else
-    f = p.sil / (p.alfl2 + xmsq) - sub;
-  const double spp = mirror ? p.mspp : p.spp;
-  if (spp != 0.) f = f + xm * (mirror ? p.mdptrat : p.dptrat) * f;
-  return f;
+  const double zvsq = xmsq * q.rvi2;
+  const double sub = q.co2 ? (2. - xmsq * rbndsq) * q.f4bnd : q.f4bnd;
+  double f = zvsq <= 4096. ? (q.siv_a3 + zvsq * q.siv_b3) - sub
+                           : q.sil * recip_nr(q.alfl2 + xmsq) - sub;
+  f = f + xm * (image ? q.mdptrat : q.dptrat) * f;
+  return (j >= lo && j <= hi) ? f : 0.;
 }
 
-// The line's F4 constants in the arithmetic of the evaluation.
+// One side of a line held in an adder's registers.
 template <typename T>
-struct F4Reg {
-  T sil, sa3, sb3, alfl2, rvi2, f4bnd, dptrat, rbndsq, rdd;
-  double xnui, bnd;
+struct F4Reg;
+
+template <>
+struct F4Reg<double> {
+  double sil, sa3, sb3, alfl2, rvi2, f4bnd, dptrat, xnui;
   int co2;
-  bool lc;
 };
 
-template <typename T>
-__device__ __forceinline__ F4Reg<T> f4_load(const F4Line& p, bool mirror, double bndsq) {
-  F4Reg<T> r;
-  r.sil = (T)p.sil;
-  r.sa3 = (T)p.siv_a3;
-  r.sb3 = (T)p.siv_b3;
-  r.alfl2 = (T)p.alfl2;
-  r.rvi2 = (T)p.rvi2;
-  r.f4bnd = (T)p.f4bnd;
-  r.dptrat = (T)(mirror ? p.mdptrat : p.dptrat);
-  r.rbndsq = (T)(1. / bndsq);
-  r.rdd = (T)(p.sil / (bndsq * (p.alfl2 + bndsq)));  // SIL/(B^2 (alpha_L^2+B^2))
-  r.bnd = sqrt(bndsq);
-  r.xnui = mirror ? p.mxnui : p.xnui;
+template <>
+struct F4Reg<float> {
+  float sil, sa3, sb3, alfl2, rvi2, f4bnd, rdd, dptrat, dlt, php, phm, mpf, mmf, k0;
+  int co2;
+};
+
+__device__ __forceinline__ void f4_load(F4Reg<double>& r, const F4Line& p, int m, int) {
+  r.sil = p.sil;
+  r.sa3 = p.siv_a3;
+  r.sb3 = p.siv_b3;
+  r.alfl2 = p.alfl2;
+  r.rvi2 = p.rvi2;
+  r.f4bnd = p.f4bnd;
+  r.dptrat = m ? p.mdptrat : p.dptrat;
+  r.xnui = m ? p.mxnui : p.xnui;
   r.co2 = p.co2;
-  r.lc = (mirror ? p.mspp : p.spp) != 0.;
-  return r;
 }
 
-// F4 at window point j: the offset to the line centre is formed in FP64
-// (grid position minus centre), the shape in T.
-template <typename T>
-__device__ __forceinline__ T f4_at(const F4Reg<T>& r, int j, double dvr4) {
-  const double xd = double(j - 1) * dvr4 - r.xnui;
-  const T xm = (T)xd;
-  const T xmsq = xm * xm;
-  const T zvsq = xmsq * r.rvi2;
-  T f;
-  if (zvsq <= (T)4096.) {
-    const T sub = r.co2 ? ((T)2. - xmsq * r.rbndsq) * r.f4bnd : r.f4bnd;
+// j0: the adder's first window point; k0 = j0 - jc is a float so that
+// j - jc at the adder's later points is an exact float sum.
+__device__ __forceinline__ void f4_load(F4Reg<float>& r, const F4Line& p, int m, int j0) {
+  const F4Side32& sd = p.s32[m];
+  r.sil = p.sil32;
+  r.sa3 = p.sa3_32;
+  r.sb3 = p.sb3_32;
+  r.alfl2 = p.alfl2_32;
+  r.rvi2 = p.rvi2_32;
+  r.f4bnd = p.f4bnd32;
+  r.rdd = p.rdd32;
+  r.dptrat = sd.dptrat;
+  r.dlt = sd.dlt;
+  r.php = sd.php;
+  r.phm = sd.phm;
+  r.mpf = sd.mpf;
+  r.mmf = sd.mmf;
+  r.k0 = (float)(j0 - sd.jc);
+  r.co2 = p.co2;
+}
+
+// F4 at window point j (FP64: CONVF4's expression).
+__device__ __forceinline__ double f4_at(const F4Reg<double>& r, int j, float, double dvr4,
+                                        double rbndsq, float, float, float) {
+  const double xm = double(j - 1) * dvr4 - r.xnui;
+  const double xmsq = xm * xm;
+  const double zvsq = xmsq * r.rvi2;
+  const double sub = r.co2 ? (2. - xmsq * rbndsq) * r.f4bnd : r.f4bnd;
+  double f;
+  if (zvsq <= 4096.)
     f = (r.sa3 + zvsq * r.sb3) - sub;
-  } else if constexpr (sizeof(T) == 8) {
-    // FP64: the reference's expression, L(x) - L(B) (CONVF4 :3990-4009)
-    const T sub = r.co2 ? ((T)2. - xmsq * r.rbndsq) * r.f4bnd : r.f4bnd;
-    f = r.sil / (r.alfl2 + xmsq) - sub;
-  } else {
-    // FP32: the same difference without cancellation near the bound B,
-    // with d = x^2 - B^2 = -(B-|x|)(B+|x|) formed in FP64:
-    //   non-CO2  L(x) - L(B)                = -SIL d / ((a^2+x^2)(a^2+B^2))
-    //   CO2      L(x) - (2 - x^2/B^2) L(B)  = SIL d (a^2+d) / (B^2 (a^2+B^2)(a^2+x^2))
-    const double ax = fabs(xd);
-    const T d = (T)(-((r.bnd - ax) * (r.bnd + ax)));
-    const T den = r.alfl2 + xmsq;
-    if (r.co2)
-      f = r.rdd * d * (r.alfl2 + d) / den;
-    else
-      f = -(r.rdd * (T)(r.bnd * r.bnd)) * d / den;
-  }
-  if (r.lc) f = f + xm * r.dptrat * f;
-  return f;
+  else
+    f = r.sil * recip_nr(r.alfl2 + xmsq) - sub;
+  return f + xm * r.dptrat * f;
 }
 
-// compensated sum in FP32; FP64 sums need no compensation here
-template <typename T>
-__device__ __forceinline__ void kahan_add(T& sum, T& c, T x) {
-  if constexpr (sizeof(T) == 8) {
-    sum += x;
+// F4 at window point j = j0 + kq - k0 (FP32).  Beyond the quadratic core
+// the bound is subtracted without cancellation, with v = B^2 - x^2 = u (2B - u):
+//   non-CO2  L(x) - L(B)               =  F4BND v / (a^2 + x^2)
+//   CO2      L(x) - (2 - x^2/B^2) L(B) =  (F4BND/B^2) v (v - a^2) / (a^2 + x^2)
+__device__ __forceinline__ float f4_at(const F4Reg<float>& r, int, float kq, double, double,
+                                       float dvr4f, float bndf, float rbndsqf) {
+  const float xm = kq * dvr4f - r.dlt;
+  const float xmsq = xm * xm;
+  const float zvsq = xmsq * r.rvi2;
+  float f;
+  if (zvsq <= 4096.f) {
+    const float sub = r.co2 ? (2.f - xmsq * rbndsqf) * r.f4bnd : r.f4bnd;
+    f = (r.sa3 + zvsq * r.sb3) - sub;
   } else {
-    const T y = x - c;
-    const T t = sum + y;
-    c = (t - sum) - y;
-    sum = t;
+    const float u = (xm >= 0.f ? (r.mpf - kq) + r.php : (r.mmf + kq) + r.phm) * dvr4f;
+    const float v = u * (2.f * bndf - u);
+    const float rden = recip_nr(r.alfl2 + xmsq);
+    f = r.co2 ? (r.rdd * v) * (v - r.alfl2) * rden : (r.f4bnd * v) * rden;
+  }
+  return f + xm * r.dptrat * f;
+}
+
+// A far-wing CTA is one deciding warp plus kFwAdders threads that own the
+// window's points (point j belongs to adder (j-1) % kFwAdders).
+constexpr int kFwAdders = 224;
+constexpr int kFwThreads = kFwAdders + 32;
+constexpr int kFwPts = (kLimOut + kFwAdders - 1) / kFwAdders;  // window points per adder
+constexpr int kFwSmem = 2 * (int)kR4Stride * (int)sizeof(double);  // two R4 buffers
+constexpr int kFwBatch = 4;  // lines the deciding warp evaluates together
+
+// Sum, in list order, of both sides of lines cl[idx(0..n-1)] at point jj
+// into acc, where a line counts only if use(k) holds.
+template <typename Idx, typename Use>
+__device__ __forceinline__ void f4_sum_lines(const F4Line* cl, int n, Idx idx, Use use, int jj,
+                                             double dvr4, double rbndsq, double& acc) {
+  for (int a = 0; a < n; a += kFwBatch) {
+    double f[kFwBatch], g[kFwBatch];
+    int img = 0;
+#pragma unroll
+    for (int u = 0; u < kFwBatch; u++) {
+      const int k = idx(a + u < n ? a + u : n - 1);
+      const F4Line& q = cl[k];
+      const bool on = a + u < n && use(k);
+      f[u] = on ? f4_side(q, false, jj, dvr4, rbndsq) : 0.;
+      img |= on ? (q.has & 2) : 0;
+      g[u] = 0.;
+    }
+    if (__any_sync(__activemask(), img)) {
+#pragma unroll
+      for (int u = 0; u < kFwBatch; u++) {
+        const int k = idx(a + u < n ? a + u : n - 1);
+        const bool on = a + u < n && use(k);
+        g[u] = on ? f4_side(cl[k], true, jj, dvr4, rbndsq) : 0.;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kFwBatch; u++) {
+      acc += f[u];
+      acc += g[u];
+    }
   }
 }
 
-constexpr int kFwThreads = 256;
-constexpr int kFwPts = (kLimOut + kFwThreads - 1) / kFwThreads;  // window points per thread
-
+// The CTA works in phases separated by one barrier.  In phase t the deciding
+// warp takes chunk t (32 consecutive lines of the layer's shrunk list) and
+// decides every line exactly as CONVF4's in-order test against the partial
+// R4 at its point JJ, where that partial R4 is
+//     R4 through chunk t-2   (buffer written in phase t-1)
+//   + chunk t-1's accepted lines, evaluated at JJ directly
+//   + the earlier accepted lines of chunk t, evaluated at JJ directly;
+// meanwhile the adders evaluate chunk t-1's accepted lines over the whole
+// window and write R4 through chunk t-1 into the other buffer.  The in-chunk
+// order dependence is resolved speculatively: every line is first decided
+// against the lines accepted on their own partial R4 alone; the lowest line
+// whose decision differs from that guess is exact, so the guess is corrected
+// there and the lines above it re-decided, until no line differs.
 template <typename T>
-__global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_layer) {
-  const int gw = blockIdx.x;
+__global__ void __launch_bounds__(kFwThreads, 3)
+    k_far_wing(Work w, const int32_t* win_order, const int32_t* win_layer) {
+  extern __shared__ double fw_r4[];  // [2][kR4Stride]
+  __shared__ F4Line cl[2][kChunk];
+  __shared__ int s_idx[2][kChunk];
+  __shared__ int s_live[kChunk];
+  __shared__ int s_nacc[2];
+  __shared__ int s_state[2];  // by phase parity: a chunk was decided
+  const int gw = win_order[blockIdx.x];
   const int l = win_layer[gw];
   const LayerDev& L = w.L[l];
-  const WinDev W = w.win[gw];
-  __shared__ double R4s[kR4Stride];
-  __shared__ F4Line cl[kChunk];
-  __shared__ int s_nacc, s_term;
-  __shared__ int s_acc[kChunk];
-  for (int j = threadIdx.x; j < kR4Stride; j += blockDim.x) R4s[j] = 0.;
-  if (threadIdx.x == 0) s_term = 0;
-  __syncthreads();
-  const double dvr4 = L.dvr4, bnd = L.bound4, bndsq = bnd * bnd;
-  const double recpi = 1. / (2. * asin(1.));
-  const double zsq = 64. * 64.;
-  const double A3 = (1. + 2. * zsq) / ((1. + zsq) * (1. + zsq));
-  const double B3 = -1. / ((1. + zsq) * (1. + zsq));
+  const WinDev& W = w.win[gw];
+  for (int j = threadIdx.x; j < 2 * kR4Stride; j += kFwThreads) fw_r4[j] = 0.;
+  const double dvr4 = L.dvr4, bnd = L.bound4, bndsq = bnd * bnd, rbndsq = 1. / bndsq;
   const int npt = W.nptr4;
   const int64_t S = L.off_shr;
   const int64_t ns = w.s_count[l];
   const int64_t nb9 = w.b9_count[l];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int term = 0;
+  const unsigned full = 0xffffffffu;
+  // deciding warp's position in the shrunk list (uniform over its lanes)
+  int64_t b = -1, c0 = 0, b1 = 0;
+  bool dmore = false;
+  auto next_block = [&]() {
+    for (b = b + 1; b < nb9; b++) {
+      c0 = w.b9_start[L.off_blk9 + b];
+      b1 = (b + 1 < nb9) ? w.b9_start[L.off_blk9 + b + 1] : ns;
+      if (!(w.s_vnu[S + b1 - 1] < W.vlo)) return true;  // RDLIN4 skips VMAX < VLO (:3815)
+    }
+    return false;
+  };
+  // raw values of the deciding warp's next line, loaded one phase ahead
+  double n_sp = 0., n_spp = 0., n_ad = 0., n_al = 0., n_v = 0.;
+  int n_co2 = 0;
+  auto prefetch = [&]() {
+    const int64_t i = c0 + lane;
+    if (dmore && i < b1) {
+      n_sp = w.s_sp[S + i];
+      n_spp = w.s_spp[S + i];
+      n_ad = w.s_epp[S + i];
+      n_al = w.s_alfa[S + i];
+      n_v = w.s_vnu[S + i];
+      n_co2 = w.s_co2[S + i];
+    }
+  };
+  if (warp == 0) {
+    dmore = next_block();
+    prefetch();
+  }
+  __syncthreads();
+  int rb = 0;      // buffer holding R4 through chunk t-2 in phase t
+  int prv = 0;     // chunk buffer decided in the previous phase
+  bool have_prev = false;
   unsigned long long nevals = 0;
-  for (int64_t b = 0; b < nb9 && !term; b++) {
-    const int64_t b0 = w.b9_start[L.off_blk9 + b];
-    const int64_t b1 = (b + 1 < nb9) ? w.b9_start[L.off_blk9 + b + 1] : ns;
-    if (w.s_vnu[S + b1 - 1] < W.vlo) continue;  // RDLIN4 skips blocks with VMAX < VLO (:3815)
-    for (int64_t c0 = b0; c0 < b1; c0 += kChunk) {
-      // every thread has finished with the previous chunk's shared state
-      // before warp 0 rewrites it
-      __syncthreads();
-      if (warp == 0) {
+  for (int ph = 0;; ph++) {
+    const double* R4r = fw_r4 + rb * kR4Stride;
+    double* R4w = fw_r4 + (rb ^ 1) * kR4Stride;
+    if (warp == 0) {
+      int decided = 0;
+      if (dmore) {
+        const int nb = prv ^ 1;
         const int64_t i = c0 + lane;
-        bool cand = false;
-        double speak = 0., base = 0.;
-        int jj = 1;
-        F4Line p;
+        bool ok = false;
+        double speak = 0., r = 0., vnu = 0., spp = 0.;
+        int jj = 1, has = 0;
+        F4Line& p = cl[nb][lane];  // built in place in shared memory
         p.has = 0;
         if (i < b1) {
-          const double sp = w.s_sp[S + i], spp = w.s_spp[S + i];
-          cand = !(sp == 0. && spp == 0.);
-          const double ad = w.s_epp[S + i], al = w.s_alfa[S + i], v = w.s_vnu[S + i];
+          const double recpi = 1. / (2. * asin(1.));
+          const double zsq = 64. * 64.;
+          const double A3 = (1. + 2. * zsq) / ((1. + zsq) * (1. + zsq));
+          const double B3 = -1. / ((1. + zsq) * (1. + zsq));
+          const double sp = n_sp;
+          spp = n_spp;
+          ok = !(sp == 0. && spp == 0.);
+          const double ad = n_ad, al = n_al, v = n_v;
           const double zeta = al / (al + ad);
           long iz = fint(100. * zeta + kONEPL);
           iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);  // zeta in [0,1]; guards bad input
           const double zd = 100. * zeta - double(iz - 1);
-          const double alfav = (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (al + ad);
+          const double alfav =
+              (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (al + ad);
           const double ralfv = 1. / alfav;
           const double sil = sp * recpi * al;
           const double siv = (al * ralfv) * sp * recpi * ralfv;
@@ -586,7 +716,8 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
           long jjl = fint((v - W.v1r4) / dvr4 + 1.);
           jjl = jjl < 1 ? 1 : (jjl > npt ? npt : jjl);
           jj = (int)jjl;
-          p.vnu = v;
+          vnu = v;
+          const double dptrat = spp != 0. ? spp / (sp * alfav) : 0.;
           p.xnui = v - W.v1r4;
           p.sil = sil;
           p.siv_a3 = siv * A3;
@@ -594,86 +725,156 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
           p.alfl2 = al * al;
           p.rvi2 = 1. / (alfav * alfav);
           p.f4bnd = sil / (al * al + bndsq);
-          p.spp = spp;
-          p.dptrat = spp / (sp * alfav);
-          p.co2 = w.s_co2[S + i];
+          p.dptrat = dptrat;
+          p.co2 = n_co2;
           const long jmin = fint((p.xnui - bnd) / dvr4 + 2.);
           const long jmax = fint((p.xnui + bnd) / dvr4 + 1.);
-          p.jmin = (int)(jmin < 1 ? 1 : (jmin > npt + 1 ? npt + 1 : jmin));
-          p.jmax = (int)(jmax > npt ? npt : (jmax < 0 ? 0 : jmax));
           const bool beyond = jmin > npt;  // GO TO 60: no wing, no image
-          if (!beyond && p.jmax >= p.jmin) p.has |= 1;
+          p.jmin = (int)(jmin < 1 ? 1 : jmin);
+          p.jmax = (int)(jmax > npt ? npt : jmax);
+          if (beyond || p.jmax < p.jmin) p.jmin = 1, p.jmax = 0;
+          else p.has |= 1;
+          p.mxnui = -v - W.v1r4;
+          p.mdptrat = -dptrat;
+          p.mjmin = 1;
+          p.mjmax = 0;
           if (!beyond && v > 0. && v <= 25.) {  // Van Vleck-Weisskopf image (:4014-4024)
-            p.mxnui = -v - W.v1r4;
-            p.mspp = -spp;
-            p.mdptrat = -spp / (sp * alfav);
             const long mjmin = fint((p.mxnui - bnd) / dvr4 + 2.);
             const long mjmax = fint((p.mxnui + bnd) / dvr4 + 1.);
-            p.mjmin = (int)(mjmin < 1 ? 1 : mjmin);
-            p.mjmax = (int)(mjmax > npt ? npt : mjmax);
-            if (mjmin <= npt && p.mjmax >= p.mjmin) p.has |= 2;
+            if (mjmin <= npt && (mjmax > npt ? npt : mjmax) >= (mjmin < 1 ? 1 : mjmin)) {
+              p.mjmin = (int)(mjmin < 1 ? 1 : mjmin);
+              p.mjmax = (int)(mjmax > npt ? npt : mjmax);
+              p.has |= 2;
+            }
           }
-          base = R4s[jj];
+          has = p.has;
+          if constexpr (sizeof(T) == 4) {
+            p.sil32 = (float)p.sil;
+            p.sa3_32 = (float)p.siv_a3;
+            p.sb3_32 = (float)p.siv_b3;
+            p.alfl2_32 = (float)p.alfl2;
+            p.rvi2_32 = (float)p.rvi2;
+            p.f4bnd32 = (float)p.f4bnd;
+            p.rdd32 = (float)(p.f4bnd * rbndsq);
+            const double rdv = 1. / dvr4;
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+              if (!(has & (1 << m))) continue;
+              F4Side32& sd = p.s32[m];
+              const double xn = m ? p.mxnui : p.xnui;
+              const double jc = floor(xn * rdv + 1.5);
+              const double dl = xn - (jc - 1.) * dvr4;
+              const double tp = (bnd + dl) * rdv, tm = (bnd - dl) * rdv;
+              const double mp = floor(tp), mm = floor(tm);
+              sd.jc = (int32_t)jc;
+              sd.dlt = (float)dl;
+              sd.php = (float)(tp - mp);
+              sd.phm = (float)(tm - mm);
+              sd.mpf = (float)mp;
+              sd.mmf = (float)mm;
+              sd.dptrat = (float)(m ? p.mdptrat : p.dptrat);
+            }
+          }
+          if (ok) r = R4r[jj];
         }
-        cl[lane] = p;
         __syncwarp();
-        double partial = 0.;
-        int term_at = kChunk;
-        for (int k = 0; k < kChunk; k++) {
-          if (c0 + k >= b1) break;
-          const bool ck = __shfl_sync(0xffffffffu, cand, k);
-          if (!ck) {
-            if (lane == k) s_acc[k] = 0;
-            continue;
+        // chunk t-1's accepted lines, not yet in the R4 buffer
+        const int np = have_prev ? s_nacc[prv] : 0;
+        f4_sum_lines(
+            cl[prv], np, [&](int a) { return s_idx[prv][a]; }, [&](int) { return ok; }, jj, dvr4,
+            rbndsq, r);
+        const double dptmn = W.dptmn, dptfc = L.dptfc;
+        bool live = ok && !(speak <= (dptmn + dptfc * r) && spp == 0.);
+        const unsigned lm = __ballot_sync(full, live);
+        // earlier lines of this chunk accepted on their own partial R4
+        if (live) s_live[__popc(lm & ((1u << lane) - 1u))] = lane;
+        __syncwarp();
+        double part = r;  // continues the running sum in CONVF4's order
+        f4_sum_lines(
+            cl[nb], __popc(lm), [&](int a) { return s_live[a]; },
+            [&](int k) { return ok && k < lane; }, jj, dvr4, rbndsq, part);
+        bool acc = ok && !(speak <= (dptmn + dptfc * part) && spp == 0.);
+        unsigned mis = __ballot_sync(full, acc != live);
+        while (mis) {
+          const int f = __ffs(mis) - 1;  // every line below f is decided exactly
+          const bool af = __shfl_sync(full, acc, f);
+          if (ok && lane > f) {
+            const double v = f4_side(cl[nb][f], false, jj, dvr4, rbndsq) +
+                             f4_side(cl[nb][f], true, jj, dvr4, rbndsq);
+            part += af ? v : -v;
+            acc = !(speak <= (dptmn + dptfc * part) && spp == 0.);
           }
-          int acc = 0;
-          if (lane == k) {
-            const double r = base + partial;
-            acc = !(speak <= (W.dptmn + L.dptfc * r) && p.spp == 0.);
-          }
-          acc = __shfl_sync(0xffffffffu, acc, k);
-          if (lane == k) s_acc[k] = acc;
-          if (!acc) continue;
-          const F4Line& q = cl[k];
-          if (q.vnu >= W.vnulst) {  // end of convolution (:3928, IHI=-1)
-            term_at = k;
-            if (lane == k) s_acc[k] = 0;
-            break;
-          }
-          if (lane > k && (c0 + lane) < b1 && cand) {
-            if ((q.has & 1) && jj >= q.jmin && jj <= q.jmax) partial += f4_eval(q, false, jj, dvr4, bndsq);
-            if ((q.has & 2) && jj >= q.mjmin && jj <= q.mjmax) partial += f4_eval(q, true, jj, dvr4, bndsq);
-          }
+          if (lane == f) live = acc;
+          mis = __ballot_sync(full, acc != live) & ~((2u << f) - 1u);
         }
-        if (lane == 0) {
-          int n = 0;
-          const int lim = (int)((b1 - c0) < kChunk ? (b1 - c0) : kChunk);
-          for (int k = 0; k < lim && k < term_at; k++)
-            if (s_acc[k] && cl[k].has) s_acc[n++] = k;
-          s_nacc = n;
-          if (term_at < kChunk) s_term = 1;
+        // the first accepted line at or beyond VNULST ends the window (:3928, IHI=-1)
+        const unsigned tm = __ballot_sync(full, acc && vnu >= W.vnulst);
+        const int lim = tm ? __ffs(tm) - 1 : kChunk;
+        const unsigned am = __ballot_sync(full, acc && has != 0 && lane < lim);
+        if ((am >> lane) & 1u) s_idx[nb][__popc(am & ((1u << lane) - 1u))] = lane;
+        if (lane == 0) s_nacc[nb] = __popc(am);
+        decided = 1;
+        if (tm) {
+          dmore = false;
+        } else {
+          c0 += kChunk;
+          if (c0 >= b1) dmore = next_block();
+          prefetch();
         }
       }
-      __syncthreads();
-      const int nacc = s_nacc;
-      if (nacc > 0) {
-        // each thread owns window points j = 1 + tid + 256 q; the line's
-        // constants are held in registers while it sweeps them
-        T acc[kFwPts], cmp[kFwPts];
+      if (lane == 0) s_state[ph & 1] = decided;
+    } else if (have_prev) {
+      // adders: chunk t-1's accepted lines over the whole window
+      const int ad = (int)threadIdx.x - 32;
+      const int na = s_nacc[prv];
+      if constexpr (sizeof(T) == 8) {
+        // FP64: each point summed in shared memory line by line, line
+        // before image, in CONVF4's order
 #pragma unroll
-        for (int q = 0; q < kFwPts; q++) acc[q] = cmp[q] = (T)0.;
-        for (int a = 0; a < nacc; a++) {
-          const F4Line& pl = cl[s_acc[a]];
+        for (int q = 0; q < kFwPts; q++) {
+          const int j = 1 + ad + kFwAdders * q;
+          if (j <= npt) R4w[j] = R4r[j];
+        }
+        for (int a = 0; a < na; a++) {
+          const F4Line& pl = cl[prv][s_idx[prv][a]];
+#pragma unroll 1
+          for (int m = 0; m < 2; m++) {
+            const int lo = m ? pl.mjmin : pl.jmin, hi = m ? pl.mjmax : pl.jmax;
+            // this adder's points j = 1 + ad + kFwAdders q inside [lo, hi]
+            const int qlo = (lo - 1 - ad <= 0) ? 0 : (lo - 2 - ad) / kFwAdders + 1;
+            const int qhi = (hi - 1 - ad < 0) ? -1 : (hi - 1 - ad) / kFwAdders;
+            if (qhi < qlo) continue;
+            F4Reg<double> rg;
+            f4_load(rg, pl, m, 0);
+#pragma unroll 2
+            for (int q = qlo; q <= qhi; q++) {
+              const int j = 1 + ad + kFwAdders * q;
+              R4w[j] += f4_at(rg, j, 0.f, dvr4, rbndsq, 0.f, 0.f, 0.f);
+            }
+            nevals += (unsigned)(qhi - qlo + 1);
+          }
+        }
+      } else {
+        // split precision: the chunk's lines summed in FP32 registers, the
+        // chunk total added to the FP64 R4
+        const float dvr4f = (float)dvr4, bndf = (float)bnd, rbndsqf = (float)rbndsq;
+        float acc[kFwPts];
+#pragma unroll
+        for (int q = 0; q < kFwPts; q++) acc[q] = 0.f;
+        for (int a = 0; a < na; a++) {
+          const F4Line& pl = cl[prv][s_idx[prv][a]];
 #pragma unroll 1
           for (int m = 0; m < 2; m++) {
             if (!(pl.has & (1 << m))) continue;
             const int lo = m ? pl.mjmin : pl.jmin, hi = m ? pl.mjmax : pl.jmax;
-            const F4Reg<T> r = f4_load<T>(pl, m == 1, bndsq);
+            F4Reg<float> rg;
+            f4_load(rg, pl, m, 1 + ad);
 #pragma unroll
             for (int q = 0; q < kFwPts; q++) {
-              const int j = 1 + (int)threadIdx.x + kFwThreads * q;
+              const int j = 1 + ad + kFwAdders * q;
               if (j >= lo && j <= hi) {
-                kahan_add(acc[q], cmp[q], f4_at<T>(r, j, dvr4));
+                acc[q] += f4_at(rg, j, rg.k0 + (float)(kFwAdders * q), dvr4, rbndsq, dvr4f,
+                                bndf, rbndsqf);
                 nevals++;
               }
             }
@@ -681,17 +882,20 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
         }
 #pragma unroll
         for (int q = 0; q < kFwPts; q++) {
-          const int j = 1 + (int)threadIdx.x + kFwThreads * q;
-          if (j <= npt) R4s[j] += (double)acc[q] - (double)cmp[q];
+          const int j = 1 + ad + kFwAdders * q;
+          if (j <= npt) R4w[j] = R4r[j] + (double)acc[q];
         }
       }
-      __syncthreads();
-      term = s_term;
-      if (term) break;
     }
+    __syncthreads();
+    const int decided = s_state[ph & 1];
+    if (have_prev) rb ^= 1;
+    prv ^= 1;
+    have_prev = decided != 0;
+    if (!decided) break;
   }
   if (nevals) atomicAdd(&w.counters[0], nevals);
-  __syncthreads();
+  double* R4s = fw_r4 + rb * kR4Stride;
   double* out = w.r4 + (int64_t)gw * kR4Stride;
   if (L.jrad == 1) {
     // radiation field applied to R4 (LBLF4 :3726-3758)
@@ -713,7 +917,7 @@ __global__ void __launch_bounds__(256) k_far_wing(Work w, const int32_t* win_lay
     }
     __syncthreads();
   }
-  for (int j = threadIdx.x; j < kR4Stride; j += blockDim.x) out[j] = (j >= 1 && j <= npt) ? R4s[j] : 0.;
+  for (int j = threadIdx.x; j < kR4Stride; j += kFwThreads) out[j] = (j >= 1 && j <= npt) ? R4s[j] : 0.;
 }
 
 // =========================================================================
@@ -1358,6 +1562,13 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
 void init_kernel_attributes() {
   cudaFuncSetAttribute(k_combine_od, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        3 * 2400 * (int)sizeof(double));
+  // two R4 buffers per CTA; the largest carveout lets several CTAs share an SM
+  cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
+  cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
+  cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
 }
 
 void upload_voicon() {
@@ -1389,13 +1600,13 @@ cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_b
   return cudaGetLastError();
 }
 
-cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_layer,
-                            int precision, cudaStream_t s) {
+cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
+                            const int32_t* win_layer, int precision, cudaStream_t s) {
   if (nwin_total <= 0) return cudaSuccess;
   if (precision == LBL_PREC_SPLIT)
-    k_far_wing<float><<<nwin_total, kFwThreads, 0, s>>>(w, win_layer);
+    k_far_wing<float><<<nwin_total, kFwThreads, kFwSmem, s>>>(w, win_order, win_layer);
   else
-    k_far_wing<double><<<nwin_total, kFwThreads, 0, s>>>(w, win_layer);
+    k_far_wing<double><<<nwin_total, kFwThreads, kFwSmem, s>>>(w, win_order, win_layer);
   return cudaGetLastError();
 }
 

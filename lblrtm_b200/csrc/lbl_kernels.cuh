@@ -79,8 +79,8 @@ void upload_voicon();
 cudaError_t launch_far_scale(const Work& w, const DevLines& ln, int64_t max_far, cudaStream_t s);
 cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_base,
                           int64_t nblk_total, cudaStream_t s);
-cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_layer,
-                            int precision, cudaStream_t s);
+cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
+                            const int32_t* win_layer, int precision, cudaStream_t s);
 cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
