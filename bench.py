@@ -307,6 +307,7 @@ def gpu_arm(a):
         roof_merge["frac"] = roof_merge["achieved"] / hbm_peak
     launches = sum(v[1] for v in stats.values()) // max(nstep, 1)
     stage_ms = {k: round(v[0] / nstep, 4) for k, v in stats.items()}
+    stage_work = {k: v[2] / nstep for k, v in stats.items() if v[2]}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -330,7 +331,7 @@ def gpu_arm(a):
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replica x{world}"},
             "roofline": roofline, "roofline_merge": roof_merge,
-            "stage_ms": stage_ms,
+            "stage_ms": stage_ms, "stage_work": stage_work,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

@@ -183,11 +183,13 @@ struct Batch {
   int32_t* d_win_order = nullptr;  // far-wing windows, most expensive first
   int32_t* d_panel_layer = nullptr;
   int64_t* d_panel_base = nullptr;
-  int64_t* d_tile_prefix = nullptr;
+  int64_t* d_panel_rng = nullptr;  // candidate near-wing lines of every panel
+  double* d_panel_segs = nullptr;  // RADFNI segments of every panel
+  int32_t* d_panel_nseg = nullptr;
   int64_t* d_blk_base = nullptr;
   int64_t nblk_total = 0;
   int32_t nwin_total = 0;
-  int64_t npanel_total = 0, ntiles = 0, max_far = 0, max_r3 = 0, max_r2 = 0;
+  int64_t npanel_total = 0, max_far = 0;
   int64_t od_total = 0;
 };
 
@@ -210,7 +212,6 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   int64_t o_r1 = 0, o_r2 = 0, o_r3 = 0, o_od = 0, o_pan = 0, o_win = 0, o_far = 0, o_near = 0,
           o_b9 = 0, o_abs = 0;
   B.ld.resize(n);
-  std::vector<int64_t> tile_prefix(3 * n + 1, 0);
   std::vector<int64_t> blk_base(n + 1, 0);
   for (int l = 0; l < n; l++) {
     LayerDev& d = B.plans[l].d;
@@ -240,16 +241,10 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
     o_b9 += nfar / 1000 + 2;
     o_abs += (d.icntnm ? d.nptabs : 0) + 8;
     B.max_far = std::max(B.max_far, nfar);
-    B.max_r3 = std::max(B.max_r3, d.n_r3);
-    B.max_r2 = std::max(B.max_r2, d.n_r2);
-    const int64_t ng[3] = {d.n_r1, d.n_r2, d.n_r3};
-    for (int k = 0; k < 3; k++)
-      tile_prefix[3 * l + k + 1] = tile_prefix[3 * l + k] + (ng[k] + 1023) / 1024;
     B.ld[l] = d;
   }
   B.nwin_total = (int32_t)o_win;
   B.npanel_total = o_pan;
-  B.ntiles = tile_prefix[3 * n];
   B.od_total = o_od;
   B.nblk_total = blk_base[n];
   const int64_t nbt = B.nblk_total + 1;
@@ -279,13 +274,12 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<double>(o_near + 1);
   for (int k = 0; k < 5; k++) lay.add<int32_t>(o_near + 1);
   lay.add<int8_t>(o_near + 1);
-  lay.add<double>(o_r1);
-  lay.add<double>(o_r2);
-  lay.add<double>(o_r3);
   lay.add<double>(o_abs);
   lay.add<double>(o_od);
-  lay.add<int64_t>(3 * n + 1);
-  lay.add<int32_t>(4);
+  lay.add<int64_t>(2 * o_pan + 2);
+  lay.add<double>(3 * kPanelSegMax * (o_pan + 1));
+  lay.add<int32_t>(o_pan + 1);
+  lay.add<int32_t>(8);
   lay.add<int32_t>(nbt * kSegMaxBlk);
   lay.add<int32_t>(nbt * kSegMaxBlk);
   lay.add<int32_t>(nbt);
@@ -334,13 +328,12 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   w.n_j3 = A.take<int32_t>(o_near + 1);
   w.n_pconv = A.take<int32_t>(o_near + 1);
   w.n_ok = A.take<int8_t>(o_near + 1);
-  w.r1 = A.take<double>(o_r1);
-  w.r2 = A.take<double>(o_r2);
-  w.r3 = A.take<double>(o_r3);
   w.absrb = A.take<double>(o_abs);
   w.od = A.take<double>(o_od);
-  B.d_tile_prefix = A.take<int64_t>(3 * n + 1);
-  w.status = A.take<int32_t>(4);
+  B.d_panel_rng = A.take<int64_t>(2 * o_pan + 2);
+  B.d_panel_segs = A.take<double>(3 * kPanelSegMax * (o_pan + 1));
+  B.d_panel_nseg = A.take<int32_t>(o_pan + 1);
+  w.status = A.take<int32_t>(8);
   w.c_raw = A.take<int32_t>(nbt * kSegMaxBlk);
   w.c_out = A.take<int32_t>(nbt * kSegMaxBlk);
   w.seg_blk = A.take<int32_t>(nbt);
@@ -376,7 +369,8 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   h_pbase[n] = o_pan;
   // Far-wing windows are launched most expensive first so that the long
   // ones do not start last.  Cost estimate: lines within the window's reach
-  // times the points one line covers.
+  // (each is decided in order) times a fixed per-line decision cost plus the
+  // points one line covers.
   std::vector<int32_t> h_word(std::max<int64_t>(o_win, 1), 0);
   {
     std::vector<double> cost(o_win);
@@ -387,7 +381,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
       const LayerDev& d = B.ld[h_wlay[k]];
       const double nl = double(std::lower_bound(vb, ve, W.vnulst) - std::lower_bound(vb, ve, W.vlo));
       const double span = std::min<double>(W.nptr4, 2. * d.bound4 / d.dvr4 + 1.);
-      cost[k] = nl * (span + 64.);
+      cost[k] = nl * (span + 8000.);
       h_word[k] = (int32_t)k;
     }
     std::stable_sort(h_word.begin(), h_word.begin() + o_win,
@@ -408,8 +402,6 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
     CK(cudaMemcpyAsync(B.d_win_layer, h_wlay.data(), sizeof(int32_t) * o_win,
                        cudaMemcpyHostToDevice, s));
   }
-  CK(cudaMemcpyAsync(B.d_tile_prefix, tile_prefix.data(), sizeof(int64_t) * (3 * n + 1),
-                     cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(B.d_blk_base, blk_base.data(), sizeof(int64_t) * (n + 1),
                      cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(w.status, 0, 4 * sizeof(int32_t), s));
@@ -423,8 +415,6 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
 int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   cudaStream_t s = ctx->stream;
   const Work& w = B.w;
-  double npts = 0.;
-  for (auto& d : B.ld) npts += (double)d.npts;
   {
     StageTimer t(ctx, "far_scale", 1);
     CK(launch_far_scale(w, ctx->dl, B.max_far, s));
@@ -447,12 +437,10 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, s));
   }
   {
-    StageTimer t(ctx, "grids", 1);
-    CK(launch_grids(w, ctx->dl, ctx->sh, B.d_tile_prefix, B.ntiles, precision, s));
-  }
-  {
-    StageTimer t(ctx, "combine", 3);
-    CK(launch_combine(w, B.max_r3, B.max_r2, B.npanel_total, B.d_panel_layer, B.d_panel_base, s));
+    // near-wing sums, PANEL combination and optical depth in one pass
+    StageTimer t(ctx, "panels", 3);
+    CK(launch_panels(w, ctx->dl, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
+                     B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
   }
   int32_t st[4] = {0, 0, 0, 0};
   unsigned long long cnt[8];
@@ -460,8 +448,7 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   CK(cudaMemcpyAsync(cnt, w.counters, sizeof(cnt), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   ctx->stage("far_wing").work += (double)cnt[0];
-  ctx->stage("grids").work += (double)cnt[1];
-  ctx->stage("combine").work += npts;
+  ctx->stage("panels").work += (double)cnt[1];
   if (st[0] == 2)
     return fail(ctx, LBL_E_RANGE,
                 "far-wing line file too sparse: a LINF4 segment spans more than 48 TAPE3 panels");
@@ -558,7 +545,7 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
   build_shape_tables(t);
   const size_t nd = kNfmx + 1;
   char* mem = nullptr;
-  if (cudaMalloc(&mem, 5 * nd * (sizeof(double) + sizeof(float)) + 1024) != cudaSuccess) {
+  if (cudaMalloc(&mem, 9 * nd * sizeof(double) + 1024) != cudaSuccess) {
     delete t;
     delete ctx;
     return LBL_E_NOMEM;
@@ -566,16 +553,18 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
   ctx->shape_mem = mem;
   const double* src[5] = {t->f1, t->f2, t->f3, t->fg, t->xver};
   double* dd = reinterpret_cast<double*>(mem);
-  float* ff = reinterpret_cast<float*>(mem + 5 * nd * sizeof(double));
-  std::vector<float> tmp(nd);
-  for (int k = 0; k < 5; k++) {
+  double* pk = dd + ((5 * nd + 3) & ~size_t(3));  // records 32-byte aligned
+  for (int k = 0; k < 5; k++)
     cudaMemcpy(dd + k * nd, src[k], nd * sizeof(double), cudaMemcpyHostToDevice);
-    for (size_t i = 0; i < nd; i++) tmp[i] = (float)src[k][i];
-    cudaMemcpy(ff + k * nd, tmp.data(), nd * sizeof(float), cudaMemcpyHostToDevice);
+  std::vector<double> rec(4 * nd, 0.);
+  for (size_t i = 0; i < nd; i++) {
+    rec[4 * i] = t->f1[i];
+    rec[4 * i + 1] = t->fg[i];
+    rec[4 * i + 2] = t->xver[i];
   }
+  cudaMemcpy(pk, rec.data(), 4 * nd * sizeof(double), cudaMemcpyHostToDevice);
   delete t;
-  ctx->sh = DevShapes{dd, dd + nd, dd + 2 * nd, dd + 3 * nd, dd + 4 * nd,
-                      ff, ff + nd, ff + 2 * nd, ff + 3 * nd, ff + 4 * nd};
+  ctx->sh = DevShapes{dd, dd + nd, dd + 2 * nd, dd + 3 * nd, dd + 4 * nd, pk};
   if (cudaGetLastError() != cudaSuccess) {
     lbl_ctx_destroy(ctx);
     return LBL_E_CUDA;

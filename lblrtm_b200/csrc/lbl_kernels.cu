@@ -9,6 +9,7 @@
 // only shift indices by multiples of 2400/600/150).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -1099,12 +1100,6 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
   // lines of the range beyond the walked panels are not used
 }
 
-// =========================================================================
-// CNVFNV gather onto the three grids (src/oprop.f90:1283-1351).  Each CTA
-// owns 256 consecutive points of one grid of one layer; candidate lines are
-// found by binary search on the sorted TAPE3 centres and staged in shared
-// memory; every thread sums the lines whose window covers its point.
-// =========================================================================
 __device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double x) {
   while (lo < hi) {
     int64_t m = (lo + hi) >> 1;
@@ -1112,143 +1107,6 @@ __device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double
     else hi = m;
   }
   return lo;
-}
-
-struct NearStage {
-  double zint, zslope, s0, s1, s2, sppsp;
-  int64_t lo, hi, pofs;  // global window; pofs = panel offset on this grid
-};
-
-constexpr int kGridTile = 1024;  // points per CTA (4 per thread)
-
-template <typename T>
-__device__ __forceinline__ const T* shape_table(const DevShapes& sh, int k) {
-  if constexpr (sizeof(T) == 8)
-    return k == 0 ? sh.f1 : k == 1 ? sh.f2 : k == 2 ? sh.f3 : k == 3 ? sh.fg : sh.xver;
-  else
-    return k == 0 ? sh.f1s : k == 1 ? sh.f2s : k == 2 ? sh.f3s : k == 3 ? sh.fgs : sh.xvers;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_grids(Work w, DevLines ln, DevShapes sh,
-                                               const int64_t* tile_prefix, int ntp) {
-  // tile -> (layer, grid) by binary search of the prefix (3 entries per layer)
-  const int64_t t = blockIdx.x;
-  int lo = 0, hi = ntp;
-  while (lo < hi) {
-    int m = (lo + hi) >> 1;
-    if (tile_prefix[m + 1] <= t) lo = m + 1;
-    else hi = m;
-  }
-  const int idx = lo;
-  const int l = idx / 3, grid = idx % 3;
-  const LayerDev& L = w.L[l];
-  const int64_t g0 = 1 + (t - tile_prefix[idx]) * kGridTile;
-  const int64_t ng = grid == 0 ? L.n_r1 : (grid == 1 ? L.n_r2 : L.n_r3);
-  const double dvk = grid == 0 ? L.dv : (grid == 1 ? L.dvr2 : L.dvr3);
-  const double conf = grid == 0 ? 1. : (grid == 1 ? L.conf2 : L.conf3);
-  const double reach = (grid == 0 ? 4. : (grid == 1 ? 16. : 64.)) * L.alfmax +
-                       (grid == 0 ? 2. : (grid == 1 ? 8. : 32.)) * L.dv + fabs(L.rhorat) * 1.0;
-  const int64_t g1e = (g0 + kGridTile - 1 < ng) ? g0 + kGridTile - 1 : ng;
-  __shared__ int64_t s_lo, s_hi;
-  if (threadIdx.x == 0)
-    s_lo = lower_bound_d(ln.vnu, L.near_lo, L.near_hi, L.vft0 + double(g0 - 1) * dvk - reach);
-  if (threadIdx.x == 32)
-    s_hi = lower_bound_d(ln.vnu, L.near_lo, L.near_hi, L.vft0 + double(g1e - 1) * dvk + reach);
-  __syncthreads();
-  const int64_t clo = s_lo, chi = s_hi;
-  __shared__ NearStage st[256];
-  __shared__ int s_n;
-  constexpr int PT = kGridTile / 256;
-  T acc[PT];
-  double acc64[PT];
-#pragma unroll
-  for (int q = 0; q < PT; q++) {
-    acc[q] = (T)0.;
-    acc64[q] = 0.;
-  }
-  const T* tf2 = shape_table<T>(sh, 1);
-  const T* tf3 = shape_table<T>(sh, 2);
-  for (int64_t c0 = clo; c0 < chi; c0 += 256) {
-    if (threadIdx.x == 0) s_n = 0;
-    __syncthreads();
-    const int64_t i = c0 + threadIdx.x;
-    if (i < chi) {
-      const int64_t slot = L.off_near + (i - L.near_lo);
-      if (w.n_ok[slot]) {
-        NearStage q;
-        q.zint = w.n_zint[slot];
-        q.zslope = w.n_zslope[slot];
-        const double* sv = w.n_str + 5 * slot;
-        // panel-local window, shifted to the global grid by the line's panel
-        const int32_t sh2 = grid == 0 ? 0 : (grid == 1 ? w.n_j2[slot] : w.n_j3[slot]);
-        const int64_t pofs = (int64_t)w.n_pconv[slot] * (grid == 0 ? 2400 : (grid == 1 ? 600 : 150));
-        q.pofs = pofs;
-        q.lo = w.n_jmin1[slot] - sh2 + pofs;
-        q.hi = w.n_jmax1[slot] - sh2 + pofs;
-        if (grid == 0) {
-          q.s0 = sv[0];
-          q.s1 = sv[3];
-          q.s2 = sv[4];
-        } else {
-          q.s0 = sv[grid];
-          q.s1 = q.s2 = 0.;
-        }
-        q.sppsp = w.n_sppsp[slot];
-        if (q.hi >= g0 && q.lo <= g1e) {
-          const int k = atomicAdd(&s_n, 1);
-          st[k] = q;
-        }
-      }
-    }
-    __syncthreads();
-    const int n = s_n;
-    if (grid == 0) {
-      // R1 (DV grid): F1 + FG + VERFN terms, whose negative VERFN part
-      // cancels the Doppler core in the wings -- evaluated in FP64 in every
-      // precision mode
-      for (int k = 0; k < n; k++) {
-        const NearStage& q = st[k];
-#pragma unroll
-        for (int qq = 0; qq < PT; qq++) {
-          const int64_t g = g0 + threadIdx.x + 256 * qq;
-          if (g > g1e || g < q.lo || g > q.hi) continue;
-          const double zf = (double(g - q.pofs - 1) - q.zint) * q.zslope;
-          long iz = fint(fabs(zf) + 1.5);
-          iz = iz > kNfmx ? kNfmx : iz;  // window limits keep iz <= 2501
-          double v = q.s0 * sh.f1[iz] + q.s1 * sh.fg[iz] + q.s2 * sh.xver[iz];
-          if (q.sppsp != 0.) v = v + v * (4. / 2000. * q.sppsp * zf);  // (:1322-1351)
-          acc64[qq] += v;
-        }
-      }
-    } else {
-      const T* tf = grid == 1 ? tf2 : tf3;
-      const double clc = grid == 1 ? 16. / 2000. : 64. / 2000.;
-      for (int k = 0; k < n; k++) {
-        const NearStage& q = st[k];
-        const T s0 = (T)q.s0;
-#pragma unroll
-        for (int qq = 0; qq < PT; qq++) {
-          const int64_t g = g0 + threadIdx.x + 256 * qq;
-          if (g > g1e || g < q.lo || g > q.hi) continue;
-          // table position from the FP64 offset to the line centre
-          const double zf = (double(g - q.pofs - 1) - q.zint * conf) * q.zslope;
-          long iz = fint(fabs(zf) + 1.5);
-          iz = iz > kNfmx ? kNfmx : iz;
-          T v = s0 * tf[iz];
-          if (q.sppsp != 0.) v = v + v * (T)(clc * q.sppsp * zf);  // (:1322-1351)
-          acc[qq] += v;
-        }
-      }
-    }
-    __syncthreads();
-  }
-  double* out = grid == 0 ? w.r1 + L.off_r1 : (grid == 1 ? w.r2 + L.off_r2 : w.r3 + L.off_r3);
-#pragma unroll
-  for (int qq = 0; qq < PT; qq++) {
-    const int64_t g = g0 + threadIdx.x + 256 * qq;
-    if (g <= g1e) out[g] = grid == 0 ? acc64[qq] : (double)acc[qq];
-  }
 }
 
 // =========================================================================
@@ -1358,30 +1216,6 @@ __device__ __forceinline__ double xint_at(double v1a, double v2a, double dva, co
   return -A[J - 1] * b1 + A[J] * (1. - C + b2) + A[J + 1] * (C + b1) - A[J + 2] * b2;
 }
 
-__global__ void k_combine_r3(Work w) {
-  const int l = blockIdx.y;
-  const LayerDev& L = w.L[l];
-  const int64_t g = 1 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g > L.n_r3) return;
-  // panel owning R3 point g: panel 0 covers 1..155, panel p>=1 covers
-  // 150p+6..150p+155 (N1R3/N2R3, src/oprop.f90:474-486)
-  int64_t p = (g <= 155) ? 0 : (g - 6) / 150;
-  if (p >= L.npanel) return;
-  const long I = (long)(g - 150 * p);
-  const long n1 = (p == 0) ? 1 : 6;
-  const double vft = w.vft[L.off_panel + p];
-  double add = 0.;
-  if (L.ilblf4 >= 1 && L.nwin > 0) {
-    const int wi = w.win_of[L.off_panel + p];
-    const WinDev& W = w.win[L.off_win + wi];
-    add += xint_at(W.v1r4, W.v2r4, L.dvr4, w.r4 + (L.off_win + wi) * kR4Stride, vft, L.dvr3, I,
-                   n1, 155);
-  }
-  if (L.icntnm >= 1)
-    add += xint_at(L.v1abs, L.v2abs, L.dvabs, w.absrb + L.off_abs, vft, L.dvr3, I, n1, 155);
-  w.r3[L.off_r3 + g] += add;
-}
-
 constexpr double X00 = -7. / 128., X01 = 105. / 128., X02 = 35. / 128., X03 = -5. / 128.,
                  X10 = -1. / 16., X11 = 9. / 16.;
 
@@ -1393,72 +1227,316 @@ __device__ __forceinline__ double interp4(const double* R, int64_t J, int r) {
   return X03 * R[J - 1] + X02 * R[J] + X01 * R[J + 1] + X00 * R[J + 2];
 }
 
-__global__ void k_combine_r2(Work w) {
-  const int l = blockIdx.y;
-  const LayerDev& L = w.L[l];
-  const int64_t g = 5 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g > L.n_r2 - 3) return;
-  const int64_t J3 = (g - 1) / 4 + 1;
-  const int r = (int)((g - 1) % 4);
-  w.r2[L.off_r2 + g] += interp4(w.r3 + L.off_r3, J3, r);
+// Global grid index ranges of one panel (panel p of layer L):
+//   R1 points whose OD the panel writes, the R2 points their 4-point
+//   interpolation reads, and the R3 points those R2 points read.
+struct PanelRange {
+  int64_t a1, b1, a2, b2, a3, b3;
+  long nhi;
+};
+
+__device__ __forceinline__ PanelRange panel_range(const LayerDev& L, int64_t p) {
+  PanelRange r;
+  r.nhi = (p == L.npanel - 1) ? (long)(L.npts - 2400 * (L.npanel - 1) + 32) : 2432;
+  r.a1 = 2400 * p + 33;
+  r.b1 = 2400 * p + r.nhi;
+  r.a2 = (r.a1 - 1) / 4;          // J2 - 1 of the first point
+  r.b2 = (r.b1 - 1) / 4 + 3;      // J2 + 2 of the last point
+  if (r.b2 > L.n_r2) r.b2 = L.n_r2;
+  // R2 points that receive R3 are 5 .. n_r2-3 (PANEL :1459-1480)
+  const int64_t c2 = r.a2 < 5 ? 5 : r.a2;
+  const int64_t d2 = r.b2 > L.n_r2 - 3 ? L.n_r2 - 3 : r.b2;
+  r.a3 = (c2 - 1) / 4;
+  if (r.a3 < 1) r.a3 = 1;
+  r.b3 = (d2 - 1) / 4 + 3;
+  if (r.b3 > L.n_r3) r.b3 = L.n_r3;
+  return r;
 }
 
-// One CTA per (layer, panel): radiation segments (RADFNI restarted each
-// panel) built by thread 0 in shared memory, then the panel's points.
-__global__ void __launch_bounds__(256) k_combine_od(Work w, const int32_t* panel_layer,
-                                                    const int64_t* panel_base) {
+// Candidate near-wing lines of every panel: TAPE3 lines whose centre lies
+// within the widest (R3) window reach of the panel's R3 span.
+__global__ void k_panel_ranges(Work w, DevLines ln, const int32_t* panel_layer,
+                               const int64_t* panel_base, int64_t npanel_total, int64_t* rng) {
+  const int64_t gp = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gp >= npanel_total) return;
+  const int l = panel_layer[gp];
+  const LayerDev& L = w.L[l];
+  const PanelRange R = panel_range(L, gp - panel_base[l]);
+  const double reach = 64. * L.alfmax + 32. * L.dv + fabs(L.rhorat) * 1.0;
+  rng[2 * gp] = lower_bound_d(ln.vnu, L.near_lo, L.near_hi,
+                              L.vft0 + double(R.a3 - 1) * L.dvr3 - reach);
+  rng[2 * gp + 1] = lower_bound_d(ln.vnu, L.near_lo, L.near_hi,
+                                  L.vft0 + double(R.b3 - 1) * L.dvr3 + reach);
+}
+
+// A staged near-wing line: its windows on the three grids (global points)
+// and the constants of CNVFNV's three sums (src/oprop.f90:1283-1351).
+struct PanelLine {
+  double zint, zslope, sppsp, s0, sg, sx, s2, s3;
+  int64_t lo1, hi1, lo2, hi2, lo3, hi3;
+  int32_t pc;  // convolution panel of the line
+};
+
+constexpr int kPanelThreads = 256;
+constexpr int kPanelStage = 128;  // lines staged per batch
+constexpr int kP1 = 10;           // R1 points per thread (2560 >= 2400)
+constexpr int kP2 = 3;            // R2 points per thread (768 >= 603)
+constexpr int kSegMax = kPanelSegMax;  // RADFNI segments kept per panel
+constexpr int kSegCap = 64;       // segments a CTA builds at a time when a panel has more
+
+// RADFNI segments of every panel (restarted each panel, src/oprop.f90:
+// 2297-2475), one thread per panel: [start point, value, slope] each; a
+// panel needing more than kSegMax keeps a count of -1 and builds its own.
+__global__ void k_panel_segs(Work w, const int32_t* panel_layer, const int64_t* panel_base,
+                             int64_t npanel_total, double* segs, int32_t* nseg) {
+  const int64_t gp = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gp >= npanel_total) return;
+  const int l = panel_layer[gp];
+  const LayerDev& L = w.L[l];
+  if (L.jrad != 0) return;
+  const int64_t p = gp - panel_base[l];
+  const long nhi = (p == L.npanel - 1) ? (long)(L.npts - 2400 * (L.npanel - 1) + 32) : 2432;
+  const double DV = L.dv;
+  const double vft = w.vft[L.off_panel + p];
+  double vitst = vft + double(33 - 1) * DV - DV, rdlast = -1.;
+  long n2 = 32;
+  int ns = 0;
+  double* out = segs + gp * (3 * kSegMax);
+  do {
+    const long n1 = n2 + 1;
+    const double vi = vft + double(n1 - 1) * DV;
+    double rdel;
+    const double rv = radfni(vi, DV, L.xkt, vitst, rdel, rdlast);
+    n2 = fint((vitst - vft) / DV + 0.001);
+    if (n2 > nhi) n2 = nhi;
+    if (ns == kSegMax) {
+      ns = -1;
+      break;
+    }
+    out[3 * ns] = double(n1);
+    out[3 * ns + 1] = rv;
+    out[3 * ns + 2] = rdel;
+    ns++;
+  } while (n2 < nhi);
+  nseg[gp] = ns;
+}
+
+// PANEL (src/oprop.f90:1371-1561) fused with the near-wing sums, one CTA
+// per panel: the panel's R1, R2 and R3 points are summed from its lines in
+// file order (each thread owns fixed points, held in shared memory), R3
+// gets the far wing and continuum by XINT (:515-519) and feeds R2 by
+// 4-point interpolation, and the optical depth R1 + interpolated R2, times
+// the radiation term, is written out.  The three grids never leave the SM.
+__global__ void __launch_bounds__(kPanelThreads, 4)
+    k_panel_od(Work w, DevLines ln, DevShapes sh, const int32_t* panel_layer,
+               const int64_t* panel_base, const int64_t* rng, const double* segs,
+               const int32_t* nseg) {
   const int64_t gp = blockIdx.x;
   const int l = panel_layer[gp];
   const LayerDev& L = w.L[l];
   const int64_t p = gp - panel_base[l];
-  const double DV = L.dv;
-  const double vft = w.vft[L.off_panel + p];
-  const long nhi = (p == L.npanel - 1) ? (long)(L.npts - 2400 * (L.npanel - 1) + 32) : 2432;
-  extern __shared__ double segbuf[];  // [start, radvi, rdel] * nseg
+  const PanelRange R = panel_range(L, p);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned full = 0xffffffffu;
+  __shared__ PanelLine st[kPanelStage];
+  __shared__ int s_wcnt[kPanelThreads / 32];
+  __shared__ double s1[kP1 * kPanelThreads];
+  __shared__ double s2[kP2 * kPanelThreads];
+  __shared__ double s3[kPanelThreads];
+  __shared__ double seg[3 * kSegCap];  // [start, radvi, rdel] per segment
   __shared__ int s_nseg;
-  const int maxseg = 2400;
-  if (L.jrad == 0) {
-    if (threadIdx.x == 0) {
-      const double v1p = vft + double(33 - 1) * DV;
-      double vi = v1p - DV, vitst = vi, rdlast = -1.;
-      long n1 = 32, n2 = 32;
-      int ns = 0;
-      do {
-        n1 = n2 + 1;
-        vi = vft + double(n1 - 1) * DV;
-        double rdel;
-        double rv = radfni(vi, DV, L.xkt, vitst, rdel, rdlast);
-        n2 = fint((vitst - vft) / DV + 0.001);
-        if (n2 > nhi) n2 = nhi;
-        if (ns < maxseg) {
-          segbuf[3 * ns] = double(n1);
-          segbuf[3 * ns + 1] = rv;
-          segbuf[3 * ns + 2] = rdel;
-          ns++;
+  __shared__ long s_n2;
+  // each thread owns local points tid + 256 q of every grid
+  const int n1p = (int)(R.b1 - R.a1 + 1), n2p = (int)(R.b2 - R.a2 + 1),
+            n3p = (int)(R.b3 - R.a3 + 1);
+  for (int i = tid; i < kP1 * kPanelThreads; i += kPanelThreads) s1[i] = 0.;
+  for (int i = tid; i < kP2 * kPanelThreads; i += kPanelThreads) s2[i] = 0.;
+  s3[tid] = 0.;
+  const int64_t clo = rng[2 * gp], chi = rng[2 * gp + 1];
+  for (int64_t c0 = clo; c0 < chi; c0 += kPanelStage) {
+    // stage the batch's accepted lines in file order
+    bool keep = false;
+    PanelLine q;
+    if (tid < kPanelStage && c0 + tid < chi) {
+      const int64_t slot = L.off_near + (c0 + tid - L.near_lo);
+      if (w.n_ok[slot]) {
+        const double* sv = w.n_str + 5 * slot;
+        const int64_t pc = w.n_pconv[slot];
+        const int64_t j1a = w.n_jmin1[slot], j1b = w.n_jmax1[slot];
+        const int64_t j2 = w.n_j2[slot], j3 = w.n_j3[slot];
+        q.zint = w.n_zint[slot];
+        q.zslope = w.n_zslope[slot];
+        q.sppsp = w.n_sppsp[slot];
+        q.s0 = sv[0];
+        q.s2 = sv[1];
+        q.s3 = sv[2];
+        q.sg = sv[3];
+        q.sx = sv[4];
+        q.pc = (int32_t)pc;
+        // panel-local windows shifted to the global grids by the line's panel
+        q.lo1 = j1a + 2400 * pc;
+        q.hi1 = j1b + 2400 * pc;
+        q.lo2 = j1a - j2 + 600 * pc;
+        q.hi2 = j1b - j2 + 600 * pc;
+        q.lo3 = j1a - j3 + 150 * pc;
+        q.hi3 = j1b - j3 + 150 * pc;
+        keep = (q.hi1 >= R.a1 && q.lo1 <= R.b1) || (q.hi2 >= R.a2 && q.lo2 <= R.b2) ||
+               (q.hi3 >= R.a3 && q.lo3 <= R.b3);
+      }
+    }
+    const unsigned bal = __ballot_sync(full, keep);
+    if (lane == 0) s_wcnt[warp] = __popc(bal);
+    __syncthreads();
+    int base = 0, n = 0;
+#pragma unroll
+    for (int k = 0; k < kPanelThreads / 32; k++) {
+      base += k < warp ? s_wcnt[k] : 0;
+      n += s_wcnt[k];
+    }
+    if (keep) st[base + __popc(bal & ((1u << lane) - 1u))] = q;
+    __syncthreads();
+    for (int k = 0; k < n; k++) {
+      const PanelLine& ql = st[k];
+      // R1 (DV grid): F1 + FG + VERFN terms
+      if (ql.hi1 >= R.a1 && ql.lo1 <= R.b1) {
+        const int lo = (int)((ql.lo1 > R.a1 ? ql.lo1 : R.a1) - R.a1);
+        const int hi = (int)((ql.hi1 < R.b1 ? ql.hi1 : R.b1) - R.a1);
+        const int off = (int)(R.a1 - 2400 * (int64_t)ql.pc - 1);  // g - pofs - 1 at i = 0
+        int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
+#pragma unroll 2
+        for (; i <= hi; i += kPanelThreads) {
+          const double zf = (double(off + i) - ql.zint) * ql.zslope;
+          int iz = (int)(fabs(zf) + 1.5);
+          iz = iz > kNfmx ? kNfmx : iz;
+          const double2 fab = *reinterpret_cast<const double2*>(sh.r1p + 4 * iz);
+          double v = ql.s0 * fab.x + ql.sg * fab.y + ql.sx * sh.r1p[4 * iz + 2];
+          if (ql.sppsp != 0.) v = v + v * (4. / 2000. * ql.sppsp * zf);  // (:1322-1351)
+          s1[i] += v;
         }
-      } while (n2 < nhi);
-      s_nseg = ns;
+      }
+      // R2 (4 DV): F2
+      if (ql.hi2 >= R.a2 && ql.lo2 <= R.b2) {
+        const int lo = (int)((ql.lo2 > R.a2 ? ql.lo2 : R.a2) - R.a2);
+        const int hi = (int)((ql.hi2 < R.b2 ? ql.hi2 : R.b2) - R.a2);
+        const int off = (int)(R.a2 - 600 * (int64_t)ql.pc - 1);
+        int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
+        for (; i <= hi; i += kPanelThreads) {
+          const double zf = (double(off + i) - ql.zint * L.conf2) * ql.zslope;
+          int iz = (int)(fabs(zf) + 1.5);
+          iz = iz > kNfmx ? kNfmx : iz;
+          double v = ql.s2 * sh.f2[iz];
+          if (ql.sppsp != 0.) v = v + v * (16. / 2000. * ql.sppsp * zf);
+          s2[i] += v;
+        }
+      }
+      // R3 (16 DV): F3
+      if (ql.hi3 >= R.a3 && ql.lo3 <= R.b3) {
+        const int lo = (int)((ql.lo3 > R.a3 ? ql.lo3 : R.a3) - R.a3);
+        const int hi = (int)((ql.hi3 < R.b3 ? ql.hi3 : R.b3) - R.a3);
+        if (tid >= lo && tid <= hi) {
+          const int off = (int)(R.a3 - 150 * (int64_t)ql.pc - 1);
+          const double zf = (double(off + tid) - ql.zint * L.conf3) * ql.zslope;
+          int iz = (int)(fabs(zf) + 1.5);
+          iz = iz > kNfmx ? kNfmx : iz;
+          double v = ql.s3 * sh.f3[iz];
+          if (ql.sppsp != 0.) v = v + v * (64. / 2000. * ql.sppsp * zf);
+          s3[tid] += v;
+        }
+      }
     }
     __syncthreads();
   }
-  const double* r1 = w.r1 + L.off_r1;
-  const double* r2 = w.r2 + L.off_r2;
-  for (long I = 33 + threadIdx.x; I <= nhi; I += blockDim.x) {
-    const int64_t g = 2400 * p + I;
-    const int64_t J2 = (g - 1) / 4 + 1;
-    const int r = (int)((g - 1) % 4);
-    double od = r1[g] + interp4(r2, J2, r);
-    if (L.jrad == 0) {
-      int lo = 0, hi = s_nseg - 1;
+  // R3 += XINT(R4 of the owning panel's window) + XINT(ABSRB): R3 point g
+  // belongs to panel 0 for g <= 155, else to panel (g-6)/150 (N1R3/N2R3,
+  // src/oprop.f90:474-486)
+  if (tid < n3p) {
+    const int64_t g = R.a3 + tid;
+    const int64_t po = (g <= 155) ? 0 : (g - 6) / 150;
+    if (po < L.npanel) {
+      const long I = (long)(g - 150 * po);
+      const long n1 = (po == 0) ? 1 : 6;
+      const double vft = w.vft[L.off_panel + po];
+      double add = 0.;
+      if (L.ilblf4 >= 1 && L.nwin > 0) {
+        const int wi = w.win_of[L.off_panel + po];
+        const WinDev& W = w.win[L.off_win + wi];
+        add += xint_at(W.v1r4, W.v2r4, L.dvr4, w.r4 + (L.off_win + wi) * kR4Stride, vft, L.dvr3,
+                       I, n1, 155);
+      }
+      if (L.icntnm >= 1)
+        add += xint_at(L.v1abs, L.v2abs, L.dvabs, w.absrb + L.off_abs, vft, L.dvr3, I, n1, 155);
+      s3[tid] += add;
+    }
+  }
+  __syncthreads();
+  // R2 += 4-point interpolation of R3 (PANEL :1459-1480)
+  for (int i = tid; i < n2p; i += kPanelThreads) {
+    const int64_t g = R.a2 + i;
+    if (g >= 5 && g <= L.n_r2 - 3) s2[i] += interp4(s3 - R.a3, (g - 1) / 4 + 1, (int)((g - 1) % 4));
+  }
+  __syncthreads();
+  // OD = R1 + 4-point interpolation of R2 (PANEL :1482-1519), times the
+  // radiation term, piecewise linear over the panel's RADFNI segments
+  double* od_out = w.od + L.off_od;
+  const double* r2 = s2 - R.a2;
+  if (L.jrad != 0) {
+    for (int i = tid; i < n1p; i += kPanelThreads) {
+      const int64_t g = R.a1 + i;
+      od_out[g - 33] = s1[i] + interp4(r2, (g - 1) / 4 + 1, (int)((g - 1) % 4));
+    }
+    return;
+  }
+  const int nsg = nseg[gp];
+  const double* sgp = segs + gp * (3 * kSegMax);
+  // thread 0's RADFNI state when the panel builds its own segments
+  double vitst = 0., rdlast = -1.;
+  long n2 = 32;
+  const double DV = L.dv;
+  const double vft = w.vft[L.off_panel + p];
+  if (tid == 0) vitst = vft + double(33 - 1) * DV - DV;
+  for (;;) {
+    if (nsg >= 0) {
+      for (int k = tid; k < 3 * nsg; k += kPanelThreads) seg[k] = sgp[k];
+      if (tid == 0) {
+        s_nseg = nsg;
+        s_n2 = R.nhi;
+      }
+    } else if (tid == 0) {
+      int ns = 0;
+      do {
+        const long n1 = n2 + 1;
+        const double vi = vft + double(n1 - 1) * DV;
+        double rdel;
+        const double rv = radfni(vi, DV, L.xkt, vitst, rdel, rdlast);
+        n2 = fint((vitst - vft) / DV + 0.001);
+        if (n2 > R.nhi) n2 = R.nhi;
+        seg[3 * ns] = double(n1);
+        seg[3 * ns + 1] = rv;
+        seg[3 * ns + 2] = rdel;
+        ns++;
+      } while (n2 < R.nhi && ns < kSegCap);
+      s_nseg = ns;
+      s_n2 = n2;
+    }
+    __syncthreads();
+    const int ns = s_nseg;
+    const long ilo = (long)seg[0], ihi = s_n2;
+    for (int i = tid; i < n1p; i += kPanelThreads) {
+      const int64_t g = R.a1 + i;
+      const long I = (long)(g - 2400 * p);
+      if (I < ilo || I > ihi) continue;
+      double od = s1[i] + interp4(r2, (g - 1) / 4 + 1, (int)((g - 1) % 4));
+      int lo = 0, hi = ns - 1;
       while (lo < hi) {
-        int m = (lo + hi + 1) >> 1;
-        if (segbuf[3 * m] <= double(I)) lo = m;
+        const int m = (lo + hi + 1) >> 1;
+        if (seg[3 * m] <= double(I)) lo = m;
         else hi = m - 1;
       }
-      const double rad = segbuf[3 * lo + 1] + double(I - (long)segbuf[3 * lo]) * segbuf[3 * lo + 2];
-      od = od * rad;
+      od = od * (seg[3 * lo + 1] + double(I - (long)seg[3 * lo]) * seg[3 * lo + 2]);
+      od_out[g - 33] = od;
     }
-    w.od[L.off_od + (g - 33)] = od;
+    if (ihi >= R.nhi) break;
+    __syncthreads();  // the next batch overwrites the segments
   }
 }
 
@@ -1560,11 +1638,11 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
 }  // namespace
 
 void init_kernel_attributes() {
-  cudaFuncSetAttribute(k_combine_od, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       3 * 2400 * (int)sizeof(double));
   // two R4 buffers per CTA; the largest carveout lets several CTAs share an SM
   cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
   cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
+  cudaFuncSetAttribute(k_panel_od, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
                        cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1621,32 +1699,17 @@ cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, do
   return cudaGetLastError();
 }
 
-cudaError_t launch_grids(const Work& w, const DevLines& ln, const DevShapes& sh,
-                         const int64_t* tile_prefix, int64_t ntiles, int precision,
-                         cudaStream_t s) {
-  // The near-wing sums stay FP64 in every mode: the reference decomposition
-  // cancels in them (negative VERFN term; negative lobes of the 4-point
-  // PANEL interpolation where a line's R2/R3 window ends), which FP32 cannot
-  // resolve at a 1e-4 relative bar where the optical depth is small.
-  (void)precision;
-  if (ntiles <= 0) return cudaSuccess;
-  k_grids<double><<<(unsigned)ntiles, 256, 0, s>>>(w, ln, sh, tile_prefix, 3 * w.nlay);
-  return cudaGetLastError();
-}
 
-cudaError_t launch_combine(const Work& w, int64_t max_r3, int64_t max_r2, int64_t npanel_total,
-                           const int32_t* panel_layer, const int64_t* panel_base,
-                           cudaStream_t s) {
-  if (max_r3 > 0) {
-    dim3 g3((unsigned)((max_r3 + 255) / 256), (unsigned)w.nlay);
-    k_combine_r3<<<g3, 256, 0, s>>>(w);
-  }
-  if (max_r2 > 0) {
-    dim3 g2((unsigned)((max_r2 + 255) / 256), (unsigned)w.nlay);
-    k_combine_r2<<<g2, 256, 0, s>>>(w);
-  }
-  k_combine_od<<<(unsigned)npanel_total, 256, 3 * 2400 * sizeof(double), s>>>(w, panel_layer,
-                                                                             panel_base);
+cudaError_t launch_panels(const Work& w, const DevLines& ln, const DevShapes& sh,
+                          int64_t npanel_total, const int32_t* panel_layer,
+                          const int64_t* panel_base, int64_t* rng, double* segs,
+                          int32_t* nseg, cudaStream_t s) {
+  if (npanel_total <= 0) return cudaSuccess;
+  const unsigned nb = (unsigned)((npanel_total + 127) / 128);
+  k_panel_ranges<<<nb, 128, 0, s>>>(w, ln, panel_layer, panel_base, npanel_total, rng);
+  k_panel_segs<<<nb, 128, 0, s>>>(w, panel_layer, panel_base, npanel_total, segs, nseg);
+  k_panel_od<<<(unsigned)npanel_total, kPanelThreads, 0, s>>>(w, ln, sh, panel_layer, panel_base,
+                                                              rng, segs, nseg);
   return cudaGetLastError();
 }
 

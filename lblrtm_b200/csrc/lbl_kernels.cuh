@@ -22,7 +22,7 @@ struct DevLines {
 // Line-shape tables, 1-based, kNfmx+1 entries each (device pointers).
 struct DevShapes {
   const double *f1, *f2, *f3, *fg, *xver;
-  const float *f1s, *f2s, *f3s, *fgs, *xvers;
+  const double* r1p;  // F1, FG, XVER, 0 per table index (one 32-byte record)
 };
 
 // Continuum coefficient table (device pointers).
@@ -84,12 +84,11 @@ cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* wi
 cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
-cudaError_t launch_grids(const Work& w, const DevLines& ln, const DevShapes& sh,
-                         const int64_t* tile_prefix, int64_t ntiles, int precision,
-                         cudaStream_t s);
-cudaError_t launch_combine(const Work& w, int64_t max_r3, int64_t max_r2, int64_t npanel_total,
-                           const int32_t* panel_layer, const int64_t* panel_base,
-                           cudaStream_t s);
+cudaError_t launch_panels(const Work& w, const DevLines& ln, const DevShapes& sh,
+                          int64_t npanel_total, const int32_t* panel_layer,
+                          const int64_t* panel_base, int64_t* rng, double* segs,
+                          int32_t* nseg, cudaStream_t s);
+constexpr int kPanelSegMax = 48;  // RADFNI segments kept per panel (3 doubles each)
 // One merge step (EMINIT when first) for the layer whose LayerDev is Ld.
 cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const double* od,
                          int64_t npts, int first, double dv_old, int64_t n_old,
