@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -81,6 +82,10 @@ struct lbl_ctx {
   DevLines dl{};
   void* line_mem = nullptr;
   size_t line_cap = 0;  // bytes of line_mem (grow-only)
+  // pinned copies of the device status and work counters, read after the
+  // caller's final synchronisation
+  int32_t* h_stat = nullptr;
+  unsigned long long* h_cnt = nullptr;
   bool have_lines = false;
   // tables
   DevShapes sh{};
@@ -196,6 +201,7 @@ struct Batch {
 // Plan layers [0,n), lay their buffers out in the arena, upload the plans.
 int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n, int jrad_in,
                   int* jrad_out, Batch& B) {
+  const auto t_host = std::chrono::steady_clock::now();
   HostLines H{ctx->h_vnu.data(), ctx->h_sp.data(), ctx->h_pshift.data(), ctx->h_mol.data(),
               ctx->h_iflg.data(), (int64_t)ctx->h_vnu.size(), ctx->h_bs.data(),
               (int64_t)ctx->h_bs.size() - 1, ctx->max_abs_pshift};
@@ -408,6 +414,10 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   CK(cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), s));
   // the host vectors must live until the copies finish
   CK(cudaStreamSynchronize(s));
+  if (ctx->prof)
+    ctx->stage("host_plan").ms +=
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host)
+            .count();
   return LBL_OK;
 }
 
@@ -442,17 +452,22 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     CK(launch_panels(w, ctx->dl, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
                      B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
   }
-  int32_t st[4] = {0, 0, 0, 0};
-  unsigned long long cnt[8];
-  CK(cudaMemcpyAsync(st, w.status, sizeof(st), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(cnt, w.counters, sizeof(cnt), cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
-  ctx->stage("far_wing").work += (double)cnt[0];
-  ctx->stage("panels").work += (double)cnt[1];
-  if (st[0] == 2)
+  CK(cudaMemcpyAsync(ctx->h_stat, w.status, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ctx->h_cnt, w.counters, 8 * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, s));
+  return LBL_OK;
+}
+
+// After the stream has been synchronised: the device status of the last
+// run_od and its work counters.
+int finish_od(lbl_ctx* ctx) {
+  ctx->stage("far_wing").work += (double)ctx->h_cnt[0];
+  ctx->stage("panels").work += (double)ctx->h_cnt[1];
+  const int32_t st = ctx->h_stat[0];
+  if (st == 2)
     return fail(ctx, LBL_E_RANGE,
                 "far-wing line file too sparse: a LINF4 segment spans more than 48 TAPE3 panels");
-  if (st[0] != 0) return fail(ctx, LBL_E_CUDA, "device status " + std::to_string(st[0]));
+  if (st != 0) return fail(ctx, LBL_E_CUDA, "device status " + std::to_string(st));
   return LBL_OK;
 }
 
@@ -541,6 +556,14 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
   }
   upload_voicon();
   init_kernel_attributes();
+  void* hs = nullptr;
+  if (cudaMallocHost(&hs, 64 + 8 * sizeof(unsigned long long)) != cudaSuccess) {
+    delete ctx;
+    return LBL_E_NOMEM;
+  }
+  std::memset(hs, 0, 64 + 8 * sizeof(unsigned long long));
+  ctx->h_stat = static_cast<int32_t*>(hs);
+  ctx->h_cnt = reinterpret_cast<unsigned long long*>(static_cast<char*>(hs) + 64);
   ShapeTables* t = new ShapeTables;
   build_shape_tables(t);
   const size_t nd = kNfmx + 1;
@@ -576,6 +599,7 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
 int lbl_ctx_destroy(lbl_ctx* ctx) {
   if (!ctx) return LBL_E_ARG;
   cudaSetDevice(ctx->device);
+  if (ctx->h_stat) cudaFreeHost(ctx->h_stat);
   if (ctx->line_mem) cudaFree(ctx->line_mem);
   if (ctx->shape_mem) cudaFree(ctx->shape_mem);
   if (ctx->ck_mem) cudaFree(ctx->ck_mem);
@@ -731,6 +755,8 @@ int lbl_layer_od(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, int32
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   harvest(ctx);
+  rc = finish_od(ctx);
+  if (rc) return rc;
   *jrad = jout;
   return LBL_OK;
 }
@@ -807,7 +833,7 @@ int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nla
   }
   CK(cudaStreamSynchronize(ctx->stream));
   harvest(ctx);
-  return LBL_OK;
+  return finish_od(ctx);
 }
 
 int lbl_forward_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, const int32_t* nlay,
