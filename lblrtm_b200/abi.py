@@ -87,6 +87,14 @@ def make_run(**kw):
     return r
 
 
+def make_layers_like(layers):
+    """A new lbl_layer array holding a copy of layers."""
+    n = len(layers)
+    arr = (Layer * n)()
+    C.memmove(arr, layers, C.sizeof(Layer) * n)
+    return arr
+
+
 def make_layers(profile):
     """Array of lbl_layer from a profile dict of numpy arrays."""
     n = len(profile["pave"])

@@ -92,6 +92,9 @@ struct lbl_ctx {
   void* shape_mem = nullptr;
   DevMtckd ck{};
   void* ck_mem = nullptr;
+  // Jacobian work space (grow-only)
+  char* jac_mem = nullptr;
+  size_t jac_cap = 0;
   bool have_ck = false;
   Arena arena;
   // merge buffers (ping-pong)
@@ -600,6 +603,7 @@ int lbl_ctx_destroy(lbl_ctx* ctx) {
   if (!ctx) return LBL_E_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->h_stat) cudaFreeHost(ctx->h_stat);
+  if (ctx->jac_mem) cudaFree(ctx->jac_mem);
   if (ctx->line_mem) cudaFree(ctx->line_mem);
   if (ctx->shape_mem) cudaFree(ctx->shape_mem);
   if (ctx->ck_mem) cudaFree(ctx->ck_mem);
@@ -866,9 +870,153 @@ int lbl_forward_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, const
 int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nlay,
                  const int32_t* mols, int32_t nq, double* rad, double* jac, int64_t npts,
                  int32_t precision) {
-  (void)run; (void)layers; (void)nlay; (void)mols; (void)nq; (void)rad; (void)jac; (void)npts;
-  (void)precision;
-  return fail(ctx, LBL_E_ARG, "lbl_jacobian: not available in this build");
+  if (!ctx) return LBL_E_ARG;
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  if (!layers || nlay < 1 || !jac || nq < 0 || nq >= kJacMaxParams || (nq > 0 && !mols))
+    return fail(ctx, LBL_E_ARG, "lbl_jacobian: bad argument");
+  if (run->iemit != 1 || run->ipathl != 1)
+    return fail(ctx, LBL_E_ARG, "lbl_jacobian: upwelling radiance only (IEMIT=1, IPATHL=1)");
+  for (int k = 0; k < nq; k++)
+    if (mols[k] < 1 || mols[k] > LBL_WKDIM)
+      return fail(ctx, LBL_E_ARG, "lbl_jacobian: molecule number out of range");
+  cudaSetDevice(ctx->device);
+  std::string e;
+  rc = dv_rule(*run, layers, nlay, &e);
+  if (rc) return fail(ctx, rc, e);
+  if (layer_npts(*run, layers[nlay - 1].dv) != npts)
+    return fail(ctx, LBL_E_ARG, "npts does not match the last layer's grid");
+  const int np = 1 + nq;
+  // layer grids: optical depths are stored layer after layer
+  std::vector<int64_t> nl(nlay), off(nlay + 1, 0);
+  for (int l = 0; l < nlay; l++) {
+    nl[l] = layer_npts(*run, layers[l].dv);
+    off[l + 1] = off[l] + nl[l];
+  }
+  const int64_t ntot = off[nlay];
+  // layers a..nlay-1 share the top grid; rows of lower layers are carried
+  // through each merge step up to a
+  int a = 0;
+  for (int l = 1; l < nlay; l++)
+    if (layers[l].dv != layers[l - 1].dv) a = l;
+  // work space: dtau per parameter, the minus pass, output rows, two
+  // buffers of carried rows, two (R, T) pairs, layer offsets
+  const size_t n_dtau = (size_t)np * ntot, n_rows = (size_t)np * nlay * npts,
+               n_low = (size_t)np * std::max(a, 1) * npts;
+  const size_t need = 8 * (n_dtau + ntot + n_rows + 2 * n_low + 4 * (size_t)npts + nlay) + 8 * 256;
+  if (need > ctx->jac_cap) {
+    if (ctx->jac_mem) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      cudaFree(ctx->jac_mem);
+    }
+    ctx->jac_mem = nullptr;
+    ctx->jac_cap = 0;
+    char* m = nullptr;
+    if (cudaMalloc(&m, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, LBL_E_NOMEM, "lbl_jacobian: work space");
+    }
+    ctx->jac_mem = m;
+    ctx->jac_cap = need;
+  }
+  size_t used = 0;
+  auto take = [&](size_t n) {
+    used = (used + 255) & ~size_t(255);
+    double* p = reinterpret_cast<double*>(ctx->jac_mem + used);
+    used += n * 8;
+    return p;
+  };
+  double* dtau = take(n_dtau);
+  double* tmp = take(ntot);
+  double* rows = take(n_rows);
+  double* low[2] = {take(n_low), take(n_low)};
+  double* rt[4] = {take(npts), take(npts), take(npts), take(npts)};
+  int64_t* d_off = reinterpret_cast<int64_t*>(take(nlay));
+  cudaStream_t s = ctx->stream;
+  // dtau/dp of every layer by central differences of whole-profile optical
+  // depths: each layer's depth depends only on its own parameters
+  const double dT = 0.1, dq = 0.01;
+  std::vector<lbl_layer> Lp(layers, layers + nlay), Lm(layers, layers + nlay);
+  for (int k = 0; k < np; k++) {
+    double h;
+    for (int l = 0; l < nlay; l++) {
+      Lp[l] = layers[l];
+      Lm[l] = layers[l];
+      if (k == 0) {
+        Lp[l].tave += dT;
+        Lm[l].tave -= dT;
+      } else {
+        Lp[l].wk[mols[k - 1] - 1] *= 1. + dq;
+        Lm[l].wk[mols[k - 1] - 1] *= 1. - dq;
+      }
+    }
+    h = k == 0 ? 2. * dT : std::log(1. + dq) - std::log(1. - dq);
+    for (int side = 0; side < 2; side++) {
+      Batch Bs;
+      rc = prepare_batch(ctx, *run, side ? Lm.data() : Lp.data(), nlay, run->jrad, nullptr, Bs);
+      if (rc) return rc;
+      rc = run_od(ctx, *run, Bs, precision);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(side ? tmp : dtau + (size_t)k * ntot, Bs.w.od, 8 * ntot,
+                         cudaMemcpyDeviceToDevice, s));
+      CK(cudaStreamSynchronize(s));
+      rc = finish_od(ctx);
+      if (rc) return rc;
+    }
+    CK(launch_jac_diff(dtau + (size_t)k * ntot, tmp, ntot, 1. / h, s));
+  }
+  // nominal optical depths, kept in the batch for the merge
+  Batch B;
+  rc = prepare_batch(ctx, *run, layers, nlay, run->jrad, nullptr, B);
+  if (rc) return rc;
+  rc = run_od(ctx, *run, B, precision);
+  if (rc) return rc;
+  std::vector<int64_t> hoff(nlay);
+  for (int l = 0; l < nlay; l++) hoff[l] = B.ld[l].off_od;
+  CK(cudaMemcpyAsync(d_off, hoff.data(), 8 * nlay, cudaMemcpyHostToDevice, s));
+  {
+    StageTimer t(ctx, "jacobian", 0);
+    int cur = 0, lc = 0;
+    double dv_old = 0.;
+    int64_t n_old = 0;
+    for (int l = 0; l < nlay; l++) {
+      const LayerDev& d = B.ld[l];
+      if (l > 0 && d.dv > dv_old) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
+      // carry the rows of layers below l onto layer l's grid
+      if (l > 0 && l <= a) {
+        for (int k = 0; k < np; k++)
+          CK(launch_jac_prop(B.d_ld + l, B.w.od + d.off_od, d.npts, dv_old, n_old,
+                             low[lc] + (size_t)k * a * npts, low[lc ^ 1] + (size_t)k * a * npts,
+                             npts, l, s));
+        lc ^= 1;
+      }
+      double* dp[kJacMaxParams];
+      const double* tp[kJacMaxParams];
+      for (int k = 0; k < np; k++) {
+        dp[k] = (l < a) ? low[lc] + ((size_t)k * a + l) * npts
+                        : rows + ((size_t)k * nlay + l) * npts;
+        tp[k] = dtau + (size_t)k * ntot + off[l];
+      }
+      const int nxt = cur ^ 2;
+      const double tbnd = (l == 0) ? run->tmpbnd : 0.;
+      CK(launch_jac_layer(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
+                          dv_old, n_old, rt[cur], rt[cur + 1], rt[nxt], rt[nxt + 1], tbnd,
+                          run->bndemi, layers[l].tzu, dp, tp, np, s));
+      cur = nxt;
+      dv_old = d.dv;
+      n_old = d.npts;
+    }
+    CK(launch_jac_top(B.w.od, d_off, nlay, a, np, npts, rows, low[lc], s));
+    if (rad) {
+      rc = copy_out(ctx, rad, rt[cur], sizeof(double) * npts);
+      if (rc) return rc;
+    }
+  }
+  rc = copy_out(ctx, jac, rows, sizeof(double) * n_rows);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s));
+  harvest(ctx);
+  return finish_od(ctx);
 }
 
 int lbl_profile(lbl_ctx* ctx, int32_t enable) {

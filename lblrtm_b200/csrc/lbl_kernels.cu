@@ -1635,6 +1635,171 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
   tr_out[f] = (double)tr * to;
 }
 
+// =========================================================================
+// Radiance Jacobians (the reference's analytic-Jacobian path, EMDT/EMADMG
+// src/xmerge.f90:4406-5782 with TDERIVup/QDERIVup :5786-6144): the forward
+// merge of one layer together with the derivative of that layer's merged
+// radiance with respect to each parameter p,
+//   d_p = dR/dtau * dtau/dp  +  [p = T] dE/dB * dB/dT
+// where dtau/dp comes from optical depths at perturbed parameters (the
+// reference's own layer-derivative route) and the rest is differentiated
+// by hand.  All FP64.
+// =========================================================================
+constexpr int kJacMaxPar = 8;
+
+// dB/dT of PLANCK (src/xmerge.f90:968-1017) at temperature t, both branches
+__device__ __forceinline__ double planck_dt(double vi, double t) {
+  if (!(t > 0.)) return 0.;
+  const double xkt = t / kRADCN2;
+  const double x = vi / xkt;
+  if (x < 1e-2) return kRADCN1 * (vi * vi) / kRADCN2 * (1. + x) / ((1. + 0.5 * x) * (1. + 0.5 * x));
+  if (x > 80.) return 0.;
+  const double e = exp(-x);
+  return kRADCN1 * (vi * vi * vi) * e / (1. - e) * (x / t) / (1. - e);
+}
+
+struct JacRows {
+  double* d[kJacMaxPar];        // per parameter: this layer's row
+  const double* dtau[kJacMaxPar];  // per parameter: dtau/dp of this layer
+  int np;
+};
+
+__global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const double* od,
+                            int first, double dv_old, int64_t n_old, const double* rad_in,
+                            const double* tr_in, double* rad_out, double* tr_out, double tbnd,
+                            double emis, double tzu, JacRows rows) {
+  const LayerDev& L = *Lp;
+  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= L.npts) return;
+  const double DV = L.dv;
+  const int64_t p = f / 2400;
+  const double vi = (vft_panel[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
+  const double xkt = L.tave / kRADCN2;
+  const double xkta = tzu / kRADCN2;
+  const double tau = od[f];
+  const bool clamped = tau < -kODLO;
+  const double o = clamped ? -kODLO : tau;
+  const double tr = exp(-o);
+  double fi, dfi;
+  if (o <= kODLO) {
+    fi = o / 6.;
+    dfi = 1. / 6.;
+  } else {
+    fi = 1. - 2. * (tr / (tr - 1.) + 1. / o);
+    dfi = -2. * (tr / ((tr - 1.) * (tr - 1.)) - 1. / (o * o));
+  }
+  const double bb = planck(vi, xkt);
+  const double bbd = (xkta > 0.) ? planck(vi, xkta) - bb : 0.;
+  const double em = (1. - tr) * (bb + bbd * fi);
+  const double dem_do = tr * (bb + bbd * fi) + (1. - tr) * bbd * dfi;
+  const double dem_db = (1. - tr) * (xkta > 0. ? 1. - fi : 1.);
+  double rad, trn, dr_do;
+  if (first) {
+    const double bs = tbnd > 0. ? planck(vi, tbnd / kRADCN2) * emis : 0.;
+    rad = em + tr * bs;
+    trn = tr;
+    dr_do = dem_do - tr * bs;
+  } else {
+    const long itype = (dv_old == DV) ? 0 : fint(DV / (dv_old - DV) + 0.5);
+    double ro, to;
+    auto R = [&](int64_t c) { return rad_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+    auto TR = [&](int64_t c) { return tr_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+    const int64_t LL = itype + 1;
+    const int64_t q = f / LL, r = f % LL;
+    if (itype == 0) {
+      ro = R(f);
+      to = TR(f);
+    } else if (r == 0) {
+      ro = R(q * itype);
+      to = TR(q * itype);
+    } else {
+      const int64_t ipl = q * itype + r - 1;
+      const double P = 1.0 - double(r) / double(LL);
+      const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
+      const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
+      ro = a1 * R(ipl - 1) + a2 * R(ipl) + a3 * R(ipl + 1) + a4 * R(ipl + 2);
+      to = a1 * TR(ipl - 1) + a2 * TR(ipl) + a3 * TR(ipl + 1) + a4 * TR(ipl + 2);
+    }
+    rad = tr * ro + em;
+    trn = tr * to;
+    dr_do = -tr * ro + dem_do;
+  }
+  rad_out[f] = rad;
+  tr_out[f] = trn;
+  const double dbt = dem_db * planck_dt(vi, L.tave);
+  for (int k = 0; k < rows.np; k++) {
+    double d = clamped ? 0. : dr_do * rows.dtau[k][f];
+    if (k == 0) d += dbt;
+    rows.d[k][f] = d;
+  }
+}
+
+// Rows of lower layers carried through merge step k: row <- T_k * regrid(row)
+// (RADNN's interpolation onto layer k's grid, then layer k's transmittance).
+// Row r of the input lives at in + r*stride on grid k-1, output likewise on
+// grid k.
+__global__ void k_jac_prop(const LayerDev* Lp, const double* od, double dv_old, int64_t n_old,
+                           const double* in, double* out, int64_t stride) {
+  const LayerDev& L = *Lp;
+  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= L.npts) return;
+  const double* x = in + (int64_t)blockIdx.y * stride;
+  const double DV = L.dv;
+  double tau = od[f];
+  if (tau < -kODLO) tau = -kODLO;
+  const double tr = exp(-tau);
+  const long itype = (dv_old == DV) ? 0 : fint(DV / (dv_old - DV) + 0.5);
+  auto X = [&](int64_t c) { return x[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+  double v;
+  const int64_t LL = itype + 1;
+  const int64_t q = f / LL, r = f % LL;
+  if (itype == 0) {
+    v = X(f);
+  } else if (r == 0) {
+    v = X(q * itype);
+  } else {
+    const int64_t ipl = q * itype + r - 1;
+    const double P = 1.0 - double(r) / double(LL);
+    const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
+    const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
+    v = a1 * X(ipl - 1) + a2 * X(ipl) + a3 * X(ipl + 1) + a4 * X(ipl + 2);
+  }
+  out[(int64_t)blockIdx.y * stride + f] = tr * v;
+}
+
+// Top segment of layers a..L-1 sharing the top grid: each layer's row is
+// carried to the top by the transmittance of the layers above it,
+// accumulated downward point by point; rows of layers below a (already on
+// the top grid, through layer a) take the product above layer a.
+//   rows[(k*nlay + l)*n + i]  (in: d_p of layer l >= a, out: Jacobian row)
+//   low[(k*a + j)*n + i]      (rows j < a carried through layer a)
+__global__ void k_jac_top(const double* od, const int64_t* od_off, int nlay, int a, int np,
+                          int64_t n, double* rows, const double* low) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double c = 1.;
+  for (int m = nlay - 1; m >= a; m--) {
+    for (int k = 0; k < np; k++) {
+      double* r = rows + ((int64_t)k * nlay + m) * n + i;
+      *r = *r * c;
+    }
+    if (m == a) {
+      for (int k = 0; k < np; k++)
+        for (int j = 0; j < a; j++)
+          rows[((int64_t)k * nlay + j) * n + i] = low[((int64_t)k * a + j) * n + i] * c;
+    }
+    double tau = od[od_off[m] + i];
+    if (tau < -kODLO) tau = -kODLO;
+    c *= exp(-tau);
+  }
+}
+
+// (tau(p+) - tau(p-)) / h, in place into plus
+__global__ void k_jac_diff(double* plus, const double* minus, int64_t n, double rh) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) plus[i] = (plus[i] - minus[i]) * rh;
+}
+
 }  // namespace
 
 void init_kernel_attributes() {
@@ -1725,6 +1890,51 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
   else
     k_merge<double><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
                                        rad_out, tr_out, tbnd, emis, iemit, tzu);
+  return cudaGetLastError();
+}
+
+}  // namespace lbl
+
+namespace lbl {
+
+cudaError_t launch_jac_layer(const LayerDev* Ld, const double* vft_panel, const double* od,
+                             int64_t npts, int first, double dv_old, int64_t n_old,
+                             const double* rad_in, const double* tr_in, double* rad_out,
+                             double* tr_out, double tbnd, double emis, double tzu,
+                             double* const* d, const double* const* dtau, int np,
+                             cudaStream_t s) {
+  if (np < 1 || np > kJacMaxPar) return cudaErrorInvalidValue;
+  JacRows rows;
+  rows.np = np;
+  for (int k = 0; k < kJacMaxPar; k++) {
+    rows.d[k] = k < np ? d[k] : nullptr;
+    rows.dtau[k] = k < np ? dtau[k] : nullptr;
+  }
+  k_jac_layer<<<(unsigned)((npts + 255) / 256), 256, 0, s>>>(
+      Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in, rad_out, tr_out, tbnd, emis, tzu,
+      rows);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_jac_prop(const LayerDev* Ld, const double* od, int64_t npts, double dv_old,
+                            int64_t n_old, const double* in, double* out, int64_t stride,
+                            int nrows, cudaStream_t s) {
+  if (nrows <= 0) return cudaSuccess;
+  dim3 g((unsigned)((npts + 255) / 256), (unsigned)nrows);
+  k_jac_prop<<<g, 256, 0, s>>>(Ld, od, dv_old, n_old, in, out, stride);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_jac_top(const double* od, const int64_t* od_off, int nlay, int a, int np,
+                           int64_t n, double* rows, const double* low, cudaStream_t s) {
+  k_jac_top<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(od, od_off, nlay, a, np, n, rows, low);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_jac_diff(double* plus, const double* minus, int64_t n, double rh,
+                            cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_jac_diff<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(plus, minus, n, rh);
   return cudaGetLastError();
 }
 

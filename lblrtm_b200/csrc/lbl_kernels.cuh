@@ -95,6 +95,24 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
                          cudaStream_t s, int precision = LBL_PREC_FP64);
+// Radiance Jacobians: one layer's forward merge plus its derivative rows,
+// the carrying of lower layers' rows through one merge step, the top
+// segment's transmittance products, and a central difference.
+cudaError_t launch_jac_layer(const LayerDev* Ld, const double* vft_panel, const double* od,
+                             int64_t npts, int first, double dv_old, int64_t n_old,
+                             const double* rad_in, const double* tr_in, double* rad_out,
+                             double* tr_out, double tbnd, double emis, double tzu,
+                             double* const* d, const double* const* dtau, int np,
+                             cudaStream_t s);
+cudaError_t launch_jac_prop(const LayerDev* Ld, const double* od, int64_t npts, double dv_old,
+                            int64_t n_old, const double* in, double* out, int64_t stride,
+                            int nrows, cudaStream_t s);
+cudaError_t launch_jac_top(const double* od, const int64_t* od_off, int nlay, int a, int np,
+                           int64_t n, double* rows, const double* low, cudaStream_t s);
+cudaError_t launch_jac_diff(double* plus, const double* minus, int64_t n, double rh,
+                            cudaStream_t s);
+constexpr int kJacMaxParams = 8;
+
 void init_kernel_attributes();
 
 }  // namespace lbl
