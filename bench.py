@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--nlines", type=int, default=50000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-workers", type=int, default=0)
+    p.add_argument("--no-jacobian", action="store_true")
     return p.parse_args()
 
 
@@ -183,6 +184,53 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def jacobian_leg(ctx, prec, torch):
+    """Config 3: temperature, H2O and O3 Jacobians of the TOA radiance for all
+    60 layers (3 x 60 rows over 650-2500 cm-1, 200,000 lines), by the
+    adjoint-style path (lbl_jacobian) against the plain central-difference
+    cost, (2 x 3 x 60 + 1) fixed-grid forwards, timed from one forward."""
+    from lblrtm_b200 import gpu
+    cfg = configs.config3()
+    run = abi.make_run(**cfg["run"])
+    layers = abi.make_layers(cfg["profile"])
+    mols = list(cfg["jac_mols"])
+    ctx.upload_lines(abi.LinesHandle(cfg["lines"]))
+    dv, _ = gpu.dv_rule(run, layers)
+    n = gpu.layer_npts(run, dv[-1])
+    rad = torch.empty(n, dtype=torch.float64, device="cuda")
+    tr = torch.empty_like(rad)
+    jac = torch.empty((1 + len(mols), len(layers), n), dtype=torch.float64, device="cuda")
+    # forward (warm, then timed with events)
+    ctx.forward(run, layers, precision=prec, rad=rad, tr=tr)
+    fwd = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.forward(run, layers, precision=prec, rad=rad, tr=tr)
+        e1.record()
+        e1.synchronize()
+        fwd.append(e0.elapsed_time(e1))
+    fwd_ms = sum(fwd) / len(fwd)
+    ctx.jacobian(run, layers, mols, precision=prec, rad=rad, jac=jac)
+    jt = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.jacobian(run, layers, mols, precision=prec, rad=rad, jac=jac)
+        torch.cuda.synchronize()
+        jt.append(1e3 * (time.perf_counter() - t0))
+    jac_ms = sum(jt) / len(jt)
+    nfd = 2 * len(mols) * len(layers) + 2 * len(layers) + 1
+    rows = (1 + len(mols)) * len(layers)
+    del jac
+    return {"config": "config3: 60 layers, 650-2500 cm-1, 200,000 lines; d/dT and d/dln q "
+                      "(H2O, O3) per layer", "rows": rows, "npts_top": int(n),
+            "ms_per_jacobian_set": jac_ms, "jacobian_sets_per_s": 1e3 / jac_ms,
+            "forward_ms": fwd_ms, "fd_forwards": nfd, "fd_ms_estimate": fwd_ms * nfd,
+            "speedup_vs_fd": fwd_ms * nfd / jac_ms,
+            "timing": "wall clock around the synchronous call (host planning included)"}
+
+
 def gpu_arm(a):
     import torch
     from lblrtm_b200 import gpu
@@ -309,6 +357,10 @@ def gpu_arm(a):
     stage_ms = {k: round(v[0] / nstep, 4) for k, v in stats.items()}
     stage_work = {k: v[2] / nstep for k, v in stats.items() if v[2]}
 
+    jleg = None
+    if not a.no_jacobian:
+        jleg = jacobian_leg(ctx, prec, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         workers = a.cpu_workers or default_workers()
@@ -336,6 +388,7 @@ def gpu_arm(a):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
+            "jacobian": jleg,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

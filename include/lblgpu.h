@@ -244,11 +244,18 @@ int lbl_forward_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
 
 /* Jacobians of the top-of-atmosphere radiance of one profile with respect
  * to each layer's temperature (K) and the log column amount of the listed
- * molecules, computed by one forward sweep plus one reverse (adjoint) sweep
- * through the merge and the line shapes.  Output layout:
+ * molecules (the reference's analytic-Jacobian path, IMRG=40-43: layer
+ * optical-depth derivatives TDERIVup/QDERIVup, merge derivatives EMDT/
+ * EMADMG, src/xmerge.f90:4406-6144).  Optical-depth derivatives are central
+ * differences (T +-0.1 K, amount +-1 %) of two whole-profile passes per
+ * parameter; the merge is differentiated by hand and each layer's row is
+ * carried to the top through the later layers' transmittance and grid
+ * changes.  Upwelling radiance only (IEMIT=1, IPATHL=1); at most 7 molecules.
+ * Output layout (host or device):
  *   jac[(k*nlay + l)*npts + i]  k=0: d rad_i / d T_l,
  *                               k=1..nq: d rad_i / d ln W_{mols[k-1]},l
- * on the last layer's grid.  rad (optional) receives the forward result. */
+ * on the last layer's grid.  rad (optional) receives the forward result.
+ * layers[].dv/itype are computed here (lbl_dv_rule) and written back. */
 int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
                  int32_t nlay, const int32_t* mols, int32_t nq, double* rad,
                  double* jac, int64_t npts, int32_t precision);

@@ -187,13 +187,16 @@ class Context:
                                          _ptr(trb), n, precision), "forward")
         return rad, trb
 
-    def jacobian(self, run, layers, mols, precision=abi.PREC_SPLIT):
+    def jacobian(self, run, layers, mols, precision=abi.PREC_FP64, rad=None, jac=None):
+        """TOA radiance and its Jacobians, shape (1 + len(mols), nlay, npts):
+        row 0 d rad/d T_l, row k d rad/d ln W_{mols[k-1]},l.  rad/jac may be
+        given (numpy arrays or CUDA tensors of that size)."""
         dv, _ = dv_rule(run, layers)
         n = layer_npts(run, dv[-1])
         nl = len(layers)
-        m = (C.c_int32 * len(mols))(*mols)
-        rad = np.zeros(n)
-        jac = np.zeros((1 + len(mols), nl, n))
+        m = (C.c_int32 * max(len(mols), 1))(*mols)
+        rad = np.zeros(n) if rad is None else rad
+        jac = np.zeros((1 + len(mols), nl, n)) if jac is None else jac
         self._check(self.lib.lbl_jacobian(self.h, C.byref(run), layers, nl, m, len(mols),
                                           _ptr(rad), _ptr(jac), n, precision), "jacobian")
         return rad, jac
