@@ -199,74 +199,130 @@ __global__ void k_far_scale(Work w, DevLines ln) {
 // are merged in groups of width DVR4/2 (non-CO2 and CO2 separately); a
 // shrunk block is written once it holds >= 1000 lines or at the end.
 // =========================================================================
-__device__ void shrink_segment(const Work& w, const LayerDev& L, int64_t lo, int64_t hi,
-                               int64_t& out) {
+// State of one SHRINK walk over raw far-wing lines in file order.
+struct ShrinkWalk {
+  double vlmt = 0.;
+  bool started = false;
+  double sal = 0., sad = 0., ss = 0., sv = 0., sc = 0.;      // non-CO2 group
+  double sal2 = 0., sad2 = 0., ss2 = 0., sv2 = 0., sc2 = 0.; // CO2 group
+  int64_t raw = 0, out = 0;  // lines taken, shrunk lines written
+};
+
+// First usable raw line in far slots [from, limit) of the layer (F = slot
+// base), searched by the whole warp 32 slots at a time; its centre in v.
+__device__ bool next_valid_vnu(const Work& w, int64_t F, int64_t from, int64_t limit, double& v) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t c = from; c < limit; c += 32) {
+    const int64_t s = c + lane;
+    const unsigned m = __ballot_sync(0xffffffffu, s < limit && w.f_ok[F + s]);
+    if (m) {
+      v = __shfl_sync(0xffffffffu, s < limit ? w.f_vnu[F + s] : 0., __ffs(m) - 1);
+      return true;
+    }
+  }
+  return false;
+}
+
+// SHRINK (src/oprop.f90:3508-3640) over far slots [a, e) by one warp: the
+// lines are loaded 32 at a time and taken in file order with every lane
+// holding the same walk state.  A group of lines within DVR4/2 of the group
+// limit is merged into one strength-weighted line (non-CO2 and CO2
+// separately); coupled lines pass through.  The group closes when the next
+// usable line (looked up before `limit`) lies beyond the limit.  WRITE
+// stores the shrunk lines at shrunk slot S + out.
+template <bool WRITE>
+__device__ void shrink_walk(const Work& w, const LayerDev& L, int64_t a, int64_t e, int64_t limit,
+                            int64_t S, ShrinkWalk& st) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   const double dvh = L.dvr4 / 2.;
-  int64_t first = lo;
-  while (first < hi && !w.f_ok[L.off_far + first]) first++;
-  if (first >= hi) return;
-  double vlmt = w.f_vnu[L.off_far + first] + dvh;
-  double sal = 0., sad = 0., ss = 0., sv = 0., sc = 0.;
-  double sal2 = 0., sad2 = 0., ss2 = 0., sv2 = 0., sc2 = 0.;
-  const int64_t S = L.off_shr;
-  int64_t cur = first;
-  while (cur < hi) {
-    const int64_t c = L.off_far + cur;
-    int64_t nxt = cur + 1;
-    while (nxt < hi && !w.f_ok[L.off_far + nxt]) nxt++;
-    double sp = w.f_sp[c], spp = w.f_spp[c];
-    if (sp < 1.0e-35) {
-      sp = 0.0;
-      spp = 0.0;
+  const int64_t F = L.off_far;
+  auto emit = [&](double vnu, double sp, double alfa, double epp, double spp, int co2) {
+    if (WRITE && lane == 0) {
+      w.s_vnu[S + st.out] = vnu;
+      w.s_sp[S + st.out] = sp;
+      w.s_alfa[S + st.out] = alfa;
+      w.s_epp[S + st.out] = epp;
+      w.s_spp[S + st.out] = spp;
+      w.s_co2[S + st.out] = (int8_t)co2;
     }
-    const double vnu = w.f_vnu[c];
-    if (spp != 0.0) {
-      w.s_vnu[S + out] = vnu;
-      w.s_sp[S + out] = sp;
-      w.s_alfa[S + out] = w.f_alfa[c];
-      w.s_epp[S + out] = w.f_epp[c];
-      w.s_spp[S + out] = spp;
-      w.s_co2[S + out] = w.f_co2[c];
-      out++;
-    } else if (!w.f_co2[c]) {
-      sv = sv + vnu * sp;
-      ss = ss + sp;
-      sal = sal + sp * w.f_alfa[c];
-      sad = sad + sp * w.f_epp[c];
-      sc = sc + spp;
-    } else {
-      sv2 = sv2 + vnu * sp;
-      ss2 = ss2 + sp;
-      sal2 = sal2 + sp * w.f_alfa[c];
-      sad2 = sad2 + sp * w.f_epp[c];
-      sc2 = sc2 + spp;
-    }
-    bool close = true;
-    if (nxt < hi && w.f_vnu[L.off_far + nxt] <= vlmt) close = false;
-    if (close) {
-      vlmt = vnu + dvh;
-      if (ss > 0.) {
-        w.s_sp[S + out] = ss;
-        w.s_alfa[S + out] = sal / ss;
-        w.s_epp[S + out] = sad / ss;
-        w.s_vnu[S + out] = sv / ss;
-        w.s_spp[S + out] = sc;
-        w.s_co2[S + out] = 0;
-        out++;
-        sal = sad = ss = sv = sc = 0.;
+    st.out++;
+  };
+  for (int64_t c = a; c < e; c += 32) {
+    const int64_t s = c + lane;
+    const bool valid = s < e && w.f_ok[F + s];
+    double v = 0., sp = 0., spp = 0., al = 0., ep = 0.;
+    int co2 = 0;
+    if (valid) {
+      v = w.f_vnu[F + s];
+      sp = w.f_sp[F + s];
+      spp = w.f_spp[F + s];
+      if (sp < 1.0e-35) {
+        sp = 0.;
+        spp = 0.;
       }
-      if (ss2 > 0.) {
-        w.s_sp[S + out] = ss2;
-        w.s_alfa[S + out] = sal2 / ss2;
-        w.s_epp[S + out] = sad2 / ss2;
-        w.s_vnu[S + out] = sv2 / ss2;
-        w.s_spp[S + out] = sc2;
-        w.s_co2[S + out] = 1;
-        out++;
-        sal2 = sad2 = ss2 = sv2 = sc2 = 0.;
+      co2 = w.f_co2[F + s];
+      if (WRITE) {
+        al = w.f_alfa[F + s];
+        ep = w.f_epp[F + s];
       }
     }
-    cur = nxt;
+    const unsigned m = __ballot_sync(full, valid);
+    for (unsigned bits = m; bits; bits &= bits - 1) {
+      const int i = __ffs(bits) - 1;
+      const double vi = __shfl_sync(full, v, i);
+      const double spi = __shfl_sync(full, sp, i);
+      const double sppi = __shfl_sync(full, spp, i);
+      const int co2i = __shfl_sync(full, co2, i);
+      double ali = 0., epi = 0.;
+      if (WRITE) {
+        ali = __shfl_sync(full, al, i);
+        epi = __shfl_sync(full, ep, i);
+      }
+      const unsigned rest = bits & (bits - 1);
+      double vn = 0.;
+      bool hn;
+      if (rest) {
+        vn = __shfl_sync(full, v, __ffs(rest) - 1);
+        hn = true;
+      } else {
+        // the first usable line after this chunk's part of [a, e)
+        hn = next_valid_vnu(w, F, (c + 32 < e) ? c + 32 : e, limit, vn);
+      }
+      if (!st.started) {
+        st.vlmt = vi + dvh;
+        st.started = true;
+      }
+      st.raw++;
+      if (sppi != 0.0) {
+        emit(vi, spi, ali, epi, sppi, co2i);
+      } else if (!co2i) {
+        st.sv = st.sv + vi * spi;
+        st.ss = st.ss + spi;
+        st.sal = st.sal + spi * ali;
+        st.sad = st.sad + spi * epi;
+        st.sc = st.sc + sppi;
+      } else {
+        st.sv2 = st.sv2 + vi * spi;
+        st.ss2 = st.ss2 + spi;
+        st.sal2 = st.sal2 + spi * ali;
+        st.sad2 = st.sad2 + spi * epi;
+        st.sc2 = st.sc2 + sppi;
+      }
+      if (!(hn && vn <= st.vlmt)) {
+        st.vlmt = vi + dvh;
+        if (st.ss > 0.) {
+          if (WRITE) emit(st.sv / st.ss, st.ss, st.sal / st.ss, st.sad / st.ss, st.sc, 0);
+          else st.out++;
+          st.sal = st.sad = st.ss = st.sv = st.sc = 0.;
+        }
+        if (st.ss2 > 0.) {
+          if (WRITE) emit(st.sv2 / st.ss2, st.ss2, st.sal2 / st.ss2, st.sad2 / st.ss2, st.sc2, 1);
+          else st.out++;
+          st.sal2 = st.sad2 = st.ss2 = st.sv2 = st.sc2 = 0.;
+        }
+      }
+    }
   }
 }
 
@@ -287,9 +343,11 @@ __device__ __forceinline__ int64_t far_slot_end(const LayerDev& L, const int64_t
   return e > n ? n : e;
 }
 
+// One warp per (layer, start block).
 __global__ void k_shr_count(Work w, const int64_t* bs, const int64_t* blk_base, int nlay) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  // thread -> (layer, local start block) through the per-layer block base
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  // warp -> (layer, local start block) through the per-layer block base
   int lo = 0, hi = nlay;
   while (lo < hi) {
     int m = (lo + hi) >> 1;
@@ -304,60 +362,23 @@ __global__ void k_shr_count(Work w, const int64_t* bs, const int64_t* blk_base, 
   if (bl >= nb) return;
   int32_t* craw = w.c_raw + (blk_base[l] + bl) * kSegMaxBlk;
   int32_t* cout = w.c_out + (blk_base[l] + bl) * kSegMaxBlk;
-  const double dvh = L.dvr4 / 2.;
-  const int64_t F = L.off_far;
-  int32_t raw = 0, out = 0;
-  double ss = 0., ss2 = 0.;
-  bool open = false;  // a group is pending
-  double vlmt = 0.;
+  const int64_t nfar = L.far_hi - L.far_lo;
+  ShrinkWalk st;
   int k = 0;
   for (int64_t b = L.fblk_lo + bl; b < L.fblk_hi && k < kSegMaxBlk; b++, k++) {
-    const int64_t a = far_slot_begin(L, bs, b), e = far_slot_end(L, bs, b);
-    int64_t last_valid = -1;
-    for (int64_t s = a; s < e; s++)
-      if (w.f_ok[F + s]) last_valid = s;
-    for (int64_t s = a; s < e; s++) {
-      if (!w.f_ok[F + s]) continue;
-      double sp = w.f_sp[F + s], spp = w.f_spp[F + s];
-      if (sp < 1.0e-35) {
-        sp = 0.;
-        spp = 0.;
-      }
-      const double v = w.f_vnu[F + s];
-      if (!open) {
-        vlmt = (raw == 0) ? v + dvh : vlmt;
-        open = true;
-      }
-      raw++;
-      if (spp != 0.) out++;
-      else if (!w.f_co2[F + s]) ss = ss + sp;
-      else ss2 = ss2 + sp;
-      if (s == last_valid) {
-        // outputs if the segment were closed at the end of this panel
-        craw[k] = raw;
-        cout[k] = out + (ss > 0.) + (ss2 > 0.);
-      }
-      // real close decision, looking at the next valid line (any panel)
-      int64_t nx = s + 1;
-      const int64_t nfar = L.far_hi - L.far_lo;
-      while (nx < nfar && !w.f_ok[F + nx]) nx++;
-      const bool close = !(nx < nfar && w.f_vnu[F + nx] <= vlmt);
-      if (close) {
-        out += (ss > 0.) + (ss2 > 0.);
-        ss = ss2 = 0.;
-        vlmt = v + dvh;
-      }
+    shrink_walk<false>(w, L, far_slot_begin(L, bs, b), far_slot_end(L, bs, b), nfar, 0, st);
+    // the segment's raw and output counts were it closed at this block's end
+    if (lane == 0) {
+      craw[k] = (int32_t)st.raw;
+      cout[k] = (int32_t)(st.out + (st.ss > 0.) + (st.ss2 > 0.));
     }
-    if (last_valid < 0) {
-      craw[k] = raw;
-      cout[k] = out + (ss > 0.) + (ss2 > 0.);
-    }
-    if (raw >= 1000) {
+    if (st.raw >= 1000) {
       k++;
       break;
     }
   }
-  for (; k < kSegMaxBlk; k++) craw[k] = -1;  // not reached
+  if (lane == 0)
+    for (; k < kSegMaxBlk; k++) craw[k] = -1;  // not reached
 }
 
 __global__ void k_shr_plan(Work w, const int64_t* blk_base) {
@@ -403,8 +424,9 @@ __global__ void k_shr_plan(Work w, const int64_t* blk_base) {
   w.b9_count[l] = nb9;
 }
 
+// One warp per segment.
 __global__ void k_shr_write(Work w, const int64_t* bs, const int64_t* seg_base, int nlay) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lo = 0, hi = nlay;
   while (lo < hi) {
     int m = (lo + hi) >> 1;
@@ -418,8 +440,10 @@ __global__ void k_shr_write(Work w, const int64_t* bs, const int64_t* seg_base, 
   if (w.s_count[l] < 0 || sgi >= w.seg_count[l]) return;
   const int64_t b0 = L.fblk_lo + w.seg_blk[L.off_seg + sgi];
   const int64_t b1 = b0 + w.seg_nblk[L.off_seg + sgi];
-  int64_t out = w.seg_out[L.off_seg + sgi];
-  shrink_segment(w, L, far_slot_begin(L, bs, b0), far_slot_end(L, bs, b1 - 1), out);
+  ShrinkWalk st;
+  st.out = w.seg_out[L.off_seg + sgi];
+  const int64_t e = far_slot_end(L, bs, b1 - 1);
+  shrink_walk<true>(w, L, far_slot_begin(L, bs, b0), e, e, L.off_shr, st);
 }
 
 // =========================================================================
@@ -1836,9 +1860,10 @@ cudaError_t launch_far_scale(const Work& w, const DevLines& ln, int64_t max_far,
 cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_base,
                           int64_t nblk_total, cudaStream_t s) {
   if (nblk_total > 0) {
-    k_shr_count<<<(unsigned)((nblk_total + 127) / 128), 128, 0, s>>>(w, bs, blk_base, w.nlay);
+    // one warp per start block, then one warp per segment
+    k_shr_count<<<(unsigned)((nblk_total + 3) / 4), 128, 0, s>>>(w, bs, blk_base, w.nlay);
     k_shr_plan<<<(w.nlay + 31) / 32, 32, 0, s>>>(w, blk_base);
-    k_shr_write<<<(unsigned)((nblk_total + 127) / 128), 128, 0, s>>>(w, bs, blk_base, w.nlay);
+    k_shr_write<<<(unsigned)((nblk_total + 3) / 4), 128, 0, s>>>(w, bs, blk_base, w.nlay);
   }
   return cudaGetLastError();
 }
