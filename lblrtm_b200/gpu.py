@@ -187,6 +187,30 @@ class Context:
                                          _ptr(trb), n, precision), "forward")
         return rad, trb
 
+    def forward_batch(self, run, profiles, precision=abi.PREC_FP64):
+        """Many profiles in one call: profiles is a list of lbl_layer arrays.
+        Returns a list of (rad, tr) per profile on each profile's top grid."""
+        counts = [len(p) for p in profiles]
+        allL = (abi.Layer * sum(counts))()
+        k = 0
+        for p in profiles:
+            C.memmove(C.byref(allL, k * C.sizeof(abi.Layer)), p, C.sizeof(abi.Layer) * len(p))
+            k += len(p)
+        total = 0
+        for p in profiles:
+            q = abi.make_layers_like(p)
+            dv, _ = dv_rule(run, q)
+            total += layer_npts(run, dv[-1])
+        rad = np.zeros(total)
+        tr = np.zeros(total)
+        off = np.zeros(len(profiles) + 1, dtype=np.int64)
+        nl = (C.c_int32 * len(profiles))(*counts)
+        self._check(self.lib.lbl_forward_batch(self.h, C.byref(run), allL, nl, len(profiles),
+                                               _ptr(rad), _ptr(tr),
+                                               off.ctypes.data_as(C.POINTER(C.c_int64)), total,
+                                               precision), "forward_batch")
+        return [(rad[off[i]:off[i + 1]], tr[off[i]:off[i + 1]]) for i in range(len(profiles))]
+
     def jacobian(self, run, layers, mols, precision=abi.PREC_FP64, rad=None, jac=None):
         """TOA radiance and its Jacobians, shape (1 + len(mols), nlay, npts):
         row 0 d rad/d T_l, row k d rad/d ln W_{mols[k-1]},l.  rad/jac may be
