@@ -629,9 +629,33 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   if (n > 0 && (!L->vnu || !L->sp || !L->alfa || !L->epp || !L->mol || !L->hwhms ||
                 !L->tmpalf || !L->pshift || !L->iflg))
     return fail(ctx, LBL_E_ARG, "NULL line array");
-  for (int64_t i = 1; i < n; i++)
-    if (!(L->vnu[i] >= L->vnu[i - 1]))
-      return fail(ctx, LBL_E_UNSORTED, "line centres not ascending at record " + std::to_string(i));
+  // Line-coupling records (IFLG < 0) follow their line and carry Y/G
+  // coefficients in the centre field (RDLIN :818-837, LNCOR1 :1039-1061):
+  // they are skipped in the order check, and the searchable copy of the
+  // centres repeats the previous line's there.
+  std::vector<double> vs(L->vnu, L->vnu + n);
+  {
+    double last = 0.;
+    bool have = false;
+    for (int64_t i = 0; i < n; i++) {
+      if (L->iflg[i] < 0) {
+        if (i == 0 || (L->iflg[i - 1] != 1 && L->iflg[i - 1] != 3))
+          return fail(ctx, LBL_E_FORMAT,
+                      "coupling record without a coupled line at record " + std::to_string(i));
+        vs[i] = last;
+        continue;
+      }
+      if (have && !(L->vnu[i] >= last))
+        return fail(ctx, LBL_E_UNSORTED,
+                    "line centres not ascending at record " + std::to_string(i));
+      last = L->vnu[i];
+      have = true;
+    }
+    for (int64_t i = 0; i < n; i++)
+      if ((L->iflg[i] == 1 || L->iflg[i] == 3) && (i + 1 >= n || L->iflg[i + 1] >= 0))
+        return fail(ctx, LBL_E_FORMAT,
+                    "coupled line without its coefficient record at record " + std::to_string(i));
+  }
   std::vector<int64_t> bs;
   if (L->nblock > 0 && L->block_start) {
     bs.assign(L->block_start, L->block_start + L->nblock + 1);
@@ -644,7 +668,7 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
     if (bs[b + 1] < bs[b]) return fail(ctx, LBL_E_ARG, "block_start not increasing");
     if (bs[b + 1] - bs[b] > 250) return fail(ctx, LBL_E_NREC, "RDLIN; NREC GT LIMIN");
   }
-  ctx->h_vnu.assign(L->vnu, L->vnu + n);
+  ctx->h_vnu = vs;
   ctx->h_sp.assign(L->sp, L->sp + n);
   ctx->h_pshift.assign(L->pshift, L->pshift + n);
   ctx->h_mol.assign(L->mol, L->mol + n);
@@ -655,7 +679,7 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
     ctx->max_abs_pshift = std::max(ctx->max_abs_pshift, std::fabs((double)L->pshift[i]));
   cudaSetDevice(ctx->device);
   const size_t nn = (size_t)std::max<int64_t>(n, 1) + 2;  // +2: coupling record reads
-  size_t bytes = nn * (8 + 6 * 4 + 2 * 4) + bs.size() * 8 + 16 * 256;  // 10 aligned arrays
+  size_t bytes = nn * (2 * 8 + 6 * 4 + 2 * 4) + bs.size() * 8 + 16 * 256;  // 11 aligned arrays
   // the line buffer grows only; work already queued on the stream that
   // reads the old lines is ordered before the copies below
   if (!ctx->line_mem || bytes > ctx->line_cap) {
@@ -681,6 +705,7 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   };
   DevLines d;
   d.vnu = reinterpret_cast<double*>(take(nn * 8));
+  d.vraw = reinterpret_cast<double*>(take(nn * 8));
   d.sp = reinterpret_cast<float*>(take(nn * 4));
   d.alfa = reinterpret_cast<float*>(take(nn * 4));
   d.epp = reinterpret_cast<float*>(take(nn * 4));
@@ -694,7 +719,8 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   d.nblk = (int64_t)bs.size() - 1;
   cudaStream_t st = ctx->stream;
   if (n > 0) {
-    CK(cudaMemcpyAsync((void*)d.vnu, L->vnu, n * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.vnu, ctx->h_vnu.data(), n * 8, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((void*)d.vraw, L->vnu, n * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void*)d.sp, L->sp, n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void*)d.alfa, L->alfa, n * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync((void*)d.epp, L->epp, n * 4, cudaMemcpyHostToDevice, st));

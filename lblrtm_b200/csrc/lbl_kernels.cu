@@ -111,7 +111,7 @@ __device__ void coupling(const DevLines& ln, int64_t i, int iflag, int ilc, doub
                          double tmpdif, bool linf4, double& yi, double& gi, double& g1,
                          double& g2) {
   double A[5], B[5];
-  A[1] = ln.vnu[i + 1];
+  A[1] = ln.vraw[i + 1];
   B[1] = (double)ln.sp[i + 1];
   A[2] = (double)ln.alfa[i + 1];
   B[2] = (double)ln.epp[i + 1];

@@ -12,7 +12,8 @@ constexpr int kSegMaxBlk = 48;  // panels a LINF4 segment may span
 
 // Resident TAPE3 lines (device pointers).
 struct DevLines {
-  const double* vnu;
+  const double* vnu;   // centres, coupling records holding the previous line's
+  const double* vraw;  // centres as given (coupling records: Y coefficient)
   const float *sp, *alfa, *epp, *hwhms, *tmpalf, *pshift;
   const int32_t *mol, *iflg;
   const int64_t* bs;  // panel starts, nblk+1

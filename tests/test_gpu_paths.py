@@ -71,3 +71,86 @@ def test_forward_batch_matches_single_profiles(gpu_ctx):
         assert len(rad) == len(ref)
         assert np.array_equal(rad, ref)
         assert np.array_equal(tr, tref)
+
+
+def coupled_lines(n, v1, v2, seed, frac=0.05):
+    """Synthetic lines where a fraction carry line coupling: IFLG=1 (Y, G) or
+    IFLG=3 (width coefficients), each followed by its coefficient record
+    (IFLG=-1; the four-temperature values packed into the record's fields as
+    the reference reads them, LNCOR1 :1039-1061).  Block boundaries never
+    split a line from its record."""
+    base = configs.gen_lines(n, v1, v2, seed=seed, mols=configs.MOLS)
+    rng = np.random.default_rng(seed + 100)
+    pick = rng.random(n) < frac
+    kind = np.where(rng.random(n) < 0.5, 1, 3)
+    recs = {k: [] for k in base}
+    for i in range(n):
+        for k in base:
+            recs[k].append(base[k][i])
+        if not pick[i]:
+            continue
+        recs["iflg"][-1] = int(kind[i])
+        amp = 0.05 if kind[i] == 1 else 0.02
+        a = rng.uniform(-amp, amp, 4)
+        b = rng.uniform(-amp / 10, amp / 10, 4)
+        recs["vnu"].append(a[0])
+        recs["sp"].append(b[0])
+        recs["alfa"].append(a[1])
+        recs["epp"].append(b[1])
+        recs["mol"].append(np.frombuffer(np.float32(a[2]).tobytes(), dtype=np.int32)[0])
+        recs["hwhms"].append(b[2])
+        recs["tmpalf"].append(a[3])
+        recs["pshift"].append(b[3])
+        recs["iflg"].append(-1)
+    lines = {k: np.asarray(v, dtype=base[k].dtype) for k, v in recs.items()}
+    nrec = len(lines["vnu"])
+    bs = [0]
+    while bs[-1] < nrec:
+        b = min(bs[-1] + 250, nrec)
+        if b < nrec and lines["iflg"][b] < 0:
+            b -= 1
+        bs.append(b)
+    lines["block_start"] = np.asarray(bs, dtype=np.int64)
+    return lines
+
+
+@pytest.fixture(scope="module")
+def coupled(gpu_ctx):
+    lines = coupled_lines(4000, 600.0, 700.0, seed=11)
+    prof = configs.atmosphere(6, ptop=300.0)
+    run = abi.make_run(v1=610.0, v2=690.0, iemit=1, ilblf4=1, tmpbnd=290.0, bndemi=0.98)
+    lays = abi.make_layers(prof)
+    gpu.dv_rule(run, lays)
+    lh = abi.LinesHandle(lines)
+    gpu_ctx.upload_lines(lh)
+    return run, lays, lh
+
+
+@pytest.mark.parametrize("layer", range(6))
+def test_line_coupling_layer_fp64(gpu_ctx, coupled, layer):
+    run, lays, lh = coupled
+    ref, _ = O.layer_od(run, lays[layer], lh, jrad=0)
+    od, _ = gpu_ctx.layer_od(run, lays[layer], jrad=0)
+    e = floored_err(od, ref)
+    assert e.max() < RTOL_FP64, (layer, e.max(), int(e.argmax()))
+
+
+def test_line_coupling_changes_the_spectrum(gpu_ctx, coupled):
+    run, lays, lh = coupled
+    plain = dict(lh.a)
+    keep = plain["iflg"] >= 0
+    plain = {k: (v[keep] if k != "block_start" else None) for k, v in plain.items()}
+    plain.pop("block_start")
+    plain["iflg"] = np.zeros(int(keep.sum()), np.int32)
+    gpu_ctx.upload_lines(abi.LinesHandle(plain))
+    od0, _ = gpu_ctx.layer_od(run, lays[0], jrad=0)
+    gpu_ctx.upload_lines(lh)
+    od1, _ = gpu_ctx.layer_od(run, lays[0], jrad=0)
+    assert np.max(np.abs(od1 - od0) / np.abs(od0)) > 1e-4
+
+
+def test_coupling_record_without_line_is_rejected(gpu_ctx):
+    bad = configs.gen_lines(600, 600.0, 700.0, seed=12)
+    bad["iflg"][10] = -1
+    with pytest.raises(gpu.LblError):
+        gpu_ctx.upload_lines(abi.LinesHandle(bad))
