@@ -54,7 +54,7 @@ def build(verbose=False):
         objs.append(obj)
     lib = os.path.join(OUT, "liblblgpu.so")
     if _newer(lib, objs):
-        _run([NVCC, *ARCH, "-shared", "-o", lib, *objs, "-lcudart"])
+        _run([NVCC, *ARCH, "-shared", "-o", lib, *objs, "-lcudart", "-lpthread"])
     return lib
 
 

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lblgpu.h"
@@ -209,14 +210,31 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
               ctx->h_iflg.data(), (int64_t)ctx->h_vnu.size(), ctx->h_bs.data(),
               (int64_t)ctx->h_bs.size() - 1, ctx->max_abs_pshift};
   B.plans.resize(n);
+  // the JRAD switch carries from layer to layer (OPDPTH :6211); everything
+  // else in a layer's plan depends on that layer alone, so layers are
+  // planned on several host threads
+  std::vector<int> jin(n);
   int jrad = jrad_in;
   for (int l = 0; l < n; l++) {
-    std::string e;
-    int rc = plan_layer(R, layers[l], jrad, H, &B.plans[l], &e);
-    if (rc != LBL_OK) return fail(ctx, rc, "layer " + std::to_string(l) + ": " + e);
-    jrad = B.plans[l].d.jrad;
+    jin[l] = jrad;
+    jrad = next_jrad(R, layers[l], jrad);
   }
   if (jrad_out) *jrad_out = jrad;
+  std::vector<int> rcs(n, LBL_OK);
+  std::vector<std::string> errs(n);
+  auto plan_range = [&](int a, int b) {
+    for (int l = a; l < b; l++) rcs[l] = plan_layer(R, layers[l], jin[l], H, &B.plans[l], &errs[l]);
+  };
+  const int nth = std::min<int>(n / 4, 8);
+  if (nth <= 1) {
+    plan_range(0, n);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < nth; t++) th.emplace_back(plan_range, n * t / nth, n * (t + 1) / nth);
+    for (auto& x : th) x.join();
+  }
+  for (int l = 0; l < n; l++)
+    if (rcs[l] != LBL_OK) return fail(ctx, rcs[l], "layer " + std::to_string(l) + ": " + errs[l]);
   // offsets
   int64_t o_r1 = 0, o_r2 = 0, o_r3 = 0, o_od = 0, o_pan = 0, o_win = 0, o_far = 0, o_near = 0,
           o_b9 = 0, o_abs = 0;

@@ -871,10 +871,31 @@ __global__ void __launch_bounds__(kFwThreads, 3)
             if (qhi < qlo) continue;
             F4Reg<double> rg;
             f4_load(rg, pl, m, 0);
+            // the offset to the line centre advances by kFwAdders points a
+            // step (CONVF4 accumulates XJJ the same way); the bound term and
+            // the coupling factor are fixed per line
+            const double step = double(kFwAdders) * dvr4;
+            double xm = double(ad + kFwAdders * qlo) * dvr4 - rg.xnui;
+            if (!rg.co2 && rg.dptrat == 0.) {
 #pragma unroll 2
-            for (int q = qlo; q <= qhi; q++) {
-              const int j = 1 + ad + kFwAdders * q;
-              R4w[j] += f4_at(rg, j, 0.f, dvr4, rbndsq, 0.f, 0.f, 0.f);
+              for (int q = qlo; q <= qhi; q++, xm += step) {
+                const double xmsq = xm * xm;
+                const double zvsq = xmsq * rg.rvi2;
+                const double f = zvsq <= 4096. ? (rg.sa3 + zvsq * rg.sb3) - rg.f4bnd
+                                               : rg.sil * recip_nr(rg.alfl2 + xmsq) - rg.f4bnd;
+                R4w[1 + ad + kFwAdders * q] += f;
+              }
+            } else {
+#pragma unroll 2
+              for (int q = qlo; q <= qhi; q++, xm += step) {
+                const double xmsq = xm * xm;
+                const double zvsq = xmsq * rg.rvi2;
+                const double sub = rg.co2 ? (2. - xmsq * rbndsq) * rg.f4bnd : rg.f4bnd;
+                double f = zvsq <= 4096. ? (rg.sa3 + zvsq * rg.sb3) - sub
+                                         : rg.sil * recip_nr(rg.alfl2 + xmsq) - sub;
+                f = f + xm * rg.dptrat * f;
+                R4w[1 + ad + kFwAdders * q] += f;
+              }
             }
             nevals += (unsigned)(qhi - qlo + 1);
           }
