@@ -313,8 +313,31 @@ def gpu_arm(a):
         e2e_s = float(t.item())
     e2e_value = world * pts / e2e_s
 
-    # ---- roofline of the dominant kernel (far wing) ----
+    # ---- rooflines ----
     nstep = a.steps
+    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    traffic_file = os.path.join(ROOT, "profiles", "traffic_config1.json")
+    try:
+        traffic_db = json.load(open(traffic_file))
+    except (OSError, ValueError):
+        traffic_db = {}
+    # dominant kernel: the fused near-wing/PANEL kernel, one launch per step;
+    # algorithmic bytes = the optical depth it must write (8 B per layer point)
+    pn = stats.get("panels", (0.0, 0, 0.0))
+    pn_ms = pn[0] / max(pn[1], 1)
+    pn_bytes = 8.0 * pts
+    pn_gbs = pn_bytes / (pn_ms / 1e3) / 1e9 if pn_ms > 0 else None
+    roofline = {
+        "bound": "hbm", "kernel": "k_panel_od (CNVFNV sums + XINT + PANEL + RADFNI)",
+        "achieved": pn_gbs, "peak": hbm_peak, "unit": "GB/s",
+        "frac": (pn_gbs / hbm_peak) if pn_gbs else None,
+        "traffic": traffic_db.get("k_panel_od"),
+        "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650",
+        "work": f"{pn_bytes:.4g} B of optical depth written per launch (8 B x layer points)",
+        "launch_ms": pn_ms,
+    }
+    # far wing: FP pipe roofline (line-point evaluations x 8 flops)
     fw = stats.get("far_wing", (0.0, 0, 0.0))
     fw_ms = fw[0] / max(fw[1], 1)
     evals = fw[2] / nstep
@@ -322,19 +345,12 @@ def gpu_arm(a):
     lanes = FP64_LANES if prec == abi.PREC_FP64 else FP32_LANES
     peak_tf = N_SM * lanes * 2 * 1965e6 / 1e12
     achieved_tf = fw_flops / (fw_ms / 1e3) / 1e12 if fw_ms > 0 else None
-    traffic = None
-    tf_path = os.path.join(ROOT, "profiles", "far_wing_traffic.json")
-    if os.path.exists(tf_path):
-        try:
-            traffic = json.load(open(tf_path)).get(a.precision)
-        except (OSError, ValueError):
-            traffic = None
-    roofline = {
+    roof_fw = {
         "bound": "fp64" if prec == abi.PREC_FP64 else "fp32",
         "kernel": "k_far_wing (LBLF4/CONVF4 far wing)",
         "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
         "frac": (achieved_tf / peak_tf) if achieved_tf else None,
-        "traffic": traffic,
+        "traffic": traffic_db.get("k_far_wing") if prec == abi.PREC_FP64 else None,
         "peak_source": f"nominal {'FP64' if lanes == 64 else 'FP32'} vector rate: "
                        f"{N_SM} SMs x {lanes} lanes x 2 x 1965 MHz (MEASURED_PEAKS.json "
                        "holds HBM and bf16 only)",
@@ -342,8 +358,6 @@ def gpu_arm(a):
         "launch_ms": fw_ms,
     }
     # HBM roofline of the merge (bytes: FP64 OD read + R,T in/out per point)
-    peaks = json.load(open(PEAKS_FILE)) if os.path.exists(PEAKS_FILE) else {}
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
     mg = stats.get("merge", (0.0, 0, 0.0))
     merge_bytes = mg[2] / nstep * (8 + 16 + 16)
     merge_ms = mg[0] / nstep
@@ -382,7 +396,7 @@ def gpu_arm(a):
                        "layer_points_per_step": pts, "precision": a.precision,
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": f"replica x{world}"},
-            "roofline": roofline, "roofline_merge": roof_merge,
+            "roofline": roofline, "roofline_far_wing": roof_fw, "roofline_merge": roof_merge,
             "stage_ms": stage_ms, "stage_work": stage_work,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),

@@ -469,7 +469,12 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   }
   {
     // near-wing sums, PANEL combination and optical depth in one pass
-    StageTimer t(ctx, "panels", 3);
+    StageTimer t(ctx, "panel_prep", 2);
+    CK(launch_panel_prep(w, ctx->dl, B.npanel_total, B.d_panel_layer, B.d_panel_base,
+                         B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
+  }
+  {
+    StageTimer t(ctx, "panels", 1);
     CK(launch_panels(w, ctx->dl, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
                      B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
   }

@@ -1911,14 +1911,21 @@ cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, do
 }
 
 
+cudaError_t launch_panel_prep(const Work& w, const DevLines& ln, int64_t npanel_total,
+                              const int32_t* panel_layer, const int64_t* panel_base, int64_t* rng,
+                              double* segs, int32_t* nseg, cudaStream_t s) {
+  if (npanel_total <= 0) return cudaSuccess;
+  const unsigned nb = (unsigned)((npanel_total + 127) / 128);
+  k_panel_ranges<<<nb, 128, 0, s>>>(w, ln, panel_layer, panel_base, npanel_total, rng);
+  k_panel_segs<<<nb, 128, 0, s>>>(w, panel_layer, panel_base, npanel_total, segs, nseg);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_panels(const Work& w, const DevLines& ln, const DevShapes& sh,
                           int64_t npanel_total, const int32_t* panel_layer,
                           const int64_t* panel_base, int64_t* rng, double* segs,
                           int32_t* nseg, cudaStream_t s) {
   if (npanel_total <= 0) return cudaSuccess;
-  const unsigned nb = (unsigned)((npanel_total + 127) / 128);
-  k_panel_ranges<<<nb, 128, 0, s>>>(w, ln, panel_layer, panel_base, npanel_total, rng);
-  k_panel_segs<<<nb, 128, 0, s>>>(w, panel_layer, panel_base, npanel_total, segs, nseg);
   k_panel_od<<<(unsigned)npanel_total, kPanelThreads, 0, s>>>(w, ln, sh, panel_layer, panel_base,
                                                               rng, segs, nseg);
   return cudaGetLastError();

@@ -85,6 +85,9 @@ cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* wi
 cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
+cudaError_t launch_panel_prep(const Work& w, const DevLines& ln, int64_t npanel_total,
+                              const int32_t* panel_layer, const int64_t* panel_base, int64_t* rng,
+                              double* segs, int32_t* nseg, cudaStream_t s);
 cudaError_t launch_panels(const Work& w, const DevLines& ln, const DevShapes& sh,
                           int64_t npanel_total, const int32_t* panel_layer,
                           const int64_t* panel_base, int64_t* rng, double* segs,
