@@ -235,6 +235,9 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   }
   for (int l = 0; l < n; l++)
     if (rcs[l] != LBL_OK) return fail(ctx, rcs[l], "layer " + std::to_string(l) + ": " + errs[l]);
+  for (int l = 0; l < n; l++)
+    if (B.plans[l].d.n_r1 >= (int64_t(1) << 31) - 64)
+      return fail(ctx, LBL_E_RANGE, "layer " + std::to_string(l) + ": more than 2^31 points");
   // offsets
   int64_t o_r1 = 0, o_r2 = 0, o_r3 = 0, o_od = 0, o_pan = 0, o_win = 0, o_far = 0, o_near = 0,
           o_b9 = 0, o_abs = 0;

@@ -560,21 +560,6 @@ __device__ __forceinline__ void f4_load(F4Reg<float>& r, const F4Line& p, int m,
   r.co2 = p.co2;
 }
 
-// F4 at window point j (FP64: CONVF4's expression).
-__device__ __forceinline__ double f4_at(const F4Reg<double>& r, int j, float, double dvr4,
-                                        double rbndsq, float, float, float) {
-  const double xm = double(j - 1) * dvr4 - r.xnui;
-  const double xmsq = xm * xm;
-  const double zvsq = xmsq * r.rvi2;
-  const double sub = r.co2 ? (2. - xmsq * rbndsq) * r.f4bnd : r.f4bnd;
-  double f;
-  if (zvsq <= 4096.)
-    f = (r.sa3 + zvsq * r.sb3) - sub;
-  else
-    f = r.sil * recip_nr(r.alfl2 + xmsq) - sub;
-  return f + xm * r.dptrat * f;
-}
-
 // F4 at window point j = j0 + kq - k0 (FP32).  Beyond the quadratic core
 // the bound is subtracted without cancellation, with v = B^2 - x^2 = u (2B - u):
 //   non-CO2  L(x) - L(B)               =  F4BND v / (a^2 + x^2)
@@ -603,6 +588,8 @@ constexpr int kFwAdders = 224;
 constexpr int kFwThreads = kFwAdders + 32;
 constexpr int kFwPts = (kLimOut + kFwAdders - 1) / kFwAdders;  // window points per adder
 constexpr int kFwSmem = 2 * (int)kR4Stride * (int)sizeof(double);  // two R4 buffers
+// split precision adds one FP32 accumulator per adder point
+constexpr int kFwSmem32 = kFwSmem + kFwPts * kFwAdders * (int)sizeof(float);
 constexpr int kFwBatch = 4;  // lines the deciding warp evaluates together
 
 // Sum, in list order, of both sides of lines cl[idx(0..n-1)] at point jj
@@ -665,6 +652,10 @@ __global__ void __launch_bounds__(kFwThreads, 3)
   const LayerDev& L = w.L[l];
   const WinDev& W = w.win[gw];
   for (int j = threadIdx.x; j < 2 * kR4Stride; j += kFwThreads) fw_r4[j] = 0.;
+  if constexpr (sizeof(T) == 4) {
+    float* acc32 = reinterpret_cast<float*>(fw_r4 + 2 * kR4Stride);
+    for (int j = threadIdx.x; j < kFwPts * kFwAdders; j += kFwThreads) acc32[j] = 0.f;
+  }
   const double dvr4 = L.dvr4, bnd = L.bound4, bndsq = bnd * bnd, rbndsq = 1. / bndsq;
   const int npt = W.nptr4;
   const int64_t S = L.off_shr;
@@ -901,35 +892,32 @@ __global__ void __launch_bounds__(kFwThreads, 3)
           }
         }
       } else {
-        // split precision: the chunk's lines summed in FP32 registers, the
-        // chunk total added to the FP64 R4
+        // split precision: the chunk's lines summed in FP32 in shared memory
+        // (each adder its own points), the chunk total added to the FP64 R4
+        float* acc32 = reinterpret_cast<float*>(fw_r4 + 2 * kR4Stride) + ad;
         const float dvr4f = (float)dvr4, bndf = (float)bnd, rbndsqf = (float)rbndsq;
-        float acc[kFwPts];
-#pragma unroll
-        for (int q = 0; q < kFwPts; q++) acc[q] = 0.f;
         for (int a = 0; a < na; a++) {
           const F4Line& pl = cl[prv][s_idx[prv][a]];
 #pragma unroll 1
           for (int m = 0; m < 2; m++) {
-            if (!(pl.has & (1 << m))) continue;
             const int lo = m ? pl.mjmin : pl.jmin, hi = m ? pl.mjmax : pl.jmax;
+            const int qlo = (lo - 1 - ad <= 0) ? 0 : (lo - 2 - ad) / kFwAdders + 1;
+            const int qhi = (hi - 1 - ad < 0) ? -1 : (hi - 1 - ad) / kFwAdders;
+            if (qhi < qlo) continue;
             F4Reg<float> rg;
             f4_load(rg, pl, m, 1 + ad);
-#pragma unroll
-            for (int q = 0; q < kFwPts; q++) {
-              const int j = 1 + ad + kFwAdders * q;
-              if (j >= lo && j <= hi) {
-                acc[q] += f4_at(rg, j, rg.k0 + (float)(kFwAdders * q), dvr4, rbndsq, dvr4f,
-                                bndf, rbndsqf);
-                nevals++;
-              }
-            }
+#pragma unroll 2
+            for (int q = qlo; q <= qhi; q++)
+              acc32[kFwAdders * q] += f4_at(rg, 0, rg.k0 + (float)(kFwAdders * q), dvr4, rbndsq,
+                                            dvr4f, bndf, rbndsqf);
+            nevals += (unsigned)(qhi - qlo + 1);
           }
         }
 #pragma unroll
         for (int q = 0; q < kFwPts; q++) {
           const int j = 1 + ad + kFwAdders * q;
-          if (j <= npt) R4w[j] = R4r[j] + (double)acc[q];
+          if (j <= npt) R4w[j] = R4r[j] + (double)acc32[kFwAdders * q];
+          acc32[kFwAdders * q] = 0.f;
         }
       }
     }
@@ -1275,26 +1263,29 @@ __device__ __forceinline__ double interp4(const double* R, int64_t J, int r) {
 // Global grid index ranges of one panel (panel p of layer L):
 //   R1 points whose OD the panel writes, the R2 points their 4-point
 //   interpolation reads, and the R3 points those R2 points read.
+// Grid indices of a layer fit in 32 bits (a layer holds fewer than 2^31
+// points, checked on the host); the panel kernels use 32-bit arithmetic.
 struct PanelRange {
-  int64_t a1, b1, a2, b2, a3, b3;
-  long nhi;
+  int32_t a1, b1, a2, b2, a3, b3;
+  int32_t nhi;
 };
 
-__device__ __forceinline__ PanelRange panel_range(const LayerDev& L, int64_t p) {
+__device__ __forceinline__ PanelRange panel_range(const LayerDev& L, int32_t p) {
   PanelRange r;
-  r.nhi = (p == L.npanel - 1) ? (long)(L.npts - 2400 * (L.npanel - 1) + 32) : 2432;
+  const int32_t npanel = (int32_t)L.npanel, n_r2 = (int32_t)L.n_r2, n_r3 = (int32_t)L.n_r3;
+  r.nhi = (p == npanel - 1) ? (int32_t)(L.npts - 2400 * (L.npanel - 1) + 32) : 2432;
   r.a1 = 2400 * p + 33;
   r.b1 = 2400 * p + r.nhi;
   r.a2 = (r.a1 - 1) / 4;          // J2 - 1 of the first point
   r.b2 = (r.b1 - 1) / 4 + 3;      // J2 + 2 of the last point
-  if (r.b2 > L.n_r2) r.b2 = L.n_r2;
+  if (r.b2 > n_r2) r.b2 = n_r2;
   // R2 points that receive R3 are 5 .. n_r2-3 (PANEL :1459-1480)
-  const int64_t c2 = r.a2 < 5 ? 5 : r.a2;
-  const int64_t d2 = r.b2 > L.n_r2 - 3 ? L.n_r2 - 3 : r.b2;
+  const int32_t c2 = r.a2 < 5 ? 5 : r.a2;
+  const int32_t d2 = r.b2 > n_r2 - 3 ? n_r2 - 3 : r.b2;
   r.a3 = (c2 - 1) / 4;
   if (r.a3 < 1) r.a3 = 1;
   r.b3 = (d2 - 1) / 4 + 3;
-  if (r.b3 > L.n_r3) r.b3 = L.n_r3;
+  if (r.b3 > n_r3) r.b3 = n_r3;
   return r;
 }
 
@@ -1306,7 +1297,7 @@ __global__ void k_panel_ranges(Work w, DevLines ln, const int32_t* panel_layer,
   if (gp >= npanel_total) return;
   const int l = panel_layer[gp];
   const LayerDev& L = w.L[l];
-  const PanelRange R = panel_range(L, gp - panel_base[l]);
+  const PanelRange R = panel_range(L, (int32_t)(gp - panel_base[l]));
   const double reach = 64. * L.alfmax + 32. * L.dv + fabs(L.rhorat) * 1.0;
   rng[2 * gp] = lower_bound_d(ln.vnu, L.near_lo, L.near_hi,
                               L.vft0 + double(R.a3 - 1) * L.dvr3 - reach);
@@ -1318,7 +1309,7 @@ __global__ void k_panel_ranges(Work w, DevLines ln, const int32_t* panel_layer,
 // and the constants of CNVFNV's three sums (src/oprop.f90:1283-1351).
 struct PanelLine {
   double zint, zslope, sppsp, s0, sg, sx, s2, s3;
-  int64_t lo1, hi1, lo2, hi2, lo3, hi3;
+  int32_t lo1, hi1, lo2, hi2, lo3, hi3;
   int32_t pc;  // convolution panel of the line
 };
 
@@ -1379,8 +1370,9 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
   const int64_t gp = blockIdx.x;
   const int l = panel_layer[gp];
   const LayerDev& L = w.L[l];
-  const int64_t p = gp - panel_base[l];
+  const int32_t p = (int32_t)(gp - panel_base[l]);
   const PanelRange R = panel_range(L, p);
+  const int32_t n_r2 = (int32_t)L.n_r2;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const unsigned full = 0xffffffffu;
   __shared__ PanelLine st[kPanelStage];
@@ -1406,9 +1398,9 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
       const int64_t slot = L.off_near + (c0 + tid - L.near_lo);
       if (w.n_ok[slot]) {
         const double* sv = w.n_str + 5 * slot;
-        const int64_t pc = w.n_pconv[slot];
-        const int64_t j1a = w.n_jmin1[slot], j1b = w.n_jmax1[slot];
-        const int64_t j2 = w.n_j2[slot], j3 = w.n_j3[slot];
+        const int32_t pc = w.n_pconv[slot];
+        const int32_t j1a = w.n_jmin1[slot], j1b = w.n_jmax1[slot];
+        const int32_t j2 = w.n_j2[slot], j3 = w.n_j3[slot];
         q.zint = w.n_zint[slot];
         q.zslope = w.n_zslope[slot];
         q.sppsp = w.n_sppsp[slot];
@@ -1417,7 +1409,7 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
         q.s3 = sv[2];
         q.sg = sv[3];
         q.sx = sv[4];
-        q.pc = (int32_t)pc;
+        q.pc = pc;
         // panel-local windows shifted to the global grids by the line's panel
         q.lo1 = j1a + 2400 * pc;
         q.hi1 = j1b + 2400 * pc;
@@ -1444,9 +1436,9 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
       const PanelLine& ql = st[k];
       // R1 (DV grid): F1 + FG + VERFN terms
       if (ql.hi1 >= R.a1 && ql.lo1 <= R.b1) {
-        const int lo = (int)((ql.lo1 > R.a1 ? ql.lo1 : R.a1) - R.a1);
-        const int hi = (int)((ql.hi1 < R.b1 ? ql.hi1 : R.b1) - R.a1);
-        const int off = (int)(R.a1 - 2400 * (int64_t)ql.pc - 1);  // g - pofs - 1 at i = 0
+        const int lo = (ql.lo1 > R.a1 ? ql.lo1 : R.a1) - R.a1;
+        const int hi = (ql.hi1 < R.b1 ? ql.hi1 : R.b1) - R.a1;
+        const int off = R.a1 - 2400 * ql.pc - 1;  // g - pofs - 1 at i = 0
         int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
 #pragma unroll 2
         for (; i <= hi; i += kPanelThreads) {
@@ -1461,9 +1453,9 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
       }
       // R2 (4 DV): F2
       if (ql.hi2 >= R.a2 && ql.lo2 <= R.b2) {
-        const int lo = (int)((ql.lo2 > R.a2 ? ql.lo2 : R.a2) - R.a2);
-        const int hi = (int)((ql.hi2 < R.b2 ? ql.hi2 : R.b2) - R.a2);
-        const int off = (int)(R.a2 - 600 * (int64_t)ql.pc - 1);
+        const int lo = (ql.lo2 > R.a2 ? ql.lo2 : R.a2) - R.a2;
+        const int hi = (ql.hi2 < R.b2 ? ql.hi2 : R.b2) - R.a2;
+        const int off = R.a2 - 600 * ql.pc - 1;
         int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
         for (; i <= hi; i += kPanelThreads) {
           const double zf = (double(off + i) - ql.zint * L.conf2) * ql.zslope;
@@ -1476,10 +1468,10 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
       }
       // R3 (16 DV): F3
       if (ql.hi3 >= R.a3 && ql.lo3 <= R.b3) {
-        const int lo = (int)((ql.lo3 > R.a3 ? ql.lo3 : R.a3) - R.a3);
-        const int hi = (int)((ql.hi3 < R.b3 ? ql.hi3 : R.b3) - R.a3);
+        const int lo = (ql.lo3 > R.a3 ? ql.lo3 : R.a3) - R.a3;
+        const int hi = (ql.hi3 < R.b3 ? ql.hi3 : R.b3) - R.a3;
         if (tid >= lo && tid <= hi) {
-          const int off = (int)(R.a3 - 150 * (int64_t)ql.pc - 1);
+          const int off = R.a3 - 150 * ql.pc - 1;
           const double zf = (double(off + tid) - ql.zint * L.conf3) * ql.zslope;
           int iz = (int)(fabs(zf) + 1.5);
           iz = iz > kNfmx ? kNfmx : iz;
@@ -1495,8 +1487,8 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
   // belongs to panel 0 for g <= 155, else to panel (g-6)/150 (N1R3/N2R3,
   // src/oprop.f90:474-486)
   if (tid < n3p) {
-    const int64_t g = R.a3 + tid;
-    const int64_t po = (g <= 155) ? 0 : (g - 6) / 150;
+    const int32_t g = R.a3 + tid;
+    const int32_t po = (g <= 155) ? 0 : (g - 6) / 150;
     if (po < L.npanel) {
       const long I = (long)(g - 150 * po);
       const long n1 = (po == 0) ? 1 : 6;
@@ -1516,8 +1508,8 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
   __syncthreads();
   // R2 += 4-point interpolation of R3 (PANEL :1459-1480)
   for (int i = tid; i < n2p; i += kPanelThreads) {
-    const int64_t g = R.a2 + i;
-    if (g >= 5 && g <= L.n_r2 - 3) s2[i] += interp4(s3 - R.a3, (g - 1) / 4 + 1, (int)((g - 1) % 4));
+    const int32_t g = R.a2 + i;
+    if (g >= 5 && g <= n_r2 - 3) s2[i] += interp4(s3 - R.a3, (g - 1) / 4 + 1, (g - 1) % 4);
   }
   __syncthreads();
   // OD = R1 + 4-point interpolation of R2 (PANEL :1482-1519), times the
@@ -1526,8 +1518,8 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
   const double* r2 = s2 - R.a2;
   if (L.jrad != 0) {
     for (int i = tid; i < n1p; i += kPanelThreads) {
-      const int64_t g = R.a1 + i;
-      od_out[g - 33] = s1[i] + interp4(r2, (g - 1) / 4 + 1, (int)((g - 1) % 4));
+      const int32_t g = R.a1 + i;
+      od_out[g - 33] = s1[i] + interp4(r2, (g - 1) / 4 + 1, (g - 1) % 4);
     }
     return;
   }
@@ -1565,19 +1557,19 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
     }
     __syncthreads();
     const int ns = s_nseg;
-    const long ilo = (long)seg[0], ihi = s_n2;
+    const int32_t ilo = (int32_t)seg[0], ihi = (int32_t)s_n2;
     for (int i = tid; i < n1p; i += kPanelThreads) {
-      const int64_t g = R.a1 + i;
-      const long I = (long)(g - 2400 * p);
+      const int32_t g = R.a1 + i;
+      const int32_t I = g - 2400 * p;
       if (I < ilo || I > ihi) continue;
-      double od = s1[i] + interp4(r2, (g - 1) / 4 + 1, (int)((g - 1) % 4));
+      double od = s1[i] + interp4(r2, (g - 1) / 4 + 1, (g - 1) % 4);
       int lo = 0, hi = ns - 1;
       while (lo < hi) {
         const int m = (lo + hi + 1) >> 1;
         if (seg[3 * m] <= double(I)) lo = m;
         else hi = m - 1;
       }
-      od = od * (seg[3 * lo + 1] + double(I - (long)seg[3 * lo]) * seg[3 * lo + 2]);
+      od = od * (seg[3 * lo + 1] + double(I - (int32_t)seg[3 * lo]) * seg[3 * lo + 2]);
       od_out[g - 33] = od;
     }
     if (ihi >= R.nhi) break;
@@ -1850,7 +1842,7 @@ __global__ void k_jac_diff(double* plus, const double* minus, int64_t n, double 
 void init_kernel_attributes() {
   // two R4 buffers per CTA; the largest carveout lets several CTAs share an SM
   cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
-  cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
+  cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem32);
   cudaFuncSetAttribute(k_panel_od, cudaFuncAttributePreferredSharedMemoryCarveout,
                        cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1893,7 +1885,7 @@ cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* wi
                             const int32_t* win_layer, int precision, cudaStream_t s) {
   if (nwin_total <= 0) return cudaSuccess;
   if (precision == LBL_PREC_SPLIT)
-    k_far_wing<float><<<nwin_total, kFwThreads, kFwSmem, s>>>(w, win_order, win_layer);
+    k_far_wing<float><<<nwin_total, kFwThreads, kFwSmem32, s>>>(w, win_order, win_layer);
   else
     k_far_wing<double><<<nwin_total, kFwThreads, kFwSmem, s>>>(w, win_order, win_layer);
   return cudaGetLastError();
