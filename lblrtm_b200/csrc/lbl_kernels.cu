@@ -1597,43 +1597,59 @@ __device__ __forceinline__ T planck_t(double vi, double xkt) {
   }
 }
 
+// Point f of the finer grid from the previous layer's field x (n_old
+// points): a copy where the grids agree, else RADNN's 4-point Lagrange
+// interpolation at P = 1 - r/(ITYPE+1) (ITYPE = DV/(DV_old-DV) rounded).
+// 32-bit indices: layers hold fewer than 2^31 points.
+__device__ __forceinline__ void merge_regrid(const double* x, const double* y, int32_t n_old,
+                                             int32_t f, int32_t itype, double& xo, double& yo) {
+  auto cl = [&](int32_t c) { return c < 0 ? 0 : (c >= n_old ? n_old - 1 : c); };
+  if (itype == 0) {
+    xo = x[cl(f)];
+    if (y) yo = y[cl(f)];
+    return;
+  }
+  const int32_t LL = itype + 1;
+  const int32_t q = f / LL, r = f - q * LL;
+  if (r == 0) {
+    xo = x[cl(q * itype)];
+    if (y) yo = y[cl(q * itype)];
+    return;
+  }
+  const int32_t ipl = q * itype + r - 1;
+  const double P = 1.0 - double(r) / double(LL);
+  const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
+  const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
+  const int32_t c0 = cl(ipl - 1), c1 = cl(ipl), c2 = cl(ipl + 1), c3 = cl(ipl + 2);
+  xo = a1 * x[c0] + a2 * x[c1] + a3 * x[c2] + a4 * x[c3];
+  if (y) yo = a1 * y[c0] + a2 * y[c1] + a3 * y[c2] + a4 * y[c3];
+}
+
 template <typename T>
 __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const double* od,
-                        int first, double dv_old, int64_t n_old, const double* rad_in,
+                        int first, double dv_old, int64_t n_old64, const double* rad_in,
                         const double* tr_in, double* rad_out, double* tr_out, double tbnd,
                         double emis, int iemit, double tzu) {
   const LayerDev& L = *Lp;
-  const int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= L.npts) return;
+  const int32_t f = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (f >= (int32_t)L.npts) return;
+  const int32_t n_old = (int32_t)n_old64;
   const double DV = L.dv;
-  const int64_t p = f / 2400;
+  const int32_t p = f / 2400;
   const double vi = (vft_panel[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
   const double odv = od[f];
+  const int32_t itype = (first || dv_old == DV) ? 0 : (int32_t)fint(DV / (dv_old - DV) + 0.5);
   if (iemit == 0) {
-    // ABINIT / ABSMRG: optical depths add (regrid below)
-    double old = 0.;
-    if (!first) {
-      const double dvk = DV;
-      long itype = (dv_old == dvk) ? 0 : fint(dvk / (dv_old - dvk) + 0.5);
-      const int64_t LL = itype + 1;
-      const int64_t q = f / LL, r = f % LL;
-      auto O = [&](int64_t c) { return rad_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
-      if (r == 0) {
-        old = O(q * itype);
-      } else {
-        const int64_t ipl = q * itype + r - 1;
-        const double P = 1.0 - double(r) / double(LL);
-        const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
-        const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
-        old = a1 * O(ipl - 1) + a2 * O(ipl) + a3 * O(ipl + 1) + a4 * O(ipl + 2);
-      }
-    }
+    // ABINIT / ABSMRG: optical depths add
+    double old = 0., unused = 0.;
+    if (!first) merge_regrid(rad_in, nullptr, n_old, f, itype, old, unused);
     rad_out[f] = odv + old;
     if (tr_out) tr_out[f] = 0.;
     return;
   }
   const double xkt = L.tave / kRADCN2;
   const double xkta = tzu / kRADCN2;
+  // EMIN: linear-in-tau source over the layer (src/xmerge.f90:1795-1855)
   T o = (T)odv;
   if (o < (T)-kODLO) o = (T)-kODLO;
   const T tr = exp(-o);
@@ -1642,32 +1658,15 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
   const T bbd = (xkta > 0.) ? planck_t<T>(vi, xkta) - bb : (T)0.;
   T em = ((T)1. - tr) * (bb + bbd * fi);
   if (first) {
+    // EMINIT: boundary emission (:2436-2484)
     if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2) * (T)emis;
     rad_out[f] = (double)em;
     tr_out[f] = (double)tr;
     return;
   }
-  const double dvk = DV;
-  const long itype = (dv_old == dvk) ? 0 : fint(dvk / (dv_old - dvk) + 0.5);
-  const int64_t LL = itype + 1;
-  const int64_t q = f / LL, r = f % LL;
-  auto R = [&](int64_t c) { return rad_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
-  auto TR = [&](int64_t c) { return tr_in[c < 0 ? 0 : (c >= n_old ? n_old - 1 : c)]; };
+  // RADNN (IPATH=1): R = T_layer R_old + E, T = T_layer T_old
   double ro, to;
-  if (itype == 0) {
-    ro = R(f);
-    to = TR(f);
-  } else if (r == 0) {
-    ro = R(q * itype);
-    to = TR(q * itype);
-  } else {
-    const int64_t ipl = q * itype + r - 1;
-    const double P = 1.0 - double(r) / double(LL);
-    const double a1 = -P * (P - 1.0) * (P - 2.0) / 6.0, a2 = (P * P - 1.0) * (P - 2.0) * 0.5;
-    const double a3 = -P * (P + 1.0) * (P - 2.0) * 0.5, a4 = P * (P * P - 1.0) / 6.0;
-    ro = a1 * R(ipl - 1) + a2 * R(ipl) + a3 * R(ipl + 1) + a4 * R(ipl + 2);
-    to = a1 * TR(ipl - 1) + a2 * TR(ipl) + a3 * TR(ipl + 1) + a4 * TR(ipl + 2);
-  }
+  merge_regrid(rad_in, tr_in, n_old, f, itype, ro, to);
   rad_out[f] = (double)tr * ro + (double)em;
   tr_out[f] = (double)tr * to;
 }
@@ -1928,6 +1927,7 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
                          cudaStream_t s, int precision) {
+  if (npts >= (int64_t(1) << 31) || n_old >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
   const unsigned nb = (unsigned)((npts + 255) / 256);
   if (precision == LBL_PREC_SPLIT)
     k_merge<float><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
