@@ -652,6 +652,7 @@ int lbl_set_stream(lbl_ctx* ctx, void* stream) {
 int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   if (!ctx || !L || L->n < 0) return fail(ctx, LBL_E_ARG, "bad lines");
   const int64_t n = L->n;
+  if (n >= (int64_t(1) << 31) - 8) return fail(ctx, LBL_E_RANGE, "more than 2^31 line records");
   if (n > 0 && (!L->vnu || !L->sp || !L->alfa || !L->epp || !L->mol || !L->hwhms ||
                 !L->tmpalf || !L->pshift || !L->iflg))
     return fail(ctx, LBL_E_ARG, "NULL line array");

@@ -205,66 +205,93 @@ struct ShrinkWalk {
   bool started = false;
   double sal = 0., sad = 0., ss = 0., sv = 0., sc = 0.;      // non-CO2 group
   double sal2 = 0., sad2 = 0., ss2 = 0., sv2 = 0., sc2 = 0.; // CO2 group
-  int64_t raw = 0, out = 0;  // lines taken, shrunk lines written
+  int32_t raw = 0, out = 0;  // lines taken, shrunk lines written
 };
 
-// First usable raw line in far slots [from, limit) of the layer (F = slot
-// base), searched by the whole warp 32 slots at a time; its centre in v.
-__device__ bool next_valid_vnu(const Work& w, int64_t F, int64_t from, int64_t limit, double& v) {
+// One layer's raw far-wing lines (LINF4 scaling) and shrunk-line outputs,
+// indexed by 32-bit slot within the layer.
+struct FarSlots {
+  const int8_t *ok, *co2;
+  const double *vnu, *sp, *spp, *alfa, *epp;
+  double *s_vnu, *s_sp, *s_alfa, *s_epp, *s_spp;
+  int8_t* s_co2;
+};
+
+__device__ __forceinline__ FarSlots far_slots(const Work& w, const LayerDev& L) {
+  FarSlots f;
+  const int64_t F = L.off_far, S = L.off_shr;
+  f.ok = w.f_ok + F;
+  f.co2 = w.f_co2 + F;
+  f.vnu = w.f_vnu + F;
+  f.sp = w.f_sp + F;
+  f.spp = w.f_spp + F;
+  f.alfa = w.f_alfa + F;
+  f.epp = w.f_epp + F;
+  f.s_vnu = w.s_vnu + S;
+  f.s_sp = w.s_sp + S;
+  f.s_alfa = w.s_alfa + S;
+  f.s_epp = w.s_epp + S;
+  f.s_spp = w.s_spp + S;
+  f.s_co2 = w.s_co2 + S;
+  return f;
+}
+
+// First usable raw line in slots [from, limit), searched by the whole warp
+// 32 slots at a time; its centre in v.
+__device__ bool next_valid_vnu(const FarSlots& fs, int32_t from, int32_t limit, double& v) {
   const int lane = threadIdx.x & 31;
-  for (int64_t c = from; c < limit; c += 32) {
-    const int64_t s = c + lane;
-    const unsigned m = __ballot_sync(0xffffffffu, s < limit && w.f_ok[F + s]);
+  for (int32_t c = from; c < limit; c += 32) {
+    const int32_t s = c + lane;
+    const unsigned m = __ballot_sync(0xffffffffu, s < limit && fs.ok[s]);
     if (m) {
-      v = __shfl_sync(0xffffffffu, s < limit ? w.f_vnu[F + s] : 0., __ffs(m) - 1);
+      v = __shfl_sync(0xffffffffu, s < limit ? fs.vnu[s] : 0., __ffs(m) - 1);
       return true;
     }
   }
   return false;
 }
 
-// SHRINK (src/oprop.f90:3508-3640) over far slots [a, e) by one warp: the
-// lines are loaded 32 at a time and taken in file order with every lane
-// holding the same walk state.  A group of lines within DVR4/2 of the group
-// limit is merged into one strength-weighted line (non-CO2 and CO2
-// separately); coupled lines pass through.  The group closes when the next
-// usable line (looked up before `limit`) lies beyond the limit.  WRITE
-// stores the shrunk lines at shrunk slot S + out.
+// SHRINK (src/oprop.f90:3508-3640) over slots [a, e) by one warp: the lines
+// are loaded 32 at a time and taken in file order with every lane holding
+// the same walk state.  A group of lines within DVR4/2 of the group limit is
+// merged into one strength-weighted line (non-CO2 and CO2 separately);
+// coupled lines pass through.  The group closes when the next usable line
+// (looked up before `limit`) lies beyond the limit.  WRITE stores the
+// shrunk lines at shrunk slot `out`.
 template <bool WRITE>
-__device__ void shrink_walk(const Work& w, const LayerDev& L, int64_t a, int64_t e, int64_t limit,
-                            int64_t S, ShrinkWalk& st) {
+__device__ void shrink_walk(const FarSlots& fs, const LayerDev& L, int32_t a, int32_t e,
+                            int32_t limit, ShrinkWalk& st) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const double dvh = L.dvr4 / 2.;
-  const int64_t F = L.off_far;
   auto emit = [&](double vnu, double sp, double alfa, double epp, double spp, int co2) {
     if (WRITE && lane == 0) {
-      w.s_vnu[S + st.out] = vnu;
-      w.s_sp[S + st.out] = sp;
-      w.s_alfa[S + st.out] = alfa;
-      w.s_epp[S + st.out] = epp;
-      w.s_spp[S + st.out] = spp;
-      w.s_co2[S + st.out] = (int8_t)co2;
+      fs.s_vnu[st.out] = vnu;
+      fs.s_sp[st.out] = sp;
+      fs.s_alfa[st.out] = alfa;
+      fs.s_epp[st.out] = epp;
+      fs.s_spp[st.out] = spp;
+      fs.s_co2[st.out] = (int8_t)co2;
     }
     st.out++;
   };
-  for (int64_t c = a; c < e; c += 32) {
-    const int64_t s = c + lane;
-    const bool valid = s < e && w.f_ok[F + s];
+  for (int32_t c = a; c < e; c += 32) {
+    const int32_t s = c + lane;
+    const bool valid = s < e && fs.ok[s];
     double v = 0., sp = 0., spp = 0., al = 0., ep = 0.;
     int co2 = 0;
     if (valid) {
-      v = w.f_vnu[F + s];
-      sp = w.f_sp[F + s];
-      spp = w.f_spp[F + s];
+      v = fs.vnu[s];
+      sp = fs.sp[s];
+      spp = fs.spp[s];
       if (sp < 1.0e-35) {
         sp = 0.;
         spp = 0.;
       }
-      co2 = w.f_co2[F + s];
+      co2 = fs.co2[s];
       if (WRITE) {
-        al = w.f_alfa[F + s];
-        ep = w.f_epp[F + s];
+        al = fs.alfa[s];
+        ep = fs.epp[s];
       }
     }
     const unsigned m = __ballot_sync(full, valid);
@@ -287,7 +314,7 @@ __device__ void shrink_walk(const Work& w, const LayerDev& L, int64_t a, int64_t
         hn = true;
       } else {
         // the first usable line after this chunk's part of [a, e)
-        hn = next_valid_vnu(w, F, (c + 32 < e) ? c + 32 : e, limit, vn);
+        hn = next_valid_vnu(fs, (c + 32 < e) ? c + 32 : e, limit, vn);
       }
       if (!st.started) {
         st.vlmt = vi + dvh;
@@ -362,11 +389,13 @@ __global__ void k_shr_count(Work w, const int64_t* bs, const int64_t* blk_base, 
   if (bl >= nb) return;
   int32_t* craw = w.c_raw + (blk_base[l] + bl) * kSegMaxBlk;
   int32_t* cout = w.c_out + (blk_base[l] + bl) * kSegMaxBlk;
-  const int64_t nfar = L.far_hi - L.far_lo;
+  const int32_t nfar = (int32_t)(L.far_hi - L.far_lo);
+  const FarSlots fs = far_slots(w, L);
   ShrinkWalk st;
   int k = 0;
   for (int64_t b = L.fblk_lo + bl; b < L.fblk_hi && k < kSegMaxBlk; b++, k++) {
-    shrink_walk<false>(w, L, far_slot_begin(L, bs, b), far_slot_end(L, bs, b), nfar, 0, st);
+    shrink_walk<false>(fs, L, (int32_t)far_slot_begin(L, bs, b), (int32_t)far_slot_end(L, bs, b),
+                       nfar, st);
     // the segment's raw and output counts were it closed at this block's end
     if (lane == 0) {
       craw[k] = (int32_t)st.raw;
@@ -441,9 +470,9 @@ __global__ void k_shr_write(Work w, const int64_t* bs, const int64_t* seg_base, 
   const int64_t b0 = L.fblk_lo + w.seg_blk[L.off_seg + sgi];
   const int64_t b1 = b0 + w.seg_nblk[L.off_seg + sgi];
   ShrinkWalk st;
-  st.out = w.seg_out[L.off_seg + sgi];
-  const int64_t e = far_slot_end(L, bs, b1 - 1);
-  shrink_walk<true>(w, L, far_slot_begin(L, bs, b0), e, e, L.off_shr, st);
+  st.out = (int32_t)w.seg_out[L.off_seg + sgi];
+  const int32_t e = (int32_t)far_slot_end(L, bs, b1 - 1);
+  shrink_walk<true>(far_slots(w, L), L, (int32_t)far_slot_begin(L, bs, b0), e, e, st);
 }
 
 // =========================================================================
@@ -1003,8 +1032,9 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
   const int npanel = (int)L.npanel;
   bool stopped = false;
   for (int64_t b = L.blk_lo; b < L.blk_hi; b++) {
-    int64_t a = ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo;
-    int64_t e = ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi;
+    // 32-bit line indices (the line file holds fewer than 2^31 records)
+    const int32_t a = (int32_t)(ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo);
+    const int32_t e = (int32_t)(ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi);
     const int pread = s_pread;
     const double VFT = w.vft[L.off_panel + pread];
     const int wi = L.nwin > 0 ? w.win_of[L.off_panel + pread] : -1;
@@ -1013,12 +1043,12 @@ __global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
       s_stop_at = 1 << 30;
     }
     __syncthreads();
-    const int64_t i = a + threadIdx.x;
+    const int32_t i = a + (int32_t)threadIdx.x;
     int pfit = -1;
     bool ok = false;
     unsigned long long ntrip = 0;
     double zslope = 0., bhw = 0., vline = 0.;
-    int64_t slot = i - L.near_lo + L.off_near;
+    const int64_t slot = (int64_t)(i - (int32_t)L.near_lo) + L.off_near;
     if (i < e && !stopped && ln.iflg[i] >= 0) {
       const int mcode = ln.mol[i];
       const int m = mcode % 100, iso = (mcode % 1000) / 100;
