@@ -86,6 +86,11 @@ struct lbl_ctx {
   // pinned copies of the device status and work counters, read after the
   // caller's final synchronisation
   int32_t* h_stat = nullptr;
+  // pinned image of the plan tables and the event of its last upload
+  char* stage_host = nullptr;
+  size_t stage_cap = 0;
+  cudaEvent_t stage_ev = nullptr;
+  bool stage_ev_set = false;
   unsigned long long* h_cnt = nullptr;
   bool have_lines = false;
   // tables
@@ -288,6 +293,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<WinDev>(std::max<int64_t>(o_win, 1));
   lay.add<int32_t>(std::max<int64_t>(o_win, 1));
   lay.add<int32_t>(std::max<int64_t>(o_win, 1));
+  lay.add<int64_t>(n + 1);
   lay.add<double>(std::max<int64_t>(o_win, 1) * kR4Stride);
   for (int k = 0; k < 5; k++) lay.add<double>(o_far + 1);
   lay.add<int8_t>(o_far + 1);
@@ -316,7 +322,6 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<int32_t>(nbt);
   lay.add<int64_t>(nbt);
   lay.add<int64_t>(n);
-  lay.add<int64_t>(n + 1);
   lay.add<unsigned long long>(8);
   CK(ctx->arena.reserve(lay.bytes + 4096));
   Arena& A = ctx->arena;
@@ -330,6 +335,9 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   WinDev* d_win = A.take<WinDev>(std::max<int64_t>(o_win, 1));
   B.d_win_layer = A.take<int32_t>(std::max<int64_t>(o_win, 1));
   B.d_win_order = A.take<int32_t>(std::max<int64_t>(o_win, 1));
+  B.d_blk_base = A.take<int64_t>(n + 1);
+  // everything up to here is the plan, uploaded in one copy
+  const size_t upload_bytes = (size_t)(reinterpret_cast<char*>(B.d_blk_base + n + 1) - A.base);
   w.r4 = A.take<double>(std::max<int64_t>(o_win, 1) * kR4Stride);
   w.f_vnu = A.take<double>(o_far + 1);
   w.f_sp = A.take<double>(o_far + 1);
@@ -370,27 +378,45 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   w.seg_nblk = A.take<int32_t>(nbt);
   w.seg_out = A.take<int64_t>(nbt);
   w.seg_count = A.take<int64_t>(n);
-  B.d_blk_base = A.take<int64_t>(n + 1);
   w.counters = A.take<unsigned long long>(8);
   w.L = B.d_ld;
   w.nlay = n;
   w.vft = d_vft;
   w.win_of = d_win_of;
   w.win = d_win;
-  // host-side staging of the plan tables
-  std::vector<double> h_vft(o_pan);
-  std::vector<int32_t> h_wof(o_pan), h_play(o_pan), h_wlay(std::max<int64_t>(o_win, 1));
-  std::vector<int64_t> h_pbase(n + 1);
-  std::vector<WinDev> h_win(std::max<int64_t>(o_win, 1));
+  // The plan tables are written into a pinned host image of the start of
+  // the arena and sent in one copy; the image is reused once the previous
+  // call's copy has completed.
+  cudaStream_t s = ctx->stream;
+  if (ctx->stage_ev_set) CK(cudaEventSynchronize(ctx->stage_ev));
+  if (upload_bytes > ctx->stage_cap) {
+    if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
+    ctx->stage_host = nullptr;
+    ctx->stage_cap = 0;
+    void* hp = nullptr;
+    CK(cudaMallocHost(&hp, upload_bytes));
+    ctx->stage_host = static_cast<char*>(hp);
+    ctx->stage_cap = upload_bytes;
+  }
+  auto host = [&](const void* dptr) {
+    return ctx->stage_host + (reinterpret_cast<const char*>(dptr) - A.base);
+  };
+  std::memcpy(host(B.d_ld), B.ld.data(), sizeof(LayerDev) * n);
+  double* h_vft = reinterpret_cast<double*>(host(d_vft));
+  int32_t* h_wof = reinterpret_cast<int32_t*>(host(d_win_of));
+  int32_t* h_play = reinterpret_cast<int32_t*>(host(B.d_panel_layer));
+  int64_t* h_pbase = reinterpret_cast<int64_t*>(host(B.d_panel_base));
+  WinDev* h_win = reinterpret_cast<WinDev*>(host(d_win));
+  int32_t* h_wlay = reinterpret_cast<int32_t*>(host(B.d_win_layer));
+  int32_t* h_word = reinterpret_cast<int32_t*>(host(B.d_win_order));
+  std::memcpy(host(B.d_blk_base), blk_base.data(), sizeof(int64_t) * (n + 1));
   for (int l = 0; l < n; l++) {
     const LayerPlan& P = B.plans[l];
     const LayerDev& d = B.ld[l];
     h_pbase[l] = d.off_panel;
-    for (int64_t p = 0; p < d.npanel; p++) {
-      h_vft[d.off_panel + p] = P.vft[p];
-      h_wof[d.off_panel + p] = P.win_of[p];
-      h_play[d.off_panel + p] = l;
-    }
+    std::memcpy(h_vft + d.off_panel, P.vft.data(), sizeof(double) * d.npanel);
+    std::memcpy(h_wof + d.off_panel, P.win_of.data(), sizeof(int32_t) * d.npanel);
+    std::fill(h_play + d.off_panel, h_play + d.off_panel + d.npanel, l);
     for (int k = 0; k < d.nwin; k++) {
       h_win[d.off_win + k] = P.win[k];
       h_wlay[d.off_win + k] = l;
@@ -401,7 +427,6 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   // ones do not start last.  Cost estimate: lines within the window's reach
   // (each is decided in order) times a fixed per-line decision cost plus the
   // points one line covers.
-  std::vector<int32_t> h_word(std::max<int64_t>(o_win, 1), 0);
   {
     std::vector<double> cost(o_win);
     const double* vb = ctx->h_vnu.data();
@@ -414,30 +439,14 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
       cost[k] = nl * (span + 8000.);
       h_word[k] = (int32_t)k;
     }
-    std::stable_sort(h_word.begin(), h_word.begin() + o_win,
+    std::stable_sort(h_word, h_word + o_win,
                      [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
   }
-  cudaStream_t s = ctx->stream;
-  CK(cudaMemcpyAsync(B.d_ld, B.ld.data(), sizeof(LayerDev) * n, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(d_vft, h_vft.data(), sizeof(double) * o_pan, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(d_win_of, h_wof.data(), sizeof(int32_t) * o_pan, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(B.d_panel_layer, h_play.data(), sizeof(int32_t) * o_pan,
-                     cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(B.d_panel_base, h_pbase.data(), sizeof(int64_t) * (n + 1),
-                     cudaMemcpyHostToDevice, s));
-  if (o_win > 0) {
-    CK(cudaMemcpyAsync(d_win, h_win.data(), sizeof(WinDev) * o_win, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(B.d_win_order, h_word.data(), sizeof(int32_t) * o_win,
-                       cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(B.d_win_layer, h_wlay.data(), sizeof(int32_t) * o_win,
-                       cudaMemcpyHostToDevice, s));
-  }
-  CK(cudaMemcpyAsync(B.d_blk_base, blk_base.data(), sizeof(int64_t) * (n + 1),
-                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(A.base, ctx->stage_host, upload_bytes, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->stage_ev, s));
+  ctx->stage_ev_set = true;
   CK(cudaMemsetAsync(w.status, 0, 4 * sizeof(int32_t), s));
   CK(cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), s));
-  // the host vectors must live until the copies finish
-  CK(cudaStreamSynchronize(s));
   if (ctx->prof)
     ctx->stage("host_plan").ms +=
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host)
@@ -592,6 +601,11 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
   }
   std::memset(hs, 0, 64 + 8 * sizeof(unsigned long long));
   ctx->h_stat = static_cast<int32_t*>(hs);
+  if (cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaFreeHost(hs);
+    delete ctx;
+    return LBL_E_CUDA;
+  }
   ctx->h_cnt = reinterpret_cast<unsigned long long*>(static_cast<char*>(hs) + 64);
   ShapeTables* t = new ShapeTables;
   build_shape_tables(t);
@@ -629,6 +643,8 @@ int lbl_ctx_destroy(lbl_ctx* ctx) {
   if (!ctx) return LBL_E_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->h_stat) cudaFreeHost(ctx->h_stat);
+  if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
+  if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
   if (ctx->jac_mem) cudaFree(ctx->jac_mem);
   if (ctx->line_mem) cudaFree(ctx->line_mem);
   if (ctx->shape_mem) cudaFree(ctx->shape_mem);
