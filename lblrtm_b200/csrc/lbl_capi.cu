@@ -550,20 +550,39 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
   for (auto& d : B.ld) mx = std::max<size_t>(mx, d.npts);
   int rc = ensure_merge_buffers(ctx, mx + 8);
   if (rc) return rc;
+  // Consecutive layers on one grid go to one launch (at most kMergeRunMax).
+  std::vector<std::pair<int, int>> runs;
+  for (int l = 0; l < n;) {
+    const LayerDev& d = B.ld[l];
+    if (l > 0 && d.dv > B.ld[l - 1].dv) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
+    int e = l + 1;
+    while (e < n && e - l < kMergeRunMax && B.ld[e].dv == d.dv && B.ld[e].npts == d.npts) e++;
+    runs.push_back({l, e});
+    l = e;
+  }
   int cur = 0;
   double dv_old = 0.;
   int64_t n_old = 0;
-  StageTimer tm(ctx, "merge", n);
-  for (int l = 0; l < n; l++) {
+  StageTimer tm(ctx, "merge", (int64_t)runs.size());
+  for (auto [l, e] : runs) {
     const LayerDev& d = B.ld[l];
-    ctx->stage("merge").work += (double)d.npts;
+    if (n_old >= (int64_t(1) << 31)) return fail(ctx, LBL_E_RANGE, "layer grid of 2^31 or more points");
+    MergeRun m{};
+    m.nl = e - l;
+    m.first = (l == 0);
+    m.itype = (l == 0 || dv_old == d.dv) ? 0 : (int32_t)(long)(d.dv / (dv_old - d.dv) + 0.5);
+    m.n_old = (int32_t)n_old;
+    for (int k = l; k < e; k++) {
+      m.od_off[k - l] = B.ld[k].off_od;
+      m.tave[k - l] = B.ld[k].tave;
+      m.tzu[k - l] = layers[k].tzu;
+      ctx->stage("merge").work += (double)B.ld[k].npts;
+    }
     const int nxt = cur ^ 2;
     const double tbnd = (l == 0 && R.ipathl == 1) ? R.tmpbnd : 0.;
-    CK(launch_merge(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
-                    dv_old, n_old, ctx->mbuf[cur], ctx->mbuf[cur + 1], ctx->mbuf[nxt],
-                    ctx->mbuf[nxt + 1], tbnd, R.bndemi, R.iemit, layers[l].tzu, ctx->stream,
-                    precision));
-    if (l > 0 && d.dv > dv_old) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
+    CK(launch_merge_run(m, B.w.vft + d.off_panel, B.w.od, d.npts, d.dv, ctx->mbuf[cur],
+                        ctx->mbuf[cur + 1], ctx->mbuf[nxt], ctx->mbuf[nxt + 1], tbnd, R.bndemi,
+                        R.iemit, ctx->stream, precision));
     cur = nxt;
     dv_old = d.dv;
     n_old = d.npts;

@@ -203,8 +203,9 @@ __global__ void k_far_scale(Work w, DevLines ln) {
 struct ShrinkWalk {
   double vlmt = 0.;
   bool started = false;
-  double sal = 0., sad = 0., ss = 0., sv = 0., sc = 0.;      // non-CO2 group
-  double sal2 = 0., sad2 = 0., ss2 = 0., sv2 = 0., sc2 = 0.; // CO2 group
+  bool pn = false, pc = false;  // the open group holds a line of positive strength
+  double sal = 0., sad = 0., ss = 0., sv = 0.;      // open non-CO2 group (WRITE)
+  double sal2 = 0., sad2 = 0., ss2 = 0., sv2 = 0.;  // open CO2 group (WRITE)
   int32_t raw = 0, out = 0;  // lines taken, shrunk lines written
 };
 
@@ -251,30 +252,28 @@ __device__ bool next_valid_vnu(const FarSlots& fs, int32_t from, int32_t limit, 
   return false;
 }
 
-// SHRINK (src/oprop.f90:3508-3640) over slots [a, e) by one warp: the lines
-// are loaded 32 at a time and taken in file order with every lane holding
-// the same walk state.  A group of lines within DVR4/2 of the group limit is
-// merged into one strength-weighted line (non-CO2 and CO2 separately);
-// coupled lines pass through.  The group closes when the next usable line
-// (looked up before `limit`) lies beyond the limit.  WRITE stores the
-// shrunk lines at shrunk slot `out`.
+// SHRINK (src/oprop.f90:3508-3640) over slots [a, e) by one warp, 32
+// slots at a time.  A group takes lines in file order while the next usable
+// line (looked up before `limit`) lies within the group limit; the line
+// where it does not closes the group and sets the next limit to its own
+// centre + DVR4/2.  Non-CO2 and CO2 lines of a group are merged separately
+// into strength-weighted lines (emitted when the group holds a line of
+// positive strength); coupled lines pass through where they stand.
+//   * closures: found in order with one ballot each against the limit the
+//     previous closure set (warp-uniform state);
+//   * sums (WRITE): the lane that ends a group adds its lines in file order
+//     (the walk's own order), starting from the sums carried over from the
+//     previous chunk when the group began there;
+//   * outputs: every lane's count (coupled line, group lines) is prefix-
+//     summed over the warp, so the shrunk lines land in walk order at
+//     shrunk slot `out`.
 template <bool WRITE>
 __device__ void shrink_walk(const FarSlots& fs, const LayerDev& L, int32_t a, int32_t e,
                             int32_t limit, ShrinkWalk& st) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
   const double dvh = L.dvr4 / 2.;
-  auto emit = [&](double vnu, double sp, double alfa, double epp, double spp, int co2) {
-    if (WRITE && lane == 0) {
-      fs.s_vnu[st.out] = vnu;
-      fs.s_sp[st.out] = sp;
-      fs.s_alfa[st.out] = alfa;
-      fs.s_epp[st.out] = epp;
-      fs.s_spp[st.out] = spp;
-      fs.s_co2[st.out] = (int8_t)co2;
-    }
-    st.out++;
-  };
   for (int32_t c = a; c < e; c += 32) {
     const int32_t s = c + lane;
     const bool valid = s < e && fs.ok[s];
@@ -295,61 +294,102 @@ __device__ void shrink_walk(const FarSlots& fs, const LayerDev& L, int32_t a, in
       }
     }
     const unsigned m = __ballot_sync(full, valid);
-    for (unsigned bits = m; bits; bits &= bits - 1) {
-      const int i = __ffs(bits) - 1;
-      const double vi = __shfl_sync(full, v, i);
-      const double spi = __shfl_sync(full, sp, i);
-      const double sppi = __shfl_sync(full, spp, i);
-      const int co2i = __shfl_sync(full, co2, i);
-      double ali = 0., epi = 0.;
-      if (WRITE) {
-        ali = __shfl_sync(full, al, i);
-        epi = __shfl_sync(full, ep, i);
-      }
-      const unsigned rest = bits & (bits - 1);
-      double vn = 0.;
-      bool hn;
-      if (rest) {
-        vn = __shfl_sync(full, v, __ffs(rest) - 1);
-        hn = true;
-      } else {
-        // the first usable line after this chunk's part of [a, e)
-        hn = next_valid_vnu(fs, (c + 32 < e) ? c + 32 : e, limit, vn);
-      }
-      if (!st.started) {
-        st.vlmt = vi + dvh;
-        st.started = true;
-      }
-      st.raw++;
-      if (sppi != 0.0) {
-        emit(vi, spi, ali, epi, sppi, co2i);
-      } else if (!co2i) {
-        st.sv = st.sv + vi * spi;
-        st.ss = st.ss + spi;
-        st.sal = st.sal + spi * ali;
-        st.sad = st.sad + spi * epi;
-        st.sc = st.sc + sppi;
-      } else {
-        st.sv2 = st.sv2 + vi * spi;
-        st.ss2 = st.ss2 + spi;
-        st.sal2 = st.sal2 + spi * ali;
-        st.sad2 = st.sad2 + spi * epi;
-        st.sc2 = st.sc2 + sppi;
-      }
-      if (!(hn && vn <= st.vlmt)) {
-        st.vlmt = vi + dvh;
-        if (st.ss > 0.) {
-          if (WRITE) emit(st.sv / st.ss, st.ss, st.sal / st.ss, st.sad / st.ss, st.sc, 0);
-          else st.out++;
-          st.sal = st.sad = st.ss = st.sv = st.sc = 0.;
-        }
-        if (st.ss2 > 0.) {
-          if (WRITE) emit(st.sv2 / st.ss2, st.ss2, st.sal2 / st.ss2, st.sad2 / st.ss2, st.sc2, 1);
-          else st.out++;
-          st.sal2 = st.sad2 = st.ss2 = st.sv2 = st.sc2 = 0.;
-        }
-      }
+    if (!m) continue;
+    const int first = __ffs(m) - 1, last = 31 - __clz(m);
+    // centre of the next usable line (after the chunk for the last lane)
+    const unsigned up = m & ~(below | (1u << lane));
+    double vn = __shfl_sync(full, v, up ? __ffs(up) - 1 : lane);
+    bool hn = up != 0;
+    double vx = 0.;
+    const bool hx = next_valid_vnu(fs, (c + 32 < e) ? c + 32 : e, limit, vx);
+    if (lane == last) {
+      hn = hx;
+      vn = vx;
     }
+    if (!st.started) {
+      st.vlmt = __shfl_sync(full, v, first) + dvh;
+      st.started = true;
+    }
+    st.raw += __popc(m);
+    unsigned cl = 0;  // lanes that close a group
+    for (int pos = first; pos <= last;) {
+      const unsigned q = __ballot_sync(full, valid && lane >= pos && !(hn && vn <= st.vlmt));
+      if (!q) break;
+      const int k = __ffs(q) - 1;
+      cl |= 1u << k;
+      st.vlmt = __shfl_sync(full, v, k) + dvh;
+      pos = k + 1;
+    }
+    const bool cpl = valid && spp != 0.;
+    const unsigned mN = __ballot_sync(full, valid && !cpl && !co2 && sp > 0.);
+    const unsigned mC = __ballot_sync(full, valid && !cpl && co2 && sp > 0.);
+    const bool isc = (cl >> lane) & 1u;
+    const bool ends = isc || (lane == last);  // a closure or the chunk's open tail
+    const unsigned prevs = cl & below;
+    const int gs = prevs ? 32 - __clz(prevs) : 0;  // first lane of this lane's group
+    const unsigned rng = (lane == 31 ? full : ((2u << lane) - 1u)) & ~((1u << gs) - 1u);
+    const bool carry = prevs == 0;  // the group began before this chunk
+    const bool gN = ends && (((mN & rng) != 0u) || (carry && st.pn));
+    const bool gC = ends && (((mC & rng) != 0u) || (carry && st.pc));
+    const int ec = (cpl ? 1 : 0) + (isc ? (gN ? 1 : 0) + (gC ? 1 : 0) : 0);
+    const unsigned b0 = __ballot_sync(full, ec & 1), b1 = __ballot_sync(full, ec & 2);
+    const bool open = !((cl >> last) & 1u);
+    if (WRITE) {
+      double sv = 0., ss = 0., sal = 0., sad = 0., sv2 = 0., ss2 = 0., sal2 = 0., sad2 = 0.;
+      if (ends && carry) {
+        sv = st.sv; ss = st.ss; sal = st.sal; sad = st.sad;
+        sv2 = st.sv2; ss2 = st.ss2; sal2 = st.sal2; sad2 = st.sad2;
+      }
+      const int len = ends ? lane - gs + 1 : 0;
+      const int maxlen = __reduce_max_sync(full, (unsigned)len);
+      const int kind = (valid && !cpl) ? (co2 ? 2 : 1) : 0;
+      for (int t = 0; t < maxlen; t++) {
+        const int src = (gs + t) & 31;
+        const double vi = __shfl_sync(full, v, src);
+        const double spi = __shfl_sync(full, sp, src);
+        const double ali = __shfl_sync(full, al, src);
+        const double epi = __shfl_sync(full, ep, src);
+        const int ki = __shfl_sync(full, kind, src);
+        if (t < len) {
+          if (ki == 1) {
+            sv = sv + vi * spi;
+            ss = ss + spi;
+            sal = sal + spi * ali;
+            sad = sad + spi * epi;
+          } else if (ki == 2) {
+            sv2 = sv2 + vi * spi;
+            ss2 = ss2 + spi;
+            sal2 = sal2 + spi * ali;
+            sad2 = sad2 + spi * epi;
+          }
+        }
+      }
+      int o = st.out + __popc(b0 & below) + 2 * __popc(b1 & below);
+      auto put = [&](double vnu, double spv, double alfa, double epp, double sppv, int c2) {
+        fs.s_vnu[o] = vnu;
+        fs.s_sp[o] = spv;
+        fs.s_alfa[o] = alfa;
+        fs.s_epp[o] = epp;
+        fs.s_spp[o] = sppv;
+        fs.s_co2[o] = (int8_t)c2;
+        o++;
+      };
+      if (cpl) put(v, sp, al, ep, spp, co2);
+      if (isc && gN) put(sv / ss, ss, sal / ss, sad / ss, 0., 0);
+      if (isc && gC) put(sv2 / ss2, ss2, sal2 / ss2, sad2 / ss2, 0., 1);
+      st.sv = open ? __shfl_sync(full, sv, last) : 0.;
+      st.ss = open ? __shfl_sync(full, ss, last) : 0.;
+      st.sal = open ? __shfl_sync(full, sal, last) : 0.;
+      st.sad = open ? __shfl_sync(full, sad, last) : 0.;
+      st.sv2 = open ? __shfl_sync(full, sv2, last) : 0.;
+      st.ss2 = open ? __shfl_sync(full, ss2, last) : 0.;
+      st.sal2 = open ? __shfl_sync(full, sal2, last) : 0.;
+      st.sad2 = open ? __shfl_sync(full, sad2, last) : 0.;
+    }
+    st.out += __popc(b0) + 2 * __popc(b1);
+    const bool pn = __shfl_sync(full, gN, last), pc = __shfl_sync(full, gC, last);
+    st.pn = open && pn;
+    st.pc = open && pc;
   }
 }
 
@@ -399,7 +439,7 @@ __global__ void k_shr_count(Work w, const int64_t* bs, const int64_t* blk_base, 
     // the segment's raw and output counts were it closed at this block's end
     if (lane == 0) {
       craw[k] = (int32_t)st.raw;
-      cout[k] = (int32_t)(st.out + (st.ss > 0.) + (st.ss2 > 0.));
+      cout[k] = (int32_t)(st.out + (st.pn ? 1 : 0) + (st.pc ? 1 : 0));
     }
     if (st.raw >= 1000) {
       k++;
@@ -1701,6 +1741,51 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
   tr_out[f] = (double)tr * to;
 }
 
+// k_merge over m.nl consecutive layers on one grid (each layer's arithmetic
+// as in k_merge, in the same order); the next layer's optical depth is
+// fetched while this one merges.
+template <typename T>
+__global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const double* vft_panel,
+                                                   const double* od, int32_t npts, double DV,
+                                                   const double* rad_in, const double* tr_in,
+                                                   double* rad_out, double* tr_out, double tbnd,
+                                                   double emis, int iemit) {
+  const int32_t f = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (f >= npts) return;
+  const int32_t p = f / 2400;
+  const double vi = (vft_panel[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
+  double ro = 0., to = 1.;
+  if (!m.first) merge_regrid(rad_in, iemit ? tr_in : nullptr, m.n_old, f, m.itype, ro, to);
+  double odn = od[m.od_off[0] + f];
+  for (int l = 0; l < m.nl; l++) {
+    const double odv = odn;
+    if (l + 1 < m.nl) odn = od[m.od_off[l + 1] + f];
+    if (iemit == 0) {
+      ro = (m.first && l == 0) ? odv : odv + ro;
+      continue;
+    }
+    const double xkt = m.tave[l] / kRADCN2;
+    const double xkta = m.tzu[l] / kRADCN2;
+    T o = (T)odv;
+    if (o < (T)-kODLO) o = (T)-kODLO;
+    const T tr = exp(-o);
+    const T fi = (o <= (T)kODLO) ? o / (T)6. : (T)1. - (T)2. * (tr / (tr - (T)1.) + (T)1. / o);
+    const T bb = planck_t<T>(vi, xkt);
+    const T bbd = (xkta > 0.) ? planck_t<T>(vi, xkta) - bb : (T)0.;
+    T em = ((T)1. - tr) * (bb + bbd * fi);
+    if (m.first && l == 0) {
+      if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2) * (T)emis;
+      ro = (double)em;
+      to = (double)tr;
+    } else {
+      ro = (double)tr * ro + (double)em;
+      to = (double)tr * to;
+    }
+  }
+  rad_out[f] = ro;
+  if (tr_out) tr_out[f] = iemit ? to : 0.;
+}
+
 // =========================================================================
 // Radiance Jacobians (the reference's analytic-Jacobian path, EMDT/EMADMG
 // src/xmerge.f90:4406-5782 with TDERIVup/QDERIVup :5786-6144): the forward
@@ -1965,6 +2050,23 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
   else
     k_merge<double><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
                                        rad_out, tr_out, tbnd, emis, iemit, tzu);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const double* od,
+                             int64_t npts, double dv, const double* rad_in, const double* tr_in,
+                             double* rad_out, double* tr_out, double tbnd, double emis, int iemit,
+                             cudaStream_t s, int precision) {
+  if (m.nl < 1 || m.nl > kMergeRunMax) return cudaErrorInvalidValue;
+  if (npts >= (int64_t(1) << 31) || m.n_old < 0) return cudaErrorInvalidValue;
+  if (npts <= 0) return cudaSuccess;
+  const unsigned nb = (unsigned)((npts + 255) / 256);
+  if (precision == LBL_PREC_SPLIT)
+    k_merge_run<float><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)npts, dv, rad_in, tr_in,
+                                          rad_out, tr_out, tbnd, emis, iemit);
+  else
+    k_merge_run<double><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)npts, dv, rad_in, tr_in,
+                                           rad_out, tr_out, tbnd, emis, iemit);
   return cudaGetLastError();
 }
 

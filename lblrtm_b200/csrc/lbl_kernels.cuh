@@ -99,6 +99,24 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
                          cudaStream_t s, int precision = LBL_PREC_FP64);
+// Consecutive layers on one grid merged in one pass: the first may be the
+// bottom layer (EMINIT) or regrid the field below it (RADNN ITYPE>0); the
+// rest share its grid, so the radiance and transmittance stay in registers
+// from layer to layer and each layer's optical depth is read once.
+constexpr int kMergeRunMax = 32;
+struct MergeRun {
+  int32_t nl;                    // layers in this launch (1..kMergeRunMax)
+  int32_t first;                 // the launch starts at the bottom layer
+  int32_t itype;                 // regrid of the incoming field (0: same grid)
+  int32_t n_old;                 // points of the incoming field
+  int64_t od_off[kMergeRunMax];  // each layer's optical depths in Work::od
+  double tave[kMergeRunMax];
+  double tzu[kMergeRunMax];
+};
+cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const double* od,
+                             int64_t npts, double dv, const double* rad_in, const double* tr_in,
+                             double* rad_out, double* tr_out, double tbnd, double emis, int iemit,
+                             cudaStream_t s, int precision);
 // Radiance Jacobians: one layer's forward merge plus its derivative rows,
 // the carrying of lower layers' rows through one merge step, the top
 // segment's transmittance products, and a central difference.

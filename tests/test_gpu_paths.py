@@ -73,6 +73,32 @@ def test_forward_batch_matches_single_profiles(gpu_ctx):
         assert np.array_equal(tr, tref)
 
 
+@pytest.mark.parametrize("iemit", [1, 0])
+def test_forward_merge_runs_match_layer_by_layer(gpu_ctx, iemit):
+    """lbl_forward merges consecutive layers on one grid in one launch; on
+    this 70-layer profile the top 39 layers share a grid, so that run is
+    split into launches of 32 and 7.  The result must be lbl_merge_layer
+    applied layer by layer (optical depths from lbl_layer_od with the JRAD
+    chain the forward uses)."""
+    cfg = configs.config1(nlines=3000)
+    gpu_ctx.upload_lines(abi.LinesHandle(cfg["lines"]))
+    run = abi.make_run(v1=600.0, v2=700.0, iemit=iemit, ilblf4=1, tmpbnd=290.0, bndemi=0.98)
+    lays = abi.make_layers(configs.atmosphere(70))
+    dv, _ = gpu.dv_rule(run, lays)
+    assert max(sum(1 for d in dv if d == x) for x in set(dv)) > 32
+    rad = tr = None
+    dv_old = 0.0
+    j = run.jrad
+    for l in range(len(lays)):
+        od, j = gpu_ctx.layer_od(run, lays[l], jrad=j)
+        rad, tr = gpu_ctx.merge_layer(run, lays[l], l == 0, dv_old, rad, tr, od)
+        dv_old = lays[l].dv
+    frad, ftr = gpu_ctx.forward(run, abi.make_layers_like(lays))
+    assert len(frad) == len(rad)
+    assert np.max(np.abs(frad - rad) / np.abs(rad)) < 1e-12
+    assert np.max(np.abs(ftr - tr)) < 1e-12
+
+
 def coupled_lines(n, v1, v2, seed, frac=0.05):
     """Synthetic lines where a fraction carry line coupling: IFLG=1 (Y, G) or
     IFLG=3 (width coefficients), each followed by its coefficient record
