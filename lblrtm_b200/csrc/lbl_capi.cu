@@ -310,6 +310,9 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<double>(o_near + 1);
   for (int k = 0; k < 5; k++) lay.add<int32_t>(o_near + 1);
   lay.add<int8_t>(o_near + 1);
+  lay.add<double>(o_near + 1);
+  lay.add<double>(o_near + 1);
+  lay.add<int8_t>(o_near + 1);
   lay.add<double>(o_abs);
   lay.add<double>(o_od);
   lay.add<int64_t>(2 * o_pan + 2);
@@ -366,6 +369,9 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   w.n_j3 = A.take<int32_t>(o_near + 1);
   w.n_pconv = A.take<int32_t>(o_near + 1);
   w.n_ok = A.take<int8_t>(o_near + 1);
+  w.n_reach = A.take<double>(o_near + 1);
+  w.n_speak = A.take<double>(o_near + 1);
+  w.n_pre = A.take<int8_t>(o_near + 1);
   w.absrb = A.take<double>(o_abs);
   w.od = A.take<double>(o_od);
   B.d_panel_rng = A.take<int64_t>(2 * o_pan + 2);
@@ -471,8 +477,16 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     CK(launch_far_wing(w, B.nwin_total, B.d_win_order, B.d_win_layer, precision, s));
   }
   {
-    StageTimer t(ctx, "near_scale", 1);
-    CK(launch_near_scale(w, ctx->dl, s));
+    StageTimer t(ctx, "near_scale", 2);
+    int64_t max_near = 0, max_panel = 0, max_win = 0;
+    for (const LayerDev& d : B.ld) {
+      max_near = std::max<int64_t>(max_near, d.near_hi - d.near_lo);
+      max_panel = std::max<int64_t>(max_panel, d.npanel);
+      max_win = std::max<int64_t>(max_win, d.nwin);
+    }
+    if (near_walk_smem(max_panel, max_win) > kNearWalkSmemMax)
+      return fail(ctx, LBL_E_RANGE, "layer grid too long for the near-wing panel walk");
+    CK(launch_near_scale(w, ctx->dl, max_near, max_panel, max_win, s));
   }
   if (R.icntnm) {
     if (!ctx->have_ck) return fail(ctx, LBL_E_NOTREADY, "continuum table not uploaded");
@@ -574,8 +588,7 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     m.n_old = (int32_t)n_old;
     for (int k = l; k < e; k++) {
       m.od_off[k - l] = B.ld[k].off_od;
-      m.tave[k - l] = B.ld[k].tave;
-      m.tzu[k - l] = layers[k].tzu;
+      m.t[k - l] = emin_temps(B.ld[k].tave, layers[k].tzu);
       ctx->stage("merge").work += (double)B.ld[k].npts;
     }
     const int nxt = cur ^ 2;

@@ -20,8 +20,6 @@ namespace lbl {
 
 namespace {
 
-constexpr double kRADCN1 = 1.191042722E-12;  // src/phys_consts.f90:73
-constexpr double kRADCN2 = 1.4387752;        // src/phys_consts.f90:74
 constexpr double kONEPL = 1.001, kONEMI = 0.999;
 constexpr double kHWDXF = 4. / 0.002;        // HWF1/DXF1
 constexpr double kODLO = 0.06;               // od_lo, src/lblparams.f90:47
@@ -88,15 +86,16 @@ __device__ double radfni(double vi, double dvi, double xkt, double& vinew, doubl
   return out;
 }
 
-// Planck function (PLANCK, src/xmerge.f90:968-1017)
-__device__ __forceinline__ double planck(double vi, double xkt) {
+// Planck function (PLANCK, src/xmerge.f90:968-1017) at XKT = T/RADCN2,
+// with the exponent's argument VI/XKT taken as VI*rk (rk = RADCN2/T).
+__device__ __forceinline__ double planck(double vi, double xkt, double rk) {
   double v = 0.;
   if (xkt > 0.0) {
-    double x = vi / xkt;
+    const double x = vi * rk;
     if (x < 1e-2) {
       v = (vi * vi) * xkt / (1. + 0.5 * x);
     } else if (x <= 80.) {
-      double e = exp(-x);
+      const double e = exp(-x);
       v = (vi * vi * vi) * e / (1. - e);
     }
   }
@@ -1058,147 +1057,217 @@ __device__ int block_max_scan(int v, int* sh) {
   return r;
 }
 
-__global__ void __launch_bounds__(256) k_near_scale(Work w, DevLines ln) {
+// RDLIN/LNCOR1 per near-wing line and layer, everything that does not
+// depend on the TAPE3 panel being read (src/oprop.f90:678-1197): strength
+// scaling and rejection, widths, the Voigt interpolation index and the
+// CNVFNV sub-function strengths (written to their final slots), the reach
+// 64 ALFV + VNU of the VFT cut and the peak SPEAK of the R4 test.  Flags:
+// bit 0 the line survives these tests, bit 1 it is subject to the R4 test.
+// The shifted centre waits in n_zint for k_near_walk.
+__global__ void __launch_bounds__(256) k_near_lines(Work w, DevLines ln) {
+  const int l = blockIdx.y;
+  const LayerDev& L = w.L[l];
+  const int32_t k = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+  const int32_t nn = (int32_t)(L.near_hi - L.near_lo);
+  if (k >= nn) return;
+  const int32_t i = (int32_t)L.near_lo + k;
+  const int64_t slot = (int64_t)k + L.off_near;
+  const double DV = L.dv;
+  int8_t fl = 0;
+  if (ln.iflg[i] >= 0) {
+    const int mcode = ln.mol[i];
+    const int m = mcode % 100, iso = (mcode % 1000) / 100;
+    double sui = 0.;
+    bool rej = !(m >= 1 && m <= 47 && iso >= 1 && iso <= c_isomax[m]);
+    if (!rej) {
+      const double wkm = (m <= L.nmol) ? L.wk[m] : 0.;
+      sui = (double)ln.sp[i] * wkm;
+      if (L.jrad == 1) sui = sui * radfn(ln.vnu[i], L.xkt);
+      if (sui == 0.) rej = true;
+    }
+    if (!rej) {
+      const int iflag = ln.iflg[i];
+      double yi = 0., gi = 0., g1 = 0., g2 = 0.;
+      if (iflag == 1 || iflag == 3)
+        coupling(ln, i, iflag, L.ilc_n, L.rectlc_n, L.tmpdif_n, false, yi, gi, g1, g2);
+      const double vnu = ln.vnu[i] + L.rhorat * (double)ln.pshift[i];
+      const double tmpcor = pow(L.tratio, (double)ln.tmpalf[i]);
+      const double a0 = air_width(ln, i, m) * tmpcor;
+      const double hs = (double)ln.hwhms[i] * tmpcor;
+      double alfl = a0 * (L.rhorat - L.rhoslf[m]) + hs * L.rhoslf[m];
+      if (iflag == 3) alfl = alfl * (1.0 - g1 * L.pavp0 - g2 * L.pavp2);
+      const double alfad = vnu * L.alfd1[m][iso];
+      const double zeta = alfl / (alfl + alfad);
+      const double fz = 100. * zeta;
+      long iz = fint(fz + kONEPL);
+      iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);
+      const double zd = fz - double(iz - 1);
+      double alfv = (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (alfl + alfad);
+      if (alfv < DV) alfv = DV;
+      if (alfv > L.alfmax) alfv = L.alfmax;
+      const double reach = 64. * alfv + vnu;  // HWF3*ALFV+VNU (:1120)
+      const double recalf = 1. / alfv;
+      double epp = (double)ln.epp[i];
+      if (epp <= -1.001) epp = fabs(epp);
+      if (epp > -0.999)
+        sui = sui * L.scor[m][iso] * exp(-epp * L.betacr_n) * (1. + exp(-vnu / L.xkt));
+      const double sp = sui * (1. + gi * L.pavp2);
+      const double sppsp = (sui * yi * L.pavp0) / sp;
+      bool r4test = false;
+      double speak = 0.;
+      if (iflag == 0) {
+        speak = sui * recalf;
+        if (L.dvr4 <= 0.) {
+          if (speak <= L.dptmn) rej = true;
+        } else {
+          r4test = (sppsp == 0.);
+        }
+      }
+      if (!rej) {
+        // strengths of the sub-functions (CNVFNV :1270-1282)
+        const double depth = sp * recalf;
+        double* str = w.n_str + 5 * slot;
+        const double* cf[5] = {c_cf1, c_cf2, c_cf3, c_cgauss, c_cer};
+#pragma unroll
+        for (int q = 0; q < 5; q++) str[q] = depth * (cf[q][iz - 1] + zd * (cf[q][iz] - cf[q][iz - 1]));
+        w.n_sppsp[slot] = sppsp;
+        w.n_zslope[slot] = recalf * L.wavdxf;
+        w.n_zint[slot] = vnu;
+        w.n_reach[slot] = reach;
+        w.n_speak[slot] = speak;
+        fl = (int8_t)(1 | (r4test ? 2 : 0));
+      }
+    }
+  }
+  w.n_pre[slot] = fl;
+}
+
+// The read-panel walk of LNCOR1 (one CTA per layer, TAPE3 panels in order):
+// the R4 rejection uses the window current when a line's TAPE3 panel is
+// read, which is the first panel able to hold all earlier accepted lines
+// (JMAX1 <= MAX1), and CNVFNV convolves each line in the panel current when
+// it reaches it.  Panel origins, window limits and the current window's R4
+// sit in shared memory; the next TAPE3 panel's line values are fetched
+// while this one is walked.
+__global__ void __launch_bounds__(256) k_near_walk(Work w, DevLines ln) {
+  extern __shared__ double sm[];
   const int l = blockIdx.x;
   const LayerDev& L = w.L[l];
-  __shared__ int s_pmax, s_stop_at;
+  const int npanel = (int)L.npanel, nwin = (int)L.nwin;
+  double* s_vft = sm;
+  double* s_v1r4 = s_vft + npanel;
+  double* s_r4 = s_v1r4 + nwin;
+  int32_t* s_wof = reinterpret_cast<int32_t*>(s_r4 + kR4Stride);
+  int32_t* s_nptr4 = s_wof + npanel;
+  __shared__ int s_pmax, s_stop_at, s_pread;
   __shared__ int s_scan[32];
-  __shared__ int s_pread;
-  if (threadIdx.x == 0) {
-    s_pread = 0;
+  const int tid = threadIdx.x;
+  for (int k = tid; k < npanel; k += blockDim.x) {
+    s_vft[k] = w.vft[L.off_panel + k];
+    s_wof[k] = nwin > 0 ? w.win_of[L.off_panel + k] : -1;
   }
-  __syncthreads();
+  for (int k = tid; k < nwin; k += blockDim.x) {
+    s_v1r4[k] = w.win[L.off_win + k].v1r4;
+    s_nptr4[k] = w.win[L.off_win + k].nptr4;
+  }
+  if (tid == 0) s_pread = 0;
   const double DV = L.dv;
-  const int npanel = (int)L.npanel;
-  bool stopped = false;
-  for (int64_t b = L.blk_lo; b < L.blk_hi; b++) {
+  // one TAPE3 panel's line values for this thread's line
+  struct Pre {
+    int64_t slot;
+    double vnu, reach, speak, zslope;
+    int fl;
+    bool in;
+  };
+  auto fetch = [&](int64_t b, Pre& q) {
     // 32-bit line indices (the line file holds fewer than 2^31 records)
     const int32_t a = (int32_t)(ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo);
     const int32_t e = (int32_t)(ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi);
+    const int32_t i = a + (int32_t)tid;
+    q.in = i < e;
+    q.slot = (int64_t)(i - (int32_t)L.near_lo) + L.off_near;
+    q.fl = 0;
+    if (q.in) {
+      q.fl = w.n_pre[q.slot];
+      q.vnu = w.n_zint[q.slot];
+      q.reach = w.n_reach[q.slot];
+      q.speak = w.n_speak[q.slot];
+      q.zslope = w.n_zslope[q.slot];
+    }
+  };
+  Pre cur;
+  if (L.blk_lo < L.blk_hi) fetch(L.blk_lo, cur);
+  bool stopped = false;
+  int rwin = -1;  // window whose R4 is in shared memory
+  __syncthreads();
+  for (int64_t b = L.blk_lo; b < L.blk_hi; b++) {
+    Pre nxt;
+    nxt.in = false;
+    if (b + 1 < L.blk_hi) fetch(b + 1, nxt);
     const int pread = s_pread;
-    const double VFT = w.vft[L.off_panel + pread];
-    const int wi = L.nwin > 0 ? w.win_of[L.off_panel + pread] : -1;
-    if (threadIdx.x == 0) {
+    const double VFT = s_vft[pread];
+    const int wi = nwin > 0 ? s_wof[pread] : -1;
+    if (wi >= 0 && wi != rwin && L.dvr4 > 0.) {
+      const double* r4 = w.r4 + (L.off_win + wi) * kR4Stride;
+      for (int k = tid; k <= s_nptr4[wi]; k += blockDim.x) s_r4[k] = r4[k];
+      rwin = wi;
+    }
+    if (tid == 0) {
       s_pmax = pread;
       s_stop_at = 1 << 30;
     }
     __syncthreads();
-    const int32_t i = a + (int32_t)threadIdx.x;
-    int pfit = -1;
-    bool ok = false;
-    unsigned long long ntrip = 0;
-    double zslope = 0., bhw = 0., vline = 0.;
-    const int64_t slot = (int64_t)(i - (int32_t)L.near_lo) + L.off_near;
-    if (i < e && !stopped && ln.iflg[i] >= 0) {
-      const int mcode = ln.mol[i];
-      const int m = mcode % 100, iso = (mcode % 1000) / 100;
-      double sui = 0.;
-      bool rej = !(m >= 1 && m <= 47 && iso >= 1 && iso <= c_isomax[m]);
-      if (!rej) {
-        const double wkm = (m <= L.nmol) ? L.wk[m] : 0.;
-        sui = (double)ln.sp[i] * wkm;
-        if (L.jrad == 1) sui = sui * radfn(ln.vnu[i], L.xkt);
-        if (sui == 0.) rej = true;
-      }
-      if (!rej) {
-        const int iflag = ln.iflg[i];
-        double yi = 0., gi = 0., g1 = 0., g2 = 0.;
-        if (iflag == 1 || iflag == 3)
-          coupling(ln, i, iflag, L.ilc_n, L.rectlc_n, L.tmpdif_n, false, yi, gi, g1, g2);
-        const double vnu = ln.vnu[i] + L.rhorat * (double)ln.pshift[i];
-        const double tmpcor = pow(L.tratio, (double)ln.tmpalf[i]);
-        const double a0 = air_width(ln, i, m) * tmpcor;
-        const double hs = (double)ln.hwhms[i] * tmpcor;
-        double alfl = a0 * (L.rhorat - L.rhoslf[m]) + hs * L.rhoslf[m];
-        if (iflag == 3) alfl = alfl * (1.0 - g1 * L.pavp0 - g2 * L.pavp2);
-        const double alfad = vnu * L.alfd1[m][iso];
-        const double zeta = alfl / (alfl + alfad);
-        const double fz = 100. * zeta;
-        long iz = fint(fz + kONEPL);
-        iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);
-        const double zd = fz - double(iz - 1);
-        double alfv = (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (alfl + alfad);
-        if (alfv < DV) alfv = DV;
-        if (alfv > L.alfmax) alfv = L.alfmax;
-        if (64. * alfv + vnu < VFT) rej = true;  // HWF3*ALFV+VNU < VFT (:1120)
-        double recalf = 0.;
-        if (!rej) {
-          recalf = 1. / alfv;
-          double epp = (double)ln.epp[i];
-          if (epp <= -1.001) epp = fabs(epp);
-          if (epp > -0.999)
-            sui = sui * L.scor[m][iso] * exp(-epp * L.betacr_n) * (1. + exp(-vnu / L.xkt));
-          const double sp = sui * (1. + gi * L.pavp2);
-          const double sppsp = (sui * yi * L.pavp0) / sp;
-          if (iflag == 0) {
-            const double speak = sui * recalf;
-            if (L.dvr4 <= 0.) {
-              if (speak <= L.dptmn) rej = true;
-            } else {
-              const WinDev& W = w.win[L.off_win + wi];
-              long jj = fint((vnu - W.v1r4) / L.dvr4 + 1.);
-              jj = jj < 1 ? 1 : (jj > W.nptr4 ? W.nptr4 : jj);
-              const double r4 = w.r4[(L.off_win + wi) * kR4Stride + jj];
-              if (speak <= (L.dptmn + L.dptfc * r4) && sppsp == 0.) rej = true;
-            }
-          }
-          if (!rej) {
-            // strengths of the sub-functions (CNVFNV :1270-1282)
-            const double depth = sp * recalf;
-            double* str = w.n_str + 5 * slot;
-            const double* cf[5] = {c_cf1, c_cf2, c_cf3, c_cgauss, c_cer};
-#pragma unroll
-            for (int k = 0; k < 5; k++) str[k] = depth * (cf[k][iz - 1] + zd * (cf[k][iz] - cf[k][iz - 1]));
-            w.n_sppsp[slot] = sppsp;
-            zslope = recalf * L.wavdxf;
-            bhw = kHWDXF / zslope;
-            vline = vnu;
-            ok = true;
-            // first panel whose buffer holds the line's R1 window (JMAX1 <= MAX1)
-            int p = pread;
-            const long excess = jmax1_at(vnu, w.vft[L.off_panel + p], DV, bhw) - L.max1;
-            if (excess > 0) p += (int)((excess + 2399) / 2400);
-            if (p > npanel) p = npanel;
-            while (p > pread && jmax1_at(vnu, w.vft[L.off_panel + p - 1], DV, bhw) <= L.max1) p--;
-            while (p < npanel && jmax1_at(vnu, w.vft[L.off_panel + p], DV, bhw) > L.max1) p++;
-            pfit = p;
-          }
-        }
-      }
+    bool ok = cur.in && !stopped && (cur.fl & 1) && !(cur.reach < VFT);  // :1120
+    if (ok && (cur.fl & 2) && wi >= 0) {
+      long jj = fint((cur.vnu - s_v1r4[wi]) / L.dvr4 + 1.);
+      jj = jj < 1 ? 1 : (jj > s_nptr4[wi] ? s_nptr4[wi] : jj);
+      if (cur.speak <= (L.dptmn + L.dptfc * s_r4[jj])) ok = false;
     }
+    int pfit = -1;
+    double bhw = 0.;
     if (ok) {
-      if (pfit >= npanel) atomicMin(&s_stop_at, (int)threadIdx.x);
+      bhw = kHWDXF / cur.zslope;
+      // first panel whose buffer holds the line's R1 window (JMAX1 <= MAX1)
+      int p = pread;
+      const long excess = jmax1_at(cur.vnu, s_vft[p], DV, bhw) - L.max1;
+      if (excess > 0) p += (int)((excess + 2399) / 2400);
+      if (p > npanel) p = npanel;
+      while (p > pread && jmax1_at(cur.vnu, s_vft[p - 1], DV, bhw) <= L.max1) p--;
+      while (p < npanel && jmax1_at(cur.vnu, s_vft[p], DV, bhw) > L.max1) p++;
+      pfit = p;
+      if (pfit >= npanel) atomicMin(&s_stop_at, tid);
     }
     __syncthreads();
     const int stop_at = s_stop_at;
-    if (ok && (int)threadIdx.x >= stop_at) ok = false;   // never reached by CNVFNV
+    if (ok && tid >= stop_at) ok = false;  // never reached by CNVFNV
     // CNVFNV convolves a line in the panel current when it reaches it: the
     // read panel or later, as far as the earlier lines of the panel pushed it
     const int pconv = max(pread, block_max_scan(ok ? pfit : -1, s_scan));
     if (ok) {
       atomicMax(&s_pmax, pfit);
       // window limits and offsets in that panel's own coordinates (:1283-1305)
-      const double zint = (vline - w.vft[L.off_panel + pconv]) / DV;
+      const double zint = (cur.vnu - s_vft[pconv]) / DV;
       const long jmax1 = fint(zint + bhw + 1.5);
       const long jmin1 = fint(zint - bhw + 1.5);
       const double rs = zint < 0.0 ? -0.5 : 0.5;
       const long j2 = fint(zint * (1. - L.conf2) + rs);
       const long j3 = fint(zint * (1. - L.conf3) + rs);
+      const int64_t slot = cur.slot;
       w.n_zint[slot] = zint;
-      w.n_zslope[slot] = zslope;
       w.n_jmin1[slot] = (int32_t)jmin1;
       w.n_jmax1[slot] = (int32_t)jmax1;
       w.n_j2[slot] = (int32_t)j2;
       w.n_j3[slot] = (int32_t)j3;
       w.n_pconv[slot] = pconv;
-      ntrip = (unsigned long long)(jmax1 - jmin1 + 1);
+      const unsigned long long ntrip = (unsigned long long)(jmax1 - jmin1 + 1);
       if (ntrip) atomicAdd(&w.counters[1], ntrip);
     }
-    if (i < e) w.n_ok[slot] = ok ? 1 : 0;
+    if (cur.in) w.n_ok[cur.slot] = ok ? 1 : 0;
     __syncthreads();
-    if (threadIdx.x == 0) s_pread = s_pmax;
+    if (tid == 0) s_pread = s_pmax;
     if (stop_at != (1 << 30)) stopped = true;
     __syncthreads();
+    cur = nxt;
   }
   // lines of the range beyond the walked panels are not used
 }
@@ -1223,10 +1292,8 @@ __global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn) {
   for (int64_t j = threadIdx.x; j < L.nptabs + 8; j += blockDim.x) absrb[j] = 0.;
   if (!L.icntnm) return;
   __syncthreads();
-  double wtot = 0.;
   const double h2o_fac = L.h2o_fac;  // WK(1)/WTOT of CONTNM (contnm.f90:261)
   if (!((L.v2 > -20.0) && (L.v1 < 20000.) && ((xself > 0.) || (xfrgn > 0)))) return;
-  (void)wtot;
   const double wv1 = L.v1abs, wv2 = L.v2abs, dva = L.dvabs;
   auto wvn = [&](int64_t i) { return ck.v0 + ck.dv * double(i - 1); };
   __shared__ int64_t s_i1, s_i2;
@@ -1653,18 +1720,33 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
 // =========================================================================
 // Planck function in the arithmetic T, from an FP64 wavenumber.
 template <typename T>
-__device__ __forceinline__ T planck_t(double vi, double xkt) {
+__device__ __forceinline__ T planck_t(double vi, double xkt, double rk) {
   if constexpr (sizeof(T) == 8) {
-    return planck(vi, xkt);
+    return planck(vi, xkt, rk);
   } else {
     if (!(xkt > 0.0)) return 0.f;
-    const float x = (float)(vi / xkt);
+    const float x = (float)(vi * rk);
     const float v = (float)vi;
     float b = 0.f;
     if (x < 1e-2f) b = (v * v) * (float)xkt / (1.f + 0.5f * x);
     else if (x <= 80.f) b = (v * v * v) / expm1f(x);
     return b * (float)kRADCN1;
   }
+}
+
+// EMIN at one point (src/xmerge.f90:1795-1855): the layer's transmittance
+// and linear-in-tau emission.  The source function's weight
+// F = 1 - 2 (T/(T-1) + 1/tau) is taken over one common denominator.
+template <typename T>
+__device__ __forceinline__ void emin_point(double odv, double vi, const EminT& t, T& tr, T& em) {
+  T o = (T)odv;
+  if (o < (T)-kODLO) o = (T)-kODLO;
+  tr = exp(-o);
+  const T d = tr - (T)1.;
+  const T fi = (o <= (T)kODLO) ? o * (T)(1. / 6.) : (T)1. - (T)2. * ((tr * o + d) / (d * o));
+  const T bb = planck_t<T>(vi, t.xkt, t.rk);
+  const T bbd = (t.xkta > 0.) ? planck_t<T>(vi, t.xkta, t.rka) - bb : (T)0.;
+  em = ((T)1. - tr) * (bb + bbd * fi);
 }
 
 // Point f of the finer grid from the previous layer's field x (n_old
@@ -1717,19 +1799,11 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
     if (tr_out) tr_out[f] = 0.;
     return;
   }
-  const double xkt = L.tave / kRADCN2;
-  const double xkta = tzu / kRADCN2;
-  // EMIN: linear-in-tau source over the layer (src/xmerge.f90:1795-1855)
-  T o = (T)odv;
-  if (o < (T)-kODLO) o = (T)-kODLO;
-  const T tr = exp(-o);
-  const T fi = (o <= (T)kODLO) ? o / (T)6. : (T)1. - (T)2. * (tr / (tr - (T)1.) + (T)1. / o);
-  const T bb = planck_t<T>(vi, xkt);
-  const T bbd = (xkta > 0.) ? planck_t<T>(vi, xkta) - bb : (T)0.;
-  T em = ((T)1. - tr) * (bb + bbd * fi);
+  T tr, em;
+  emin_point<T>(odv, vi, emin_temps(L.tave, tzu), tr, em);
   if (first) {
     // EMINIT: boundary emission (:2436-2484)
-    if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2) * (T)emis;
+    if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2, kRADCN2 / tbnd) * (T)emis;
     rad_out[f] = (double)em;
     tr_out[f] = (double)tr;
     return;
@@ -1764,17 +1838,10 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
       ro = (m.first && l == 0) ? odv : odv + ro;
       continue;
     }
-    const double xkt = m.tave[l] / kRADCN2;
-    const double xkta = m.tzu[l] / kRADCN2;
-    T o = (T)odv;
-    if (o < (T)-kODLO) o = (T)-kODLO;
-    const T tr = exp(-o);
-    const T fi = (o <= (T)kODLO) ? o / (T)6. : (T)1. - (T)2. * (tr / (tr - (T)1.) + (T)1. / o);
-    const T bb = planck_t<T>(vi, xkt);
-    const T bbd = (xkta > 0.) ? planck_t<T>(vi, xkta) - bb : (T)0.;
-    T em = ((T)1. - tr) * (bb + bbd * fi);
+    T tr, em;
+    emin_point<T>(odv, vi, m.t[l], tr, em);
     if (m.first && l == 0) {
-      if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2) * (T)emis;
+      if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2, kRADCN2 / tbnd) * (T)emis;
       ro = (double)em;
       to = (double)tr;
     } else {
@@ -1825,8 +1892,8 @@ __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const d
   const double DV = L.dv;
   const int64_t p = f / 2400;
   const double vi = (vft_panel[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
-  const double xkt = L.tave / kRADCN2;
-  const double xkta = tzu / kRADCN2;
+  const EminT t = emin_temps(L.tave, tzu);
+  const double xkta = t.xkta;
   const double tau = od[f];
   const bool clamped = tau < -kODLO;
   const double o = clamped ? -kODLO : tau;
@@ -1836,17 +1903,18 @@ __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const d
     fi = o / 6.;
     dfi = 1. / 6.;
   } else {
-    fi = 1. - 2. * (tr / (tr - 1.) + 1. / o);
-    dfi = -2. * (tr / ((tr - 1.) * (tr - 1.)) - 1. / (o * o));
+    const double d = tr - 1.;
+    fi = 1. - 2. * ((tr * o + d) / (d * o));
+    dfi = -2. * (tr / (d * d) - 1. / (o * o));
   }
-  const double bb = planck(vi, xkt);
-  const double bbd = (xkta > 0.) ? planck(vi, xkta) - bb : 0.;
+  const double bb = planck(vi, t.xkt, t.rk);
+  const double bbd = (xkta > 0.) ? planck(vi, xkta, t.rka) - bb : 0.;
   const double em = (1. - tr) * (bb + bbd * fi);
   const double dem_do = tr * (bb + bbd * fi) + (1. - tr) * bbd * dfi;
   const double dem_db = (1. - tr) * (xkta > 0. ? 1. - fi : 1.);
   double rad, trn, dr_do;
   if (first) {
-    const double bs = tbnd > 0. ? planck(vi, tbnd / kRADCN2) * emis : 0.;
+    const double bs = tbnd > 0. ? planck(vi, tbnd / kRADCN2, kRADCN2 / tbnd) * emis : 0.;
     rad = em + tr * bs;
     trn = tr;
     dr_do = dem_do - tr * bs;
@@ -1957,6 +2025,8 @@ void init_kernel_attributes() {
   // two R4 buffers per CTA; the largest carveout lets several CTAs share an SM
   cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
   cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem32);
+  cudaFuncSetAttribute(k_near_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kNearWalkSmemMax);
   cudaFuncSetAttribute(k_panel_od, cudaFuncAttributePreferredSharedMemoryCarveout,
                        cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -2005,8 +2075,16 @@ cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* wi
   return cudaGetLastError();
 }
 
-cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s) {
-  k_near_scale<<<w.nlay, 256, 0, s>>>(w, ln);
+cudaError_t launch_near_scale(const Work& w, const DevLines& ln, int64_t max_near,
+                              int64_t max_panel, int64_t max_win, cudaStream_t s) {
+  if (w.nlay > 65535) return cudaErrorInvalidValue;
+  if (max_near > 0) {
+    const dim3 g((unsigned)((max_near + 255) / 256), (unsigned)w.nlay);
+    k_near_lines<<<g, 256, 0, s>>>(w, ln);
+  }
+  const size_t smem = near_walk_smem(max_panel, max_win);
+  if (smem > kNearWalkSmemMax) return cudaErrorInvalidValue;
+  k_near_walk<<<w.nlay, 256, smem, s>>>(w, ln);
   return cudaGetLastError();
 }
 

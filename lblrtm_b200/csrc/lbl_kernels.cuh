@@ -66,6 +66,8 @@ struct Work {
   int32_t *n_jmin1, *n_jmax1, *n_j2, *n_j3;  // in the convolution panel's coordinates
   int32_t* n_pconv;      // panel in which CNVFNV convolves the line
   int8_t* n_ok;
+  double *n_reach, *n_speak;  // k_near_lines -> k_near_walk
+  int8_t* n_pre;
   // grids
   double *r1, *r2, *r3;
   double* absrb;
@@ -82,7 +84,16 @@ cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_b
                           int64_t nblk_total, cudaStream_t s);
 cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
                             const int32_t* win_layer, int precision, cudaStream_t s);
-cudaError_t launch_near_scale(const Work& w, const DevLines& ln, cudaStream_t s);
+// Near-wing line scaling: per line and layer (k_near_lines), then the
+// read-panel walk per layer (k_near_walk) with the layer's panel origins,
+// window limits and current R4 in shared memory.
+inline size_t near_walk_smem(int64_t npanel, int64_t nwin) {
+  return (size_t)(npanel + nwin + kR4Stride) * sizeof(double) +
+         (size_t)(npanel + nwin) * sizeof(int32_t);
+}
+constexpr size_t kNearWalkSmemMax = 220 * 1024;
+cudaError_t launch_near_scale(const Work& w, const DevLines& ln, int64_t max_near,
+                              int64_t max_panel, int64_t max_win, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
 cudaError_t launch_panel_prep(const Work& w, const DevLines& ln, int64_t npanel_total,
@@ -99,6 +110,16 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
                          cudaStream_t s, int precision = LBL_PREC_FP64);
+constexpr double kRADCN1 = 1.191042722E-12;  // src/phys_consts.f90:73
+constexpr double kRADCN2 = 1.4387752;        // src/phys_consts.f90:74
+// Temperatures of one EMIN step: XKT = T/RADCN2 and RADCN2/T for the layer
+// and for its upper boundary (XKTA; zero when the boundary is absent).
+struct EminT {
+  double xkt, rk, xkta, rka;
+};
+__host__ __device__ inline EminT emin_temps(double tave, double tzu) {
+  return {tave / kRADCN2, kRADCN2 / tave, tzu / kRADCN2, kRADCN2 / tzu};
+}
 // Consecutive layers on one grid merged in one pass: the first may be the
 // bottom layer (EMINIT) or regrid the field below it (RADNN ITYPE>0); the
 // rest share its grid, so the radiance and transmittance stay in registers
@@ -110,8 +131,7 @@ struct MergeRun {
   int32_t itype;                 // regrid of the incoming field (0: same grid)
   int32_t n_old;                 // points of the incoming field
   int64_t od_off[kMergeRunMax];  // each layer's optical depths in Work::od
-  double tave[kMergeRunMax];
-  double tzu[kMergeRunMax];
+  EminT t[kMergeRunMax];
 };
 cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const double* od,
                              int64_t npts, double dv, const double* rad_in, const double* tr_in,
