@@ -244,6 +244,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
     if (B.plans[l].d.n_r1 >= (int64_t(1) << 31) - 64)
       return fail(ctx, LBL_E_RANGE, "layer " + std::to_string(l) + ": more than 2^31 points");
   // offsets
+  int64_t o_nblk = 0;
   int64_t o_r1 = 0, o_r2 = 0, o_r3 = 0, o_od = 0, o_pan = 0, o_win = 0, o_far = 0, o_near = 0,
           o_b9 = 0, o_abs = 0;
   B.ld.resize(n);
@@ -260,6 +261,8 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
     d.off_far = o_far;
     d.off_shr = o_far;
     d.off_near = o_near;
+    d.off_nblk = o_nblk;
+    o_nblk += d.blk_hi - d.blk_lo;
     d.off_blk9 = o_b9;
     d.off_abs = o_abs;
     d.off_seg = blk_base[l];
@@ -310,9 +313,8 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<double>(o_near + 1);
   for (int k = 0; k < 5; k++) lay.add<int32_t>(o_near + 1);
   lay.add<int8_t>(o_near + 1);
-  lay.add<double>(o_near + 1);
-  lay.add<double>(o_near + 1);
-  lay.add<int8_t>(o_near + 1);
+  lay.add<NearPre>(o_near + 1);
+  lay.add<int2>(o_nblk + 1);
   lay.add<double>(o_abs);
   lay.add<double>(o_od);
   lay.add<int64_t>(2 * o_pan + 2);
@@ -369,9 +371,8 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   w.n_j3 = A.take<int32_t>(o_near + 1);
   w.n_pconv = A.take<int32_t>(o_near + 1);
   w.n_ok = A.take<int8_t>(o_near + 1);
-  w.n_reach = A.take<double>(o_near + 1);
-  w.n_speak = A.take<double>(o_near + 1);
-  w.n_pre = A.take<int8_t>(o_near + 1);
+  w.n_pre = A.take<NearPre>(o_near + 1);
+  w.n_blk = A.take<int2>(o_nblk + 1);
   w.absrb = A.take<double>(o_abs);
   w.od = A.take<double>(o_od);
   B.d_panel_rng = A.take<int64_t>(2 * o_pan + 2);
@@ -477,16 +478,17 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     CK(launch_far_wing(w, B.nwin_total, B.d_win_order, B.d_win_layer, precision, s));
   }
   {
-    StageTimer t(ctx, "near_scale", 2);
-    int64_t max_near = 0, max_panel = 0, max_win = 0;
+    StageTimer t(ctx, "near_scale", 3);
+    int64_t max_near = 0, max_panel = 0, max_win = 0, max_nblk = 0;
     for (const LayerDev& d : B.ld) {
       max_near = std::max<int64_t>(max_near, d.near_hi - d.near_lo);
       max_panel = std::max<int64_t>(max_panel, d.npanel);
       max_win = std::max<int64_t>(max_win, d.nwin);
+      max_nblk = std::max<int64_t>(max_nblk, d.blk_hi - d.blk_lo);
     }
     if (near_walk_smem(max_panel, max_win) > kNearWalkSmemMax)
       return fail(ctx, LBL_E_RANGE, "layer grid too long for the near-wing panel walk");
-    CK(launch_near_scale(w, ctx->dl, max_near, max_panel, max_win, s));
+    CK(launch_near_scale(w, ctx->dl, max_near, max_panel, max_win, max_nblk, s));
   }
   if (R.icntnm) {
     if (!ctx->have_ck) return fail(ctx, LBL_E_NOTREADY, "continuum table not uploaded");

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdint>
 #include <cstdio>
 
@@ -996,7 +997,10 @@ __global__ void __launch_bounds__(kFwThreads, 3)
     have_prev = decided != 0;
     if (!decided) break;
   }
-  if (nevals) atomicAdd(&w.counters[0], nevals);
+  // one counter update per warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nevals += __shfl_xor_sync(0xffffffffu, nevals, o);
+  if ((threadIdx.x & 31) == 0 && nevals) atomicAdd(&w.counters[0], nevals);
   double* R4s = fw_r4 + rb * kR4Stride;
   double* out = w.r4 + (int64_t)gw * kR4Stride;
   if (L.jrad == 1) {
@@ -1061,9 +1065,8 @@ __device__ int block_max_scan(int v, int* sh) {
 // depend on the TAPE3 panel being read (src/oprop.f90:678-1197): strength
 // scaling and rejection, widths, the Voigt interpolation index and the
 // CNVFNV sub-function strengths (written to their final slots), the reach
-// 64 ALFV + VNU of the VFT cut and the peak SPEAK of the R4 test.  Flags:
-// bit 0 the line survives these tests, bit 1 it is subject to the R4 test.
-// The shifted centre waits in n_zint for k_near_walk.
+// 64 ALFV + VNU of the VFT cut, the peak SPEAK of the R4 test and the first
+// panel able to hold the line's R1 window, all in one NearPre record.
 __global__ void __launch_bounds__(256) k_near_lines(Work w, DevLines ln) {
   const int l = blockIdx.y;
   const LayerDev& L = w.L[l];
@@ -1073,7 +1076,7 @@ __global__ void __launch_bounds__(256) k_near_lines(Work w, DevLines ln) {
   const int32_t i = (int32_t)L.near_lo + k;
   const int64_t slot = (int64_t)k + L.off_near;
   const double DV = L.dv;
-  int8_t fl = 0;
+  NearPre pre = {0., 0., 0., 0, -1};  // flags 0: rejected
   if (ln.iflg[i] >= 0) {
     const int mcode = ln.mol[i];
     const int m = mcode % 100, iso = (mcode % 1000) / 100;
@@ -1131,145 +1134,248 @@ __global__ void __launch_bounds__(256) k_near_lines(Work w, DevLines ln) {
 #pragma unroll
         for (int q = 0; q < 5; q++) str[q] = depth * (cf[q][iz - 1] + zd * (cf[q][iz] - cf[q][iz - 1]));
         w.n_sppsp[slot] = sppsp;
-        w.n_zslope[slot] = recalf * L.wavdxf;
-        w.n_zint[slot] = vnu;
-        w.n_reach[slot] = reach;
-        w.n_speak[slot] = speak;
-        fl = (int8_t)(1 | (r4test ? 2 : 0));
+        const double zslope = recalf * L.wavdxf;
+        const double bhw = kHWDXF / zslope;
+        // First panel whose buffer holds the line's R1 window (JMAX1 <=
+        // MAX1).  JMAX1 falls as the panel origin rises, so the panel the
+        // reference settles on from read panel P is the later of P and this.
+        const double* vft = w.vft + L.off_panel;
+        const int npanel = (int)L.npanel;
+        int p = 0;
+        const long excess = jmax1_at(vnu, vft[0], DV, bhw) - L.max1;
+        if (excess > 0) p = (int)min((excess + 2399) / 2400, (long)npanel);
+        while (p > 0 && jmax1_at(vnu, vft[p - 1], DV, bhw) <= L.max1) p--;
+        while (p < npanel && jmax1_at(vnu, vft[p], DV, bhw) > L.max1) p++;
+        w.n_zslope[slot] = zslope;
+        // the R4 point of the R4 test in the window of that panel, which
+        // is the read panel's window for most lines
+        int32_t wj = -1;  // none
+        if (r4test && L.nwin > 0 && L.nwin < 32768) {
+          const int wq = w.win_of[L.off_panel + (p < npanel ? p : npanel - 1)];
+          const WinDev& W = w.win[L.off_win + wq];
+          long jj = fint((vnu - W.v1r4) / L.dvr4 + 1.);
+          jj = jj < 1 ? 1 : (jj > W.nptr4 ? W.nptr4 : jj);
+          wj = (int32_t)((wq << 16) | (int)jj);
+        }
+        pre = {vnu, reach, speak, (p << 2) | 1 | (r4test ? 2 : 0), wj};
       }
     }
   }
-  w.n_pre[slot] = fl;
+  w.n_pre[slot] = pre;
 }
 
-// The read-panel walk of LNCOR1 (one CTA per layer, TAPE3 panels in order):
-// the R4 rejection uses the window current when a line's TAPE3 panel is
-// read, which is the first panel able to hold all earlier accepted lines
-// (JMAX1 <= MAX1), and CNVFNV convolves each line in the panel current when
-// it reaches it.  Panel origins, window limits and the current window's R4
-// sit in shared memory; the next TAPE3 panel's line values are fetched
-// while this one is walked.
-__global__ void __launch_bounds__(256) k_near_walk(Work w, DevLines ln) {
+// LNCOR1's tests that depend on the TAPE3 panel being read: the VFT cut
+// (:1120) and, for uncoupled lines, the R4 rejection against the window of
+// the read panel (:1160-1175).  r4 is that window's R4.
+__device__ __forceinline__ bool near_accept(const NearPre& r, double vft_read, int wi,
+                                            double v1r4, int nptr4, const double* r4,
+                                            double dvr4, double dptmn, double dptfc) {
+  bool ok = (r.pf_fl & 1) && !(r.reach < vft_read);
+  if (ok && (r.pf_fl & 2) && wi >= 0) {
+    long jj;
+    if ((r.wj >> 16) == wi) {
+      jj = r.wj & 0xffff;  // computed for this window by k_near_lines
+    } else {
+      jj = fint((r.vnu - v1r4) / dvr4 + 1.);
+      jj = jj < 1 ? 1 : (jj > nptr4 ? nptr4 : jj);
+    }
+    if (r.speak <= (dptmn + dptfc * r4[jj])) ok = false;
+  }
+  return ok;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The read-panel walk of LNCOR1, one warp per layer over its TAPE3 panels
+// in order.  The panel read next is the first panel able to hold the R1
+// windows of all lines accepted so far (JMAX1 <= MAX1); a line that no
+// panel can hold ends the walk (CNVFNV never reaches it or what follows).
+// Per TAPE3 panel the walk records the read panel and the first line not
+// reached; k_near_out derives everything else in parallel.  Line records
+// arrive in shared memory kWalkRing-1 panels ahead by asynchronous copies.
+__global__ void __launch_bounds__(32) k_near_walk(Work w, DevLines ln) {
   extern __shared__ double sm[];
   const int l = blockIdx.x;
+  const int lane = threadIdx.x;
+  const unsigned full = 0xffffffffu;
   const LayerDev& L = w.L[l];
   const int npanel = (int)L.npanel, nwin = (int)L.nwin;
-  double* s_vft = sm;
+  const int64_t blk_lo = L.blk_lo, nblk = L.blk_hi - L.blk_lo;
+  const int64_t near_lo = L.near_lo, near_hi = L.near_hi, off_near = L.off_near;
+  const int64_t off_win = L.off_win, off_nblk = L.off_nblk;
+  const double dvr4 = L.dvr4, dptmn = L.dptmn, dptfc = L.dptfc;
+  double* s_r4 = sm;  // first: 16-byte aligned for the asynchronous copies
+  double* s_vft = s_r4 + kR4Stride;
   double* s_v1r4 = s_vft + npanel;
-  double* s_r4 = s_v1r4 + nwin;
-  int32_t* s_wof = reinterpret_cast<int32_t*>(s_r4 + kR4Stride);
+  const size_t dbytes = ((size_t)(npanel + nwin + kR4Stride) * sizeof(double) + 31) / 32 * 32;
+  NearPre* ring = reinterpret_cast<NearPre*>(reinterpret_cast<char*>(sm) + dbytes);
+  int32_t* s_wof = reinterpret_cast<int32_t*>(ring + kWalkRing * 256);
   int32_t* s_nptr4 = s_wof + npanel;
-  __shared__ int s_pmax, s_stop_at, s_pread;
-  __shared__ int s_scan[32];
-  const int tid = threadIdx.x;
-  for (int k = tid; k < npanel; k += blockDim.x) {
+  constexpr int kBs = 64;
+  __shared__ int64_t s_bs[kBs + 1];
+  __shared__ int32_t s_rn[kWalkRing];
+  for (int k = lane; k < npanel; k += 32) {
     s_vft[k] = w.vft[L.off_panel + k];
     s_wof[k] = nwin > 0 ? w.win_of[L.off_panel + k] : -1;
   }
-  for (int k = tid; k < nwin; k += blockDim.x) {
-    s_v1r4[k] = w.win[L.off_win + k].v1r4;
-    s_nptr4[k] = w.win[L.off_win + k].nptr4;
+  for (int k = lane; k < nwin; k += 32) {
+    s_v1r4[k] = w.win[off_win + k].v1r4;
+    s_nptr4[k] = w.win[off_win + k].nptr4;
   }
-  if (tid == 0) s_pread = 0;
-  const double DV = L.dv;
-  // one TAPE3 panel's line values for this thread's line
-  struct Pre {
-    int64_t slot;
-    double vnu, reach, speak, zslope;
-    int fl;
-    bool in;
-  };
-  auto fetch = [&](int64_t b, Pre& q) {
-    // 32-bit line indices (the line file holds fewer than 2^31 records)
-    const int32_t a = (int32_t)(ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo);
-    const int32_t e = (int32_t)(ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi);
-    const int32_t i = a + (int32_t)tid;
-    q.in = i < e;
-    q.slot = (int64_t)(i - (int32_t)L.near_lo) + L.off_near;
-    q.fl = 0;
-    if (q.in) {
-      q.fl = w.n_pre[q.slot];
-      q.vnu = w.n_zint[q.slot];
-      q.reach = w.n_reach[q.slot];
-      q.speak = w.n_speak[q.slot];
-      q.zslope = w.n_zslope[q.slot];
+  // TAPE3 panel starts of panels [bs_base, bs_base + kBs]
+  int64_t bs_base = -(int64_t)kBs - 2;
+  // copy the records of near-range panel bi into ring slot bi % kWalkRing
+  auto issue = [&](int64_t bi) {
+    if (bi < nblk) {
+      const int64_t b = blk_lo + bi;
+      if (b + 1 > bs_base + kBs) {
+        __syncwarp();
+        for (int k = lane; k <= kBs; k += 32) s_bs[k] = (b + k <= L.blk_hi) ? ln.bs[b + k] : 0;
+        bs_base = b;
+        __syncwarp();
+      }
+      const int64_t a = s_bs[b - bs_base] > near_lo ? s_bs[b - bs_base] : near_lo;
+      const int64_t e = s_bs[b + 1 - bs_base] < near_hi ? s_bs[b + 1 - bs_base] : near_hi;
+      const int n = e > a ? (int)(e - a) : 0;  // at most 250 (RDLIN's LIMIN)
+      NearPre* dst = ring + (bi % kWalkRing) * 256;
+      const NearPre* src = w.n_pre + off_near + (a - near_lo);
+      for (int k = lane; k < n; k += 32) {
+        cp_async16(dst + k, src + k);
+        cp_async16(reinterpret_cast<char*>(dst + k) + 16, reinterpret_cast<const char*>(src + k) + 16);
+      }
+      if (lane == 0) s_rn[bi % kWalkRing] = n;
     }
+    cp_async_commit();
   };
-  Pre cur;
-  if (L.blk_lo < L.blk_hi) fetch(L.blk_lo, cur);
+  __syncwarp();
+  for (int64_t bi = 0; bi < kWalkRing - 1; bi++) issue(bi);
+  int pread = 0, rwin = -1;
   bool stopped = false;
-  int rwin = -1;  // window whose R4 is in shared memory
-  __syncthreads();
-  for (int64_t b = L.blk_lo; b < L.blk_hi; b++) {
-    Pre nxt;
-    nxt.in = false;
-    if (b + 1 < L.blk_hi) fetch(b + 1, nxt);
-    const int pread = s_pread;
-    const double VFT = s_vft[pread];
-    const int wi = nwin > 0 ? s_wof[pread] : -1;
-    if (wi >= 0 && wi != rwin && L.dvr4 > 0.) {
-      const double* r4 = w.r4 + (L.off_win + wi) * kR4Stride;
-      for (int k = tid; k <= s_nptr4[wi]; k += blockDim.x) s_r4[k] = r4[k];
-      rwin = wi;
+  for (int64_t bi = 0; bi < nblk; bi++) {
+    issue(bi + kWalkRing - 1);
+    cp_async_wait<kWalkRing - 1>();
+    __syncwarp();
+    const int slot = (int)(bi % kWalkRing);
+    const int n = s_rn[slot];
+    const NearPre* rb = ring + slot * 256;
+    int stop = INT_MAX;
+    if (!stopped) {
+      const double vft_read = s_vft[pread];
+      const int wi = nwin > 0 ? s_wof[pread] : -1;
+      if (wi >= 0 && wi != rwin && dvr4 > 0.) {
+        // the window's R4 (kR4Stride doubles, a multiple of 16 bytes)
+        const double* r4 = w.r4 + (off_win + wi) * kR4Stride;
+        for (int k = 2 * lane; k < (int)kR4Stride; k += 64) cp_async16(s_r4 + k, r4 + k);
+        cp_async_commit();
+        cp_async_wait<0>();
+        rwin = wi;
+        __syncwarp();
+      }
+      const double v1r4 = wi >= 0 ? s_v1r4[wi] : 0.;
+      const int nptr4 = wi >= 0 ? s_nptr4[wi] : 0;
+      int pf[8];
+      int first_out = INT_MAX;  // this lane's first accepted line no panel holds
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int k = lane + 32 * j;
+        pf[j] = -1;
+        if (k < n) {
+          const NearPre r = rb[k];
+          if (near_accept(r, vft_read, wi, v1r4, nptr4, s_r4, dvr4, dptmn, dptfc)) {
+            pf[j] = max(pread, r.pf_fl >> 2);
+            if (pf[j] >= npanel && k < first_out) first_out = k;
+          }
+        }
+      }
+      stop = __reduce_min_sync(full, first_out);
+      int pm = pread;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if (lane + 32 * j < stop) pm = max(pm, pf[j]);
+      const int pmax = __reduce_max_sync(full, pm);
+      if (lane == 0) w.n_blk[off_nblk + bi] = make_int2(pread, stop);
+      pread = pmax;
+      if (stop != INT_MAX) stopped = true;
+    } else if (lane == 0) {
+      w.n_blk[off_nblk + bi] = make_int2(-1, 0);
     }
-    if (tid == 0) {
-      s_pmax = pread;
-      s_stop_at = 1 << 30;
-    }
-    __syncthreads();
-    bool ok = cur.in && !stopped && (cur.fl & 1) && !(cur.reach < VFT);  // :1120
-    if (ok && (cur.fl & 2) && wi >= 0) {
-      long jj = fint((cur.vnu - s_v1r4[wi]) / L.dvr4 + 1.);
-      jj = jj < 1 ? 1 : (jj > s_nptr4[wi] ? s_nptr4[wi] : jj);
-      if (cur.speak <= (L.dptmn + L.dptfc * s_r4[jj])) ok = false;
-    }
-    int pfit = -1;
-    double bhw = 0.;
-    if (ok) {
-      bhw = kHWDXF / cur.zslope;
-      // first panel whose buffer holds the line's R1 window (JMAX1 <= MAX1)
-      int p = pread;
-      const long excess = jmax1_at(cur.vnu, s_vft[p], DV, bhw) - L.max1;
-      if (excess > 0) p += (int)((excess + 2399) / 2400);
-      if (p > npanel) p = npanel;
-      while (p > pread && jmax1_at(cur.vnu, s_vft[p - 1], DV, bhw) <= L.max1) p--;
-      while (p < npanel && jmax1_at(cur.vnu, s_vft[p], DV, bhw) > L.max1) p++;
-      pfit = p;
-      if (pfit >= npanel) atomicMin(&s_stop_at, tid);
-    }
-    __syncthreads();
-    const int stop_at = s_stop_at;
-    if (ok && tid >= stop_at) ok = false;  // never reached by CNVFNV
-    // CNVFNV convolves a line in the panel current when it reaches it: the
-    // read panel or later, as far as the earlier lines of the panel pushed it
-    const int pconv = max(pread, block_max_scan(ok ? pfit : -1, s_scan));
-    if (ok) {
-      atomicMax(&s_pmax, pfit);
-      // window limits and offsets in that panel's own coordinates (:1283-1305)
-      const double zint = (cur.vnu - s_vft[pconv]) / DV;
-      const long jmax1 = fint(zint + bhw + 1.5);
-      const long jmin1 = fint(zint - bhw + 1.5);
-      const double rs = zint < 0.0 ? -0.5 : 0.5;
-      const long j2 = fint(zint * (1. - L.conf2) + rs);
-      const long j3 = fint(zint * (1. - L.conf3) + rs);
-      const int64_t slot = cur.slot;
-      w.n_zint[slot] = zint;
-      w.n_jmin1[slot] = (int32_t)jmin1;
-      w.n_jmax1[slot] = (int32_t)jmax1;
-      w.n_j2[slot] = (int32_t)j2;
-      w.n_j3[slot] = (int32_t)j3;
-      w.n_pconv[slot] = pconv;
-      const unsigned long long ntrip = (unsigned long long)(jmax1 - jmin1 + 1);
-      if (ntrip) atomicAdd(&w.counters[1], ntrip);
-    }
-    if (cur.in) w.n_ok[cur.slot] = ok ? 1 : 0;
-    __syncthreads();
-    if (tid == 0) s_pread = s_pmax;
-    if (stop_at != (1 << 30)) stopped = true;
-    __syncthreads();
-    cur = nxt;
+    __syncwarp();  // the slot is refilled by the next issue
   }
-  // lines of the range beyond the walked panels are not used
+  cp_async_wait<0>();
+}
+
+// Window limits of every near-wing line (one CTA per layer and TAPE3
+// panel), from the read panel and stop line the walk recorded: the line is
+// accepted by the same tests, and CNVFNV convolves it in the panel current
+// when it reaches it: the read panel or later, as far as the earlier lines
+// of the panel pushed it (:1283-1305).
+__global__ void __launch_bounds__(256) k_near_out(Work w, DevLines ln) {
+  __shared__ int s_scan[32];
+  const int l = blockIdx.y;
+  const LayerDev& L = w.L[l];
+  const int64_t bi = blockIdx.x;
+  if (bi >= L.blk_hi - L.blk_lo) return;
+  const int64_t b = L.blk_lo + bi;
+  const int tid = threadIdx.x;
+  const int64_t a = ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo;
+  const int64_t e = ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi;
+  const int64_t i = a + tid;
+  const bool in = i < e;
+  const int64_t slot = (i - L.near_lo) + L.off_near;
+  const int2 pb = w.n_blk[L.off_nblk + bi];
+  const int pread = pb.x;
+  bool ok = false;
+  int pfit = -1;
+  NearPre r;
+  if (in && pread >= 0) {
+    r = w.n_pre[slot];
+    const int64_t pp = L.off_panel + pread;
+    const int wi = L.nwin > 0 ? w.win_of[pp] : -1;
+    double v1r4 = 0.;
+    int nptr4 = 0;
+    const double* r4 = w.r4;
+    if (wi >= 0) {
+      v1r4 = w.win[L.off_win + wi].v1r4;
+      nptr4 = w.win[L.off_win + wi].nptr4;
+      r4 = w.r4 + (L.off_win + wi) * kR4Stride;
+    }
+    ok = near_accept(r, w.vft[pp], wi, v1r4, nptr4, r4, L.dvr4, L.dptmn, L.dptfc) && tid < pb.y;
+    if (ok) pfit = max(pread, r.pf_fl >> 2);
+  }
+  const int pconv = max(pread, block_max_scan(ok ? pfit : -1, s_scan));
+  unsigned ntrip = 0;
+  if (ok) {
+    const double DV = L.dv;
+    const double bhw = kHWDXF / w.n_zslope[slot];
+    const double zint = (r.vnu - w.vft[L.off_panel + pconv]) / DV;
+    const long jmax1 = fint(zint + bhw + 1.5);
+    const long jmin1 = fint(zint - bhw + 1.5);
+    const double rs = zint < 0.0 ? -0.5 : 0.5;
+    const long j2 = fint(zint * (1. - L.conf2) + rs);
+    const long j3 = fint(zint * (1. - L.conf3) + rs);
+    w.n_zint[slot] = zint;
+    w.n_jmin1[slot] = (int32_t)jmin1;
+    w.n_jmax1[slot] = (int32_t)jmax1;
+    w.n_j2[slot] = (int32_t)j2;
+    w.n_j3[slot] = (int32_t)j3;
+    w.n_pconv[slot] = pconv;
+    ntrip = (unsigned)(jmax1 - jmin1 + 1);
+  }
+  if (in) w.n_ok[slot] = ok ? 1 : 0;
+  // one counter update per warp (a single address updated by every line
+  // would serialise the kernel)
+  const unsigned wsum = __reduce_add_sync(0xffffffffu, ntrip);
+  if ((tid & 31) == 0 && wsum) atomicAdd(&w.counters[1], (unsigned long long)wsum);
 }
 
 __device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double x) {
@@ -2076,7 +2182,8 @@ cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* wi
 }
 
 cudaError_t launch_near_scale(const Work& w, const DevLines& ln, int64_t max_near,
-                              int64_t max_panel, int64_t max_win, cudaStream_t s) {
+                              int64_t max_panel, int64_t max_win, int64_t max_nblk,
+                              cudaStream_t s) {
   if (w.nlay > 65535) return cudaErrorInvalidValue;
   if (max_near > 0) {
     const dim3 g((unsigned)((max_near + 255) / 256), (unsigned)w.nlay);
@@ -2084,7 +2191,8 @@ cudaError_t launch_near_scale(const Work& w, const DevLines& ln, int64_t max_nea
   }
   const size_t smem = near_walk_smem(max_panel, max_win);
   if (smem > kNearWalkSmemMax) return cudaErrorInvalidValue;
-  k_near_walk<<<w.nlay, 256, smem, s>>>(w, ln);
+  k_near_walk<<<w.nlay, 32, smem, s>>>(w, ln);
+  if (max_nblk > 0) k_near_out<<<dim3((unsigned)max_nblk, (unsigned)w.nlay), 256, 0, s>>>(w, ln);
   return cudaGetLastError();
 }
 

@@ -33,6 +33,17 @@ struct DevMtckd {
   int64_t n;
 };
 
+// What k_near_lines leaves for the read-panel walk about one near-wing line
+// of one layer, in one 32-byte record.
+struct NearPre {
+  double vnu;     // pressure-shifted centre
+  double reach;   // HWF3*ALFV + VNU, against the read panel's VFT
+  double speak;   // peak for the R4 test
+  int32_t pf_fl;  // first panel whose R1 buffer holds the window << 2 | flags
+                  // (bit 0: survives the panel-independent tests; bit 1: R4 test applies)
+  int32_t wj;     // window of that panel << 16 | the line's R4 point in it
+};
+
 // Work buffers of one batch of layers; offsets come from LayerDev.
 struct Work {
   const LayerDev* L;     // nlay entries
@@ -66,8 +77,8 @@ struct Work {
   int32_t *n_jmin1, *n_jmax1, *n_j2, *n_j3;  // in the convolution panel's coordinates
   int32_t* n_pconv;      // panel in which CNVFNV convolves the line
   int8_t* n_ok;
-  double *n_reach, *n_speak;  // k_near_lines -> k_near_walk
-  int8_t* n_pre;
+  NearPre* n_pre;  // k_near_lines -> k_near_walk, k_near_out
+  int2* n_blk;     // per near-range TAPE3 panel: read panel (-1 past the end), stop line
   // grids
   double *r1, *r2, *r3;
   double* absrb;
@@ -84,16 +95,19 @@ cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_b
                           int64_t nblk_total, cudaStream_t s);
 cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
                             const int32_t* win_layer, int precision, cudaStream_t s);
-// Near-wing line scaling: per line and layer (k_near_lines), then the
-// read-panel walk per layer (k_near_walk) with the layer's panel origins,
-// window limits and current R4 in shared memory.
+// Near-wing line scaling: per line and layer (k_near_lines), the read-panel
+// walk per layer (k_near_walk: one warp, the layer's panel origins, window
+// limits, current R4 and a ring of line records in shared memory), then
+// the window limits of every line (k_near_out, per TAPE3 panel).
+constexpr int kWalkRing = 4;  // TAPE3 panels of line records in flight
 inline size_t near_walk_smem(int64_t npanel, int64_t nwin) {
-  return (size_t)(npanel + nwin + kR4Stride) * sizeof(double) +
-         (size_t)(npanel + nwin) * sizeof(int32_t);
+  const size_t d = ((size_t)(npanel + nwin + kR4Stride) * sizeof(double) + 31) / 32 * 32;
+  return d + (size_t)kWalkRing * 256 * sizeof(NearPre) + (size_t)(npanel + nwin) * sizeof(int32_t);
 }
 constexpr size_t kNearWalkSmemMax = 220 * 1024;
 cudaError_t launch_near_scale(const Work& w, const DevLines& ln, int64_t max_near,
-                              int64_t max_panel, int64_t max_win, cudaStream_t s);
+                              int64_t max_panel, int64_t max_win, int64_t max_nblk,
+                              cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
 cudaError_t launch_panel_prep(const Work& w, const DevLines& ln, int64_t npanel_total,

@@ -66,6 +66,7 @@ struct LayerDev {
   int64_t off_far;            // raw far-wing line slots
   int64_t off_shr;            // shrunk line slots
   int64_t off_near;           // near-wing line slots
+  int64_t off_nblk;           // near-range TAPE3 panel slots
   int64_t off_blk9;           // shrunk-line (TAPE9) block slots
   int64_t off_abs;            // continuum (ABSRB) slots
   int64_t off_seg;            // LINF4 segment slots (one per far-range panel)
