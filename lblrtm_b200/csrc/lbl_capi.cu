@@ -13,6 +13,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -56,6 +61,67 @@ struct Layout {
   void add(size_t n) {
     bytes = ((bytes + 255) & ~size_t(255)) + n * sizeof(T);
   }
+};
+
+// Persistent host workers for the per-layer planning: tasks [0, n) are taken
+// from a shared counter by the workers and the calling thread (starting
+// threads for every call costs more than planning a profile).
+class HostPool {
+ public:
+  explicit HostPool(int nworkers) {
+    for (int t = 0; t < nworkers; t++) th_.emplace_back([this] { work(); });
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      quit_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  void run(int n, const std::function<void(int)>& f) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      f_ = &f;
+      n_ = n;
+      next_.store(0);
+      active_ = (int)th_.size();
+      gen_++;
+    }
+    cv_.notify_all();
+    for (int i; (i = next_.fetch_add(1)) < n;) f(i);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [this] { return active_ == 0; });
+  }
+
+ private:
+  void work() {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(int)>* f;
+      int n;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return quit_ || gen_ != seen; });
+        if (quit_) return;
+        seen = gen_;
+        f = f_;
+        n = n_;
+      }
+      for (int i; (i = next_.fetch_add(1)) < n;) (*f)(i);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--active_ == 0) done_.notify_all();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)>* f_ = nullptr;
+  int n_ = 0;
+  std::atomic<int> next_{0};
+  int active_ = 0;
+  uint64_t gen_ = 0;
+  bool quit_ = false;
 };
 
 bool is_device_ptr(const void* p) {
@@ -103,6 +169,7 @@ struct lbl_ctx {
   size_t jac_cap = 0;
   bool have_ck = false;
   Arena arena;
+  std::unique_ptr<HostPool> pool;  // planning workers, created on first use
   // merge buffers (ping-pong)
   double* mbuf[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t mcap = 0;
@@ -227,16 +294,17 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   if (jrad_out) *jrad_out = jrad;
   std::vector<int> rcs(n, LBL_OK);
   std::vector<std::string> errs(n);
-  auto plan_range = [&](int a, int b) {
-    for (int l = a; l < b; l++) rcs[l] = plan_layer(R, layers[l], jin[l], H, &B.plans[l], &errs[l]);
+  const std::function<void(int)> plan_one = [&](int l) {
+    rcs[l] = plan_layer(R, layers[l], jin[l], H, &B.plans[l], &errs[l]);
   };
-  const int nth = std::min<int>(n / 4, 8);
-  if (nth <= 1) {
-    plan_range(0, n);
+  if (n < 8) {
+    for (int l = 0; l < n; l++) plan_one(l);
   } else {
-    std::vector<std::thread> th;
-    for (int t = 0; t < nth; t++) th.emplace_back(plan_range, n * t / nth, n * (t + 1) / nth);
-    for (auto& x : th) x.join();
+    if (!ctx->pool) {
+      const int hw = (int)std::thread::hardware_concurrency();
+      ctx->pool = std::make_unique<HostPool>(std::max(1, std::min(hw - 1, 7)));
+    }
+    ctx->pool->run(n, plan_one);
   }
   for (int l = 0; l < n; l++)
     if (rcs[l] != LBL_OK) return fail(ctx, rcs[l], "layer " + std::to_string(l) + ": " + errs[l]);

@@ -311,12 +311,27 @@ __device__ void shrink_walk(const FarSlots& fs, const LayerDev& L, int32_t a, in
       st.started = true;
     }
     st.raw += __popc(m);
+    // Where the chunk's centres do not decrease, a line whose next usable
+    // line lies beyond its own centre + DVR4/2 closes its group under any
+    // limit set inside the chunk (such a limit is at most that bound), so
+    // after a closure a run of such lines closes in one step.
+    const unsigned forced = __ballot_sync(full, valid && !(hn && vn <= v + dvh));
+    const bool sorted = __ballot_sync(full, valid && hn && lane != last && vn < v) == 0u;
     unsigned cl = 0;  // lanes that close a group
     for (int pos = first; pos <= last;) {
       const unsigned q = __ballot_sync(full, valid && lane >= pos && !(hn && vn <= st.vlmt));
       if (!q) break;
-      const int k = __ffs(q) - 1;
+      int k = __ffs(q) - 1;
       cl |= 1u << k;
+      if (sorted) {
+        const unsigned after = m & ~((2u << k) - 1u);  // usable lanes above k
+        const unsigned nf = after & ~forced;
+        const unsigned run = nf ? (after & ((1u << (__ffs(nf) - 1)) - 1u)) : after;
+        if (run) {
+          cl |= run;
+          k = 31 - __clz(run);
+        }
+      }
       st.vlmt = __shfl_sync(full, v, k) + dvh;
       pos = k + 1;
     }
@@ -450,37 +465,52 @@ __global__ void k_shr_count(Work w, const int64_t* bs, const int64_t* blk_base, 
     for (; k < kSegMaxBlk; k++) craw[k] = -1;  // not reached
 }
 
+// One warp per layer: the LINF4 state machine over the count tables, the
+// end of each segment found by one ballot over its start panel's row.
 __global__ void k_shr_plan(Work w, const int64_t* blk_base) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = blockIdx.x;
+  const int lane = threadIdx.x;
+  const unsigned full = 0xffffffffu;
   if (l >= w.nlay) return;
   const LayerDev& L = w.L[l];
   int64_t nseg = 0, total = 0, nb9 = 0, blk_start = 0, J = 0;
+  static_assert(kSegMaxBlk <= 64, "two entries of a count row per lane");
   if (L.ilblf4 >= 1 && L.far_hi > L.far_lo) {
     const int64_t nb = L.fblk_hi - L.fblk_lo;
     int64_t b = 0;
     while (b < nb) {
       const int32_t* craw = w.c_raw + (blk_base[l] + b) * kSegMaxBlk;
       const int32_t* cout = w.c_out + (blk_base[l] + b) * kSegMaxBlk;
-      int k = 0;
-      for (;; k++) {
-        if (k >= kSegMaxBlk || craw[k] < 0) {
+      // segment b..b+k ends at the first k reaching the last panel or
+      // holding + raw >= 1000; an unreached entry (-1) or k past the row
+      // means the segment is longer than the table
+      const int k0 = lane, k1 = lane + 32;
+      const int32_t r0 = craw[k0], r1 = k1 < kSegMaxBlk ? craw[k1] : -1;
+      const bool h0 = r0 < 0 || b + k0 == nb - 1 || J + r0 >= 1000;
+      const bool h1 = r1 < 0 || b + k1 == nb - 1 || J + r1 >= 1000;
+      const unsigned m0 = __ballot_sync(full, h0), m1 = __ballot_sync(full, h1);
+      const int k = m0 ? __ffs(m0) - 1 : (m1 ? 32 + __ffs(m1) - 1 : 64);
+      const int32_t rk = k < 32 ? __shfl_sync(full, r0, k & 31) : __shfl_sync(full, r1, k & 31);
+      if (k >= kSegMaxBlk || rk < 0) {
+        if (lane == 0) {
           w.status[0] = 2;  // segment longer than the count table: fall back
           w.s_count[l] = -1;
-          return;
         }
-        if (b + k == nb - 1 || J + craw[k] >= 1000) break;
+        return;
       }
       const int64_t n = cout[k];
-      w.seg_blk[L.off_seg + nseg] = (int32_t)b;
-      w.seg_nblk[L.off_seg + nseg] = (int32_t)(k + 1);
-      w.seg_out[L.off_seg + nseg] = total;
+      if (lane == 0) {
+        w.seg_blk[L.off_seg + nseg] = (int32_t)b;
+        w.seg_nblk[L.off_seg + nseg] = (int32_t)(k + 1);
+        w.seg_out[L.off_seg + nseg] = total;
+      }
       nseg++;
       total += n;
       J += n;
       b += k + 1;
       if (J >= 1000 || b >= nb) {
         if (J > 0) {
-          w.b9_start[L.off_blk9 + nb9] = blk_start;
+          if (lane == 0) w.b9_start[L.off_blk9 + nb9] = blk_start;
           nb9++;
         }
         blk_start = total;
@@ -488,9 +518,11 @@ __global__ void k_shr_plan(Work w, const int64_t* blk_base) {
       }
     }
   }
-  w.seg_count[l] = nseg;
-  w.s_count[l] = total;
-  w.b9_count[l] = nb9;
+  if (lane == 0) {
+    w.seg_count[l] = nseg;
+    w.s_count[l] = total;
+    w.b9_count[l] = nb9;
+  }
 }
 
 // One warp per segment.
@@ -1496,11 +1528,14 @@ constexpr double X00 = -7. / 128., X01 = 105. / 128., X02 = 35. / 128., X03 = -5
                  X10 = -1. / 16., X11 = 9. / 16.;
 
 __device__ __forceinline__ double interp4(const double* R, int64_t J, int r) {
-  // value added at fine point J*4-3+r from coarse points J-1..J+2
-  if (r == 0) return R[J];
-  if (r == 1) return X00 * R[J - 1] + X01 * R[J] + X02 * R[J + 1] + X03 * R[J + 2];
-  if (r == 2) return X10 * (R[J - 1] + R[J + 2]) + X11 * (R[J] + R[J + 1]);
-  return X03 * R[J - 1] + X02 * R[J] + X01 * R[J + 1] + X00 * R[J + 2];
+  // value added at fine point J*4-3+r from coarse points J-1..J+2; the four
+  // forms are all evaluated and one selected, so neighbouring lanes (with
+  // different r) do not diverge
+  const double a = R[J - 1], b = R[J], c = R[J + 1], d = R[J + 2];
+  const double v1 = X00 * a + X01 * b + X02 * c + X03 * d;
+  const double v2 = X10 * (a + d) + X11 * (b + c);
+  const double v3 = X03 * a + X02 * b + X01 * c + X00 * d;
+  return r == 0 ? b : (r == 1 ? v1 : (r == 2 ? v2 : v3));
 }
 
 // Global grid index ranges of one panel (panel p of layer L):
@@ -2165,7 +2200,7 @@ cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_b
   if (nblk_total > 0) {
     // one warp per start block, then one warp per segment
     k_shr_count<<<(unsigned)((nblk_total + 3) / 4), 128, 0, s>>>(w, bs, blk_base, w.nlay);
-    k_shr_plan<<<(w.nlay + 31) / 32, 32, 0, s>>>(w, blk_base);
+    k_shr_plan<<<w.nlay, 32, 0, s>>>(w, blk_base);
     k_shr_write<<<(unsigned)((nblk_total + 3) / 4), 128, 0, s>>>(w, bs, blk_base, w.nlay);
   }
   return cudaGetLastError();
