@@ -170,6 +170,10 @@ struct lbl_ctx {
   bool have_ck = false;
   Arena arena;
   std::unique_ptr<HostPool> pool;  // planning workers, created on first use
+  // the result's copy-out, overlapped with the last merge launch
+  static constexpr int kOutChunks = 4;
+  cudaStream_t cstream = nullptr;
+  cudaEvent_t cev[kOutChunks + 1] = {};
   // merge buffers (ping-pong)
   double* mbuf[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t mcap = 0;
@@ -627,9 +631,25 @@ int ensure_merge_buffers(lbl_ctx* ctx, size_t n) {
   return LBL_OK;
 }
 
+// Where the merged radiance and transmittance go (host or device memory).
+struct OutSink {
+  double* rad;
+  double* tr;  // may be null
+};
+
+int ensure_copy_stream(lbl_ctx* ctx) {
+  if (ctx->cstream) return LBL_OK;
+  CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
+  for (auto& e : ctx->cev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return LBL_OK;
+}
+
 // Merge every layer of the batch bottom-up; result in mbuf[res], mbuf[res+1].
+// With a sink, the last launch runs in kOutChunks pieces and each piece is
+// copied to the sink on a second stream while the next one is merged; the
+// main stream waits for the copies.
 int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B, int n,
-              int* res, int precision) {
+              int* res, int precision, const OutSink* sink = nullptr) {
   size_t mx = 0;
   for (auto& d : B.ld) mx = std::max<size_t>(mx, d.npts);
   int rc = ensure_merge_buffers(ctx, mx + 8);
@@ -644,11 +664,17 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     runs.push_back({l, e});
     l = e;
   }
+  if (sink) {
+    const int rc2 = ensure_copy_stream(ctx);
+    if (rc2) return rc2;
+  }
+  const int nchunk = sink ? lbl_ctx::kOutChunks : 1;
   int cur = 0;
   double dv_old = 0.;
   int64_t n_old = 0;
-  StageTimer tm(ctx, "merge", (int64_t)runs.size());
-  for (auto [l, e] : runs) {
+  StageTimer tm(ctx, "merge", (int64_t)runs.size() + nchunk - 1);
+  for (size_t ri = 0; ri < runs.size(); ri++) {
+    const int l = runs[ri].first, e = runs[ri].second;
     const LayerDev& d = B.ld[l];
     if (n_old >= (int64_t(1) << 31)) return fail(ctx, LBL_E_RANGE, "layer grid of 2^31 or more points");
     MergeRun m{};
@@ -663,9 +689,41 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     }
     const int nxt = cur ^ 2;
     const double tbnd = (l == 0 && R.ipathl == 1) ? R.tmpbnd : 0.;
-    CK(launch_merge_run(m, B.w.vft + d.off_panel, B.w.od, d.npts, d.dv, ctx->mbuf[cur],
-                        ctx->mbuf[cur + 1], ctx->mbuf[nxt], ctx->mbuf[nxt + 1], tbnd, R.bndemi,
-                        R.iemit, ctx->stream, precision));
+    const bool last = ri + 1 == runs.size();
+    if (!(last && sink)) {
+      CK(launch_merge_run(m, B.w.vft + d.off_panel, B.w.od, d.npts, d.dv, ctx->mbuf[cur],
+                          ctx->mbuf[cur + 1], ctx->mbuf[nxt], ctx->mbuf[nxt + 1], tbnd, R.bndemi,
+                          R.iemit, ctx->stream, precision));
+    } else {
+      const cudaMemcpyKind kr = is_device_ptr(sink->rad) ? cudaMemcpyDeviceToDevice
+                                                          : cudaMemcpyDeviceToHost;
+      const cudaMemcpyKind kt = (sink->tr && is_device_ptr(sink->tr)) ? cudaMemcpyDeviceToDevice
+                                                                      : cudaMemcpyDeviceToHost;
+      const int64_t step = ((d.npts + nchunk - 1) / nchunk + 2399) / 2400 * 2400;
+      // all pieces are queued before the first copy: a copy to pageable
+      // host memory returns only when it is done
+      for (int c = 0; c < nchunk; c++) {
+        const int64_t lo = std::min<int64_t>(d.npts, c * step);
+        const int64_t hi = std::min<int64_t>(d.npts, lo + step);
+        CK(launch_merge_run(m, B.w.vft + d.off_panel, B.w.od, d.npts, d.dv, ctx->mbuf[cur],
+                            ctx->mbuf[cur + 1], ctx->mbuf[nxt], ctx->mbuf[nxt + 1], tbnd,
+                            R.bndemi, R.iemit, ctx->stream, precision, lo, hi));
+        CK(cudaEventRecord(ctx->cev[c], ctx->stream));
+      }
+      for (int c = 0; c < nchunk; c++) {
+        const int64_t lo = std::min<int64_t>(d.npts, c * step);
+        const int64_t hi = std::min<int64_t>(d.npts, lo + step);
+        if (hi == lo) continue;
+        CK(cudaStreamWaitEvent(ctx->cstream, ctx->cev[c], 0));
+        CK(cudaMemcpyAsync(sink->rad + lo, ctx->mbuf[nxt] + lo, sizeof(double) * (hi - lo), kr,
+                           ctx->cstream));
+        if (sink->tr)
+          CK(cudaMemcpyAsync(sink->tr + lo, ctx->mbuf[nxt + 1] + lo, sizeof(double) * (hi - lo),
+                             kt, ctx->cstream));
+      }
+      CK(cudaEventRecord(ctx->cev[nchunk], ctx->cstream));
+      CK(cudaStreamWaitEvent(ctx->stream, ctx->cev[nchunk], 0));
+    }
     cur = nxt;
     dv_old = d.dv;
     n_old = d.npts;
@@ -755,6 +813,9 @@ int lbl_ctx_destroy(lbl_ctx* ctx) {
   for (int k = 0; k < 4; k++)
     if (ctx->mbuf[k]) cudaFree(ctx->mbuf[k]);
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
+  for (auto e : ctx->cev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
   delete ctx;
   return LBL_OK;
 }
@@ -998,14 +1059,9 @@ int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nla
   rc = run_od(ctx, *run, B, precision);
   if (rc) return rc;
   int res = 0;
-  rc = run_merge(ctx, *run, layers, B, nlay, &res, precision);
+  const OutSink sink{rad, tr};
+  rc = run_merge(ctx, *run, layers, B, nlay, &res, precision, &sink);
   if (rc) return rc;
-  rc = copy_out(ctx, rad, ctx->mbuf[res], sizeof(double) * npts);
-  if (rc) return rc;
-  if (tr) {
-    rc = copy_out(ctx, tr, ctx->mbuf[res + 1], sizeof(double) * npts);
-    if (rc) return rc;
-  }
   CK(cudaStreamSynchronize(ctx->stream));
   harvest(ctx);
   return finish_od(ctx);

@@ -1961,12 +1961,13 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
 // fetched while this one merges.
 template <typename T>
 __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const double* vft_panel,
-                                                   const double* od, int32_t npts, double DV,
-                                                   const double* rad_in, const double* tr_in,
-                                                   double* rad_out, double* tr_out, double tbnd,
-                                                   double emis, int iemit) {
-  const int32_t f = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (f >= npts) return;
+                                                   const double* od, int32_t f_lo, int32_t f_hi,
+                                                   double DV, const double* rad_in,
+                                                   const double* tr_in, double* rad_out,
+                                                   double* tr_out, double tbnd, double emis,
+                                                   int iemit) {
+  const int32_t f = f_lo + (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (f >= f_hi) return;
   const int32_t p = f / 2400;
   const double vi = (vft_panel[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
   double ro = 0., to = 1.;
@@ -2277,17 +2278,19 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
 cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const double* od,
                              int64_t npts, double dv, const double* rad_in, const double* tr_in,
                              double* rad_out, double* tr_out, double tbnd, double emis, int iemit,
-                             cudaStream_t s, int precision) {
+                             cudaStream_t s, int precision, int64_t f_lo, int64_t f_hi) {
   if (m.nl < 1 || m.nl > kMergeRunMax) return cudaErrorInvalidValue;
   if (npts >= (int64_t(1) << 31) || m.n_old < 0) return cudaErrorInvalidValue;
-  if (npts <= 0) return cudaSuccess;
-  const unsigned nb = (unsigned)((npts + 255) / 256);
+  if (f_hi < 0) f_hi = npts;
+  if (f_lo < 0 || f_hi > npts || f_lo > f_hi) return cudaErrorInvalidValue;
+  if (f_hi == f_lo) return cudaSuccess;
+  const unsigned nb = (unsigned)((f_hi - f_lo + 255) / 256);
   if (precision == LBL_PREC_SPLIT)
-    k_merge_run<float><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)npts, dv, rad_in, tr_in,
-                                          rad_out, tr_out, tbnd, emis, iemit);
+    k_merge_run<float><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)f_lo, (int32_t)f_hi, dv,
+                                          rad_in, tr_in, rad_out, tr_out, tbnd, emis, iemit);
   else
-    k_merge_run<double><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)npts, dv, rad_in, tr_in,
-                                           rad_out, tr_out, tbnd, emis, iemit);
+    k_merge_run<double><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)f_lo, (int32_t)f_hi, dv,
+                                           rad_in, tr_in, rad_out, tr_out, tbnd, emis, iemit);
   return cudaGetLastError();
 }
 

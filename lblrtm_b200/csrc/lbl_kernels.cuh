@@ -147,10 +147,11 @@ struct MergeRun {
   int64_t od_off[kMergeRunMax];  // each layer's optical depths in Work::od
   EminT t[kMergeRunMax];
 };
+// Points [f_lo, f_hi) of the run's grid (f_hi < 0: to the end).
 cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const double* od,
                              int64_t npts, double dv, const double* rad_in, const double* tr_in,
                              double* rad_out, double* tr_out, double tbnd, double emis, int iemit,
-                             cudaStream_t s, int precision);
+                             cudaStream_t s, int precision, int64_t f_lo = 0, int64_t f_hi = -1);
 // Radiance Jacobians: one layer's forward merge plus its derivative rows,
 // the carrying of lower layers' rows through one merge step, the top
 // segment's transmittance products, and a central difference.
