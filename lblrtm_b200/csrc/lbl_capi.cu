@@ -533,10 +533,42 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   return LBL_OK;
 }
 
+// The second stream (plan-only kernels beside the far wing; the result's
+// copy-out) and its events, created on first use.
+int ensure_copy_stream(lbl_ctx* ctx) {
+  if (ctx->cstream) return LBL_OK;
+  CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
+  for (auto& e : ctx->cev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return LBL_OK;
+}
+
 // Optical depth of every layer of the batch into B.w.od.
 int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   cudaStream_t s = ctx->stream;
   const Work& w = B.w;
+  int64_t max_near = 0, max_panel = 0, max_win = 0, max_nblk = 0;
+  for (const LayerDev& d : B.ld) {
+    max_near = std::max<int64_t>(max_near, d.near_hi - d.near_lo);
+    max_panel = std::max<int64_t>(max_panel, d.npanel);
+    max_win = std::max<int64_t>(max_win, d.nwin);
+    max_nblk = std::max<int64_t>(max_nblk, d.blk_hi - d.blk_lo);
+  }
+  if (near_walk_smem(max_panel, max_win) > kNearWalkSmemMax)
+    return fail(ctx, LBL_E_RANGE, "layer grid too long for the near-wing panel walk");
+  if (R.icntnm && !ctx->have_ck) return fail(ctx, LBL_E_NOTREADY, "continuum table not uploaded");
+  // The work that needs only the plans and the lines (near-wing line
+  // scaling, the continuum, the panels' candidate ranges and radiation
+  // segments) runs on a second stream beside the far wing.
+  int rc = ensure_copy_stream(ctx);
+  if (rc) return rc;
+  cudaStream_t s2 = ctx->cstream;
+  CK(cudaEventRecord(ctx->cev[0], s));
+  CK(cudaStreamWaitEvent(s2, ctx->cev[0], 0));
+  CK(launch_near_lines(w, ctx->dl, max_near, s2));
+  if (R.icntnm) CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, s2));
+  CK(launch_panel_prep(w, ctx->dl, B.npanel_total, B.d_panel_layer, B.d_panel_base,
+                       B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s2));
+  CK(cudaEventRecord(ctx->cev[1], s2));
   {
     StageTimer t(ctx, "far_scale", 1);
     CK(launch_far_scale(w, ctx->dl, B.max_far, s));
@@ -549,31 +581,14 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     StageTimer t(ctx, "far_wing", B.nwin_total > 0 ? 1 : 0);
     CK(launch_far_wing(w, B.nwin_total, B.d_win_order, B.d_win_layer, precision, s));
   }
+  CK(cudaStreamWaitEvent(s, ctx->cev[1], 0));
   {
-    StageTimer t(ctx, "near_scale", 3);
-    int64_t max_near = 0, max_panel = 0, max_win = 0, max_nblk = 0;
-    for (const LayerDev& d : B.ld) {
-      max_near = std::max<int64_t>(max_near, d.near_hi - d.near_lo);
-      max_panel = std::max<int64_t>(max_panel, d.npanel);
-      max_win = std::max<int64_t>(max_win, d.nwin);
-      max_nblk = std::max<int64_t>(max_nblk, d.blk_hi - d.blk_lo);
-    }
-    if (near_walk_smem(max_panel, max_win) > kNearWalkSmemMax)
-      return fail(ctx, LBL_E_RANGE, "layer grid too long for the near-wing panel walk");
-    CK(launch_near_scale(w, ctx->dl, max_near, max_panel, max_win, max_nblk, s));
-  }
-  if (R.icntnm) {
-    if (!ctx->have_ck) return fail(ctx, LBL_E_NOTREADY, "continuum table not uploaded");
-    StageTimer t(ctx, "continuum", 1);
-    CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, s));
+    // the walk and the window limits; the per-line part ran on the second stream
+    StageTimer t(ctx, "near_scale", 3 + (R.icntnm ? 1 : 0) + 2);
+    CK(launch_near_walk(w, ctx->dl, max_panel, max_win, max_nblk, s));
   }
   {
     // near-wing sums, PANEL combination and optical depth in one pass
-    StageTimer t(ctx, "panel_prep", 2);
-    CK(launch_panel_prep(w, ctx->dl, B.npanel_total, B.d_panel_layer, B.d_panel_base,
-                         B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
-  }
-  {
     StageTimer t(ctx, "panels", 1);
     CK(launch_panels(w, ctx->dl, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
                      B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
@@ -636,13 +651,6 @@ struct OutSink {
   double* rad;
   double* tr;  // may be null
 };
-
-int ensure_copy_stream(lbl_ctx* ctx) {
-  if (ctx->cstream) return LBL_OK;
-  CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
-  for (auto& e : ctx->cev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  return LBL_OK;
-}
 
 // Merge every layer of the batch bottom-up; result in mbuf[res], mbuf[res+1].
 // With a sink, the last launch runs in kOutChunks pieces and each piece is

@@ -2217,14 +2217,19 @@ cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* wi
   return cudaGetLastError();
 }
 
-cudaError_t launch_near_scale(const Work& w, const DevLines& ln, int64_t max_near,
-                              int64_t max_panel, int64_t max_win, int64_t max_nblk,
+cudaError_t launch_near_lines(const Work& w, const DevLines& ln, int64_t max_near,
                               cudaStream_t s) {
   if (w.nlay > 65535) return cudaErrorInvalidValue;
   if (max_near > 0) {
     const dim3 g((unsigned)((max_near + 255) / 256), (unsigned)w.nlay);
     k_near_lines<<<g, 256, 0, s>>>(w, ln);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_near_walk(const Work& w, const DevLines& ln, int64_t max_panel,
+                             int64_t max_win, int64_t max_nblk, cudaStream_t s) {
+  if (w.nlay > 65535) return cudaErrorInvalidValue;
   const size_t smem = near_walk_smem(max_panel, max_win);
   if (smem > kNearWalkSmemMax) return cudaErrorInvalidValue;
   k_near_walk<<<w.nlay, 32, smem, s>>>(w, ln);

@@ -105,9 +105,10 @@ inline size_t near_walk_smem(int64_t npanel, int64_t nwin) {
   return d + (size_t)kWalkRing * 256 * sizeof(NearPre) + (size_t)(npanel + nwin) * sizeof(int32_t);
 }
 constexpr size_t kNearWalkSmemMax = 220 * 1024;
-cudaError_t launch_near_scale(const Work& w, const DevLines& ln, int64_t max_near,
-                              int64_t max_panel, int64_t max_win, int64_t max_nblk,
+cudaError_t launch_near_lines(const Work& w, const DevLines& ln, int64_t max_near,
                               cudaStream_t s);
+cudaError_t launch_near_walk(const Work& w, const DevLines& ln, int64_t max_panel,
+                             int64_t max_win, int64_t max_nblk, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
 cudaError_t launch_panel_prep(const Work& w, const DevLines& ln, int64_t npanel_total,
