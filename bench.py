@@ -115,7 +115,8 @@ def reference_arm(a):
     workers = a.cpu_workers or default_workers()
     # every step is one concurrent forward per worker: ~10 s of CPU time each
     steps = max(1, min(a.steps, 6))
-    res = cpu_run(a.nlines, workers, reps=max(1, min(a.warmup, 1)) + steps)
+    warm = max(1, min(a.warmup, 3))
+    res = cpu_run(a.nlines, workers, reps=warm + steps)
     timed = res[-steps:]
     pts = timed[0][0]
     wall = sum(r[1] for r in timed) / steps
@@ -124,7 +125,7 @@ def reference_arm(a):
             "nlines": a.nlines, "layers": 60, "precision": "fp64"}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
-        "steps": steps, "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": True,
+        "steps": steps, "warmup": warm, "ms_per_step": wall * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)", "config": cfgd,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
