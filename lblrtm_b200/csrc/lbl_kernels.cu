@@ -1890,6 +1890,51 @@ __device__ __forceinline__ void emin_point(double odv, double vi, const EminT& t
   em = ((T)1. - tr) * (bb + bbd * fi);
 }
 
+// emin_point in FP64 with the three divisions (two Planck quotients
+// e/(1-e) and the source weight's common denominator) taken from one
+// reciprocal of their product; differs from emin_point by a few units in
+// the last place.
+__device__ __forceinline__ void emin_point_1div(double odv, double vi, const EminT& t, double& tr,
+                                                double& em) {
+  double o = odv;
+  if (o < -kODLO) o = -kODLO;
+  tr = exp(-o);
+  const double d = tr - 1.;
+  const bool lin = o <= kODLO;
+  // Planck: the main branch needs e/(1-e) with e = exp(-x)
+  auto pre = [&](double xkt, double rk, double& e, double& small, int& br) {
+    br = 0;  // 0: zero, 1: small-x form, 2: main
+    e = 0.;
+    small = 0.;
+    if (xkt > 0.0) {
+      const double x = vi * rk;
+      if (x < 1e-2) {
+        br = 1;
+        small = (vi * vi) * xkt / (1. + 0.5 * x);
+      } else if (x <= 80.) {
+        br = 2;
+        e = exp(-x);
+      }
+    }
+  };
+  double e1, s1, e2, s2;
+  int b1, b2;
+  pre(t.xkt, t.rk, e1, s1, b1);
+  const bool bnd = t.xkta > 0.;
+  if (bnd) pre(t.xkta, t.rka, e2, s2, b2);
+  else b2 = 0, e2 = 0., s2 = 0.;
+  const double D1 = b1 == 2 ? 1. - e1 : 1.;
+  const double D2 = b2 == 2 ? 1. - e2 : 1.;
+  const double D3 = lin ? 1. : d * o;
+  const double r = 1. / ((D1 * D2) * D3);
+  const double v3 = (vi * vi) * vi;
+  const double bb = kRADCN1 * (b1 == 2 ? v3 * e1 * ((D2 * D3) * r) : s1);
+  const double bt = kRADCN1 * (b2 == 2 ? v3 * e2 * ((D1 * D3) * r) : s2);
+  const double bbd = bnd ? bt - bb : 0.;
+  const double fi = lin ? o * (1. / 6.) : 1. - 2. * ((tr * o + d) * ((D1 * D2) * r));
+  em = (1. - tr) * (bb + bbd * fi);
+}
+
 // Point f of the finer grid from the previous layer's field x (n_old
 // points): a copy where the grids agree, else RADNN's 4-point Lagrange
 // interpolation at P = 1 - r/(ITYPE+1) (ITYPE = DV/(DV_old-DV) rounded).
@@ -1981,7 +2026,8 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
       continue;
     }
     T tr, em;
-    emin_point<T>(odv, vi, m.t[l], tr, em);
+    if constexpr (sizeof(T) == 8) emin_point_1div(odv, vi, m.t[l], tr, em);
+    else emin_point<T>(odv, vi, m.t[l], tr, em);
     if (m.first && l == 0) {
       if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2, kRADCN2 / tbnd) * (T)emis;
       ro = (double)em;
