@@ -145,7 +145,12 @@ int lbl_ctx_create(int device, lbl_ctx** out);
 int lbl_ctx_destroy(lbl_ctx* ctx);
 /* Last error message of this context (empty if none). */
 const char* lbl_last_error(const lbl_ctx* ctx);
-/* Set the CUDA stream (cudaStream_t) used by later calls; NULL = default. */
+/* Set the CUDA stream (cudaStream_t) used by later calls; NULL = default.
+ * The context also owns one internal non-blocking stream (created on first
+ * use): the kernels that need only the layer plans run there beside the far
+ * wing, and lbl_forward copies its result out there while the last merge
+ * launch runs; both are joined to the caller's stream by events, and every
+ * call that returns results synchronises before it returns. */
 int lbl_set_stream(lbl_ctx* ctx, void* stream);
 
 /* ---- inputs ----------------------------------------------------------- */
