@@ -2001,9 +2001,9 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
   tr_out[f] = (double)tr * to;
 }
 
-// k_merge over m.nl consecutive layers on one grid (each layer's arithmetic
-// as in k_merge, in the same order); the next layer's optical depth is
-// fetched while this one merges.
+// k_merge over m.nl consecutive layers on one grid (in FP64 with EMIN's
+// quotients from one reciprocal, emin_point_1div); the next layer's optical
+// depth is fetched while this one merges.
 template <typename T>
 __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const double* vft_panel,
                                                    const double* od, int32_t f_lo, int32_t f_hi,
