@@ -1589,7 +1589,20 @@ struct PanelLine {
   double zint, zslope, sppsp, s0, sg, sx, s2, s3;
   int32_t lo1, hi1, lo2, hi2, lo3, hi3;
   int32_t pc;  // convolution panel of the line
+  uint32_t wm; // warps owning points of its R1 (bits 0-7), R2 (8-15), R3 (16-23) windows
 };
+
+// Warps of a 256-thread CTA whose threads own local points of [lo, hi]
+// (clipped to [0, n)), thread t owning the points i with i mod 256 == t.
+__device__ __forceinline__ uint32_t warps_of(int lo, int hi, int n) {
+  lo = lo < 0 ? 0 : lo;
+  hi = hi > n - 1 ? n - 1 : hi;
+  if (hi < lo) return 0u;
+  if (hi - lo >= 255) return 0xffu;
+  const int a = (lo & 255) >> 5, b = (hi & 255) >> 5;
+  const uint32_t up = 0xffu & ~((1u << a) - 1u), down = (2u << b) - 1u;
+  return ((lo >> 8) == (hi >> 8)) ? (up & down) : ((up | down) & 0xffu);
+}
 
 constexpr int kPanelThreads = 256;
 constexpr int kPanelStage = 128;  // lines staged per batch
@@ -1695,6 +1708,9 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
         q.hi2 = j1b - j2 + 600 * pc;
         q.lo3 = j1a - j3 + 150 * pc;
         q.hi3 = j1b - j3 + 150 * pc;
+        q.wm = warps_of(q.lo1 - R.a1, q.hi1 - R.a1, n1p) |
+               (warps_of(q.lo2 - R.a2, q.hi2 - R.a2, n2p) << 8) |
+               (warps_of(q.lo3 - R.a3, q.hi3 - R.a3, n3p) << 16);
         keep = (q.hi1 >= R.a1 && q.lo1 <= R.b1) || (q.hi2 >= R.a2 && q.lo2 <= R.b2) ||
                (q.hi3 >= R.a3 && q.lo3 <= R.b3);
       }
@@ -1712,8 +1728,11 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
     __syncthreads();
     for (int k = 0; k < n; k++) {
       const PanelLine& ql = st[k];
+      // a warp owning none of the line's window points skips it
+      const uint32_t wm = ql.wm >> warp;
+      if (!(wm & 0x10101u)) continue;
       // R1 (DV grid): F1 + FG + VERFN terms
-      if (ql.hi1 >= R.a1 && ql.lo1 <= R.b1) {
+      if ((wm & 1u) && ql.hi1 >= R.a1 && ql.lo1 <= R.b1) {
         const int lo = (ql.lo1 > R.a1 ? ql.lo1 : R.a1) - R.a1;
         const int hi = (ql.hi1 < R.b1 ? ql.hi1 : R.b1) - R.a1;
         const int off = R.a1 - 2400 * ql.pc - 1;  // g - pofs - 1 at i = 0
@@ -1730,7 +1749,7 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
         }
       }
       // R2 (4 DV): F2
-      if (ql.hi2 >= R.a2 && ql.lo2 <= R.b2) {
+      if ((wm & 0x100u) && ql.hi2 >= R.a2 && ql.lo2 <= R.b2) {
         const int lo = (ql.lo2 > R.a2 ? ql.lo2 : R.a2) - R.a2;
         const int hi = (ql.hi2 < R.b2 ? ql.hi2 : R.b2) - R.a2;
         const int off = R.a2 - 600 * ql.pc - 1;
@@ -1745,7 +1764,7 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
         }
       }
       // R3 (16 DV): F3
-      if (ql.hi3 >= R.a3 && ql.lo3 <= R.b3) {
+      if ((wm & 0x10000u) && ql.hi3 >= R.a3 && ql.lo3 <= R.b3) {
         const int lo = (ql.lo3 > R.a3 ? ql.lo3 : R.a3) - R.a3;
         const int hi = (ql.hi3 < R.b3 ? ql.hi3 : R.b3) - R.a3;
         if (tid >= lo && tid <= hi) {
