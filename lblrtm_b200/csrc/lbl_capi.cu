@@ -556,11 +556,16 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   if (near_walk_smem(max_panel, max_win) > kNearWalkSmemMax)
     return fail(ctx, LBL_E_RANGE, "layer grid too long for the near-wing panel walk");
   if (R.icntnm && !ctx->have_ck) return fail(ctx, LBL_E_NOTREADY, "continuum table not uploaded");
-  // The work that needs only the plans and the lines (near-wing line
-  // scaling, the continuum, the panels' candidate ranges and radiation
-  // segments) runs on a second stream beside the far wing.
   int rc = ensure_copy_stream(ctx);
   if (rc) return rc;
+  {
+    StageTimer t(ctx, "far_scale", 1);
+    CK(launch_far_scale(w, ctx->dl, B.max_far, s));
+  }
+  // The work that needs only the plans and the lines (near-wing line
+  // scaling, the continuum, the panels' candidate ranges and radiation
+  // segments) runs on a second stream beside SHRINK and the far wing; it
+  // starts after the far-wing line scaling, which heads the longer chain.
   cudaStream_t s2 = ctx->cstream;
   CK(cudaEventRecord(ctx->cev[0], s));
   CK(cudaStreamWaitEvent(s2, ctx->cev[0], 0));
@@ -569,10 +574,6 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   CK(launch_panel_prep(w, ctx->dl, B.npanel_total, B.d_panel_layer, B.d_panel_base,
                        B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s2));
   CK(cudaEventRecord(ctx->cev[1], s2));
-  {
-    StageTimer t(ctx, "far_scale", 1);
-    CK(launch_far_scale(w, ctx->dl, B.max_far, s));
-  }
   {
     StageTimer t(ctx, "shrink", 3);
     CK(launch_shrink(w, ctx->dl.bs, B.d_blk_base, B.nblk_total, s));
