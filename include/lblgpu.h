@@ -163,7 +163,11 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* lines);
 
 /* Read a TAPE3 file (Fortran unformatted, 4-byte record markers, the
  * INPUT_HEADER/INPUT_BLOCK records of struct_types.f90:106-125) and upload
- * it.  Returns the number of line records through *nlines (may be NULL). */
+ * it.  Returns the number of line records through *nlines (may be NULL).
+ * A truncated or malformed record gives LBL_E_FORMAT, a panel of more than
+ * 250 records LBL_E_NREC, descending centres LBL_E_UNSORTED.  With ctx NULL
+ * the file is read and checked the same way but nothing is uploaded (no
+ * device is needed). */
 int lbl_lines_load_tape3(lbl_ctx* ctx, const char* path, int64_t* nlines);
 
 /* Upload the H2O continuum coefficient table (CONTNM, contnm.f90:279-324). */
@@ -210,16 +214,20 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
  * only hands out buffers it already owns.  Runs the same merge kernel as
  * lbl_merge_layer on device `device` and CUDA stream `stream` (NULL =
  * default), with no context: od, rad_in, tr_in, rad_out and tr_out must all
- * be caller-owned DEVICE memory (host pointers give LBL_E_ARG), and the call
- * allocates nothing.  Its only scratch is a fixed device array inside the
+ * be caller-owned memory of device `device` (host pointers or another
+ * GPU's memory give LBL_E_ARG), and the call allocates nothing.  An output
+ * must not share memory with rad_in, tr_in or the other output (LBL_E_ARG);
+ * it may be od itself.  IEMIT must be 0 or 1; with IEMIT=0 tr_in and tr_out
+ * are not used.  Its only scratch is a fixed device array inside the
  * library, about 72 KB on every device that loads it, kept until the
  * process exits; it bounds a layer to LBL_NOALLOC_MAX_PANELS panels of 2400
  * points (19,660,800 points); longer layers return LBL_E_RANGE.  The first
- * call on a device looks up that array's device address, so make it before
- * any stream capture.  Every call rewrites all of the scratch it reads, but
- * all calls share the one array: calls that overlap on the GPU (different
- * host threads or streams) race.  The call returns after its stream has
- * finished the merge. */
+ * call on a device looks up that array's device address; make that first
+ * call before any stream capture on the device.  Every call rewrites all of
+ * the scratch it reads, but all calls share the one array: calls that
+ * overlap on the GPU (different host threads or streams) race.  The caller's
+ * current device is restored before the call returns, and the call returns
+ * after its stream has finished the merge. */
 #define LBL_NOALLOC_MAX_PANELS 8192
 int lbl_merge_layer_noalloc(int device, const lbl_run* run, const lbl_layer* layer,
                             int32_t first, double dv_old, const double* rad_in,

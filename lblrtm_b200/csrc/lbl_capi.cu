@@ -837,8 +837,16 @@ int lbl_set_stream(lbl_ctx* ctx, void* stream) {
   return LBL_OK;
 }
 
-int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
-  if (!ctx || !L || L->n < 0) return fail(ctx, LBL_E_ARG, "bad lines");
+}  // extern "C"
+
+namespace {
+// The host-side checks of a line list (the conditions RDLIN assumes or
+// STOPs on): ascending centres, coupling records after their line, TAPE3
+// panels of at most 250 records.  Fills the searchable centres (coupling
+// records repeat the previous line's centre) and the panel starts.
+int validate_lines(lbl_ctx* ctx, const lbl_lines* L, std::vector<double>* vs_out,
+                   std::vector<int64_t>* bs_out) {
+  if (!L || L->n < 0) return fail(ctx, LBL_E_ARG, "bad lines");
   const int64_t n = L->n;
   if (n >= (int64_t(1) << 31) - 8) return fail(ctx, LBL_E_RANGE, "more than 2^31 line records");
   if (n > 0 && (!L->vnu || !L->sp || !L->alfa || !L->epp || !L->mol || !L->hwhms ||
@@ -848,7 +856,8 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   // coefficients in the centre field (RDLIN :818-837, LNCOR1 :1039-1061):
   // they are skipped in the order check, and the searchable copy of the
   // centres repeats the previous line's there.
-  std::vector<double> vs(L->vnu, L->vnu + n);
+  std::vector<double>& vs = *vs_out;
+  vs.assign(L->vnu, L->vnu + n);
   {
     double last = 0.;
     bool have = false;
@@ -871,7 +880,8 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
         return fail(ctx, LBL_E_FORMAT,
                     "coupled line without its coefficient record at record " + std::to_string(i));
   }
-  std::vector<int64_t> bs;
+  std::vector<int64_t>& bs = *bs_out;
+  bs.clear();
   if (L->nblock > 0 && L->block_start) {
     bs.assign(L->block_start, L->block_start + L->nblock + 1);
     if (bs.front() != 0 || bs.back() != n) return fail(ctx, LBL_E_ARG, "block_start must span 0..n");
@@ -883,6 +893,19 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
     if (bs[b + 1] < bs[b]) return fail(ctx, LBL_E_ARG, "block_start not increasing");
     if (bs[b + 1] - bs[b] > 250) return fail(ctx, LBL_E_NREC, "RDLIN; NREC GT LIMIN");
   }
+  return LBL_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
+  if (!ctx) return LBL_E_ARG;
+  std::vector<double> vs;
+  std::vector<int64_t> bs;
+  const int vrc = validate_lines(ctx, L, &vs, &bs);
+  if (vrc) return vrc;
+  const int64_t n = L->n;
   ctx->h_vnu = vs;
   ctx->h_sp.assign(L->sp, L->sp + n);
   ctx->h_pshift.assign(L->pshift, L->pshift + n);
@@ -1300,7 +1323,7 @@ extern "C" int lbl_tape3_parse(const char* path, std::vector<double>* vnu, std::
                                std::string* err);
 
 extern "C" int lbl_lines_load_tape3(lbl_ctx* ctx, const char* path, int64_t* nlines) {
-  if (!ctx || !path) return LBL_E_ARG;
+  if (!path) return fail(ctx, LBL_E_ARG, "NULL path");
   std::vector<double> vnu;
   std::vector<float> sp, alfa, epp, hw, tmp, psh;
   std::vector<int32_t> mol, iflg;
@@ -1321,6 +1344,14 @@ extern "C" int lbl_lines_load_tape3(lbl_ctx* ctx, const char* path, int64_t* nli
   L.iflg = iflg.data();
   L.nblock = (int64_t)bs.size() - 1;
   L.block_start = bs.data();
+  if (!ctx) {
+    // no context: read and check the file only
+    std::vector<double> vs;
+    std::vector<int64_t> bchk;
+    rc = validate_lines(nullptr, &L, &vs, &bchk);
+    if (rc == LBL_OK && nlines) *nlines = L.n;
+    return rc;
+  }
   rc = lbl_lines_upload(ctx, &L);
   if (rc == LBL_OK && nlines) *nlines = L.n;
   return rc;

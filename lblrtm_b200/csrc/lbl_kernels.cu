@@ -1564,7 +1564,54 @@ __device__ __forceinline__ PanelRange panel_range(const LayerDev& L, int32_t p) 
   if (r.a3 < 1) r.a3 = 1;
   r.b3 = (d2 - 1) / 4 + 3;
   if (r.b3 > n_r3) r.b3 = n_r3;
+  // a first panel starting at or below zero wavenumber folds its grids from
+  // point 0 up (RSYM), so it sums them from there
+  if (p == 0 && L.vft0 <= 0.) r.a1 = r.a2 = r.a3 = 0;
   return r;
+}
+
+// RSYM (src/oprop.f90:2145-2200): folds the negative-wavenumber part of a
+// grid of spacing dv starting at vft <= 0 onto the positive part, in place.
+// R[i] is grid point i (its wavenumber vft + (i-1) dv); the loop reads R[0]
+// and up to R[2 IP + 1] with IP <= 32, all inside the first panel's grids.
+__device__ void rsym(double* R, double dv, double vft) {
+  long ip = fint((-vft / dv) + 1. - .000001);
+  ip = ip + 1;
+  double P = (double(ip - 1) + vft / dv) * 2.;
+  const double pst = P;
+  if (P > 1.) P = P - 1.;
+  const double wn1 = -P * (P - 1.) * (P - 2.) / 6.;
+  const double w0 = (P * P - 1.) * (P - 2.) / 2.;
+  const double w1 = -P * (P + 1.) * (P - 2.) / 2.;
+  const double w2 = P * (P * P - 1.) / 6.;
+  long k = ip;
+  const long ipmax = ip + ip - 1;
+  if (pst > 1.) {
+    double b1 = R[ip - 2], b2 = R[ip - 1], c1 = R[k], c2;
+    for (long i = ip; i <= ipmax; i++) {
+      k = k - 1;
+      c2 = c1;
+      if (k < 1) return;
+      c1 = R[k];
+      R[k] = R[k] + wn1 * R[i + 1] + w0 * R[i] + w1 * b2 + w2 * b1;
+      b1 = b2;
+      b2 = R[i];
+      if (k <= 2) continue;
+      R[i] = R[i] + wn1 * c2 + w0 * c1 + w1 * R[k - 1] + w2 * R[k - 2];
+    }
+    return;
+  }
+  double c1 = R[ip], c2 = R[ip + 1], b2 = R[ip - 1], b1;
+  for (long i = ip; i <= ipmax; i++) {
+    k = k - 1;
+    b1 = b2;
+    b2 = R[i];
+    if (k <= 1) return;
+    R[i] = R[i] + wn1 * c2 + w0 * c1 + w1 * R[k] + w2 * R[k - 1];
+    c2 = c1;
+    c1 = R[k];
+    R[k] = R[k] + wn1 * R[i + 2] + w0 * R[i + 1] + w1 * b2 + w2 * b1;
+  }
 }
 
 // Candidate near-wing lines of every panel: TAPE3 lines whose centre lies
@@ -1780,6 +1827,17 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
     }
     __syncthreads();
   }
+  // RSYM on the three grids of a first panel starting at or below zero
+  // (HIRAC1 :501-505), before the far wing and continuum are added
+  if (R.a1 == 0) {
+    if (tid == 0) {
+      const double vft = w.vft[L.off_panel];
+      rsym(s1, L.dv, vft);
+      rsym(s2, L.dvr2, vft);
+      rsym(s3, L.dvr3, vft);
+    }
+    __syncthreads();
+  }
   // R3 += XINT(R4 of the owning panel's window) + XINT(ABSRB): R3 point g
   // belongs to panel 0 for g <= 155, else to panel (g-6)/150 (N1R3/N2R3,
   // src/oprop.f90:474-486)
@@ -1816,6 +1874,7 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
   if (L.jrad != 0) {
     for (int i = tid; i < n1p; i += kPanelThreads) {
       const int32_t g = R.a1 + i;
+      if (g < 33) continue;  // below V1: a folded first panel's lower points
       od_out[g - 33] = s1[i] + interp4(r2, (g - 1) / 4 + 1, (g - 1) % 4);
     }
     return;
@@ -1858,7 +1917,7 @@ __global__ void __launch_bounds__(kPanelThreads, 4)
     for (int i = tid; i < n1p; i += kPanelThreads) {
       const int32_t g = R.a1 + i;
       const int32_t I = g - 2400 * p;
-      if (I < ilo || I > ihi) continue;
+      if (I < ilo || I > ihi || g < 33) continue;
       double od = s1[i] + interp4(r2, (g - 1) / 4 + 1, (g - 1) % 4);
       int lo = 0, hi = ns - 1;
       while (lo < hi) {
@@ -1982,6 +2041,27 @@ __device__ __forceinline__ void merge_regrid(const double* x, const double* y, i
   if (y) yo = a1 * y[c0] + a2 * y[c1] + a3 * y[c2] + a4 * y[c3];
 }
 
+// ABSMRG's regrid of the accumulated optical depth (src/xmerge.f90:437-682):
+// the interpolation of merge_regrid, except at the end of the old field.
+// ABSMRG advances its old-point counter NVS with every new point (label
+// 190); once NVS passes the old field's last point but two and no old data
+// is left, every later point takes the mean of the last two old points
+// (label 210).  Point f-1 used NVS = q*ITYPE + max(r, 1) (q, r = (f-1) divided
+// by ITYPE+1), and NVS never decreases, so point f lies in that tail when
+// NVS of point f-1 has reached n_old-2.
+__device__ __forceinline__ double absmrg_regrid(const double* x, int32_t n_old, int32_t f,
+                                                int32_t itype) {
+  if (itype > 0 && f >= 2 && n_old >= 2) {
+    const int32_t g = f - 1, LL = itype + 1;
+    const int32_t q = g / LL, r = g - q * LL;
+    const int32_t nvs = q * itype + (r > 1 ? r : 1);
+    if (nvs >= n_old - 2) return (x[n_old - 1] + x[n_old - 2]) * 0.5;
+  }
+  double xo = 0., unused = 0.;
+  merge_regrid(x, nullptr, n_old, f, itype, xo, unused);
+  return xo;
+}
+
 template <typename T>
 __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const double* od,
                         int first, double dv_old, int64_t n_old64, const double* rad_in,
@@ -1998,8 +2078,7 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
   const int32_t itype = (first || dv_old == DV) ? 0 : (int32_t)fint(DV / (dv_old - DV) + 0.5);
   if (iemit == 0) {
     // ABINIT / ABSMRG: optical depths add
-    double old = 0., unused = 0.;
-    if (!first) merge_regrid(rad_in, nullptr, n_old, f, itype, old, unused);
+    const double old = first ? 0. : absmrg_regrid(rad_in, n_old, f, itype);
     rad_out[f] = odv + old;
     if (tr_out) tr_out[f] = 0.;
     return;
@@ -2035,7 +2114,10 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
   const int32_t p = f / 2400;
   const double vi = (vft_panel[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
   double ro = 0., to = 1.;
-  if (!m.first) merge_regrid(rad_in, iemit ? tr_in : nullptr, m.n_old, f, m.itype, ro, to);
+  if (!m.first) {
+    if (iemit) merge_regrid(rad_in, tr_in, m.n_old, f, m.itype, ro, to);
+    else ro = absmrg_regrid(rad_in, m.n_old, f, m.itype);
+  }
   double odn = od[m.od_off[0] + f];
   for (int l = 0; l < m.nl; l++) {
     const double odv = odn;

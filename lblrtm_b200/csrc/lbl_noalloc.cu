@@ -10,6 +10,7 @@
 // in the file-scope device array below, whose size bounds the layer length.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -33,14 +34,38 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 unsigned char* g_scratch_ptr[kMaxDevices] = {nullptr};
 
-bool on_device(const void* p) {
+// Device memory of GPU `device` (a buffer on another GPU would be read as a
+// peer access, which faults unless peer access is enabled).
+bool on_device(const void* p, int device) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == device;
 }
+
+// Byte ranges [a, a+na) and [b, b+nb) share memory.
+bool overlap(const void* a, int64_t na, const void* b, int64_t nb) {
+  if (!a || !b || na <= 0 || nb <= 0) return false;
+  const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + (uintptr_t)nb && y < x + (uintptr_t)na;
+}
+
+// Restores the caller's current device when the call returns.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 }  // namespace
 
@@ -50,15 +75,36 @@ extern "C" int lbl_merge_layer_noalloc(int device, const lbl_run* run, const lbl
                                        double* rad_out, double* tr_out, int64_t n_new,
                                        void* stream) {
   if (!run || !layer || !od || !rad_out || device < 0 || device >= kMaxDevices) return LBL_E_ARG;
+  if (run->iemit != 0 && run->iemit != 1) return LBL_E_ARG;
   if (run->iemit == 1 && !tr_out) return LBL_E_ARG;
   if (run->iemit == 1 && run->ipathl != 1) return LBL_E_ARG;
   if (!first && (!rad_in || (run->iemit == 1 && !tr_in) || n_old < 1)) return LBL_E_ARG;
-  if (!(layer->dv > 0.) || !(run->v2 > run->v1)) return LBL_E_ARG;
+  if (!(layer->dv > 0.) || !(run->v2 > run->v1) || !(run->v1 > 0.) || n_new < 1)
+    return LBL_E_ARG;
   if (!first && layer->dv > dv_old) return LBL_E_ITYPE;
+  // the kernel reads neighbouring points of rad_in/tr_in while it writes
+  // rad_out/tr_out, so an output shares memory with no other buffer, except
+  // that it may be od itself (each point of od is read and then written by
+  // the same thread)
+  {
+    const int64_t bo = 8 * n_new, bi = first ? 0 : 8 * n_old;
+    const double* outs[2] = {rad_out, run->iemit == 1 ? tr_out : nullptr};
+    const double* ins[2] = {first ? nullptr : rad_in,
+                            (first || run->iemit != 1) ? nullptr : tr_in};
+    for (const double* o : outs)
+      for (const double* i : ins)
+        if (overlap(o, bo, i, bi)) return LBL_E_ARG;
+    if (overlap(outs[0], bo, outs[1], bo)) return LBL_E_ARG;
+    for (const double* o : outs)
+      if (o != od && overlap(o, bo, od, bo)) return LBL_E_ARG;
+  }
+  DeviceGuard guard;
   if (cudaSetDevice(device) != cudaSuccess) return LBL_E_CUDA;
-  // inputs and outputs must already be device memory: nothing is staged
-  if (!on_device(od) || !on_device(rad_out) || (tr_out && !on_device(tr_out)) ||
-      (!first && (!on_device(rad_in) || (tr_in && !on_device(tr_in)))))
+  // inputs and outputs must already be memory of this device: nothing is staged
+  if (!on_device(od, device) || !on_device(rad_out, device) ||
+      (run->iemit == 1 && !on_device(tr_out, device)) ||
+      (!first && (!on_device(rad_in, device) ||
+                  (run->iemit == 1 && !on_device(tr_in, device)))))
     return LBL_E_ARG;
   // panel origins VFT_p exactly as PANEL accumulates them; the layer's
   // length is bounded by the scratch table
@@ -113,7 +159,10 @@ extern "C" int lbl_merge_layer_noalloc(int device, const lbl_run* run, const lbl
           cudaSuccess)
     return LBL_E_CUDA;
   const double tbnd = (first && run->ipathl == 1) ? run->tmpbnd : 0.;
-  if (launch_merge(d_plan, d_vft, od, npts, first, dv_old, n_old, rad_in, tr_in, rad_out, tr_out,
+  // IEMIT=0 leaves tr_in/tr_out unused
+  const double* tin = run->iemit == 1 ? tr_in : nullptr;
+  double* tout = run->iemit == 1 ? tr_out : nullptr;
+  if (launch_merge(d_plan, d_vft, od, npts, first, dv_old, n_old, rad_in, tin, rad_out, tout,
                    tbnd, run->bndemi, run->iemit, layer->tzu, s) != cudaSuccess)
     return LBL_E_CUDA;
   // the host-side plan buffers are on this stack frame: wait for the copies

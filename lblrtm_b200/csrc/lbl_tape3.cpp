@@ -21,14 +21,18 @@
 
 namespace {
 
-bool read_record(FILE* f, std::vector<char>& buf) {
+// One Fortran record: 1 read, 0 clean end of file (no bytes left), -1 a
+// record cut short or with differing length markers.
+int read_record(FILE* f, std::vector<char>& buf) {
   int32_t n1 = 0, n2 = 0;
-  if (std::fread(&n1, 4, 1, f) != 1) return false;
-  if (n1 < 0 || n1 > (1 << 28)) return false;
+  const size_t got = std::fread(&n1, 1, 4, f);
+  if (got == 0 && std::feof(f)) return 0;
+  if (got != 4) return -1;
+  if (n1 < 0 || n1 > (1 << 28)) return -1;
   buf.resize(n1);
-  if (n1 && std::fread(buf.data(), 1, n1, f) != (size_t)n1) return false;
-  if (std::fread(&n2, 4, 1, f) != 1) return false;
-  return n1 == n2;
+  if (n1 && std::fread(buf.data(), 1, n1, f) != (size_t)n1) return -1;
+  if (std::fread(&n2, 4, 1, f) != 1) return -1;
+  return n1 == n2 ? 1 : -1;
 }
 
 template <typename T>
@@ -57,13 +61,13 @@ int lbl_tape3_parse(const char* path, std::vector<double>* vnu, std::vector<floa
     return LBL_E_ARG;
   }
   std::vector<char> rec;
-  if (!read_record(f, rec) || rec.size() < 80) {
+  if (read_record(f, rec) != 1 || rec.size() < 80) {
     std::fclose(f);
     *err = "TAPE3: missing file header record";
     return LBL_E_FORMAT;
   }
   if (rec[6 * 8 + 7] == '^') {
-    if (!read_record(f, rec)) {
+    if (read_record(f, rec) != 1) {
       std::fclose(f);
       *err = "TAPE3: missing negative-EPP record";
       return LBL_E_FORMAT;
@@ -73,7 +77,13 @@ int lbl_tape3_parse(const char* path, std::vector<double>* vnu, std::vector<floa
   bs->push_back(0);
   const size_t NL = 250;
   for (;;) {
-    if (!read_record(f, rec)) break;  // end of file
+    const int hr = read_record(f, rec);
+    if (hr == 0) break;  // end of file
+    if (hr < 0) {
+      std::fclose(f);
+      *err = "TAPE3: truncated or malformed panel header record";
+      return LBL_E_FORMAT;
+    }
     if (rec.size() != 24) {
       std::fclose(f);
       *err = "TAPE3: panel header record is not 24 bytes";
@@ -81,7 +91,7 @@ int lbl_tape3_parse(const char* path, std::vector<double>* vnu, std::vector<floa
     }
     const int32_t nrec = at<int32_t>(rec, 16);
     std::vector<char> blk;
-    if (!read_record(f, blk)) {
+    if (read_record(f, blk) != 1) {
       std::fclose(f);
       *err = "TAPE3: truncated panel";
       return LBL_E_FORMAT;

@@ -72,6 +72,9 @@ const double OD_LO = 0.06;                 // src/lblparams.f90:47
 inline long fint(double x) { return (long)x; }
 
 std::string g_err;
+// RSYM is always applied as the reference does; a test switches it off to
+// show that the fold changes the lowest points of a run starting near zero.
+bool g_rsym = true;
 int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
@@ -1360,7 +1363,7 @@ int hirac1(Layer& S, std::vector<PanelOut>& panels) {
     N2R3 = NLIM3 + (NSHIFT / 16) - 1 + 3;
     (void)N2R1;
     (void)N2R2;
-    if (VFT <= 0.) {
+    if (VFT <= 0. && g_rsym) {
       rsym(R1.at1(), DV, VFT);
       rsym(R2.at1(), DVR2, VFT);
       rsym(R3.at1(), DVR3, VFT);
@@ -1825,6 +1828,8 @@ int64_t npts_of(const lbl_run& R, double dv) {
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
+
+void orc_set_rsym(int on) { g_rsym = on != 0; }
 
 // PATH DV rule (src/lblrtm.f90:5355-5510), standard path (JTYPE=0, IOD=0).
 int orc_dv_rule(const lbl_run* R, lbl_layer* Ls, int nlay) {

@@ -70,3 +70,21 @@ def test_brightness_temperature_matches_oracle():
 def test_layer_npts_invalid():
     run = abi.make_run(v1=600.0, v2=500.0)
     assert gpu.layer_npts(run, 0.01) == -1
+
+
+def test_noalloc_rejects_bad_iemit_before_device_work():
+    """IEMIT other than 0 or 1 is refused before any CUDA call (so the GPU
+    never sees the emission branch with a NULL transmittance output)."""
+    lib = gpu.load()
+    lay = abi.Layer()
+    lay.tave = 250.0
+    lay.dv = 0.01
+    buf = [np.zeros(8) for _ in range(2)]
+    P = [C.c_void_p(b.ctypes.data) for b in buf]
+    for iemit in (2, -1):
+        run = abi.make_run(v1=600.0, v2=700.0, iemit=iemit)
+        assert lib.lbl_merge_layer_noalloc(0, C.byref(run), C.byref(lay), 1, 0.0, None, None,
+                                           0, P[0], P[1], None, 8, None) == 1
+    run = abi.make_run(v1=-5.0, v2=700.0, iemit=0)
+    assert lib.lbl_merge_layer_noalloc(0, C.byref(run), C.byref(lay), 1, 0.0, None, None, 0,
+                                       P[0], P[1], None, 8, None) == 1

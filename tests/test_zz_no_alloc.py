@@ -60,12 +60,43 @@ def test_noalloc_rejects_host_buffers_and_long_layers():
     lay = abi.Layer()
     lay.tave = 250.0
     lay.dv = 1e-5  # 1e8 points: beyond LBL_NOALLOC_MAX_PANELS * 2400
-    host = np.zeros(16)
-    P = C.c_void_p(host.ctypes.data)
+    host = [np.zeros(16) for _ in range(3)]
+    H = [C.c_void_p(h.ctypes.data) for h in host]
     assert lib.lbl_merge_layer_noalloc(0, C.byref(run), C.byref(lay), 1, 0.0, None, None, 0,
-                                       P, P, P, 16, None) == 1  # LBL_E_ARG: host memory
+                                       H[0], H[1], H[2], 16, None) == 1  # LBL_E_ARG: host memory
     import torch
-    d = torch.zeros(16, dtype=torch.float64, device="cuda")
-    D = C.c_void_p(d.data_ptr())
+    d = [torch.zeros(16, dtype=torch.float64, device="cuda") for _ in range(3)]
+    D = [C.c_void_p(t.data_ptr()) for t in d]
     assert lib.lbl_merge_layer_noalloc(0, C.byref(run), C.byref(lay), 1, 0.0, None, None, 0,
-                                       D, D, D, 16, None) == 7  # LBL_E_RANGE: too long
+                                       D[0], D[1], D[2], 16, None) == 7  # LBL_E_RANGE: too long
+
+
+def test_noalloc_rejects_aliased_outputs_and_restores_device(gpu_ctx):
+    """Outputs that overlap an input the kernel reads at neighbouring points
+    (or each other) are refused before any device work; the caller's current
+    device is left as it was."""
+    import torch
+
+    lib = gpu.load()
+    run = abi.make_run(v1=600.0, v2=700.0, iemit=1, tmpbnd=290.0)
+    lays = abi.make_layers(configs.atmosphere(2, ptop=500.0))
+    gpu.dv_rule(run, lays)
+    n0 = gpu.layer_npts(run, lays[0].dv)
+    n1 = gpu.layer_npts(run, lays[1].dv)
+    big = torch.zeros(4 * (n0 + n1), dtype=torch.float64, device="cuda")
+    od = torch.ones(n1, dtype=torch.float64, device="cuda")
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    rad_in, tr_in = big[:n0], big[n0:2 * n0]
+    before = torch.cuda.current_device()
+    # rad_out starting inside rad_in
+    rc = lib.lbl_merge_layer_noalloc(0, C.byref(run), C.byref(lays[1]), 0, lays[0].dv,
+                                     P(rad_in), P(tr_in), n0, P(od), P(big[n0 // 2:]),
+                                     P(big[2 * n0 + 2 * n1:]), n1, None)
+    assert rc == 1
+    # rad_out and tr_out overlapping
+    out = big[2 * n0:]
+    rc = lib.lbl_merge_layer_noalloc(0, C.byref(run), C.byref(lays[1]), 0, lays[0].dv,
+                                     P(rad_in), P(tr_in), n0, P(od), P(out), P(out[1:]), n1,
+                                     None)
+    assert rc == 1
+    assert torch.cuda.current_device() == before
