@@ -153,6 +153,17 @@ const char* lbl_last_error(const lbl_ctx* ctx);
  * call that returns results synchronises before it returns. */
 int lbl_set_stream(lbl_ctx* ctx, void* stream);
 
+/* Cap the device memory the context holds (lines, tables, work arenas,
+ * merge and Jacobian buffers) at `bytes`; 0 removes the cap.  The context's
+ * grow-only work buffers are released (after its stream is idle) and
+ * allocated again within the cap by later calls.  A call that would need
+ * more returns LBL_E_NOMEM (as when the device itself is full) and leaves
+ * the context usable.  The batched calls size their groups of profiles, and
+ * the Jacobians their chunks of parameters, to fit under the cap. */
+int lbl_set_memory_limit(lbl_ctx* ctx, int64_t bytes);
+/* Device memory the context holds now, in bytes (-1 for a NULL context). */
+int64_t lbl_memory_used(const lbl_ctx* ctx);
+
 /* ---- inputs ----------------------------------------------------------- */
 
 /* Copy the TAPE3 line records (host arrays) to the device, where they stay
@@ -272,6 +283,43 @@ int lbl_forward_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
 int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
                  int32_t nlay, const int32_t* mols, int32_t nq, double* rad,
                  double* jac, int64_t npts, int32_t precision);
+
+/* How the batched Jacobians obtain a layer's optical-depth derivatives. */
+typedef enum lbl_jac_mode {
+  LBL_JAC_CENTRAL = 0,    /* central differences (T +-0.1 K, amount +-1 %)
+                             merged with the exact derivative of the merge:
+                             the derivative of the discrete forward model */
+  LBL_JAC_REFERENCE = 1   /* the reference's analytic-Jacobian definitions
+                             (src/lblrtm.f90:2855-3067): a pass at T + 1 K and
+                             one per molecule with that molecule alone (other
+                             amounts zero, WK(7) added to WBROAD), merged by
+                             the TDERIVup/QDERIVup rows (src/xmerge.f90:
+                             5786-6144) from the quantities EMDT saves */
+} lbl_jac_mode;
+
+/* Forward and Jacobians of many profiles (uneven layer counts) in one call:
+ * the batched form of the reference's analytic-Jacobian run.  Each profile
+ * costs one optical-depth pass per derivative pass (LBL_JAC_REFERENCE:
+ * 1 + nq after the nominal one; LBL_JAC_CENTRAL: 2 (1 + nq)) queued back to
+ * back without host waits, then one merge sweep that forms every layer's
+ * row and carries it to the top through the later layers.  When a
+ * profile's work space for all parameters would not fit the device (or the
+ * lbl_set_memory_limit cap), the parameters are taken in chunks and the
+ * nominal pass is recomputed for each chunk.
+ *   dv_chan > 0: radiance and Jacobians are averaged over channels
+ *     [V1 + c dv_chan, V1 + (c+1) dv_chan), c < floor((V2-V1)/dv_chan) (a
+ *     boxcar instrument function); dv_chan = 0: each profile's top grid.
+ *   rad: concatenated per profile, profile p at offsets[p] (nprof+1
+ *        entries, output), rad_cap doubles available;
+ *   jac: profile p's block jac[jac_off[p] + (k*nlay[p] + l)*n_p + i]
+ *        (k = 0: d/dT_l, k = 1..nq: d/d ln W_{mols[k-1],l}), jac_off output
+ *        (nprof+1 entries), jac_cap doubles available.
+ * Host or device buffers; upwelling radiance only. */
+int lbl_adjoint_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers,
+                      const int32_t* nlay, int32_t nprof, const int32_t* mols,
+                      int32_t nq, int32_t mode, double dv_chan, double* rad,
+                      int64_t* offsets, int64_t rad_cap, double* jac,
+                      int64_t* jac_off, int64_t jac_cap, int32_t precision);
 
 /* ---- timing and work counters ------------------------------------------
  * Per-stage device time, launch count and algorithmic work of the calls

@@ -19,6 +19,9 @@ STATUS = {
 PREC_FP64 = 0
 PREC_SPLIT = 1
 
+JAC_CENTRAL = 0     # lbl_jac_mode: central differences, exact merge derivative
+JAC_REFERENCE = 1   # the reference's analytic-Jacobian definitions
+
 
 class Run(C.Structure):
     """lbl_run: TAPE5 records 1.2/1.2a/1.3/1.4 subset."""

@@ -30,18 +30,41 @@ using namespace lbl;
 
 namespace {
 
+// Device memory the context holds, against an optional cap
+// (lbl_set_memory_limit).  Allocations that would pass the cap fail with
+// cudaErrorMemoryAllocation, as a full device does.
+struct DevBudget {
+  size_t used = 0, limit = 0;  // limit 0: no cap
+  cudaError_t alloc(void** p, size_t bytes) {
+    *p = nullptr;
+    if (limit && used + bytes > limit) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) used += bytes;
+    else cudaGetLastError();
+    return e;
+  }
+  void release(void* p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    used -= std::min(used, bytes);
+  }
+};
+
 // Grow-only device arena; sub-allocations are 256-byte aligned.
 struct Arena {
   char* base = nullptr;
   size_t cap = 0, used = 0;
-  cudaError_t reserve(size_t bytes) {
+  cudaError_t reserve(size_t bytes, DevBudget& b) {
     if (bytes <= cap) return cudaSuccess;
     size_t want = std::max(bytes, cap * 3 / 2);
-    if (base) cudaFree(base);
+    b.release(base, cap);
     base = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc(&base, want);
+    void* p = nullptr;
+    cudaError_t e = b.alloc(&p, want);
+    if (e != cudaSuccess && want > bytes) e = b.alloc(&p, want = bytes);
     if (e != cudaSuccess) return e;
+    base = static_cast<char*>(p);
     cap = want;
     return cudaSuccess;
   }
@@ -134,6 +157,17 @@ bool is_device_ptr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Page-locked host memory (cudaMallocHost or registered).
+bool is_pinned(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 }  // namespace
 
 struct lbl_ctx {
@@ -149,21 +183,40 @@ struct lbl_ctx {
   DevLines dl{};
   void* line_mem = nullptr;
   size_t line_cap = 0;  // bytes of line_mem (grow-only)
-  // pinned copies of the device status and work counters, read after the
-  // caller's final synchronisation
-  int32_t* h_stat = nullptr;
+  // pinned copies of each optical-depth pass's device status and work
+  // counters (one slot per pass queued since the last synchronisation),
+  // read after the caller's final synchronisation
+  struct StatSlot {
+    int32_t status[4];
+    int32_t pad[4];
+    unsigned long long cnt[8];
+  };
+  static constexpr int kStatSlots = 512;
+  StatSlot* h_slots = nullptr;
+  int nslot = 0;
+  DevBudget mem;
   // pinned image of the plan tables and the event of its last upload
   char* stage_host = nullptr;
   size_t stage_cap = 0;
   cudaEvent_t stage_ev = nullptr;
   bool stage_ev_set = false;
-  unsigned long long* h_cnt = nullptr;
   bool have_lines = false;
   // tables
   DevShapes sh{};
   void* shape_mem = nullptr;
   DevMtckd ck{};
   void* ck_mem = nullptr;
+  size_t ck_bytes = 0;
+  // small pinned staging for per-call tables (layer offsets, channel
+  // bounds): a ring of buffers, each reused once the copy that last read it
+  // is done (small_ev is the event of the buffer handed out last)
+  static constexpr int kSmallRing = 4;
+  char* small_host[kSmallRing] = {};
+  size_t small_cap[kSmallRing] = {};
+  cudaEvent_t small_evs[kSmallRing] = {};
+  bool small_used[kSmallRing] = {};
+  int small_next = 0;
+  cudaEvent_t small_ev = nullptr;
   // Jacobian work space (grow-only)
   char* jac_mem = nullptr;
   size_t jac_cap = 0;
@@ -251,11 +304,15 @@ int fail(lbl_ctx* c, int code, const std::string& m) {
   return code;
 }
 
-#define CK(call)                                                                  \
-  do {                                                                            \
-    cudaError_t e_ = (call);                                                      \
-    if (e_ != cudaSuccess)                                                        \
-      return fail(ctx, LBL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+// A failed runtime call returns LBL_E_CUDA with the call and its message;
+// an allocation that failed (device full or the context's cap reached)
+// returns LBL_E_NOMEM.
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? LBL_E_NOMEM : LBL_E_CUDA,    \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));               \
   } while (0)
 
 // Device view of one batch of planned layers.
@@ -278,14 +335,15 @@ struct Batch {
   int64_t od_total = 0;
 };
 
-// Plan layers [0,n), lay their buffers out in the arena, upload the plans.
-int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n, int jrad_in,
-                  int* jrad_out, Batch& B) {
-  const auto t_host = std::chrono::steady_clock::now();
+// Plan layers [0,n) on the host into `plans`.  The JRAD switch runs
+// through the layers from jrad_in (one profile).
+int plan_layers(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n, int jrad_in,
+                int* jrad_out, std::vector<LayerPlan>& plans,
+                const lbl_layer* chain = nullptr) {
   HostLines H{ctx->h_vnu.data(), ctx->h_sp.data(), ctx->h_pshift.data(), ctx->h_mol.data(),
               ctx->h_iflg.data(), (int64_t)ctx->h_vnu.size(), ctx->h_bs.data(),
               (int64_t)ctx->h_bs.size() - 1, ctx->max_abs_pshift};
-  B.plans.resize(n);
+  plans.resize(n);
   // the JRAD switch carries from layer to layer (OPDPTH :6211); everything
   // else in a layer's plan depends on that layer alone, so layers are
   // planned on several host threads
@@ -293,13 +351,13 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   int jrad = jrad_in;
   for (int l = 0; l < n; l++) {
     jin[l] = jrad;
-    jrad = next_jrad(R, layers[l], jrad);
+    jrad = next_jrad(R, chain ? chain[l] : layers[l], jrad);
   }
   if (jrad_out) *jrad_out = jrad;
   std::vector<int> rcs(n, LBL_OK);
   std::vector<std::string> errs(n);
   const std::function<void(int)> plan_one = [&](int l) {
-    rcs[l] = plan_layer(R, layers[l], jin[l], H, &B.plans[l], &errs[l]);
+    rcs[l] = plan_layer(R, layers[l], jin[l], H, &plans[l], &errs[l]);
   };
   if (n < 8) {
     for (int l = 0; l < n; l++) plan_one(l);
@@ -313,8 +371,44 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   for (int l = 0; l < n; l++)
     if (rcs[l] != LBL_OK) return fail(ctx, rcs[l], "layer " + std::to_string(l) + ": " + errs[l]);
   for (int l = 0; l < n; l++)
-    if (B.plans[l].d.n_r1 >= (int64_t(1) << 31) - 64)
+    if (plans[l].d.n_r1 >= (int64_t(1) << 31) - 64)
       return fail(ctx, LBL_E_RANGE, "layer " + std::to_string(l) + ": more than 2^31 points");
+  return LBL_OK;
+}
+
+// Device bytes one planned layer adds to a batch's arena (the per-layer
+// terms of upload_batch's layout; the fixed part is under 64 KB).
+size_t layer_arena_bytes(const LayerDev& d) {
+  const size_t npanel = (size_t)d.npanel, nwin = (size_t)d.nwin;
+  const size_t nfar = (size_t)(d.far_hi - d.far_lo), nnear = (size_t)(d.near_hi - d.near_lo);
+  const size_t nblk = (size_t)(d.blk_hi - d.blk_lo), nfblk = (size_t)(d.fblk_hi - d.fblk_lo);
+  const size_t nabs = (size_t)(d.icntnm ? d.nptabs : 0) + 8;
+  return sizeof(LayerDev) + 64 + npanel * (8 + 4 + 4 + 16 + 8 * 3 * kPanelSegMax + 4) +
+         nwin * (sizeof(WinDev) + 8 + 8 * kR4Stride) + nfar * 83 + 16 * (nfar / 1000 + 2) +
+         nnear * 117 + 8 * nblk + 8 * nabs + 8 * (size_t)d.npts + (8 * kSegMaxBlk + 16) * nfblk;
+}
+
+int upload_batch(lbl_ctx* ctx, Batch& B);
+
+// Plan layers [0,n), lay their buffers out in the arena, upload the plans.
+// The JRAD chain follows `chain` when given (the nominal layers of a
+// perturbed pass), else the layers themselves.
+int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n, int jrad_in,
+                  int* jrad_out, Batch& B, const lbl_layer* chain = nullptr) {
+  const auto t_host = std::chrono::steady_clock::now();
+  int rc = plan_layers(ctx, R, layers, n, jrad_in, jrad_out, B.plans, chain);
+  if (rc) return rc;
+  rc = upload_batch(ctx, B);
+  if (ctx->prof)
+    ctx->stage("host_plan").ms +=
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host)
+            .count();
+  return rc;
+}
+
+// Lay the planned layers of B out in the arena and upload their plans.
+int upload_batch(lbl_ctx* ctx, Batch& B) {
+  const int n = (int)B.plans.size();
   // offsets
   int64_t o_nblk = 0;
   int64_t o_r1 = 0, o_r2 = 0, o_r3 = 0, o_od = 0, o_pan = 0, o_win = 0, o_far = 0, o_near = 0,
@@ -400,7 +494,7 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   lay.add<int64_t>(nbt);
   lay.add<int64_t>(n);
   lay.add<unsigned long long>(8);
-  CK(ctx->arena.reserve(lay.bytes + 4096));
+  CK(ctx->arena.reserve(lay.bytes + 4096, ctx->mem));
   Arena& A = ctx->arena;
   A.reset();
   Work& w = B.w;
@@ -526,10 +620,6 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   ctx->stage_ev_set = true;
   CK(cudaMemsetAsync(w.status, 0, 4 * sizeof(int32_t), s));
   CK(cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), s));
-  if (ctx->prof)
-    ctx->stage("host_plan").ms +=
-        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host)
-            .count();
   return LBL_OK;
 }
 
@@ -539,6 +629,31 @@ int ensure_copy_stream(lbl_ctx* ctx) {
   if (ctx->cstream) return LBL_OK;
   CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
   for (auto& e : ctx->cev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return LBL_OK;
+}
+
+int finish_od(lbl_ctx* ctx);
+
+// A pinned host buffer of at least `bytes` for a table about to be copied
+// to the device; the caller records ctx->small_ev after its copy.
+int small_pinned(lbl_ctx* ctx, size_t bytes, void** out) {
+  const int k = ctx->small_next;
+  ctx->small_next = (k + 1) % lbl_ctx::kSmallRing;
+  if (!ctx->small_evs[k])
+    CK(cudaEventCreateWithFlags(&ctx->small_evs[k], cudaEventDisableTiming));
+  if (ctx->small_used[k]) CK(cudaEventSynchronize(ctx->small_evs[k]));
+  if (bytes > ctx->small_cap[k]) {
+    if (ctx->small_host[k]) cudaFreeHost(ctx->small_host[k]);
+    ctx->small_host[k] = nullptr;
+    ctx->small_cap[k] = 0;
+    void* hp = nullptr;
+    CK(cudaMallocHost(&hp, std::max<size_t>(bytes, 1 << 16)));
+    ctx->small_host[k] = static_cast<char*>(hp);
+    ctx->small_cap[k] = std::max<size_t>(bytes, 1 << 16);
+  }
+  ctx->small_used[k] = true;
+  ctx->small_ev = ctx->small_evs[k];
+  *out = ctx->small_host[k];
   return LBL_OK;
 }
 
@@ -594,8 +709,15 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     CK(launch_panels(w, ctx->dl, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
                      B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
   }
-  CK(cudaMemcpyAsync(ctx->h_stat, w.status, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(ctx->h_cnt, w.counters, 8 * sizeof(unsigned long long),
+  if (ctx->nslot >= lbl_ctx::kStatSlots) {
+    // every slot holds a pass not yet read: drain them
+    CK(cudaStreamSynchronize(s));
+    const int rc2 = finish_od(ctx);
+    if (rc2) return rc2;
+  }
+  lbl_ctx::StatSlot* sl = ctx->h_slots + ctx->nslot++;
+  CK(cudaMemcpyAsync(sl->status, w.status, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(sl->cnt, w.counters, 8 * sizeof(unsigned long long),
                      cudaMemcpyDeviceToHost, s));
   return LBL_OK;
 }
@@ -603,9 +725,14 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
 // After the stream has been synchronised: the device status of the last
 // run_od and its work counters.
 int finish_od(lbl_ctx* ctx) {
-  ctx->stage("far_wing").work += (double)ctx->h_cnt[0];
-  ctx->stage("panels").work += (double)ctx->h_cnt[1];
-  const int32_t st = ctx->h_stat[0];
+  int32_t st = 0;
+  for (int k = 0; k < ctx->nslot; k++) {
+    const lbl_ctx::StatSlot& sl = ctx->h_slots[k];
+    ctx->stage("far_wing").work += (double)sl.cnt[0];
+    ctx->stage("panels").work += (double)sl.cnt[1];
+    if (!st) st = sl.status[0];
+  }
+  ctx->nslot = 0;
   if (st == 2)
     return fail(ctx, LBL_E_RANGE,
                 "far-wing line file too sparse: a LINF4 segment spans more than 48 TAPE3 panels");
@@ -639,10 +766,15 @@ int check_run(lbl_ctx* ctx, const lbl_run* R) {
 int ensure_merge_buffers(lbl_ctx* ctx, size_t n) {
   if (n <= ctx->mcap) return LBL_OK;
   for (int k = 0; k < 4; k++) {
-    if (ctx->mbuf[k]) cudaFree(ctx->mbuf[k]);
+    ctx->mem.release(ctx->mbuf[k], ctx->mcap * sizeof(double));
     ctx->mbuf[k] = nullptr;
   }
-  for (int k = 0; k < 4; k++) CK(cudaMalloc(&ctx->mbuf[k], n * sizeof(double)));
+  ctx->mcap = 0;
+  for (int k = 0; k < 4; k++) {
+    void* p = nullptr;
+    CK(ctx->mem.alloc(&p, n * sizeof(double)));
+    ctx->mbuf[k] = static_cast<double*>(p);
+  }
   ctx->mcap = n;
   return LBL_OK;
 }
@@ -658,7 +790,9 @@ struct OutSink {
 // copied to the sink on a second stream while the next one is merged; the
 // main stream waits for the copies.
 int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B, int n,
-              int* res, int precision, const OutSink* sink = nullptr) {
+              int* res, int precision, const OutSink* sink = nullptr, int l0 = 0) {
+  // the profile is layers [l0, l0+n) of the batch; `layers` points at its first
+  const LayerDev* ld = B.ld.data() + l0;
   size_t mx = 0;
   for (auto& d : B.ld) mx = std::max<size_t>(mx, d.npts);
   int rc = ensure_merge_buffers(ctx, mx + 8);
@@ -666,10 +800,10 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
   // Consecutive layers on one grid go to one launch (at most kMergeRunMax).
   std::vector<std::pair<int, int>> runs;
   for (int l = 0; l < n;) {
-    const LayerDev& d = B.ld[l];
-    if (l > 0 && d.dv > B.ld[l - 1].dv) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
+    const LayerDev& d = ld[l];
+    if (l > 0 && d.dv > ld[l - 1].dv) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
     int e = l + 1;
-    while (e < n && e - l < kMergeRunMax && B.ld[e].dv == d.dv && B.ld[e].npts == d.npts) e++;
+    while (e < n && e - l < kMergeRunMax && ld[e].dv == d.dv && ld[e].npts == d.npts) e++;
     runs.push_back({l, e});
     l = e;
   }
@@ -684,7 +818,7 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
   StageTimer tm(ctx, "merge", (int64_t)runs.size() + nchunk - 1);
   for (size_t ri = 0; ri < runs.size(); ri++) {
     const int l = runs[ri].first, e = runs[ri].second;
-    const LayerDev& d = B.ld[l];
+    const LayerDev& d = ld[l];
     if (n_old >= (int64_t(1) << 31)) return fail(ctx, LBL_E_RANGE, "layer grid of 2^31 or more points");
     MergeRun m{};
     m.nl = e - l;
@@ -692,9 +826,9 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     m.itype = (l == 0 || dv_old == d.dv) ? 0 : (int32_t)(long)(d.dv / (dv_old - d.dv) + 0.5);
     m.n_old = (int32_t)n_old;
     for (int k = l; k < e; k++) {
-      m.od_off[k - l] = B.ld[k].off_od;
-      m.t[k - l] = emin_temps(B.ld[k].tave, layers[k].tzu);
-      ctx->stage("merge").work += (double)B.ld[k].npts;
+      m.od_off[k - l] = ld[k].off_od;
+      m.t[k - l] = emin_temps(ld[k].tave, layers[k].tzu);
+      ctx->stage("merge").work += (double)ld[k].npts;
     }
     const int nxt = cur ^ 2;
     const double tbnd = (l == 0 && R.ipathl == 1) ? R.tmpbnd : 0.;
@@ -743,6 +877,449 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
 
 }  // namespace
 
+namespace {
+
+// Device bytes a group of profiles may take in the arena: under the
+// context's cap, what the cap leaves beside the other buffers; otherwise
+// most of the device's free memory.
+size_t group_budget(lbl_ctx* ctx, size_t merge_bytes) {
+  size_t avail;
+  const size_t others = ctx->mem.used - std::min(ctx->mem.used, ctx->arena.cap);
+  if (ctx->mem.limit) {
+    avail = ctx->mem.limit > others ? ctx->mem.limit - others : 0;
+  } else {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      fr = 0;
+    }
+    avail = fr + ctx->arena.cap;
+    const size_t keep = (size_t)2 << 30;  // left to the caller and the runtime
+    avail = avail > keep ? (avail - keep) / 10 * 9 : 0;
+  }
+  return avail > merge_bytes ? avail - merge_bytes : 0;
+}
+
+// Pinned staging of results bound for pageable host memory, so that the
+// copies out stay asynchronous and the host goes on planning; two buffers
+// alternate between groups.
+struct Bounce {
+  double* buf = nullptr;
+  size_t cap = 0;  // doubles
+  cudaEvent_t ev = nullptr;
+  struct Out {
+    double* dst;
+    size_t off, n;
+  };
+  std::vector<Out> pend;
+};
+
+// Copy a bounce buffer's pending results to their host destinations once
+// its group's copies are done.
+int bounce_flush(lbl_ctx* ctx, Bounce& b) {
+  if (b.pend.empty()) return LBL_OK;
+  CK(cudaEventSynchronize(b.ev));
+  for (const Bounce::Out& o : b.pend) std::memcpy(o.dst, b.buf + o.off, o.n * sizeof(double));
+  b.pend.clear();
+  return LBL_OK;
+}
+
+// The batched layer loop over profiles [lay0 index p] .. : profiles are
+// planned on the host one after another and gathered into groups that fit
+// the device budget; each group is uploaded in one copy, its optical depths
+// computed by one set of launches for all its layers, and its profiles
+// merged one after another, results going straight to device or pinned
+// destinations (pageable ones through a pinned bounce buffer).  Every
+// device step of a group is queued without a host wait, so the host plans
+// the next group while the device computes this one.
+int forward_groups(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers,
+                   const std::vector<int64_t>& lay0, const int64_t* offsets, double* rad,
+                   double* tr, int precision) {
+  const int nprof = (int)lay0.size() - 1;
+  size_t mx = 0;
+  for (int p = 0; p < nprof; p++)
+    for (int64_t l = lay0[p]; l < lay0[p + 1]; l++)
+      mx = std::max<size_t>(mx, (size_t)layer_npts(R, layers[l].dv));
+  int rc = ensure_merge_buffers(ctx, mx + 8);
+  if (rc) return rc;
+  const size_t budget = group_budget(ctx, 0);
+  const bool rad_host = !is_device_ptr(rad) && !is_pinned(rad);
+  const bool tr_host = tr && !is_device_ptr(tr) && !is_pinned(tr);
+  Bounce bounce[2];
+  int bi = 0;
+  std::vector<LayerPlan> cur;      // plans of the open group
+  std::vector<int> cur_prof;       // its profiles
+  size_t cur_bytes = 0;
+  auto t_host = std::chrono::steady_clock::now();
+  double host_ms = 0.;
+  auto flush = [&]() -> int {
+    if (cur_prof.empty()) return LBL_OK;
+    host_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_host)
+                   .count();
+    Batch B;
+    B.plans = std::move(cur);
+    cur.clear();
+    int rc2 = upload_batch(ctx, B);
+    if (rc2) return rc2;
+    rc2 = run_od(ctx, R, B, precision);
+    if (rc2) return rc2;
+    // results of this group bound for pageable memory go to bounce[bi]
+    Bounce& bb = bounce[bi];
+    size_t need = 0;
+    for (int p : cur_prof)
+      need += (size_t)(offsets[p + 1] - offsets[p]) * ((rad_host ? 1 : 0) + (tr_host ? 1 : 0));
+    if (need) {
+      rc2 = bounce_flush(ctx, bb);
+      if (rc2) return rc2;
+      if (need > bb.cap) {
+        if (bb.buf) cudaFreeHost(bb.buf);
+        bb.buf = nullptr;
+        bb.cap = 0;
+        void* hp = nullptr;
+        CK(cudaMallocHost(&hp, need * sizeof(double)));
+        bb.buf = static_cast<double*>(hp);
+        bb.cap = need;
+      }
+      if (!bb.ev) CK(cudaEventCreateWithFlags(&bb.ev, cudaEventDisableTiming));
+    }
+    size_t boff = 0;
+    int l0 = 0;
+    for (int p : cur_prof) {
+      const int n = (int)(lay0[p + 1] - lay0[p]);
+      const size_t np = (size_t)(offsets[p + 1] - offsets[p]);
+      OutSink sink{rad + offsets[p], tr ? tr + offsets[p] : nullptr};
+      if (rad_host) {
+        bb.pend.push_back({rad + offsets[p], boff, np});
+        sink.rad = bb.buf + boff;
+        boff += np;
+      }
+      if (tr_host) {
+        bb.pend.push_back({tr + offsets[p], boff, np});
+        sink.tr = bb.buf + boff;
+        boff += np;
+      }
+      int res = 0;
+      rc2 = run_merge(ctx, R, layers + lay0[p], B, n, &res, precision, &sink, l0);
+      if (rc2) return rc2;
+      l0 += n;
+    }
+    if (need) CK(cudaEventRecord(bb.ev, ctx->stream));
+    bi ^= 1;
+    cur_prof.clear();
+    cur_bytes = 0;
+    t_host = std::chrono::steady_clock::now();
+    return LBL_OK;
+  };
+  for (int p = 0; p < nprof && rc == LBL_OK; p++) {
+    std::vector<LayerPlan> plans;
+    const int n = (int)(lay0[p + 1] - lay0[p]);
+    rc = plan_layers(ctx, R, layers + lay0[p], n, R.jrad, nullptr, plans);
+    if (rc) break;
+    size_t bytes = 0;
+    for (const LayerPlan& P : plans) bytes += layer_arena_bytes(P.d);
+    if (!cur_prof.empty() && cur_bytes + bytes > budget) {
+      rc = flush();
+      if (rc) break;
+    }
+    if (bytes > budget) {
+      rc = fail(ctx, LBL_E_NOMEM, "profile " + std::to_string(p) + " needs " +
+                                      std::to_string(bytes >> 20) + " MiB of work space, " +
+                                      std::to_string(budget >> 20) + " MiB available");
+      break;
+    }
+    for (LayerPlan& P : plans) cur.push_back(std::move(P));
+    cur_prof.push_back(p);
+    cur_bytes += bytes;
+  }
+  if (rc == LBL_OK) rc = flush();
+  if (ctx->prof) ctx->stage("host_plan").ms += host_ms;
+  cudaError_t se = cudaStreamSynchronize(ctx->stream);
+  for (Bounce& b : bounce) {
+    if (rc == LBL_OK && se == cudaSuccess) rc = bounce_flush(ctx, b);
+    if (b.buf) cudaFreeHost(b.buf);
+    if (b.ev) cudaEventDestroy(b.ev);
+  }
+  if (rc) return rc;
+  if (se != cudaSuccess) return fail(ctx, LBL_E_CUDA, cudaGetErrorString(se));
+  harvest(ctx);
+  return finish_od(ctx);
+}
+
+}  // namespace
+
+namespace {
+
+int check_jac_args(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layers,
+                   const int32_t* nlay, int nprof, const int32_t* mols, int nq, int mode) {
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
+  if (!layers || !nlay || nprof < 1 || nq < 0 || nq >= kJacMaxParams || (nq > 0 && !mols))
+    return fail(ctx, LBL_E_ARG, "Jacobians: bad argument");
+  if (mode != LBL_JAC_CENTRAL && mode != LBL_JAC_REFERENCE)
+    return fail(ctx, LBL_E_ARG, "Jacobians: mode must be LBL_JAC_CENTRAL or LBL_JAC_REFERENCE");
+  if (run->iemit != 1 || run->ipathl != 1)
+    return fail(ctx, LBL_E_ARG, "Jacobians: upwelling radiance only (IEMIT=1, IPATHL=1)");
+  for (int p = 0; p < nprof; p++)
+    if (nlay[p] < 1) return fail(ctx, LBL_E_ARG, "Jacobians: profile without layers");
+  for (int k = 0; k < nq; k++)
+    if (mols[k] < 1 || mols[k] > LBL_WKDIM)
+      return fail(ctx, LBL_E_ARG, "Jacobians: molecule number out of range");
+  return LBL_OK;
+}
+
+// Device results of jac_profile (pointers into the Jacobian work space).
+struct JacOut {
+  double* rad = nullptr;   // TOA radiance on the top grid (npts)
+  double* rows = nullptr;  // rows (k - k0)*nlay*npts + l*npts + i
+  int64_t npts = 0;
+  int nlay = 0;
+  std::vector<double> top_vft;     // panel origins of the top layer
+  double top_dv = 0.;
+  double* chan_rad = nullptr;      // channel means (jac_channels)
+  double* chan_rows = nullptr;
+};
+
+// Sizes of one profile's Jacobian work space for nk parameters at once.
+struct JacSizes {
+  int64_t ntot, npts;
+  int a;  // layers a..nlay-1 share the top grid
+  size_t bytes(int nk, int nlay, int64_t nchan) const {
+    const size_t rows = (size_t)nk * nlay * npts, low = (size_t)nk * std::max(a, 1) * npts;
+    const size_t chan = nchan > 0 ? (size_t)(nk * nlay + 2) * nchan + 32 : 0;
+    return 8 * ((size_t)nk * ntot + ntot + rows + 2 * low + 4 * (size_t)npts + nlay + chan) +
+           16 * 256;
+  }
+};
+
+JacSizes jac_sizes(const lbl_run& R, const lbl_layer* layers, int nlay) {
+  JacSizes z{0, layer_npts(R, layers[nlay - 1].dv), 0};
+  for (int l = 0; l < nlay; l++) {
+    z.ntot += layer_npts(R, layers[l].dv);
+    if (l > 0 && layers[l].dv != layers[l - 1].dv) z.a = l;
+  }
+  return z;
+}
+
+// Parameters one profile can take at once within the memory budget (the
+// optical-depth passes are recomputed for each chunk of parameters when not
+// all fit); 0 when even one does not.
+int jac_chunk(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int nlay, int np,
+              int64_t nchan) {
+  const JacSizes z = jac_sizes(R, layers, nlay);
+  // arena of one pass: estimated from the layer grids and the line count
+  const size_t arena = (size_t)z.ntot * 16 + (size_t)nlay * ctx->h_vnu.size() * 200 +
+                       ((size_t)64 << 20);
+  size_t avail;
+  const size_t held = ctx->mem.used - std::min(ctx->mem.used, ctx->arena.cap + ctx->jac_cap);
+  if (ctx->mem.limit) {
+    avail = ctx->mem.limit > held ? ctx->mem.limit - held : 0;
+  } else {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      fr = 0;
+    }
+    avail = fr + ctx->arena.cap + ctx->jac_cap;
+    const size_t keep = (size_t)2 << 30;
+    avail = avail > keep ? avail - keep : 0;
+  }
+  avail = avail > arena ? avail - arena : 0;
+  for (int nk = np; nk >= 1; nk--)
+    if (z.bytes(nk, nlay, nchan) <= avail) return nk;
+  return 0;
+}
+
+// One profile's TOA radiance and the Jacobian rows of parameters [k0, k1)
+// (0: temperature, k: molecule mols[k-1]) on its top grid, left in the
+// Jacobian work space.  Every step is queued on the stream without a host
+// wait (the caller synchronises), so the host plans each optical-depth pass
+// while the device runs the previous one.
+//   LBL_JAC_CENTRAL:   dtau/dp by central differences of whole-profile
+//                      optical depths (T +-0.1 K, amount +-1 %; a layer's
+//                      depth depends only on its own parameters, so one pass
+//                      serves every layer), merged with the exact derivative
+//                      of EMIN/EMINIT/RADNN;
+//   LBL_JAC_REFERENCE: the reference's analytic-Jacobian definitions
+//                      (src/lblrtm.f90:2855-3067): one pass at T + 1 K and one
+//                      per molecule with that molecule alone (other amounts
+//                      zero, WK(7) added to WBROAD), merged by the
+//                      TDERIVup/QDERIVup rows (src/xmerge.f90:5786-6144).
+// Each layer's row is carried to the top through the later layers' regrid
+// and transmittance.
+int jac_profile(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers, int nlay,
+                const int32_t* mols, int k0, int k1, int mode, int precision, int64_t nchan,
+                JacOut& o) {
+  const int nk = k1 - k0;
+  const JacSizes z = jac_sizes(R, layers, nlay);
+  const int64_t npts = z.npts, ntot = z.ntot;
+  const int a = z.a;
+  std::vector<int64_t> off(nlay + 1, 0);
+  for (int l = 0; l < nlay; l++) off[l + 1] = off[l] + layer_npts(R, layers[l].dv);
+  const size_t need = z.bytes(nk, nlay, nchan);
+  if (need > ctx->jac_cap) {
+    if (ctx->jac_mem) CK(cudaStreamSynchronize(ctx->stream));
+    ctx->mem.release(ctx->jac_mem, ctx->jac_cap);
+    ctx->jac_mem = nullptr;
+    ctx->jac_cap = 0;
+    void* m = nullptr;
+    CK(ctx->mem.alloc(&m, need));
+    ctx->jac_mem = static_cast<char*>(m);
+    ctx->jac_cap = need;
+  }
+  size_t used = 0;
+  auto take = [&](size_t n) {
+    used = (used + 255) & ~size_t(255);
+    double* p = reinterpret_cast<double*>(ctx->jac_mem + used);
+    used += n * 8;
+    return p;
+  };
+  const size_t n_rows = (size_t)nk * nlay * npts, n_low = (size_t)nk * std::max(a, 1) * npts;
+  double* dtau = take((size_t)nk * ntot);
+  double* tmp = take(ntot);
+  double* rows = take(n_rows);
+  double* low[2] = {take(n_low), take(n_low)};
+  double* rt[4] = {take(npts), take(npts), take(npts), take(npts)};
+  int64_t* d_off = reinterpret_cast<int64_t*>(take(nlay));
+  // channel means, then the channel bounds (nchan + 1 entries)
+  o.chan_rows = take(nchan > 0 ? (size_t)nk * nlay * nchan + nchan + 9 : 0);
+  o.chan_rad = take(nchan > 0 ? (size_t)nchan + 8 : 0);
+  cudaStream_t s = ctx->stream;
+  int rc;
+  std::vector<lbl_layer> Lp(layers, layers + nlay), Lm(layers, layers + nlay);
+  const double dT = 0.1, dq = 0.01;
+  for (int k = k0; k < k1; k++) {
+    double* dst = dtau + (size_t)(k - k0) * ntot;
+    for (int l = 0; l < nlay; l++) {
+      Lp[l] = layers[l];
+      Lm[l] = layers[l];
+      if (mode == LBL_JAC_CENTRAL) {
+        if (k == 0) {
+          Lp[l].tave += dT;
+          Lm[l].tave -= dT;
+        } else {
+          Lp[l].wk[mols[k - 1] - 1] *= 1. + dq;
+          Lm[l].wk[mols[k - 1] - 1] *= 1. - dq;
+        }
+      } else if (k == 0) {
+        Lp[l].tave += 1.;
+      } else {
+        const int m = mols[k - 1];
+        for (int j = 0; j < LBL_WKDIM; j++) Lp[l].wk[j] = 0.;
+        Lp[l].wk[m - 1] = layers[l].wk[m - 1];
+        Lp[l].wbroad = layers[l].wbroad + layers[l].wk[6];
+      }
+    }
+    const int nside = mode == LBL_JAC_CENTRAL ? 2 : 1;
+    for (int side = 0; side < nside; side++) {
+      Batch Bs;
+      // every pass keeps the nominal JRAD chain of the layers
+      rc = prepare_batch(ctx, R, side ? Lm.data() : Lp.data(), nlay, R.jrad, nullptr, Bs,
+                         layers);
+      if (rc) return rc;
+      rc = run_od(ctx, R, Bs, precision);
+      if (rc) return rc;
+      CK(cudaMemcpyAsync(side ? tmp : dst, Bs.w.od, 8 * ntot, cudaMemcpyDeviceToDevice, s));
+    }
+    if (mode == LBL_JAC_CENTRAL) {
+      const double h = k == 0 ? 2. * dT : std::log(1. + dq) - std::log(1. - dq);
+      CK(launch_jac_diff(dst, tmp, ntot, 1. / h, s));
+    }
+  }
+  // nominal optical depths, kept in the batch for the merge
+  Batch B;
+  rc = prepare_batch(ctx, R, layers, nlay, R.jrad, nullptr, B);
+  if (rc) return rc;
+  rc = run_od(ctx, R, B, precision);
+  if (rc) return rc;
+  {
+    int64_t* hoff = nullptr;
+    rc = small_pinned(ctx, 8 * (size_t)nlay, reinterpret_cast<void**>(&hoff));
+    if (rc) return rc;
+    for (int l = 0; l < nlay; l++) hoff[l] = B.ld[l].off_od;
+    CK(cudaMemcpyAsync(d_off, hoff, 8 * nlay, cudaMemcpyHostToDevice, s));
+    CK(cudaEventRecord(ctx->small_ev, s));
+  }
+  int cur = 0;
+  {
+    StageTimer t(ctx, "jacobian", 0);
+    int lc = 0;
+    double dv_old = 0.;
+    int64_t n_old = 0;
+    for (int l = 0; l < nlay; l++) {
+      const LayerDev& d = B.ld[l];
+      if (l > 0 && d.dv > dv_old) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
+      // carry the rows of layers below l onto layer l's grid
+      if (l > 0 && l <= a) {
+        for (int k = 0; k < nk; k++)
+          CK(launch_jac_prop(B.d_ld + l, B.w.od + d.off_od, d.npts, dv_old, n_old,
+                             low[lc] + (size_t)k * a * npts, low[lc ^ 1] + (size_t)k * a * npts,
+                             npts, l, s));
+        lc ^= 1;
+      }
+      double* dp[kJacMaxParams];
+      const double* tp[kJacMaxParams];
+      for (int k = 0; k < nk; k++) {
+        dp[k] = (l < a) ? low[lc] + ((size_t)k * a + l) * npts
+                        : rows + ((size_t)k * nlay + l) * npts;
+        tp[k] = dtau + (size_t)k * ntot + off[l];
+      }
+      const int nxt = cur ^ 2;
+      const double tbnd = (l == 0) ? R.tmpbnd : 0.;
+      CK(launch_jac_layer(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
+                          dv_old, n_old, rt[cur], rt[cur + 1], rt[nxt], rt[nxt + 1], tbnd,
+                          R.bndemi, layers[l].tzu, dp, tp, nk, mode, s));
+      cur = nxt;
+      dv_old = d.dv;
+      n_old = d.npts;
+    }
+    CK(launch_jac_top(B.w.od, d_off, nlay, a, nk, npts, rows, low[lc], s));
+  }
+  o.rad = rt[cur];
+  o.rows = rows;
+  o.npts = npts;
+  o.nlay = nlay;
+  o.top_vft = B.plans[nlay - 1].vft;
+  o.top_dv = B.ld[nlay - 1].dv;
+  return LBL_OK;
+}
+
+// Means of the radiance and of `nrows` rows over channels [V1 + c dv_chan,
+// V1 + (c+1) dv_chan), c < nchan, of the top grid (the points of a channel
+// are those whose wavenumber lies in it).
+int jac_channels(lbl_ctx* ctx, const lbl_run& R, JacOut& o, int nrows, double dv_chan,
+                 int64_t nchan) {
+  int64_t* cb = nullptr;
+  int rc = small_pinned(ctx, 8 * (size_t)(nchan + 1), reinterpret_cast<void**>(&cb));
+  if (rc) return rc;
+  const double DV = o.top_dv;
+  auto vpt = [&](int64_t f) {
+    const int64_t p = f / 2400;
+    return (o.top_vft[p] + double(33 - 1) * DV) + double(f - 2400 * p) * DV;
+  };
+  for (int64_t c = 0; c <= nchan; c++) {
+    const double vc = R.v1 + double(c) * dv_chan;
+    int64_t lo = 0, hi = o.npts;
+    while (lo < hi) {
+      const int64_t m = (lo + hi) / 2;
+      if (vpt(m) < vc) lo = m + 1;
+      else hi = m;
+    }
+    cb[c] = lo;
+  }
+  for (int64_t c = 0; c < nchan; c++)
+    if (cb[c + 1] <= cb[c]) return fail(ctx, LBL_E_ARG, "a channel holds no grid point");
+  // the bounds go in the rows' space, which the channel means no longer need
+  int64_t* d_cb = reinterpret_cast<int64_t*>(o.chan_rows + (size_t)nrows * nchan);
+  static_assert(sizeof(int64_t) == sizeof(double), "bounds stored in a double array");
+  CK(cudaMemcpyAsync(d_cb, cb, 8 * (nchan + 1), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaEventRecord(ctx->small_ev, ctx->stream));
+  CK(launch_chan_mean(o.rad, o.npts, 1, d_cb, nchan, o.chan_rad, ctx->stream));
+  CK(launch_chan_mean(o.rows, o.npts, nrows, d_cb, nchan, o.chan_rows, ctx->stream));
+  return LBL_OK;
+}
+
+}  // namespace
+
 // ==========================================================================
 extern "C" {
 
@@ -764,18 +1341,18 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
   upload_voicon();
   init_kernel_attributes();
   void* hs = nullptr;
-  if (cudaMallocHost(&hs, 64 + 8 * sizeof(unsigned long long)) != cudaSuccess) {
+  const size_t slot_bytes = sizeof(lbl_ctx::StatSlot) * lbl_ctx::kStatSlots;
+  if (cudaMallocHost(&hs, slot_bytes) != cudaSuccess) {
     delete ctx;
     return LBL_E_NOMEM;
   }
-  std::memset(hs, 0, 64 + 8 * sizeof(unsigned long long));
-  ctx->h_stat = static_cast<int32_t*>(hs);
+  std::memset(hs, 0, slot_bytes);
+  ctx->h_slots = static_cast<lbl_ctx::StatSlot*>(hs);
   if (cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming) != cudaSuccess) {
     cudaFreeHost(hs);
     delete ctx;
     return LBL_E_CUDA;
   }
-  ctx->h_cnt = reinterpret_cast<unsigned long long*>(static_cast<char*>(hs) + 64);
   ShapeTables* t = new ShapeTables;
   build_shape_tables(t);
   const size_t nd = kNfmx + 1;
@@ -811,16 +1388,19 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
 int lbl_ctx_destroy(lbl_ctx* ctx) {
   if (!ctx) return LBL_E_ARG;
   cudaSetDevice(ctx->device);
-  if (ctx->h_stat) cudaFreeHost(ctx->h_stat);
+  if (ctx->h_slots) cudaFreeHost(ctx->h_slots);
   if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
   if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
-  if (ctx->jac_mem) cudaFree(ctx->jac_mem);
-  if (ctx->line_mem) cudaFree(ctx->line_mem);
+  for (int k = 0; k < lbl_ctx::kSmallRing; k++) {
+    if (ctx->small_host[k]) cudaFreeHost(ctx->small_host[k]);
+    if (ctx->small_evs[k]) cudaEventDestroy(ctx->small_evs[k]);
+  }
+  ctx->mem.release(ctx->jac_mem, ctx->jac_cap);
+  ctx->mem.release(ctx->line_mem, ctx->line_cap);
   if (ctx->shape_mem) cudaFree(ctx->shape_mem);
-  if (ctx->ck_mem) cudaFree(ctx->ck_mem);
-  if (ctx->arena.base) cudaFree(ctx->arena.base);
-  for (int k = 0; k < 4; k++)
-    if (ctx->mbuf[k]) cudaFree(ctx->mbuf[k]);
+  ctx->mem.release(ctx->ck_mem, ctx->ck_bytes);
+  ctx->mem.release(ctx->arena.base, ctx->arena.cap);
+  for (int k = 0; k < 4; k++) ctx->mem.release(ctx->mbuf[k], ctx->mcap * sizeof(double));
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
   for (auto e : ctx->cev)
     if (e) cudaEventDestroy(e);
@@ -923,12 +1503,13 @@ int lbl_lines_upload(lbl_ctx* ctx, const lbl_lines* L) {
   if (!ctx->line_mem || bytes > ctx->line_cap) {
     if (ctx->line_mem) {
       CK(cudaStreamSynchronize(ctx->stream));
-      cudaFree(ctx->line_mem);
+      ctx->mem.release(ctx->line_mem, ctx->line_cap);
     }
     ctx->line_mem = nullptr;
     ctx->line_cap = 0;
-    char* nm = nullptr;
-    CK(cudaMalloc(&nm, bytes));
+    ctx->have_lines = false;
+    void* nm = nullptr;
+    CK(ctx->mem.alloc(&nm, bytes));
     ctx->line_mem = nm;
     ctx->line_cap = bytes;
   }
@@ -981,10 +1562,16 @@ int lbl_mtckd_upload(lbl_ctx* ctx, const lbl_mtckd* T) {
       !(T->dv > 0.))
     return fail(ctx, LBL_E_ARG, "bad continuum table");
   cudaSetDevice(ctx->device);
-  if (ctx->ck_mem) cudaFree(ctx->ck_mem);
+  ctx->mem.release(ctx->ck_mem, ctx->ck_bytes);
   ctx->ck_mem = nullptr;
-  double* m = nullptr;
-  CK(cudaMalloc(&m, 3 * T->n * sizeof(double)));
+  ctx->have_ck = false;
+  void* vm = nullptr;
+  CK(ctx->mem.alloc(&vm, 3 * T->n * sizeof(double)));
+  ctx->ck_bytes = 3 * T->n * sizeof(double);
+  double* m = static_cast<double*>(vm);
+  CK(cudaMemcpy(m, T->self_absco_ref, T->n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m + T->n, T->for_absco_ref, T->n * 8, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(m + 2 * T->n, T->self_texp, T->n * 8, cudaMemcpyHostToDevice));
   ctx->ck_mem = m;
   CK(cudaMemcpy(m, T->self_absco_ref, T->n * 8, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(m + T->n, T->for_absco_ref, T->n * 8, cudaMemcpyHostToDevice));
@@ -1051,7 +1638,7 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, in
   const size_t nn = (size_t)std::max(n_new, n_old) + 8;
   rc = ensure_merge_buffers(ctx, nn);
   if (rc) return rc;
-  CK(ctx->arena.reserve(sizeof(LayerDev) + P.vft.size() * 8 + n_new * 8 + 4096));
+  CK(ctx->arena.reserve(sizeof(LayerDev) + P.vft.size() * 8 + n_new * 8 + 4096, ctx->mem));
   ctx->arena.reset();
   LayerDev* dL = ctx->arena.take<LayerDev>(1);
   double* dv = ctx->arena.take<double>(P.vft.size());
@@ -1103,42 +1690,31 @@ int lbl_forward_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, const
                       int32_t nprof, double* rad, double* tr, int64_t* offsets,
                       int64_t npts_total, int32_t precision) {
   if (!ctx) return LBL_E_ARG;
+  int rc = check_run(ctx, run);
+  if (rc) return rc;
   if (!layers || !nlay || nprof < 1 || !rad || !offsets) return fail(ctx, LBL_E_ARG, "NULL argument");
-  int64_t lay0 = 0, off = 0;
+  cudaSetDevice(ctx->device);
+  std::vector<int64_t> lay0(nprof + 1, 0);
   offsets[0] = 0;
   for (int p = 0; p < nprof; p++) {
+    if (nlay[p] < 1) return fail(ctx, LBL_E_ARG, "profile without layers");
     std::string e;
-    int rc = dv_rule(*run, layers + lay0, nlay[p], &e);
-    if (rc) return fail(ctx, rc, e);
-    off += layer_npts(*run, layers[lay0 + nlay[p] - 1].dv);
-    offsets[p + 1] = off;
-    lay0 += nlay[p];
+    rc = dv_rule(*run, layers + lay0[p], nlay[p], &e);
+    if (rc) return fail(ctx, rc, "profile " + std::to_string(p) + ": " + e);
+    offsets[p + 1] = offsets[p] + layer_npts(*run, layers[lay0[p] + nlay[p] - 1].dv);
+    lay0[p + 1] = lay0[p] + nlay[p];
   }
-  if (off > npts_total) return fail(ctx, LBL_E_ARG, "output buffer too small");
-  lay0 = 0;
-  for (int p = 0; p < nprof; p++) {
-    const int64_t n = offsets[p + 1] - offsets[p];
-    int rc = lbl_forward(ctx, run, layers + lay0, nlay[p], rad + offsets[p],
-                         tr ? tr + offsets[p] : nullptr, n, precision);
-    if (rc) return rc;
-    lay0 += nlay[p];
-  }
-  return LBL_OK;
+  if (offsets[nprof] > npts_total) return fail(ctx, LBL_E_ARG, "output buffer too small");
+  return forward_groups(ctx, *run, layers, lay0, offsets, rad, tr, precision);
 }
 
 int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nlay,
                  const int32_t* mols, int32_t nq, double* rad, double* jac, int64_t npts,
                  int32_t precision) {
   if (!ctx) return LBL_E_ARG;
-  int rc = check_run(ctx, run);
+  int rc = check_jac_args(ctx, run, layers, &nlay, 1, mols, nq, LBL_JAC_CENTRAL);
   if (rc) return rc;
-  if (!layers || nlay < 1 || !jac || nq < 0 || nq >= kJacMaxParams || (nq > 0 && !mols))
-    return fail(ctx, LBL_E_ARG, "lbl_jacobian: bad argument");
-  if (run->iemit != 1 || run->ipathl != 1)
-    return fail(ctx, LBL_E_ARG, "lbl_jacobian: upwelling radiance only (IEMIT=1, IPATHL=1)");
-  for (int k = 0; k < nq; k++)
-    if (mols[k] < 1 || mols[k] > LBL_WKDIM)
-      return fail(ctx, LBL_E_ARG, "lbl_jacobian: molecule number out of range");
+  if (!jac) return fail(ctx, LBL_E_ARG, "lbl_jacobian: NULL output");
   cudaSetDevice(ctx->device);
   std::string e;
   rc = dv_rule(*run, layers, nlay, &e);
@@ -1146,137 +1722,109 @@ int lbl_jacobian(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nl
   if (layer_npts(*run, layers[nlay - 1].dv) != npts)
     return fail(ctx, LBL_E_ARG, "npts does not match the last layer's grid");
   const int np = 1 + nq;
-  // layer grids: optical depths are stored layer after layer
-  std::vector<int64_t> nl(nlay), off(nlay + 1, 0);
-  for (int l = 0; l < nlay; l++) {
-    nl[l] = layer_npts(*run, layers[l].dv);
-    off[l + 1] = off[l] + nl[l];
-  }
-  const int64_t ntot = off[nlay];
-  // layers a..nlay-1 share the top grid; rows of lower layers are carried
-  // through each merge step up to a
-  int a = 0;
-  for (int l = 1; l < nlay; l++)
-    if (layers[l].dv != layers[l - 1].dv) a = l;
-  // work space: dtau per parameter, the minus pass, output rows, two
-  // buffers of carried rows, two (R, T) pairs, layer offsets
-  const size_t n_dtau = (size_t)np * ntot, n_rows = (size_t)np * nlay * npts,
-               n_low = (size_t)np * std::max(a, 1) * npts;
-  const size_t need = 8 * (n_dtau + ntot + n_rows + 2 * n_low + 4 * (size_t)npts + nlay) + 8 * 256;
-  if (need > ctx->jac_cap) {
-    if (ctx->jac_mem) {
-      CK(cudaStreamSynchronize(ctx->stream));
-      cudaFree(ctx->jac_mem);
-    }
-    ctx->jac_mem = nullptr;
-    ctx->jac_cap = 0;
-    char* m = nullptr;
-    if (cudaMalloc(&m, need) != cudaSuccess) {
-      cudaGetLastError();
-      return fail(ctx, LBL_E_NOMEM, "lbl_jacobian: work space");
-    }
-    ctx->jac_mem = m;
-    ctx->jac_cap = need;
-  }
-  size_t used = 0;
-  auto take = [&](size_t n) {
-    used = (used + 255) & ~size_t(255);
-    double* p = reinterpret_cast<double*>(ctx->jac_mem + used);
-    used += n * 8;
-    return p;
-  };
-  double* dtau = take(n_dtau);
-  double* tmp = take(ntot);
-  double* rows = take(n_rows);
-  double* low[2] = {take(n_low), take(n_low)};
-  double* rt[4] = {take(npts), take(npts), take(npts), take(npts)};
-  int64_t* d_off = reinterpret_cast<int64_t*>(take(nlay));
-  cudaStream_t s = ctx->stream;
-  // dtau/dp of every layer by central differences of whole-profile optical
-  // depths: each layer's depth depends only on its own parameters
-  const double dT = 0.1, dq = 0.01;
-  std::vector<lbl_layer> Lp(layers, layers + nlay), Lm(layers, layers + nlay);
-  for (int k = 0; k < np; k++) {
-    double h;
-    for (int l = 0; l < nlay; l++) {
-      Lp[l] = layers[l];
-      Lm[l] = layers[l];
-      if (k == 0) {
-        Lp[l].tave += dT;
-        Lm[l].tave -= dT;
-      } else {
-        Lp[l].wk[mols[k - 1] - 1] *= 1. + dq;
-        Lm[l].wk[mols[k - 1] - 1] *= 1. - dq;
-      }
-    }
-    h = k == 0 ? 2. * dT : std::log(1. + dq) - std::log(1. - dq);
-    for (int side = 0; side < 2; side++) {
-      Batch Bs;
-      rc = prepare_batch(ctx, *run, side ? Lm.data() : Lp.data(), nlay, run->jrad, nullptr, Bs);
-      if (rc) return rc;
-      rc = run_od(ctx, *run, Bs, precision);
-      if (rc) return rc;
-      CK(cudaMemcpyAsync(side ? tmp : dtau + (size_t)k * ntot, Bs.w.od, 8 * ntot,
-                         cudaMemcpyDeviceToDevice, s));
-      CK(cudaStreamSynchronize(s));
-      rc = finish_od(ctx);
+  const int chunk = jac_chunk(ctx, *run, layers, nlay, np, 0);
+  if (chunk < 1) return fail(ctx, LBL_E_NOMEM, "lbl_jacobian: work space");
+  for (int k0 = 0; k0 < np; k0 += chunk) {
+    const int k1 = std::min(np, k0 + chunk);
+    JacOut o;
+    rc = jac_profile(ctx, *run, layers, nlay, mols, k0, k1, LBL_JAC_CENTRAL, precision, 0, o);
+    if (rc) return rc;
+    if (rad && k0 == 0) {
+      rc = copy_out(ctx, rad, o.rad, sizeof(double) * npts);
       if (rc) return rc;
     }
-    CK(launch_jac_diff(dtau + (size_t)k * ntot, tmp, ntot, 1. / h, s));
+    rc = copy_out(ctx, jac + (size_t)k0 * nlay * npts, o.rows,
+                  sizeof(double) * (size_t)(k1 - k0) * nlay * npts);
+    if (rc) return rc;
   }
-  // nominal optical depths, kept in the batch for the merge
-  Batch B;
-  rc = prepare_batch(ctx, *run, layers, nlay, run->jrad, nullptr, B);
-  if (rc) return rc;
-  rc = run_od(ctx, *run, B, precision);
-  if (rc) return rc;
-  std::vector<int64_t> hoff(nlay);
-  for (int l = 0; l < nlay; l++) hoff[l] = B.ld[l].off_od;
-  CK(cudaMemcpyAsync(d_off, hoff.data(), 8 * nlay, cudaMemcpyHostToDevice, s));
-  {
-    StageTimer t(ctx, "jacobian", 0);
-    int cur = 0, lc = 0;
-    double dv_old = 0.;
-    int64_t n_old = 0;
-    for (int l = 0; l < nlay; l++) {
-      const LayerDev& d = B.ld[l];
-      if (l > 0 && d.dv > dv_old) return fail(ctx, LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
-      // carry the rows of layers below l onto layer l's grid
-      if (l > 0 && l <= a) {
-        for (int k = 0; k < np; k++)
-          CK(launch_jac_prop(B.d_ld + l, B.w.od + d.off_od, d.npts, dv_old, n_old,
-                             low[lc] + (size_t)k * a * npts, low[lc ^ 1] + (size_t)k * a * npts,
-                             npts, l, s));
-        lc ^= 1;
-      }
-      double* dp[kJacMaxParams];
-      const double* tp[kJacMaxParams];
-      for (int k = 0; k < np; k++) {
-        dp[k] = (l < a) ? low[lc] + ((size_t)k * a + l) * npts
-                        : rows + ((size_t)k * nlay + l) * npts;
-        tp[k] = dtau + (size_t)k * ntot + off[l];
-      }
-      const int nxt = cur ^ 2;
-      const double tbnd = (l == 0) ? run->tmpbnd : 0.;
-      CK(launch_jac_layer(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
-                          dv_old, n_old, rt[cur], rt[cur + 1], rt[nxt], rt[nxt + 1], tbnd,
-                          run->bndemi, layers[l].tzu, dp, tp, np, s));
-      cur = nxt;
-      dv_old = d.dv;
-      n_old = d.npts;
-    }
-    CK(launch_jac_top(B.w.od, d_off, nlay, a, np, npts, rows, low[lc], s));
-    if (rad) {
-      rc = copy_out(ctx, rad, rt[cur], sizeof(double) * npts);
-      if (rc) return rc;
-    }
-  }
-  rc = copy_out(ctx, jac, rows, sizeof(double) * n_rows);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(s));
+  CK(cudaStreamSynchronize(ctx->stream));
   harvest(ctx);
   return finish_od(ctx);
 }
+
+int lbl_adjoint_batch(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, const int32_t* nlay,
+                      int32_t nprof, const int32_t* mols, int32_t nq, int32_t mode,
+                      double dv_chan, double* rad, int64_t* offsets, int64_t rad_cap,
+                      double* jac, int64_t* jac_off, int64_t jac_cap, int32_t precision) {
+  if (!ctx) return LBL_E_ARG;
+  int rc = check_jac_args(ctx, run, layers, nlay, nprof, mols, nq, mode);
+  if (rc) return rc;
+  if (!rad || !offsets || !jac || !jac_off || !(dv_chan >= 0.))
+    return fail(ctx, LBL_E_ARG, "lbl_adjoint_batch: bad argument");
+  cudaSetDevice(ctx->device);
+  const int np = 1 + nq;
+  std::vector<int64_t> lay0(nprof + 1, 0), nout(nprof);
+  const int64_t nchan = dv_chan > 0. ? (int64_t)std::floor((run->v2 - run->v1) / dv_chan + 1e-9) : 0;
+  if (dv_chan > 0. && nchan < 1) return fail(ctx, LBL_E_ARG, "channel wider than the run");
+  offsets[0] = 0;
+  jac_off[0] = 0;
+  for (int p = 0; p < nprof; p++) {
+    std::string e;
+    rc = dv_rule(*run, layers + lay0[p], nlay[p], &e);
+    if (rc) return fail(ctx, rc, "profile " + std::to_string(p) + ": " + e);
+    lay0[p + 1] = lay0[p] + nlay[p];
+    nout[p] = dv_chan > 0. ? nchan : layer_npts(*run, layers[lay0[p + 1] - 1].dv);
+    offsets[p + 1] = offsets[p] + nout[p];
+    jac_off[p + 1] = jac_off[p] + (int64_t)np * nlay[p] * nout[p];
+  }
+  if (offsets[nprof] > rad_cap || jac_off[nprof] > jac_cap)
+    return fail(ctx, LBL_E_ARG, "output buffer too small");
+  for (int p = 0; p < nprof; p++) {
+    lbl_layer* L = layers + lay0[p];
+    const int nl = nlay[p];
+    const int chunk = jac_chunk(ctx, *run, L, nl, np, nchan);
+    if (chunk < 1)
+      return fail(ctx, LBL_E_NOMEM, "profile " + std::to_string(p) + ": Jacobian work space");
+    for (int k0 = 0; k0 < np; k0 += chunk) {
+      const int k1 = std::min(np, k0 + chunk);
+      JacOut o;
+      rc = jac_profile(ctx, *run, L, nl, mols, k0, k1, mode, precision, nchan, o);
+      if (rc) return rc;
+      const double* rsrc = o.rad;
+      const double* jsrc = o.rows;
+      if (dv_chan > 0.) {
+        // channel means of the radiance and of each row, into the work space
+        rc = jac_channels(ctx, *run, o, nl * (k1 - k0), dv_chan, nchan);
+        if (rc) return rc;
+        rsrc = o.chan_rad;
+        jsrc = o.chan_rows;
+      }
+      if (k0 == 0) {
+        rc = copy_out(ctx, rad + offsets[p], rsrc, sizeof(double) * nout[p]);
+        if (rc) return rc;
+      }
+      rc = copy_out(ctx, jac + jac_off[p] + (int64_t)k0 * nl * nout[p], jsrc,
+                    sizeof(double) * (size_t)(k1 - k0) * nl * nout[p]);
+      if (rc) return rc;
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  harvest(ctx);
+  return finish_od(ctx);
+}
+
+int lbl_set_memory_limit(lbl_ctx* ctx, int64_t bytes) {
+  if (!ctx || bytes < 0) return fail(ctx, LBL_E_ARG, "memory limit must be >= 0");
+  // the grow-only work buffers are released; later calls allocate them again
+  // within the cap
+  cudaSetDevice(ctx->device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->mem.release(ctx->arena.base, ctx->arena.cap);
+  ctx->arena.base = nullptr;
+  ctx->arena.cap = 0;
+  ctx->mem.release(ctx->jac_mem, ctx->jac_cap);
+  ctx->jac_mem = nullptr;
+  ctx->jac_cap = 0;
+  for (int k = 0; k < 4; k++) {
+    ctx->mem.release(ctx->mbuf[k], ctx->mcap * sizeof(double));
+    ctx->mbuf[k] = nullptr;
+  }
+  ctx->mcap = 0;
+  ctx->mem.limit = (size_t)bytes;
+  return LBL_OK;
+}
+
+int64_t lbl_memory_used(const lbl_ctx* ctx) { return ctx ? (int64_t)ctx->mem.used : -1; }
 
 int lbl_profile(lbl_ctx* ctx, int32_t enable) {
   if (!ctx) return LBL_E_ARG;

@@ -2165,10 +2165,25 @@ __device__ __forceinline__ double planck_dt(double vi, double t) {
   return kRADCN1 * (vi * vi * vi) * e / (1. - e) * (x / t) / (1. - e);
 }
 
+// PLANCK_DT (src/xmerge.f90:1019-1080): the factor of the Planck function's
+// temperature derivative at XKT, times BBVAL (EMDT passes the layer's Planck
+// value for both the layer and the upper level).
+__device__ __forceinline__ double planck_dt_ref(double vi, double xkt, double bbval) {
+  double v = 0.;
+  if (xkt > 0.0) {
+    const double viokt = vi / xkt, vtkelv = xkt * kRADCN2;
+    if (viokt <= 1e-2) v = 1. / (-vtkelv * (1. + 5e-1 * viokt));
+    else if (viokt <= 80.0) v = viokt / (vtkelv * (1. - exp(-viokt)));
+  }
+  return v * bbval;
+}
+
 struct JacRows {
   double* d[kJacMaxPar];        // per parameter: this layer's row
-  const double* dtau[kJacMaxPar];  // per parameter: dtau/dp of this layer
+  const double* dtau[kJacMaxPar];  // per parameter: dtau/dp of this layer (mode 0) or
+                                   // the perturbed run's optical depth (mode 1)
   int np;
+  int mode;                     // 0: exact merge derivative; 1: TDERIVup/QDERIVup
 };
 
 __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const double* od,
@@ -2201,12 +2216,13 @@ __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const d
   const double em = (1. - tr) * (bb + bbd * fi);
   const double dem_do = tr * (bb + bbd * fi) + (1. - tr) * bbd * dfi;
   const double dem_db = (1. - tr) * (xkta > 0. ? 1. - fi : 1.);
-  double rad, trn, dr_do;
+  double rad, trn, dr_do, rado;
   if (first) {
     const double bs = tbnd > 0. ? planck(vi, tbnd / kRADCN2, kRADCN2 / tbnd) * emis : 0.;
     rad = em + tr * bs;
     trn = tr;
     dr_do = dem_do - tr * bs;
+    rado = bs;
   } else {
     const long itype = (dv_old == DV) ? 0 : fint(DV / (dv_old - DV) + 0.5);
     double ro, to;
@@ -2231,9 +2247,35 @@ __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const d
     rad = tr * ro + em;
     trn = tr * to;
     dr_do = -tr * ro + dem_do;
+    rado = ro;
   }
   rad_out[f] = rad;
   tr_out[f] = trn;
+  if (rows.mode == 1) {
+    // the reference's layer rows (TDERIVup :6076-6110, QDERIVup :5900-5935)
+    // from the quantities EMDT saves (:4500-4540); RADO is the radiance
+    // entering the layer (the boundary emission under the first layer)
+    const double bb = planck(vi, t.xkt, t.rk);
+    const double bb_dif = xkta > 0. ? planck(vi, xkta, t.rka) - bb : 0.;
+    const double betai = (bb + bb_dif) - bb;
+    const double bbeff = bb + bb_dif * fi;
+    const double bbd = planck_dt_ref(vi, t.xkt, bb);
+    const double bbdt = xkta > 0. ? planck_dt_ref(vi, xkta, bb) : 0.;
+    const double a = (bbeff + betai * fi - rado) * tr;
+    for (int k = 0; k < rows.np; k++) {
+      const double x = rows.dtau[k][f];
+      double d;
+      if (k == 0) {
+        const double optdpt = tr > 1.e-06 ? -log(tr) : x;
+        const double dtaudt = x - optdpt;
+        d = a * dtaudt + bbd * (1. - tr) + (1. - tr) * ((bbdt - bbd) * fi + betai * dfi * dtaudt);
+      } else {
+        d = x * (a + (1. - tr) * betai * dfi);
+      }
+      rows.d[k][f] = d;
+    }
+    return;
+  }
   const double dbt = dem_db * planck_dt(vi, L.tave);
   for (int k = 0; k < rows.np; k++) {
     double d = clamped ? 0. : dr_do * rows.dtau[k][f];
@@ -2299,6 +2341,29 @@ __global__ void k_jac_top(const double* od, const int64_t* od_off, int nlay, int
     double tau = od[od_off[m] + i];
     if (tau < -kODLO) tau = -kODLO;
     c *= exp(-tau);
+  }
+}
+
+// Means of each row of x (row r at x + r n) over the channels whose points
+// are [cb[c], cb[c+1]): out[r nchan + c].  One CTA per (channel, row); the
+// points of a channel are summed in a fixed order (thread stride, then a
+// fixed reduction tree), so the result does not depend on timing.
+__global__ void __launch_bounds__(256) k_chan_mean(const double* x, int64_t n, const int64_t* cb,
+                                                   int64_t nchan, double* out) {
+  __shared__ double red[8];
+  const int64_t c = blockIdx.x, r = blockIdx.y;
+  const int64_t a = cb[c], b = cb[c + 1];
+  const double* xr = x + r * n;
+  double s = 0.;
+  for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) s += xr[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int k = 0; k < 8; k++) t += red[k];
+    out[r * nchan + c] = b > a ? t / double(b - a) : 0.;
   }
 }
 
@@ -2455,10 +2520,11 @@ cudaError_t launch_jac_layer(const LayerDev* Ld, const double* vft_panel, const 
                              const double* rad_in, const double* tr_in, double* rad_out,
                              double* tr_out, double tbnd, double emis, double tzu,
                              double* const* d, const double* const* dtau, int np,
-                             cudaStream_t s) {
+                             int mode, cudaStream_t s) {
   if (np < 1 || np > kJacMaxPar) return cudaErrorInvalidValue;
   JacRows rows;
   rows.np = np;
+  rows.mode = mode;
   for (int k = 0; k < kJacMaxPar; k++) {
     rows.d[k] = k < np ? d[k] : nullptr;
     rows.dtau[k] = k < np ? dtau[k] : nullptr;
@@ -2481,6 +2547,14 @@ cudaError_t launch_jac_prop(const LayerDev* Ld, const double* od, int64_t npts, 
 cudaError_t launch_jac_top(const double* od, const int64_t* od_off, int nlay, int a, int np,
                            int64_t n, double* rows, const double* low, cudaStream_t s) {
   k_jac_top<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(od, od_off, nlay, a, np, n, rows, low);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chan_mean(const double* x, int64_t n, int nrows, const int64_t* cb,
+                             int64_t nchan, double* out, cudaStream_t s) {
+  if (nrows <= 0 || nchan <= 0) return cudaSuccess;
+  if (nrows > 65535 || nchan >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
+  k_chan_mean<<<dim3((unsigned)nchan, (unsigned)nrows), 256, 0, s>>>(x, n, cb, nchan, out);
   return cudaGetLastError();
 }
 

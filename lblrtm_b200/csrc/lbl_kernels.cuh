@@ -161,7 +161,7 @@ cudaError_t launch_jac_layer(const LayerDev* Ld, const double* vft_panel, const 
                              const double* rad_in, const double* tr_in, double* rad_out,
                              double* tr_out, double tbnd, double emis, double tzu,
                              double* const* d, const double* const* dtau, int np,
-                             cudaStream_t s);
+                             int mode, cudaStream_t s);
 cudaError_t launch_jac_prop(const LayerDev* Ld, const double* od, int64_t npts, double dv_old,
                             int64_t n_old, const double* in, double* out, int64_t stride,
                             int nrows, cudaStream_t s);
@@ -169,6 +169,9 @@ cudaError_t launch_jac_top(const double* od, const int64_t* od_off, int nlay, in
                            int64_t n, double* rows, const double* low, cudaStream_t s);
 cudaError_t launch_jac_diff(double* plus, const double* minus, int64_t n, double rh,
                             cudaStream_t s);
+// Means of nrows rows (n points each) over channels [cb[c], cb[c+1]).
+cudaError_t launch_chan_mean(const double* x, int64_t n, int nrows, const int64_t* cb,
+                             int64_t nchan, double* out, cudaStream_t s);
 constexpr int kJacMaxParams = 8;
 
 void init_kernel_attributes();

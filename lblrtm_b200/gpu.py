@@ -42,11 +42,17 @@ SIGNATURES = {
                                     C.c_int32]),
     "lbl_jacobian": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32,
                                P_I32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
+    "lbl_adjoint_batch": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), P_I32,
+                                    C.c_int32, P_I32, C.c_int32, C.c_int32, C.c_double,
+                                    C.c_void_p, P_I64, C.c_int64, C.c_void_p, P_I64, C.c_int64,
+                                    C.c_int32]),
     "lbl_brightness_temperature": (C.c_int, [P_D, C.c_int64, C.c_double, C.c_double, P_D]),
     "lbl_merge_layer_noalloc": (C.c_int, [C.c_int, C.POINTER(abi.Run), C.POINTER(abi.Layer),
                                           C.c_int32, C.c_double, C.c_void_p, C.c_void_p,
                                           C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_int64, C.c_void_p]),
+    "lbl_set_memory_limit": (C.c_int, [C.c_void_p, C.c_int64]),
+    "lbl_memory_used": (C.c_int64, [C.c_void_p]),
     "lbl_profile": (C.c_int, [C.c_void_p, C.c_int32]),
     "lbl_profile_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, P_I32]),
 }
@@ -144,6 +150,13 @@ class Context:
         return {buf[i].name.decode(): (buf[i].ms, buf[i].launches, buf[i].work)
                 for i in range(n.value)}
 
+    def set_memory_limit(self, nbytes):
+        """Cap the device memory this context may hold (0: no cap)."""
+        self._check(self.lib.lbl_set_memory_limit(self.h, int(nbytes)), "set_memory_limit")
+
+    def memory_used(self):
+        return int(self.lib.lbl_memory_used(self.h))
+
     def set_stream(self, stream_ptr):
         self._check(self.lib.lbl_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
 
@@ -210,6 +223,48 @@ class Context:
                                                off.ctypes.data_as(C.POINTER(C.c_int64)), total,
                                                precision), "forward_batch")
         return [(rad[off[i]:off[i + 1]], tr[off[i]:off[i + 1]]) for i in range(len(profiles))]
+
+    def adjoint_batch(self, run, profiles, mols, mode=abi.JAC_REFERENCE, dv_chan=0.0,
+                      precision=abi.PREC_FP64, rad=None, jac=None):
+        """Forward and Jacobians of many profiles in one call.  Returns a list
+        of (rad, jac) per profile, jac of shape (1 + len(mols), nlay, n);
+        n is the profile's top-grid length (dv_chan = 0) or the number of
+        channels of width dv_chan.  rad/jac may be given as flat buffers
+        (numpy arrays or CUDA tensors) large enough for all profiles."""
+        counts = [len(p) for p in profiles]
+        allL = (abi.Layer * sum(counts))()
+        k = 0
+        for p in profiles:
+            C.memmove(C.byref(allL, k * C.sizeof(abi.Layer)), p, C.sizeof(abi.Layer) * len(p))
+            k += len(p)
+        np_ = 1 + len(mols)
+        if dv_chan > 0:
+            nch = int(np.floor((run.v2 - run.v1) / dv_chan + 1e-9))
+            nout = [nch] * len(profiles)
+        else:
+            nout = []
+            for p in profiles:
+                q = abi.make_layers_like(p)
+                dv, _ = dv_rule(run, q)
+                nout.append(layer_npts(run, dv[-1]))
+        nrad = sum(nout)
+        njac = sum(np_ * c * n for c, n in zip(counts, nout))
+        rad = np.zeros(nrad) if rad is None else rad
+        jac = np.zeros(njac) if jac is None else jac
+        off = np.zeros(len(profiles) + 1, dtype=np.int64)
+        joff = np.zeros(len(profiles) + 1, dtype=np.int64)
+        nl = (C.c_int32 * len(profiles))(*counts)
+        m = (C.c_int32 * max(len(mols), 1))(*mols)
+        self._check(self.lib.lbl_adjoint_batch(
+            self.h, C.byref(run), allL, nl, len(profiles), m, len(mols), int(mode),
+            C.c_double(dv_chan), _ptr(rad), off.ctypes.data_as(P_I64), int(nrad), _ptr(jac),
+            joff.ctypes.data_as(P_I64), int(njac), precision), "adjoint_batch")
+        out = []
+        for i, (c, n) in enumerate(zip(counts, nout)):
+            r = rad[off[i]:off[i + 1]]
+            j = jac[joff[i]:joff[i + 1]]
+            out.append((r, j.reshape(np_, c, n) if hasattr(j, "reshape") else j))
+        return out
 
     def jacobian(self, run, layers, mols, precision=abi.PREC_FP64, rad=None, jac=None):
         """TOA radiance and its Jacobians, shape (1 + len(mols), nlay, npts):

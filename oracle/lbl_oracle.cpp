@@ -50,6 +50,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "../include/lblgpu.h"
@@ -1520,9 +1521,15 @@ void eminit(const lbl_run& R, const lbl_layer& L, const std::vector<PanelOut>& o
 }
 
 // RADMRG + RADNN, IPATHL=1 (src/xmerge.f90:2587-2895, 2899-3130)
-int radmrg(const lbl_run& R, const lbl_layer& L, double DVL,
-           const std::vector<MPanel>& old, const std::vector<PanelOut>& od,
-           std::vector<MPanel>& out) {
+// The RADMRG/RADNN panel loop with the layer's (EM, TR) supplied per panel
+// by `layer`: EMIN for the forward merge; the analytic-Jacobian rows use the
+// same loop to regrid a field onto the layer grid (EM = 0, TR = 1) and to
+// carry a row through the layer (EM = 0, TR = the layer transmittance).
+int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
+                const std::vector<MPanel>& old, const std::vector<PanelOut>& od,
+                const std::function<void(size_t, const PanelOut&, std::vector<double>&,
+                                         std::vector<double>&)>& layer,
+                std::vector<MPanel>& out) {
   double DVK = L.dv;
   long ITYPE;
   if (DVL == DVK) ITYPE = 0;
@@ -1549,9 +1556,12 @@ int radmrg(const lbl_run& R, const lbl_layer& L, double DVL,
   double V2PO = 0., DVPO = 0.;
   size_t oi = 0;  // next old panel
   out.clear();
-  for (const PanelOut& p : od) {
+  (void)XKT;
+  (void)XKTA;
+  for (size_t pi = 0; pi < od.size(); pi++) {
+    const PanelOut& p = od[pi];
     std::vector<double> EM, TR;
-    emin(p, XKT, XKTA, EM, TR);
+    layer(pi, p, EM, TR);
     if (V2PO <= p.v2p + DVPO) {
       while (true) {
         if (oi >= old.size()) break;
@@ -1616,6 +1626,16 @@ int radmrg(const lbl_run& R, const lbl_layer& L, double DVL,
     NPE = IPLn;
   }
   return LBL_OK;
+}
+
+int radmrg(const lbl_run& R, const lbl_layer& L, double DVL,
+           const std::vector<MPanel>& old, const std::vector<PanelOut>& od,
+           std::vector<MPanel>& out) {
+  const double XKT = L.tave / RADCN2, XKTA = L.tzu / RADCN2;
+  return radmrg_core(R, L, DVL, old, od,
+                     [&](size_t, const PanelOut& p, std::vector<double>& EM,
+                         std::vector<double>& TR) { emin(p, XKT, XKTA, EM, TR); },
+                     out);
 }
 
 // ABSMRG (src/xmerge.f90:437-682): optical-depth sum with 4-point regrid.
@@ -1831,6 +1851,7 @@ const char* orc_last_error() { return g_err.c_str(); }
 
 void orc_set_rsym(int on) { g_rsym = on != 0; }
 
+
 // PATH DV rule (src/lblrtm.f90:5355-5510), standard path (JTYPE=0, IOD=0).
 int orc_dv_rule(const lbl_run* R, lbl_layer* Ls, int nlay) {
   double DV = 0.;
@@ -1989,6 +2010,222 @@ int orc_forward(const lbl_run* R, lbl_layer* Ls, int nlay, const lbl_lines* line
       }
   if (k != npts) return fail(LBL_E_ARG, "npts mismatch: oracle produced " + std::to_string(k));
   return LBL_OK;
+}
+
+// PLANCK_DT (src/xmerge.f90:1019-1080): the factor of the Planck function's
+// temperature derivative at XKT, times BBVAL (EMDT passes the layer's
+// Planck value for both the layer and the upper level).
+double PLANCK_DT_REF(double VI, double XKT, double BBVAL) {
+  double v = 0.;
+  if (XKT > 0.0) {
+    const double VIOKT = VI / XKT, VTKELV = XKT * RADCN2;
+    if (VIOKT <= 1e-2) v = 1. / (-VTKELV * (1. + 5e-1 * VIOKT));
+    else if (VIOKT <= 80.0) v = VIOKT / (VTKELV * (1. - std::exp(-VIOKT)));
+  }
+  return v * BBVAL;
+}
+
+// dB/dT of the PLANCK function's two branches at temperature t (the
+// derivative of the discrete forward model, central-difference mode).
+double planck_dt_model(double vi, double t) {
+  if (!(t > 0.)) return 0.;
+  const double xkt = t / RADCN2;
+  const double x = vi / xkt;
+  if (x < 1e-2) return RADCN1 * (vi * vi) / RADCN2 * (1. + x) / ((1. + 0.5 * x) * (1. + 0.5 * x));
+  if (x > 80.) return 0.;
+  const double e = std::exp(-x);
+  return RADCN1 * (vi * vi * vi) * e / (1. - e) * (x / t) / (1. - e);
+}
+
+// Radiance Jacobians of the upwelling top-of-atmosphere radiance with
+// respect to each layer's temperature and the log column amount of the
+// listed molecules: the reference's analytic-Jacobian path (lblrtm.f90:
+// 2855-3067: one extra OPDPTH per layer and parameter; EMDT xmerge.f90:
+// 4406-5030 saves BBEFF, BBSAV, BBASAV, BBDSAV, BBDLSAV, FSAV, dF_dtau;
+// TDERIVup :5956-6144 and QDERIVup :5786-5952 form the layer rows), each
+// row carried to the top through the later layers' RADNN regrid and
+// transmittance (the reference's TRTOTDN product on a common grid).
+//   mode 1: the reference's definitions: dtau/dT = tau(T+1 K) - tau where the
+//           layer transmittance exceeds 1e-6 (else 0); the molecule row uses
+//           the optical depth of a run with that molecule alone (other WK
+//           zero, WK(7) added to WBROAD);
+//   mode 0: central differences (T +-0.1 K, amount +-1 %) merged with the
+//           exact derivative of EMIN/EMINIT/RADNN.
+int jacobian(const lbl_run& R, lbl_layer* Ls, int nlay, const lbl_lines* lines,
+             const lbl_mtckd* ck, const int* mols, int nq, int mode, double* rad, double* jac,
+             int64_t npts) {
+  int rc = orc_dv_rule(&R, Ls, nlay);
+  if (rc != LBL_OK) return rc;
+  if (R.iemit != 1 || R.ipathl != 1) return fail(LBL_E_ARG, "upwelling radiance only");
+  Tape3 t3(lines);
+  const lbl_mtckd* cku = R.icntnm ? ck : nullptr;
+  const int np = 1 + nq;
+  std::vector<MPanel> acc;
+  std::vector<std::vector<MPanel>> rows((size_t)np * nlay);
+  int jrad = R.jrad;
+  double dv_old = 0.;
+  auto od_of = [&](const lbl_layer& L, int j, std::vector<PanelOut>& out) {
+    int jj = j;
+    return opdpth(&R, &L, t3, cku, &jj, out);
+  };
+  for (int l = 0; l < nlay; l++) {
+    const lbl_layer& L = Ls[l];
+    const int jin = jrad;
+    std::vector<PanelOut> od;
+    rc = opdpth(&R, &L, t3, cku, &jrad, od);
+    if (rc != LBL_OK) return rc;
+    // optical-depth inputs of each parameter's row
+    std::vector<std::vector<PanelOut>> dp(np);
+    for (int k = 0; k < np; k++) {
+      if (mode == 0) {
+        lbl_layer Lp = L, Lm = L;
+        double h;
+        if (k == 0) {
+          Lp.tave += 0.1;
+          Lm.tave -= 0.1;
+          h = 0.2;
+        } else {
+          Lp.wk[mols[k - 1] - 1] *= 1.01;
+          Lm.wk[mols[k - 1] - 1] *= 0.99;
+          h = std::log(1.01) - std::log(0.99);
+        }
+        std::vector<PanelOut> pp, pm;
+        if ((rc = od_of(Lp, jin, pp)) || (rc = od_of(Lm, jin, pm))) return rc;
+        for (size_t q = 0; q < pp.size(); q++)
+          for (size_t i = 0; i < pp[q].r.size(); i++) pp[q].r[i] = (pp[q].r[i] - pm[q].r[i]) / h;
+        dp[k] = std::move(pp);
+      } else {
+        lbl_layer Lq = L;
+        if (k == 0) {
+          Lq.tave = L.tave + 1.;
+        } else {
+          const int m = mols[k - 1];
+          for (int j = 0; j < LBL_WKDIM; j++) Lq.wk[j] = 0.;
+          Lq.wk[m - 1] = L.wk[m - 1];
+          Lq.wbroad = L.wbroad + L.wk[6];
+        }
+        if ((rc = od_of(Lq, jin, dp[k]))) return rc;
+      }
+    }
+    // incoming radiance on this layer's grid
+    const double XKT = L.tave / RADCN2, XKTA = L.tzu / RADCN2;
+    std::vector<MPanel> rin;
+    if (l > 0) {
+      rc = radmrg_core(R, L, dv_old, acc, od,
+                       [&](size_t, const PanelOut& p, std::vector<double>& EM,
+                           std::vector<double>& TR) {
+                         EM.assign(p.nlim + 1, 0.);
+                         TR.assign(p.nlim + 1, 1.);
+                       },
+                       rin);
+      if (rc != LBL_OK) return rc;
+    }
+    // the layer transmittance and this layer's rows, point by point as EMDT
+    std::vector<std::vector<double>> trl(od.size());
+    for (int k = 0; k < np; k++) rows[(size_t)k * nlay + l].clear();
+    const double TBND = R.tmpbnd, XKTBND = TBND / RADCN2;
+    const double rec_6 = 1. / 6.;
+    for (size_t q = 0; q < od.size(); q++) {
+      const PanelOut& p = od[q];
+      trl[q].assign(p.nlim + 1, 0.);
+      std::vector<std::vector<double>> d(np, std::vector<double>(p.nlim, 0.));
+      double VI = p.v1p;
+      for (long I = 1; I <= p.nlim; I++) {
+        const double BB = PLANCK(VI, XKT);
+        const double bb_dif = XKTA > 0. ? PLANCK(VI, XKTA) - BB : 0.;
+        const double tau = p.r[I - 1];
+        double odvi = tau;
+        const bool clamped = odvi < -OD_LO;
+        if (clamped) odvi = -OD_LO;
+        const double tr_i = std::exp(-odvi);
+        double f_i, df_i;
+        if (odvi <= OD_LO) {
+          f_i = rec_6 * odvi;
+          df_i = rec_6;
+        } else {
+          f_i = 1. - 2. * (tr_i / (tr_i - 1.) + 1. / odvi);
+          df_i = -2. * (tr_i / ((tr_i - 1.) * (tr_i - 1.)) - 1. / (odvi * odvi));
+        }
+        trl[q][I] = tr_i;
+        const double bs = (l == 0 && TBND > 0.) ? PLANCK(VI, XKTBND) * R.bndemi : 0.;
+        const double rado = l == 0 ? bs : rin[q].rad[I - 1];
+        const double bbeff = BB + bb_dif * f_i;
+        for (int k = 0; k < np; k++) {
+          const double x = dp[k][q].r[I - 1];
+          double v;
+          if (mode == 0) {
+            const double dem_do = tr_i * bbeff + (1. - tr_i) * bb_dif * df_i;
+            const double dr_do = dem_do - tr_i * rado;
+            v = clamped ? 0. : dr_do * x;
+            if (k == 0)
+              v += (1. - tr_i) * (XKTA > 0. ? 1. - f_i : 1.) * planck_dt_model(VI, L.tave);
+          } else {
+            const double betai = (BB + bb_dif) - BB;
+            if (k == 0) {
+              const double BBD = PLANCK_DT_REF(VI, XKT, BB);
+              const double bbdT = XKTA > 0. ? PLANCK_DT_REF(VI, XKTA, BB) : 0.;
+              const double optdpt = tr_i > 1.e-06 ? -std::log(tr_i) : x;
+              const double dtaudT = x - optdpt;
+              v = (bbeff + betai * f_i - rado) * dtaudT * tr_i + BBD * (1. - tr_i) +
+                  (1. - tr_i) * ((bbdT - BBD) * f_i + betai * df_i * dtaudT);
+            } else {
+              v = x * ((bbeff + betai * f_i - rado) * tr_i + (1. - tr_i) * betai * df_i);
+            }
+          }
+          d[k][I - 1] = v;
+        }
+        VI = VI + p.dvp;
+      }
+      for (int k = 0; k < np; k++)
+        rows[(size_t)k * nlay + l].push_back(
+            MPanel{p.v1p, p.v2p, p.dvp, p.nlim, d[k], std::vector<double>(p.nlim, 0.)});
+    }
+    // rows of the layers below, carried through this layer
+    if (l > 0) {
+      for (int k = 0; k < np; k++)
+        for (int j = 0; j < l; j++) {
+          std::vector<MPanel> out;
+          rc = radmrg_core(R, L, dv_old, rows[(size_t)k * nlay + j], od,
+                           [&](size_t pi, const PanelOut& p, std::vector<double>& EM,
+                               std::vector<double>& TR) {
+                             EM.assign(p.nlim + 1, 0.);
+                             TR = trl[pi];
+                           },
+                           out);
+          if (rc != LBL_OK) return rc;
+          rows[(size_t)k * nlay + j].swap(out);
+        }
+    }
+    // the forward merge
+    std::vector<MPanel> out;
+    if (l == 0) eminit(R, L, od, out);
+    else if ((rc = radmrg(R, L, dv_old, acc, od, out)) != LBL_OK) return rc;
+    acc.swap(out);
+    dv_old = L.dv;
+  }
+  int64_t k = 0;
+  for (auto& p : acc)
+    for (long i = 0; i < p.nlim; i++, k++)
+      if (k < npts && rad) rad[k] = p.rad[i];
+  if (k != npts) return fail(LBL_E_ARG, "npts mismatch: oracle produced " + std::to_string(k));
+  for (int q = 0; q < np; q++)
+    for (int l = 0; l < nlay; l++) {
+      int64_t i = 0;
+      double* dst = jac + ((int64_t)q * nlay + l) * npts;
+      for (auto& p : rows[(size_t)q * nlay + l])
+        for (long t = 0; t < p.nlim; t++, i++)
+          if (i < npts) dst[i] = p.rad[t];
+      if (i != npts) return fail(LBL_E_ARG, "Jacobian row length mismatch");
+    }
+  return LBL_OK;
+}
+
+int orc_jacobian(const lbl_run* R, lbl_layer* Ls, int nlay, const lbl_lines* lines,
+                 const lbl_mtckd* ck, const int* mols, int nq, int mode, double* rad, double* jac,
+                 int64_t npts) {
+  g_err.clear();
+  if (!R || !Ls || nlay < 1 || !jac || nq < 0 || (nq > 0 && !mols)) return fail(LBL_E_ARG, "bad argument");
+  return jacobian(*R, Ls, nlay, lines, ck, mols, nq, mode, rad, jac, npts);
 }
 
 // Shape tables for known-answer tests: which = 0..4 -> F1,F2,F3,FG,XVER.

@@ -105,3 +105,21 @@ def tips_scor(mol, iso, t):
     s = C.c_double()
     check(lib().orc_tips_scor(mol, iso, C.c_double(t), C.byref(s)))
     return s.value
+
+
+def jacobian(run, layers, lines_h, mols, mode, mtckd_h=None):
+    """TOA radiance and Jacobian rows (1 + len(mols), nlay, npts) of the
+    oracle's analytic-Jacobian restatement (mode 1: the reference's
+    definitions; mode 0: central differences)."""
+    L = lib()
+    check(L.orc_dv_rule(C.byref(run), layers, len(layers)))
+    n = npts(run, layers[len(layers) - 1].dv)
+    nl = len(layers)
+    rad = np.zeros(n)
+    jac = np.zeros((1 + len(mols), nl, n))
+    m = (C.c_int * max(len(mols), 1))(*mols)
+    ck = C.byref(mtckd_h.struct) if mtckd_h is not None else None
+    P = C.POINTER(C.c_double)
+    check(L.orc_jacobian(C.byref(run), layers, nl, C.byref(lines_h.struct), ck, m, len(mols),
+                         int(mode), rad.ctypes.data_as(P), jac.ctypes.data_as(P), C.c_int64(n)))
+    return rad, jac
