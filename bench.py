@@ -54,7 +54,14 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-workers", type=int, default=0)
     p.add_argument("--no-jacobian", action="store_true")
+    p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--no-precision", action="store_true")
+    p.add_argument("--batch-profiles", type=int, default=256)
     return p.parse_args()
+
+
+WORKLOAD = ("config1: 60 layers, 4 absorbers (H2O, CO2, O3, CH4), {nlines:,} lines, "
+            "500-1500 cm-1, upwelling TOA radiance")
 
 
 def workload(nlines):
@@ -62,6 +69,16 @@ def workload(nlines):
     run = abi.make_run(**cfg["run"])
     layers = abi.make_layers(cfg["profile"])
     return cfg, run, layers
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def layer_points(run, layers, npts_fn):
@@ -113,24 +130,27 @@ def reference_arm(a):
     if rank != 0:
         return
     workers = a.cpu_workers or default_workers()
-    # every step is one concurrent forward per worker: ~10 s of CPU time each
-    steps = max(1, min(a.steps, 6))
-    warm = max(1, min(a.warmup, 3))
+    # every step is one config-1 forward per worker, run concurrently (about
+    # 6-7 s of wall time on 16 cores); warm-up and timed steps as asked
+    steps = max(1, a.steps)
+    warm = max(0, a.warmup)
     res = cpu_run(a.nlines, workers, reps=warm + steps)
     timed = res[-steps:]
     pts = timed[0][0]
     wall = sum(r[1] for r in timed) / steps
     value = pts / wall
-    cfgd = {"workload": "config1: 60 layers, 50,000 lines, 500-1500 cm-1, upwelling TOA radiance",
-            "nlines": a.nlines, "layers": 60, "precision": "fp64"}
+    cfgd = {"workload": WORKLOAD.format(nlines=a.nlines), "nlines": a.nlines, "layers": 60,
+            "precision": "fp64"}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
         "steps": steps, "warmup": warm, "ms_per_step": wall * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)", "config": cfgd,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                         "cpu": cpu_model(),
                          "sample": f"{workers} concurrent config-1 forwards per step "
-                                   "(restated reference, C++ FP64 oracle)"},
+                                   "(restated reference, C++ FP64 oracle, one process per "
+                                   "core)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -248,6 +268,208 @@ def jacobian_leg(ctx, prec, torch):
             "timing": "wall clock around the synchronous call (host planning included)"}
 
 
+C2_SLICES = {"20-45 cm-1 (DV to 8.5e-6, continuum, image lines)": (20.0, 45.0),
+             "700-725 cm-1": (700.0, 725.0),
+             "2500-2525 cm-1 (JRAD=1 in every layer)": (2500.0, 2525.0)}
+
+
+def precision_leg(ctx):
+    """Config 2, the precision sweep: FP32/FP64-split against plain FP64 on
+    25 cm-1 slices of both sub-runs (all 60 layers, 400,000 lines over
+    10-3000 cm-1, seeded MT_CKD-layout continuum); max and RMS error of
+    every layer's optical depth (relative, above 1e-9), of its
+    transmittance, of the total transmittance and of the TOA brightness
+    temperature.  The FP64 path agrees with the FP64 oracle to 1e-9 on these
+    slices (tests/test_gpu_sweep.py)."""
+    from lblrtm_b200 import gpu
+    cfg = configs.config2()
+    ck = abi.MtckdHandle(cfg["mtckd"])
+    ctx.upload_mtckd(ck)
+    od_max = od_ss = t_max = t_ss = 0.0
+    od_n = t_n = 0
+    bt_max = bt_ss = tt_max = 0.0
+    bt_n = 0
+    per = {}
+    for name, (v1, v2) in C2_SLICES.items():
+        run = abi.make_run(**cfg["run"], v1=v1, v2=v2)
+        lays = abi.make_layers(cfg["profile"])
+        gpu.dv_rule(run, lays)
+        ctx.upload_lines(abi.LinesHandle(configs.subset_lines(cfg["lines"], v1, v2, margin=30.0)))
+        j = run.jrad
+        smax = 0.0
+        for l in range(len(lays)):
+            o64, jn = ctx.layer_od(run, lays[l], jrad=j)
+            o32, _ = ctx.layer_od(run, lays[l], jrad=j, precision=abi.PREC_SPLIT)
+            j = jn
+            e = np.abs(o32 - o64) / np.maximum(np.abs(o64), 1e-9)
+            te = np.abs(np.exp(-o32) - np.exp(-o64))
+            od_max = max(od_max, float(e.max()))
+            smax = max(smax, float(e.max()))
+            od_ss += float(np.sum(e * e))
+            od_n += e.size
+            t_max = max(t_max, float(te.max()))
+            t_ss += float(np.sum(te * te))
+            t_n += te.size
+        r64, tr64 = ctx.forward(run, abi.make_layers_like(lays))
+        r32, tr32 = ctx.forward(run, abi.make_layers_like(lays), precision=abi.PREC_SPLIT)
+        dv = lays[len(lays) - 1].dv
+        be = np.abs(gpu.brightness_temperature(r32, v1, dv) - gpu.brightness_temperature(r64, v1, dv))
+        bt_max = max(bt_max, float(be.max()))
+        bt_ss += float(np.sum(be * be))
+        bt_n += be.size
+        tt_max = max(tt_max, float(np.abs(tr32 - tr64).max()))
+        per[name] = {"od_rel_max": smax, "bt_max_K": float(be.max()),
+                     "dv_top": float(dv), "npts_top": int(len(r64))}
+    return {"config": "config2: 400,000 lines 10-3000 cm-1 (strengths 1e-28..1e-18), 60 layers, "
+                      "MT_CKD-layout continuum; 25 cm-1 slices of both sub-runs",
+            "compared": "FP32/FP64-split against plain FP64 (the FP64 path matches the FP64 "
+                        "oracle to 1e-9 on the same slices)",
+            "layer_od_rel_max": od_max, "layer_od_rel_rms": (od_ss / od_n) ** 0.5,
+            "layer_transmittance_max": t_max, "layer_transmittance_rms": (t_ss / t_n) ** 0.5,
+            "total_transmittance_max": tt_max,
+            "bt_max_K": bt_max, "bt_rms_K": (bt_ss / bt_n) ** 0.5, "slices": per}
+
+
+def config2_leg(ctx, torch):
+    """Config 2 at full size: both reference-legal sub-runs (10-1505 and
+    1505-3000 cm-1) with all 400,000 lines, FP64 and split, timed with CUDA
+    events on device buffers."""
+    from lblrtm_b200 import gpu
+    cfg = configs.config2()
+    ctx.upload_lines(abi.LinesHandle(cfg["lines"]))
+    ctx.upload_mtckd(abi.MtckdHandle(cfg["mtckd"]))
+    out = {}
+    for prec, pname in ((abi.PREC_FP64, "fp64"), (abi.PREC_SPLIT, "split")):
+        pts = 0
+        ms = 0.0
+        for v1, v2 in cfg["subruns"]:
+            run = abi.make_run(**cfg["run"], v1=v1, v2=v2)
+            lays = abi.make_layers(cfg["profile"])
+            dv, _ = gpu.dv_rule(run, lays)
+            n = gpu.layer_npts(run, dv[-1])
+            rad = torch.empty(n, dtype=torch.float64, device="cuda")
+            tr = torch.empty_like(rad)
+            ctx.forward(run, lays, precision=prec, rad=rad, tr=tr)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(2):
+                ctx.forward(run, lays, precision=prec, rad=rad, tr=tr)
+            e1.record()
+            e1.synchronize()
+            ms += e0.elapsed_time(e1) / 2
+            pts += sum(gpu.layer_npts(run, d) for d in dv)
+        out[pname] = {"ms": ms, "layer_points": pts, "layer_points_per_s": pts / (ms / 1e3)}
+    out["config"] = "config2: 60 layers, 400,000 lines, sub-runs 10-1505 and 1505-3000 cm-1"
+    return out
+
+
+def batch_leg(ctx, torch, dist, world, rank, nprof=256):
+    """Config 4: 256 perturbed profiles of 30-90 layers, 200,000 lines over
+    600-2500 cm-1, FP32/FP64-split.  The batched forward (lbl_forward_batch)
+    and the batched forward + Jacobians (lbl_adjoint_batch, the reference's
+    analytic-Jacobian definitions: d/dT and d/d ln q for H2O and O3 at every
+    layer, averaged over 1 cm-1 channels) of this rank's shard of the
+    profiles (greedy by layer points, no data-path collective), timed with
+    CUDA events, max over ranks.  The plain-FD baseline is the FP64 forward
+    per profile times (2 x 3 x layers + 1) forwards, the forward timed on a
+    sample of profiles and scaled by layer points; the brightness-
+    temperature error is split against FP64 on the same sample."""
+    from lblrtm_b200 import dist as shard_mod
+    from lblrtm_b200 import gpu
+    cfg = configs.config4(nprof=nprof)
+    run = abi.make_run(**cfg["run"])
+    profs = [abi.make_layers(p) for p in cfg["profiles"]]
+    lp = []
+    for p in profs:
+        dv, _ = gpu.dv_rule(run, abi.make_layers_like(p))
+        lp.append(sum(gpu.layer_npts(run, d) for d in dv))
+    mine = shard_mod.shard(lp, rank, world)
+    sub = [profs[i] for i in mine]
+    ctx.upload_lines(abi.LinesHandle(cfg["lines"]))
+    mols = list(cfg["jac_mols"])
+    npf = sum(gpu.layer_npts(run, gpu.dv_rule(run, abi.make_layers_like(p))[0][-1]) for p in sub)
+    rad = torch.empty(npf, dtype=torch.float64, device="cuda")
+    tr = torch.empty_like(rad)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def maxr(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up on a few profiles, then the whole shard once
+    ctx.forward_batch(run, sub[:4], precision=abi.PREC_SPLIT)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ctx.forward_batch(run, sub, precision=abi.PREC_SPLIT, rad=rad, tr=tr)
+    e1.record()
+    e1.synchronize()
+    fwd_ms = maxr(e0.elapsed_time(e1))
+    barrier()
+    nchan = int((run.v2 - run.v1) / 1.0)
+    njac = sum((1 + len(mols)) * len(p) * nchan for p in sub)
+    crad = torch.empty(len(sub) * nchan, dtype=torch.float64, device="cuda")
+    cjac = torch.empty(njac, dtype=torch.float64, device="cuda")
+    ctx.adjoint_batch(run, sub[:2], mols, mode=abi.JAC_REFERENCE, dv_chan=1.0,
+                      precision=abi.PREC_SPLIT)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ctx.adjoint_batch(run, sub, mols, mode=abi.JAC_REFERENCE, dv_chan=1.0,
+                      precision=abi.PREC_SPLIT, rad=crad, jac=cjac)
+    e1.record()
+    e1.synchronize()
+    adj_ms = maxr(e0.elapsed_time(e1))
+    barrier()
+    # plain FP64 forward on a sample (FD baseline) and the split error there
+    sample = list(range(0, nprof, max(1, nprof // 8)))[:8]
+    f64_ms, f64_pts, bt_err = 0.0, 0, 0.0
+    for i in sample:
+        p = profs[i]
+        r64, _ = ctx.forward(run, abi.make_layers_like(p))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.forward(run, abi.make_layers_like(p))
+        e1.record()
+        e1.synchronize()
+        f64_ms += e0.elapsed_time(e1)
+        f64_pts += lp[i]
+        r32 = ctx.forward_batch(run, [p], precision=abi.PREC_SPLIT)[0][0]
+        dv = gpu.dv_rule(run, abi.make_layers_like(p))[0][-1]
+        bt_err = max(bt_err, float(np.abs(gpu.brightness_temperature(r32, run.v1, dv)
+                                          - gpu.brightness_temperature(r64, run.v1, dv)).max()))
+    ms_per_pt = f64_ms / f64_pts
+    np_ = 1 + len(mols)
+    fd_ms = sum((2 * np_ * len(profs[i]) + 1) * lp[i] * ms_per_pt for i in range(nprof))
+    total_pts = sum(lp)
+    return {
+        "config": "config4: 256 profiles, 30-90 layers (seeded T and H2O perturbations), "
+                  "200,000 lines 600-2500 cm-1, fp32/fp64-split",
+        "profiles": nprof, "layers_total": sum(len(p) for p in profs),
+        "layer_points_total": int(total_pts),
+        "shard": f"{len(mine)} profiles on rank 0 of {world} (greedy by layer points)",
+        "forward_ms": fwd_ms, "forward_layer_points_per_s": total_pts / (fwd_ms / 1e3),
+        "adjoint_ms": adj_ms, "jacobian_sets_per_s": nprof / (adj_ms / 1e3),
+        "jacobian_rows": np_ * sum(len(p) for p in profs),
+        "adjoint_mode": "LBL_JAC_REFERENCE (T + 1 K pass, one pass per molecule alone; "
+                        "TDERIVup/QDERIVup rows), 1 cm-1 channel means",
+        "fd_forwards_per_profile": f"2 x {np_} x layers + 1",
+        "fd_ms_estimate": fd_ms, "speedup_vs_fd": fd_ms / adj_ms,
+        "fd_basis": f"plain FP64 lbl_forward timed on {len(sample)} profiles, "
+                    f"{ms_per_pt * 1e6:.3f} ms per 1e6 layer points",
+        "bt_err_split_vs_fp64_max_K": bt_err,
+        "timing": "CUDA events around one call over the shard (host planning included), "
+                  "max over ranks",
+    }
+
+
 def gpu_arm(a):
     import torch
     from lblrtm_b200 import gpu
@@ -350,6 +572,9 @@ def gpu_arm(a):
         "achieved": pn_gbs, "peak": hbm_peak, "unit": "GB/s",
         "frac": (pn_gbs / hbm_peak) if pn_gbs else None,
         "traffic": traffic_db.get("k_panel_od"),
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                          "from an earlier capture recorded in profiles/traffic_config1.json "
+                          "(not measured in this run)",
         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650",
         "work": f"{pn_bytes:.4g} B of optical depth written per launch (8 B x layer points)",
         "launch_ms": pn_ms,
@@ -394,12 +619,20 @@ def gpu_arm(a):
     jleg = None
     if not a.no_jacobian:
         jleg = jacobian_leg(ctx, prec, torch)
+    bleg = None
+    if not a.no_batch:
+        bleg = batch_leg(ctx, torch, dist, world, rank, nprof=a.batch_profiles)
+    pleg = c2leg = None
+    if not a.no_precision:
+        pleg = precision_leg(ctx)
+        c2leg = config2_leg(ctx, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         workers = a.cpu_workers or default_workers()
         r = cpu_run(a.nlines, workers, reps=1)[0]
         cpu = {"value": r[0] / r[1], "unit": UNIT, "cores": workers, "kind": "port",
+               "cpu": cpu_model(),
                "sample": f"{workers} concurrent config-1 forwards (restated reference, "
                          f"C++ FP64 oracle), wall {r[1]:.1f} s"}
 
@@ -410,8 +643,7 @@ def gpu_arm(a):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == abi.PREC_FP64 else "f32/f64",
             "data": "synthetic (seeded lines and atmosphere)",
-            "config": {"workload": "config1: 60 layers, 4 absorbers, 50,000 lines, "
-                                   "500-1500 cm-1, upwelling TOA radiance",
+            "config": {"workload": WORKLOAD.format(nlines=a.nlines),
                        "nlines": a.nlines, "layers": len(layers),
                        "layer_points_per_step": pts, "precision": a.precision,
                        "l2": "256 MB buffer written between timed steps",
@@ -423,6 +655,9 @@ def gpu_arm(a):
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "jacobian": jleg,
+            "batch": bleg,
+            "precision": pleg,
+            "config2": c2leg,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -201,6 +201,9 @@ struct lbl_ctx {
   cudaEvent_t stage_ev = nullptr;
   bool stage_ev_set = false;
   bool have_lines = false;
+  // fused panel kernel variant chosen by the autotuner (-1: not yet tuned)
+  int panel_variant = -1;
+  float tune_ms[kPanelVariants] = {};
   // tables
   DevShapes sh{};
   void* shape_mem = nullptr;
@@ -385,7 +388,8 @@ size_t layer_arena_bytes(const LayerDev& d) {
   const size_t nabs = (size_t)(d.icntnm ? d.nptabs : 0) + 8;
   return sizeof(LayerDev) + 64 + npanel * (8 + 4 + 4 + 16 + 8 * 3 * kPanelSegMax + 4) +
          nwin * (sizeof(WinDev) + 8 + 8 * kR4Stride) + nfar * 83 + 16 * (nfar / 1000 + 2) +
-         nnear * 117 + 8 * nblk + 8 * nabs + 8 * (size_t)d.npts + (8 * kSegMaxBlk + 16) * nfblk;
+         nnear * (117 + sizeof(NearRec) + 8) + 16 * nblk + 8 * nabs + 8 * (size_t)d.npts +
+         (8 * kSegMaxBlk + 16) * nfblk;
 }
 
 int upload_batch(lbl_ctx* ctx, Batch& B);
@@ -481,6 +485,12 @@ int upload_batch(lbl_ctx* ctx, Batch& B) {
   lay.add<int8_t>(o_near + 1);
   lay.add<NearPre>(o_near + 1);
   lay.add<int2>(o_nblk + 1);
+  lay.add<NearRec>(o_near + 1);
+  lay.add<double>(o_near + 1);
+  lay.add<int32_t>(o_nblk + 1);
+  lay.add<int32_t>(o_nblk + 1);
+  lay.add<int32_t>(n);
+  lay.add<int32_t>(n);
   lay.add<double>(o_abs);
   lay.add<double>(o_od);
   lay.add<int64_t>(2 * o_pan + 2);
@@ -539,6 +549,12 @@ int upload_batch(lbl_ctx* ctx, Batch& B) {
   w.n_ok = A.take<int8_t>(o_near + 1);
   w.n_pre = A.take<NearPre>(o_near + 1);
   w.n_blk = A.take<int2>(o_nblk + 1);
+  w.n_rec = A.take<NearRec>(o_near + 1);
+  w.n_rvnu = A.take<double>(o_near + 1);
+  w.n_bcnt = A.take<int32_t>(o_nblk + 1);
+  w.n_boff = A.take<int32_t>(o_nblk + 1);
+  w.n_cnt = A.take<int32_t>(n);
+  w.n_hw3 = A.take<int32_t>(n);
   w.absrb = A.take<double>(o_abs);
   w.od = A.take<double>(o_od);
   B.d_panel_rng = A.take<int64_t>(2 * o_pan + 2);
@@ -634,6 +650,48 @@ int ensure_copy_stream(lbl_ctx* ctx) {
 
 int finish_od(lbl_ctx* ctx);
 
+// The autotuner: on the context's first batch of at least kTuneMinPanels
+// panels, every variant of the fused panel kernel (records staged per
+// batch) runs once on that batch, timed by CUDA events on the context's
+// stream, and the fastest is kept for the context's later calls.  Every
+// variant writes the same optical depths (each point sums its lines in file
+// order), so the batch's result does not depend on which ran last.  The
+// variant can be fixed by the environment variable LBL_PANEL_VARIANT (0-2).
+constexpr int64_t kTuneMinPanels = 4096;
+int tune_panels(lbl_ctx* ctx, Batch& B, int precision) {
+  cudaStream_t s = ctx->stream;
+  if (const char* e = std::getenv("LBL_PANEL_VARIANT")) {
+    const int v = std::atoi(e);
+    if (v >= 0 && v < kPanelVariants) {
+      ctx->panel_variant = v;
+      return LBL_OK;
+    }
+  }
+  cudaEvent_t ev[kPanelVariants + 1];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  CK(cudaEventRecord(ev[0], s));
+  for (int v = 0; v < kPanelVariants; v++) {
+    CK(launch_panels(B.w, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
+                     B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, precision, v, s));
+    CK(cudaEventRecord(ev[v + 1], s));
+  }
+  CK(cudaEventSynchronize(ev[kPanelVariants]));
+  int best = 1;
+  float best_ms = 1e30f;
+  for (int v = 0; v < kPanelVariants; v++) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev[v], ev[v + 1]));
+    ctx->tune_ms[v] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  ctx->panel_variant = best;
+  return LBL_OK;
+}
+
 // A pinned host buffer of at least `bytes` for a table about to be copied
 // to the device; the caller records ctx->small_ev after its copy.
 int small_pinned(lbl_ctx* ctx, size_t bytes, void** out) {
@@ -686,8 +744,8 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   CK(cudaStreamWaitEvent(s2, ctx->cev[0], 0));
   CK(launch_near_lines(w, ctx->dl, max_near, s2));
   if (R.icntnm) CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, s2));
-  CK(launch_panel_prep(w, ctx->dl, B.npanel_total, B.d_panel_layer, B.d_panel_base,
-                       B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s2));
+  CK(launch_panel_segs(w, B.npanel_total, B.d_panel_layer, B.d_panel_base, B.d_panel_segs,
+                       B.d_panel_nseg, s2));
   CK(cudaEventRecord(ctx->cev[1], s2));
   {
     StageTimer t(ctx, "shrink", 3);
@@ -700,14 +758,21 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   CK(cudaStreamWaitEvent(s, ctx->cev[1], 0));
   {
     // the walk and the window limits; the per-line part ran on the second stream
-    StageTimer t(ctx, "near_scale", 3 + (R.icntnm ? 1 : 0) + 2);
+    StageTimer t(ctx, "near_scale", 3 + (R.icntnm ? 1 : 0) + 2 + 3);
     CK(launch_near_walk(w, ctx->dl, max_panel, max_win, max_nblk, s));
+    // accepted lines packed per layer, every panel's candidate records
+    CK(launch_near_pack(w, ctx->dl, max_nblk, B.npanel_total, B.d_panel_layer, B.d_panel_base,
+                        B.d_panel_rng, s));
+  }
+  if (ctx->panel_variant < 0 && B.npanel_total >= kTuneMinPanels) {
+    const int rc3 = tune_panels(ctx, B, precision);
+    if (rc3) return rc3;
   }
   {
     // near-wing sums, PANEL combination and optical depth in one pass
     StageTimer t(ctx, "panels", 1);
-    CK(launch_panels(w, ctx->dl, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
-                     B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, s));
+    CK(launch_panels(w, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base, B.d_panel_rng,
+                     B.d_panel_segs, B.d_panel_nseg, precision, ctx->panel_variant, s));
   }
   if (ctx->nslot >= lbl_ctx::kStatSlots) {
     // every slot holds a pass not yet read: drain them
@@ -1357,7 +1422,8 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
   build_shape_tables(t);
   const size_t nd = kNfmx + 1;
   char* mem = nullptr;
-  if (cudaMalloc(&mem, 9 * nd * sizeof(double) + 1024) != cudaSuccess) {
+  // FP64 tables, the packed R1 records, and their FP32 copies
+  if (cudaMalloc(&mem, 13 * nd * sizeof(double) + 4096) != cudaSuccess) {
     delete t;
     delete ctx;
     return LBL_E_NOMEM;
@@ -1375,8 +1441,21 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
     rec[4 * i + 2] = t->xver[i];
   }
   cudaMemcpy(pk, rec.data(), 4 * nd * sizeof(double), cudaMemcpyHostToDevice);
+  // FP32: F1, FG, XVER, 0 per index (16-byte records), then F2 and F3
+  float* fk = reinterpret_cast<float*>(pk + 4 * nd);
+  std::vector<float> rec32(4 * nd, 0.f), f23(2 * nd);
+  for (size_t i = 0; i < nd; i++) {
+    rec32[4 * i] = (float)t->f1[i];
+    rec32[4 * i + 1] = (float)t->fg[i];
+    rec32[4 * i + 2] = (float)t->xver[i];
+    f23[i] = (float)t->f2[i];
+    f23[nd + i] = (float)t->f3[i];
+  }
+  cudaMemcpy(fk, rec32.data(), 4 * nd * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(fk + 4 * nd, f23.data(), 2 * nd * sizeof(float), cudaMemcpyHostToDevice);
   delete t;
-  ctx->sh = DevShapes{dd, dd + nd, dd + 2 * nd, dd + 3 * nd, dd + 4 * nd, pk};
+  ctx->sh = DevShapes{dd, dd + nd, dd + 2 * nd, dd + 3 * nd, dd + 4 * nd, pk,
+                      reinterpret_cast<const float4*>(fk), fk + 4 * nd, fk + 5 * nd};
   if (cudaGetLastError() != cudaSuccess) {
     lbl_ctx_destroy(ctx);
     return LBL_E_CUDA;

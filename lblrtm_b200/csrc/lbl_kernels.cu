@@ -1408,6 +1408,90 @@ __global__ void __launch_bounds__(256) k_near_out(Work w, DevLines ln) {
   // would serialise the kernel)
   const unsigned wsum = __reduce_add_sync(0xffffffffu, ntrip);
   if ((tid & 31) == 0 && wsum) atomicAdd(&w.counters[1], (unsigned long long)wsum);
+  // accepted lines of this TAPE3 panel, for the packing of the layer's list
+  const int nacc = __syncthreads_count(ok ? 1 : 0);
+  if (tid == 0) w.n_bcnt[L.off_nblk + bi] = nacc;
+}
+
+// Exclusive scan of the accepted-line counts over each layer's TAPE3 panels
+// (one warp per layer): where each panel's accepted lines start in the
+// layer's packed list, and the layer's total.
+__global__ void __launch_bounds__(32) k_near_scan(Work w) {
+  const int l = blockIdx.x;
+  const int lane = threadIdx.x;
+  const LayerDev& L = w.L[l];
+  const int nb = (int)(L.blk_hi - L.blk_lo);
+  int run = 0;
+  for (int b0 = 0; b0 < nb; b0 += 32) {
+    const int b = b0 + lane;
+    const int c = b < nb ? w.n_bcnt[L.off_nblk + b] : 0;
+    int x = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += t;
+    }
+    if (b < nb) w.n_boff[L.off_nblk + b] = run + x - c;
+    run += __shfl_sync(0xffffffffu, x, 31);
+  }
+  if (lane == 0) {
+    w.n_cnt[l] = run;
+    w.n_hw3[l] = 0;
+  }
+}
+
+// Pack the accepted near-wing lines of one TAPE3 panel of one layer into
+// NearRec records at their rank in the layer's list (file order), with the
+// windows on the three global grids (the convolution panel's windows shifted
+// by 2400/600/150 points per panel), and raise the layer's widest R3
+// half-window about the line centre.
+__global__ void __launch_bounds__(256) k_near_pack(Work w, DevLines ln) {
+  __shared__ int s_wc[8];
+  const int l = blockIdx.y;
+  const LayerDev& L = w.L[l];
+  const int64_t bi = blockIdx.x;
+  if (bi >= L.blk_hi - L.blk_lo) return;
+  const int64_t b = L.blk_lo + bi;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t a = ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo;
+  const int64_t e = ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi;
+  const int64_t i = a + tid;
+  const int64_t slot = (i - L.near_lo) + L.off_near;
+  const bool ok = i < e && w.n_ok[slot];
+  const unsigned m = __ballot_sync(0xffffffffu, ok);
+  if (lane == 0) s_wc[warp] = __popc(m);
+  __syncthreads();
+  if (!ok) return;
+  int rank = w.n_boff[L.off_nblk + bi] + __popc(m & ((1u << lane) - 1u));
+  for (int k = 0; k < warp; k++) rank += s_wc[k];
+  const int32_t pc = w.n_pconv[slot];
+  const int32_t j1a = w.n_jmin1[slot], j1b = w.n_jmax1[slot];
+  const int32_t j2 = w.n_j2[slot], j3 = w.n_j3[slot];
+  const double* sv = w.n_str + 5 * slot;
+  NearRec r;
+  r.zint = w.n_zint[slot];
+  r.zslope = w.n_zslope[slot];
+  r.sppsp = w.n_sppsp[slot];
+  r.s0 = sv[0];
+  r.s2 = sv[1];
+  r.s3 = sv[2];
+  r.sg = sv[3];
+  r.sx = sv[4];
+  r.lo1 = j1a + 2400 * pc;
+  r.hi1 = j1b + 2400 * pc;
+  r.lo2 = j1a - j2 + 600 * pc;
+  r.hi2 = j1b - j2 + 600 * pc;
+  r.lo3 = j1a - j3 + 150 * pc;
+  r.hi3 = j1b - j3 + 150 * pc;
+  r.pc = pc;
+  r.pad = 0;
+  w.n_rec[L.off_near + rank] = r;
+  const double v = ln.vnu[i];
+  w.n_rvnu[L.off_near + rank] = v;
+  // R3 point of the TAPE3 centre (global index g: VFT0 + (g-1) DVR3)
+  const double c3 = (v - L.vft0) / L.dvr3 + 1.;
+  const double hw = fmax(c3 - double(r.lo3), double(r.hi3) - c3);
+  atomicMax(&w.n_hw3[l], (int)ceil(hw));
 }
 
 __device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double x) {
@@ -1614,30 +1698,22 @@ __device__ void rsym(double* R, double dv, double vft) {
   }
 }
 
-// Candidate near-wing lines of every panel: TAPE3 lines whose centre lies
-// within the widest (R3) window reach of the panel's R3 span.
-__global__ void k_panel_ranges(Work w, DevLines ln, const int32_t* panel_layer,
-                               const int64_t* panel_base, int64_t npanel_total, int64_t* rng) {
+// Candidate records of every panel: the layer's packed accepted lines whose
+// centre lies within the layer's widest R3 half-window (+2 points) of the
+// panel's R3 span; as ranks into the layer's packed list.
+__global__ void k_panel_ranges(Work w, const int32_t* panel_layer, const int64_t* panel_base,
+                               int64_t npanel_total, int64_t* rng) {
   const int64_t gp = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (gp >= npanel_total) return;
   const int l = panel_layer[gp];
   const LayerDev& L = w.L[l];
   const PanelRange R = panel_range(L, (int32_t)(gp - panel_base[l]));
-  const double reach = 64. * L.alfmax + 32. * L.dv + fabs(L.rhorat) * 1.0;
-  rng[2 * gp] = lower_bound_d(ln.vnu, L.near_lo, L.near_hi,
-                              L.vft0 + double(R.a3 - 1) * L.dvr3 - reach);
-  rng[2 * gp + 1] = lower_bound_d(ln.vnu, L.near_lo, L.near_hi,
-                                  L.vft0 + double(R.b3 - 1) * L.dvr3 + reach);
+  const double reach = double(w.n_hw3[l] + 2) * L.dvr3;
+  const double* v = w.n_rvnu + L.off_near;
+  const int64_t n = w.n_cnt[l];
+  rng[2 * gp] = lower_bound_d(v, 0, n, L.vft0 + double(R.a3 - 1) * L.dvr3 - reach);
+  rng[2 * gp + 1] = lower_bound_d(v, 0, n, L.vft0 + double(R.b3 - 1) * L.dvr3 + reach);
 }
-
-// A staged near-wing line: its windows on the three grids (global points)
-// and the constants of CNVFNV's three sums (src/oprop.f90:1283-1351).
-struct PanelLine {
-  double zint, zslope, sppsp, s0, sg, sx, s2, s3;
-  int32_t lo1, hi1, lo2, hi2, lo3, hi3;
-  int32_t pc;  // convolution panel of the line
-  uint32_t wm; // warps owning points of its R1 (bits 0-7), R2 (8-15), R3 (16-23) windows
-};
 
 // Warps of a 256-thread CTA whose threads own local points of [lo, hi]
 // (clipped to [0, n)), thread t owning the points i with i mod 256 == t.
@@ -1652,11 +1728,118 @@ __device__ __forceinline__ uint32_t warps_of(int lo, int hi, int n) {
 }
 
 constexpr int kPanelThreads = 256;
-constexpr int kPanelStage = 128;  // lines staged per batch
-constexpr int kP1 = 10;           // R1 points per thread (2560 >= 2400)
-constexpr int kP2 = 3;            // R2 points per thread (768 >= 603)
+constexpr int kP1 = 10;           // R1 points per thread (2560 >= 2433)
+constexpr int kP2 = 3;            // R2 points per thread (768 >= 611)
 constexpr int kSegMax = kPanelSegMax;  // RADFNI segments kept per panel
 constexpr int kSegCap = 64;       // segments a CTA builds at a time when a panel has more
+
+// ---- bulk copies into shared memory, completed on an mbarrier -------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+// make the initialised barriers visible to the asynchronous proxy
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// order this thread's (and, after a CTA barrier, the CTA's) generic-proxy
+// accesses of shared memory before later asynchronous-proxy writes
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// global -> shared bulk copy (no multicast); bytes a multiple of 16, both
+// addresses 16-byte aligned
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `parity` of a barrier, giving up after about a second.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  for (int it = 0; it < (1 << 24); it++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it > 16) __nanosleep(64);
+  }
+  return false;
+}
+
+// Kahan-compensated FP32 accumulation of one grid point (sum, compensation).
+__device__ __forceinline__ void kahan_add(float2& a, float v) {
+  const float y = v - a.y;
+  const float t = a.x + y;
+  a.y = (t - a.x) - y;
+  a.x = t;
+}
+
+// Adds line q's contributions to the points this thread owns on one grid:
+// local points [lo, hi] of the panel's span (thread tid owns tid + 256 k);
+// `off` maps a local point to the line's panel coordinate.  T = double:
+// FP64 sums; T = float: the table index from the same FP64 position, the
+// line shape in FP32 and a Kahan-compensated FP32 sum.
+template <typename T, int GRID>
+__device__ __forceinline__ void near_add(const NearRec& q, const DevShapes& sh, int tid, int lo,
+                                         int hi, int off, double zc, double* acc) {
+  int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
+  const double cf = GRID == 1 ? 4. / 2000. : (GRID == 2 ? 16. / 2000. : 64. / 2000.);
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll 2
+    for (; i <= hi; i += kPanelThreads) {
+      const double zf = (double(off + i) - zc) * q.zslope;
+      int iz = (int)(fabs(zf) + 1.5);
+      iz = iz > kNfmx ? kNfmx : iz;
+      double v;
+      if (GRID == 1) {
+        const double2 fab = *reinterpret_cast<const double2*>(sh.r1p + 4 * iz);
+        v = q.s0 * fab.x + q.sg * fab.y + q.sx * sh.r1p[4 * iz + 2];
+      } else {
+        v = (GRID == 2 ? q.s2 * sh.f2[iz] : q.s3 * sh.f3[iz]);
+      }
+      if (q.sppsp != 0.) v = v + v * (cf * q.sppsp * zf);  // (:1322-1351)
+      acc[i] += v;
+    }
+  } else {
+    float2* a2 = reinterpret_cast<float2*>(acc);
+    const float s0 = (float)q.s0, sg = (float)q.sg, sx = (float)q.sx;
+    const float s23 = (float)(GRID == 2 ? q.s2 : q.s3);
+    const float cs = (float)(cf * q.sppsp);
+#pragma unroll 2
+    for (; i <= hi; i += kPanelThreads) {
+      const double zf = (double(off + i) - zc) * q.zslope;
+      int iz = (int)(fabs(zf) + 1.5);
+      iz = iz > kNfmx ? kNfmx : iz;
+      float v;
+      if (GRID == 1) {
+        const float4 t = sh.r1p32[iz];
+        v = s0 * t.x + sg * t.y + sx * t.z;
+      } else {
+        v = s23 * (GRID == 2 ? sh.f2_32[iz] : sh.f3_32[iz]);
+      }
+      if (cs != 0.f) v = v + v * (cs * (float)zf);
+      kahan_add(a2[i], v);
+    }
+  }
+}
 
 // RADFNI segments of every panel (restarted each panel, src/oprop.f90:
 // 2297-2475), one thread per panel: [start point, value, slope] each; a
@@ -1701,135 +1884,124 @@ __global__ void k_panel_segs(Work w, const int32_t* panel_layer, const int64_t* 
 // gets the far wing and continuum by XINT (:515-519) and feeds R2 by
 // 4-point interpolation, and the optical depth R1 + interpolated R2, times
 // the radiation term, is written out.  The three grids never leave the SM.
-__global__ void __launch_bounds__(kPanelThreads, 4)
-    k_panel_od(Work w, DevLines ln, DevShapes sh, const int32_t* panel_layer,
-               const int64_t* panel_base, const int64_t* rng, const double* segs,
-               const int32_t* nseg) {
+//
+// The panel's candidate lines (packed 96-byte records of the layer's
+// accepted lines, in file order) arrive in batches of STAGE by bulk copies
+// into a two-buffer ring: batch b+1 is in flight while the warps add batch
+// b.  Each warp adds a record to the points it owns only where the
+// record's window reaches them.
+template <typename T, int STAGE, int MINB>
+__global__ void __launch_bounds__(kPanelThreads, MINB)
+    k_panel_od(Work w, DevShapes sh, const int32_t* panel_layer, const int64_t* panel_base,
+               const int64_t* rng, const double* segs, const int32_t* nseg) {
   const int64_t gp = blockIdx.x;
   const int l = panel_layer[gp];
   const LayerDev& L = w.L[l];
   const int32_t p = (int32_t)(gp - panel_base[l]);
   const PanelRange R = panel_range(L, p);
   const int32_t n_r2 = (int32_t)L.n_r2;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const unsigned full = 0xffffffffu;
-  __shared__ PanelLine st[kPanelStage];
-  __shared__ int s_wcnt[kPanelThreads / 32];
-  __shared__ double s1[kP1 * kPanelThreads];
-  __shared__ double s2[kP2 * kPanelThreads];
-  __shared__ double s3[kPanelThreads];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  __shared__ __align__(128) NearRec st[2][STAGE];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(16) double s1[kP1 * kPanelThreads];
+  __shared__ __align__(16) double s2[kP2 * kPanelThreads];
+  __shared__ __align__(16) double s3[kPanelThreads];
   __shared__ double seg[3 * kSegCap];  // [start, radvi, rdel] per segment
   __shared__ int s_nseg;
   __shared__ long s_n2;
-  // each thread owns local points tid + 256 q of every grid
   const int n1p = (int)(R.b1 - R.a1 + 1), n2p = (int)(R.b2 - R.a2 + 1),
             n3p = (int)(R.b3 - R.a3 + 1);
+  const int64_t clo = rng[2 * gp], chi = rng[2 * gp + 1];
+  const NearRec* src = w.n_rec + L.off_near;
+  const int nbatch = (int)((chi - clo + STAGE - 1) / STAGE);
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  auto issue = [&](int b) {  // thread 0: batch b into buffer b & 1
+    const int64_t c0 = clo + (int64_t)b * STAGE;
+    const int n = (int)((chi - c0) < STAGE ? (chi - c0) : STAGE);
+    const unsigned bytes = (unsigned)n * (unsigned)sizeof(NearRec);
+    mbar_expect_tx(&bar[b & 1], bytes);
+    bulk_g2s(st[b & 1], src + c0, bytes, &bar[b & 1]);
+  };
+  if (tid == 0 && nbatch > 0) issue(0);
+  // the grids start at zero (FP32: sum and compensation pairs)
   for (int i = tid; i < kP1 * kPanelThreads; i += kPanelThreads) s1[i] = 0.;
   for (int i = tid; i < kP2 * kPanelThreads; i += kPanelThreads) s2[i] = 0.;
   s3[tid] = 0.;
-  const int64_t clo = rng[2 * gp], chi = rng[2 * gp + 1];
-  for (int64_t c0 = clo; c0 < chi; c0 += kPanelStage) {
-    // stage the batch's accepted lines in file order
-    bool keep = false;
-    PanelLine q;
-    if (tid < kPanelStage && c0 + tid < chi) {
-      const int64_t slot = L.off_near + (c0 + tid - L.near_lo);
-      if (w.n_ok[slot]) {
-        const double* sv = w.n_str + 5 * slot;
-        const int32_t pc = w.n_pconv[slot];
-        const int32_t j1a = w.n_jmin1[slot], j1b = w.n_jmax1[slot];
-        const int32_t j2 = w.n_j2[slot], j3 = w.n_j3[slot];
-        q.zint = w.n_zint[slot];
-        q.zslope = w.n_zslope[slot];
-        q.sppsp = w.n_sppsp[slot];
-        q.s0 = sv[0];
-        q.s2 = sv[1];
-        q.s3 = sv[2];
-        q.sg = sv[3];
-        q.sx = sv[4];
-        q.pc = pc;
-        // panel-local windows shifted to the global grids by the line's panel
-        q.lo1 = j1a + 2400 * pc;
-        q.hi1 = j1b + 2400 * pc;
-        q.lo2 = j1a - j2 + 600 * pc;
-        q.hi2 = j1b - j2 + 600 * pc;
-        q.lo3 = j1a - j3 + 150 * pc;
-        q.hi3 = j1b - j3 + 150 * pc;
-        q.wm = warps_of(q.lo1 - R.a1, q.hi1 - R.a1, n1p) |
-               (warps_of(q.lo2 - R.a2, q.hi2 - R.a2, n2p) << 8) |
-               (warps_of(q.lo3 - R.a3, q.hi3 - R.a3, n3p) << 16);
-        keep = (q.hi1 >= R.a1 && q.lo1 <= R.b1) || (q.hi2 >= R.a2 && q.lo2 <= R.b2) ||
-               (q.hi3 >= R.a3 && q.lo3 <= R.b3);
-      }
+  int lost = -1;  // batch whose copy did not complete
+  for (int b = 0; b < nbatch; b++) {
+    // buffer (b+1)&1 was last read in batch b-1, which every thread has
+    // finished (barrier at the end of that batch)
+    if (tid == 0 && b + 1 < nbatch) {
+      fence_proxy_async_smem();
+      issue(b + 1);
     }
-    const unsigned bal = __ballot_sync(full, keep);
-    if (lane == 0) s_wcnt[warp] = __popc(bal);
-    __syncthreads();
-    int base = 0, n = 0;
-#pragma unroll
-    for (int k = 0; k < kPanelThreads / 32; k++) {
-      base += k < warp ? s_wcnt[k] : 0;
-      n += s_wcnt[k];
+    if (!mbar_wait_bounded(&bar[b & 1], (unsigned)((b >> 1) & 1))) {
+      lost = b;
+      break;
     }
-    if (keep) st[base + __popc(bal & ((1u << lane) - 1u))] = q;
-    __syncthreads();
+    const int64_t c0 = clo + (int64_t)b * STAGE;
+    const int n = (int)((chi - c0) < STAGE ? (chi - c0) : STAGE);
+    const NearRec* batch = st[b & 1];
     for (int k = 0; k < n; k++) {
-      const PanelLine& ql = st[k];
-      // a warp owning none of the line's window points skips it
-      const uint32_t wm = ql.wm >> warp;
-      if (!(wm & 0x10101u)) continue;
+      const NearRec& q = batch[k];
       // R1 (DV grid): F1 + FG + VERFN terms
-      if ((wm & 1u) && ql.hi1 >= R.a1 && ql.lo1 <= R.b1) {
-        const int lo = (ql.lo1 > R.a1 ? ql.lo1 : R.a1) - R.a1;
-        const int hi = (ql.hi1 < R.b1 ? ql.hi1 : R.b1) - R.a1;
-        const int off = R.a1 - 2400 * ql.pc - 1;  // g - pofs - 1 at i = 0
-        int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
-#pragma unroll 2
-        for (; i <= hi; i += kPanelThreads) {
-          const double zf = (double(off + i) - ql.zint) * ql.zslope;
-          int iz = (int)(fabs(zf) + 1.5);
-          iz = iz > kNfmx ? kNfmx : iz;
-          const double2 fab = *reinterpret_cast<const double2*>(sh.r1p + 4 * iz);
-          double v = ql.s0 * fab.x + ql.sg * fab.y + ql.sx * sh.r1p[4 * iz + 2];
-          if (ql.sppsp != 0.) v = v + v * (4. / 2000. * ql.sppsp * zf);  // (:1322-1351)
-          s1[i] += v;
-        }
+      if (q.hi1 >= R.a1 && q.lo1 <= R.b1) {
+        const int lo = (q.lo1 > R.a1 ? q.lo1 : R.a1) - R.a1;
+        const int hi = (q.hi1 < R.b1 ? q.hi1 : R.b1) - R.a1;
+        if ((warps_of(lo, hi, n1p) >> warp) & 1u)
+          near_add<T, 1>(q, sh, tid, lo, hi, R.a1 - 2400 * q.pc - 1, q.zint, s1);
       }
       // R2 (4 DV): F2
-      if ((wm & 0x100u) && ql.hi2 >= R.a2 && ql.lo2 <= R.b2) {
-        const int lo = (ql.lo2 > R.a2 ? ql.lo2 : R.a2) - R.a2;
-        const int hi = (ql.hi2 < R.b2 ? ql.hi2 : R.b2) - R.a2;
-        const int off = R.a2 - 600 * ql.pc - 1;
-        int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
-        for (; i <= hi; i += kPanelThreads) {
-          const double zf = (double(off + i) - ql.zint * L.conf2) * ql.zslope;
-          int iz = (int)(fabs(zf) + 1.5);
-          iz = iz > kNfmx ? kNfmx : iz;
-          double v = ql.s2 * sh.f2[iz];
-          if (ql.sppsp != 0.) v = v + v * (16. / 2000. * ql.sppsp * zf);
-          s2[i] += v;
-        }
+      if (q.hi2 >= R.a2 && q.lo2 <= R.b2) {
+        const int lo = (q.lo2 > R.a2 ? q.lo2 : R.a2) - R.a2;
+        const int hi = (q.hi2 < R.b2 ? q.hi2 : R.b2) - R.a2;
+        if ((warps_of(lo, hi, n2p) >> warp) & 1u)
+          near_add<T, 2>(q, sh, tid, lo, hi, R.a2 - 600 * q.pc - 1, q.zint * L.conf2, s2);
       }
       // R3 (16 DV): F3
-      if ((wm & 0x10000u) && ql.hi3 >= R.a3 && ql.lo3 <= R.b3) {
-        const int lo = (ql.lo3 > R.a3 ? ql.lo3 : R.a3) - R.a3;
-        const int hi = (ql.hi3 < R.b3 ? ql.hi3 : R.b3) - R.a3;
-        if (tid >= lo && tid <= hi) {
-          const int off = R.a3 - 150 * ql.pc - 1;
-          const double zf = (double(off + tid) - ql.zint * L.conf3) * ql.zslope;
-          int iz = (int)(fabs(zf) + 1.5);
-          iz = iz > kNfmx ? kNfmx : iz;
-          double v = ql.s3 * sh.f3[iz];
-          if (ql.sppsp != 0.) v = v + v * (64. / 2000. * ql.sppsp * zf);
-          s3[tid] += v;
-        }
+      if (q.hi3 >= R.a3 && q.lo3 <= R.b3) {
+        const int lo = (q.lo3 > R.a3 ? q.lo3 : R.a3) - R.a3;
+        const int hi = (q.hi3 < R.b3 ? q.hi3 : R.b3) - R.a3;
+        if ((warps_of(lo, hi, n3p) >> warp) & 1u)
+          near_add<T, 3>(q, sh, tid, lo, hi, R.a3 - 150 * q.pc - 1, q.zint * L.conf3, s3);
       }
+    }
+    __syncthreads();
+  }
+  if (lost >= 0) {
+    // a bulk copy did not complete: flag it, give the copies in flight
+    // (that batch and the next) another bounded wait, and leave the panel
+    // unwritten
+    if (tid == 0) atomicExch(&w.status[0], 4);
+    mbar_wait_bounded(&bar[lost & 1], (unsigned)((lost >> 1) & 1));
+    if (lost + 1 < nbatch) mbar_wait_bounded(&bar[(lost + 1) & 1], (unsigned)(((lost + 1) >> 1) & 1));
+    return;
+  }
+  if constexpr (sizeof(T) == 4) {
+    // compensated FP32 sums to FP64, each thread its own points in place
+    for (int i = tid; i < kP1 * kPanelThreads; i += kPanelThreads) {
+      const float2 a = reinterpret_cast<const float2*>(s1)[i];
+      s1[i] = (double)a.x - (double)a.y;
+    }
+    for (int i = tid; i < kP2 * kPanelThreads; i += kPanelThreads) {
+      const float2 a = reinterpret_cast<const float2*>(s2)[i];
+      s2[i] = (double)a.x - (double)a.y;
+    }
+    {
+      const float2 a = reinterpret_cast<const float2*>(s3)[tid];
+      s3[tid] = (double)a.x - (double)a.y;
     }
     __syncthreads();
   }
   // RSYM on the three grids of a first panel starting at or below zero
   // (HIRAC1 :501-505), before the far wing and continuum are added
   if (R.a1 == 0) {
+    __syncthreads();  // the grids are complete (also when no line reached the panel)
     if (tid == 0) {
       const double vft = w.vft[L.off_panel];
       rsym(s1, L.dv, vft);
@@ -2381,8 +2553,16 @@ void init_kernel_attributes() {
   cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem32);
   cudaFuncSetAttribute(k_near_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kNearWalkSmemMax);
-  cudaFuncSetAttribute(k_panel_od, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
+  {
+    const cudaFuncAttribute c = cudaFuncAttributePreferredSharedMemoryCarveout;
+    const int mx = cudaSharedmemCarveoutMaxShared;
+    cudaFuncSetAttribute(k_panel_od<double, 32, 4>, c, mx);
+    cudaFuncSetAttribute(k_panel_od<double, 64, 4>, c, mx);
+    cudaFuncSetAttribute(k_panel_od<double, 32, 5>, c, mx);
+    cudaFuncSetAttribute(k_panel_od<float, 32, 4>, c, mx);
+    cudaFuncSetAttribute(k_panel_od<float, 64, 4>, c, mx);
+    cudaFuncSetAttribute(k_panel_od<float, 32, 5>, c, mx);
+  }
   cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
                        cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -2456,24 +2636,60 @@ cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, do
 }
 
 
-cudaError_t launch_panel_prep(const Work& w, const DevLines& ln, int64_t npanel_total,
-                              const int32_t* panel_layer, const int64_t* panel_base, int64_t* rng,
-                              double* segs, int32_t* nseg, cudaStream_t s) {
+cudaError_t launch_panel_segs(const Work& w, int64_t npanel_total, const int32_t* panel_layer,
+                              const int64_t* panel_base, double* segs, int32_t* nseg,
+                              cudaStream_t s) {
   if (npanel_total <= 0) return cudaSuccess;
   const unsigned nb = (unsigned)((npanel_total + 127) / 128);
-  k_panel_ranges<<<nb, 128, 0, s>>>(w, ln, panel_layer, panel_base, npanel_total, rng);
   k_panel_segs<<<nb, 128, 0, s>>>(w, panel_layer, panel_base, npanel_total, segs, nseg);
   return cudaGetLastError();
 }
 
-cudaError_t launch_panels(const Work& w, const DevLines& ln, const DevShapes& sh,
-                          int64_t npanel_total, const int32_t* panel_layer,
-                          const int64_t* panel_base, int64_t* rng, double* segs,
-                          int32_t* nseg, cudaStream_t s) {
-  if (npanel_total <= 0) return cudaSuccess;
-  k_panel_od<<<(unsigned)npanel_total, kPanelThreads, 0, s>>>(w, ln, sh, panel_layer, panel_base,
-                                                              rng, segs, nseg);
+cudaError_t launch_near_pack(const Work& w, const DevLines& ln, int64_t max_nblk,
+                             int64_t npanel_total, const int32_t* panel_layer,
+                             const int64_t* panel_base, int64_t* rng, cudaStream_t s) {
+  if (w.nlay > 65535) return cudaErrorInvalidValue;
+  k_near_scan<<<w.nlay, 32, 0, s>>>(w);
+  if (max_nblk > 0) k_near_pack<<<dim3((unsigned)max_nblk, (unsigned)w.nlay), 256, 0, s>>>(w, ln);
+  if (npanel_total > 0)
+    k_panel_ranges<<<(unsigned)((npanel_total + 127) / 128), 128, 0, s>>>(
+        w, panel_layer, panel_base, npanel_total, rng);
   return cudaGetLastError();
+}
+
+// The panel kernel's variants: records staged per batch and the CTAs per SM
+// the registers are bounded for: (32, 4), (64, 4), (32, 5).
+int panel_stage_of(int variant) { return variant == 1 ? 64 : 32; }
+
+template <typename T>
+cudaError_t launch_panels_t(const Work& w, const DevShapes& sh, int64_t np,
+                            const int32_t* panel_layer, const int64_t* panel_base,
+                            const int64_t* rng, const double* segs, const int32_t* nseg,
+                            int variant, cudaStream_t s) {
+  const unsigned g = (unsigned)np;
+  if (variant == 1)
+    k_panel_od<T, 64, 4><<<g, kPanelThreads, 0, s>>>(w, sh, panel_layer, panel_base, rng, segs,
+                                                      nseg);
+  else if (variant == 2)
+    k_panel_od<T, 32, 5><<<g, kPanelThreads, 0, s>>>(w, sh, panel_layer, panel_base, rng, segs,
+                                                      nseg);
+  else
+    k_panel_od<T, 32, 4><<<g, kPanelThreads, 0, s>>>(w, sh, panel_layer, panel_base, rng, segs,
+                                                      nseg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_panels(const Work& w, const DevShapes& sh, int64_t npanel_total,
+                          const int32_t* panel_layer, const int64_t* panel_base,
+                          const int64_t* rng, const double* segs, const int32_t* nseg,
+                          int precision, int variant, cudaStream_t s) {
+  if (npanel_total <= 0) return cudaSuccess;
+  if (npanel_total >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
+  if (precision == LBL_PREC_SPLIT)
+    return launch_panels_t<float>(w, sh, npanel_total, panel_layer, panel_base, rng, segs, nseg,
+                                  variant, s);
+  return launch_panels_t<double>(w, sh, npanel_total, panel_layer, panel_base, rng, segs, nseg,
+                                 variant, s);
 }
 
 cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const double* od,

@@ -24,6 +24,9 @@ struct DevLines {
 struct DevShapes {
   const double *f1, *f2, *f3, *fg, *xver;
   const double* r1p;  // F1, FG, XVER, 0 per table index (one 32-byte record)
+  // FP32 copies for split precision: F1, FG, XVER, 0 per index (16 bytes), F2, F3
+  const float4* r1p32;
+  const float *f2_32, *f3_32;
 };
 
 // Continuum coefficient table (device pointers).
@@ -43,6 +46,19 @@ struct NearPre {
                   // (bit 0: survives the panel-independent tests; bit 1: R4 test applies)
   int32_t wj;     // window of that panel << 16 | the line's R4 point in it
 };
+
+// One accepted near-wing line of one layer as the fused panel kernel reads
+// it: the constants of CNVFNV's three sums (src/oprop.f90:1283-1351) and the
+// line's windows on the three global grids.  Packed by k_near_pack in file
+// order, 96 bytes (a multiple of 16, so a run of records moves with one bulk
+// copy).
+struct NearRec {
+  double zint, zslope, sppsp, s0, s2, s3, sg, sx;
+  int32_t lo1, hi1, lo2, hi2, lo3, hi3;
+  int32_t pc;   // convolution panel
+  int32_t pad;
+};
+static_assert(sizeof(NearRec) == 96, "NearRec is 96 bytes");
 
 // Work buffers of one batch of layers; offsets come from LayerDev.
 struct Work {
@@ -79,6 +95,13 @@ struct Work {
   int8_t* n_ok;
   NearPre* n_pre;  // k_near_lines -> k_near_walk, k_near_out
   int2* n_blk;     // per near-range TAPE3 panel: read panel (-1 past the end), stop line
+  // accepted near-wing lines packed in file order (slot = rank within the layer)
+  NearRec* n_rec;
+  double* n_rvnu;    // their TAPE3 centres (ascending), for the panels' candidate search
+  int32_t* n_bcnt;   // per near-range TAPE3 panel: accepted lines
+  int32_t* n_boff;   // per near-range TAPE3 panel: accepted lines of the earlier panels
+  int32_t* n_cnt;    // per layer: accepted lines
+  int32_t* n_hw3;    // per layer: widest R3 half-window of an accepted line (R3 points)
   // grids
   double *r1, *r2, *r3;
   double* absrb;
@@ -111,13 +134,22 @@ cudaError_t launch_near_walk(const Work& w, const DevLines& ln, int64_t max_pane
                              int64_t max_win, int64_t max_nblk, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
                              cudaStream_t s);
-cudaError_t launch_panel_prep(const Work& w, const DevLines& ln, int64_t npanel_total,
-                              const int32_t* panel_layer, const int64_t* panel_base, int64_t* rng,
-                              double* segs, int32_t* nseg, cudaStream_t s);
-cudaError_t launch_panels(const Work& w, const DevLines& ln, const DevShapes& sh,
-                          int64_t npanel_total, const int32_t* panel_layer,
-                          const int64_t* panel_base, int64_t* rng, double* segs,
-                          int32_t* nseg, cudaStream_t s);
+// RADFNI segments of every panel (needs only the plans).
+cudaError_t launch_panel_segs(const Work& w, int64_t npanel_total, const int32_t* panel_layer,
+                              const int64_t* panel_base, double* segs, int32_t* nseg,
+                              cudaStream_t s);
+// Pack the accepted near-wing lines of every layer (after k_near_out) and
+// find every panel's candidate records.
+cudaError_t launch_near_pack(const Work& w, const DevLines& ln, int64_t max_nblk,
+                             int64_t npanel_total, const int32_t* panel_layer,
+                             const int64_t* panel_base, int64_t* rng, cudaStream_t s);
+// Variants of the fused panel kernel the autotuner chooses among.
+constexpr int kPanelVariants = 3;
+int panel_stage_of(int variant);
+cudaError_t launch_panels(const Work& w, const DevShapes& sh, int64_t npanel_total,
+                          const int32_t* panel_layer, const int64_t* panel_base,
+                          const int64_t* rng, const double* segs, const int32_t* nseg,
+                          int precision, int variant, cudaStream_t s);
 constexpr int kPanelSegMax = 48;  // RADFNI segments kept per panel (3 doubles each)
 // One merge step (EMINIT when first) for the layer whose LayerDev is Ld.
 cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const double* od,
