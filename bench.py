@@ -503,6 +503,9 @@ def gpu_arm(a):
 
     for _ in range(a.warmup):
         ctx.forward(run, layers, precision=prec, rad=rad_d, tr=tr_d)
+    warm = ctx.profile_read()
+    tuning = {k: {"ms": v[0], "chosen": bool(v[2])} for k, v in warm.items()
+              if k.startswith("tune_")}
     ctx.profile(True)
     ctx.profile_read()
     barrier()
@@ -650,6 +653,7 @@ def gpu_arm(a):
                        "parallelism": f"replica x{world}"},
             "roofline": roofline, "roofline_far_wing": roof_fw, "roofline_merge": roof_merge,
             "stage_ms": stage_ms, "stage_work": stage_work,
+            "autotune": tuning or None,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

@@ -196,10 +196,15 @@ struct lbl_ctx {
   int nslot = 0;
   DevBudget mem;
   // pinned image of the plan tables and the event of its last upload
-  char* stage_host = nullptr;
-  size_t stage_cap = 0;
-  cudaEvent_t stage_ev = nullptr;
-  bool stage_ev_set = false;
+  // two images alternate, so that the host writes the next batch's plan
+  // while the previous upload (or captured graph) may still read the other
+  char* stage_host[2] = {nullptr, nullptr};
+  size_t stage_cap[2] = {0, 0};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  bool stage_ev_set[2] = {false, false};
+  int stage_next = 0;
+  // the executable graph of the last captured group (lbl_forward_batch)
+  cudaGraphExec_t gexec = nullptr;
   bool have_lines = false;
   // fused panel kernel variant chosen by the autotuner (-1: not yet tuned)
   int panel_variant = -1;
@@ -336,6 +341,8 @@ struct Batch {
   int32_t nwin_total = 0;
   int64_t npanel_total = 0, max_far = 0;
   int64_t od_total = 0;
+  int stage_k = 0;          // staging image holding the plan
+  size_t upload_bytes = 0;  // bytes of the plan image
 };
 
 // Plan layers [0,n) on the host into `plans`.  The JRAD switch runs
@@ -392,7 +399,8 @@ size_t layer_arena_bytes(const LayerDev& d) {
          (8 * kSegMaxBlk + 16) * nfblk;
 }
 
-int upload_batch(lbl_ctx* ctx, Batch& B);
+int upload_batch(lbl_ctx* ctx, Batch& B, bool defer = false);
+int enqueue_upload(lbl_ctx* ctx, Batch& B);
 
 // Plan layers [0,n), lay their buffers out in the arena, upload the plans.
 // The JRAD chain follows `chain` when given (the nominal layers of a
@@ -410,8 +418,9 @@ int prepare_batch(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, int n
   return rc;
 }
 
-// Lay the planned layers of B out in the arena and upload their plans.
-int upload_batch(lbl_ctx* ctx, Batch& B) {
+// Lay the planned layers of B out in the arena and upload their plans (with
+// `defer`, only write the plan image; enqueue_upload queues the copy).
+int upload_batch(lbl_ctx* ctx, Batch& B, bool defer) {
   const int n = (int)B.plans.size();
   // offsets
   int64_t o_nblk = 0;
@@ -577,18 +586,22 @@ int upload_batch(lbl_ctx* ctx, Batch& B) {
   // the arena and sent in one copy; the image is reused once the previous
   // call's copy has completed.
   cudaStream_t s = ctx->stream;
-  if (ctx->stage_ev_set) CK(cudaEventSynchronize(ctx->stage_ev));
-  if (upload_bytes > ctx->stage_cap) {
-    if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
-    ctx->stage_host = nullptr;
-    ctx->stage_cap = 0;
+  const int sk = ctx->stage_next;
+  ctx->stage_next ^= 1;
+  B.stage_k = sk;
+  B.upload_bytes = upload_bytes;
+  if (ctx->stage_ev_set[sk]) CK(cudaEventSynchronize(ctx->stage_ev[sk]));
+  if (upload_bytes > ctx->stage_cap[sk]) {
+    if (ctx->stage_host[sk]) cudaFreeHost(ctx->stage_host[sk]);
+    ctx->stage_host[sk] = nullptr;
+    ctx->stage_cap[sk] = 0;
     void* hp = nullptr;
     CK(cudaMallocHost(&hp, upload_bytes));
-    ctx->stage_host = static_cast<char*>(hp);
-    ctx->stage_cap = upload_bytes;
+    ctx->stage_host[sk] = static_cast<char*>(hp);
+    ctx->stage_cap[sk] = upload_bytes;
   }
   auto host = [&](const void* dptr) {
-    return ctx->stage_host + (reinterpret_cast<const char*>(dptr) - A.base);
+    return ctx->stage_host[sk] + (reinterpret_cast<const char*>(dptr) - A.base);
   };
   std::memcpy(host(B.d_ld), B.ld.data(), sizeof(LayerDev) * n);
   double* h_vft = reinterpret_cast<double*>(host(d_vft));
@@ -631,11 +644,23 @@ int upload_batch(lbl_ctx* ctx, Batch& B) {
     std::stable_sort(h_word, h_word + o_win,
                      [&](int32_t a, int32_t b) { return cost[a] > cost[b]; });
   }
-  CK(cudaMemcpyAsync(A.base, ctx->stage_host, upload_bytes, cudaMemcpyHostToDevice, s));
-  CK(cudaEventRecord(ctx->stage_ev, s));
-  ctx->stage_ev_set = true;
-  CK(cudaMemsetAsync(w.status, 0, 4 * sizeof(int32_t), s));
-  CK(cudaMemsetAsync(w.counters, 0, 8 * sizeof(unsigned long long), s));
+  if (defer) return LBL_OK;
+  const int rc = enqueue_upload(ctx, B);
+  if (rc) return rc;
+  CK(cudaEventRecord(ctx->stage_ev[sk], s));
+  ctx->stage_ev_set[sk] = true;
+  return LBL_OK;
+}
+
+// The device side of a batch's upload: the plan image in one copy, the
+// status and counters cleared.  Queued directly, or inside a captured graph
+// (the caller then records the staging image's event after the graph).
+int enqueue_upload(lbl_ctx* ctx, Batch& B) {
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->arena.base, ctx->stage_host[B.stage_k], B.upload_bytes,
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(B.w.status, 0, 4 * sizeof(int32_t), s));
+  CK(cudaMemsetAsync(B.w.counters, 0, 8 * sizeof(unsigned long long), s));
   return LBL_OK;
 }
 
@@ -689,6 +714,14 @@ int tune_panels(lbl_ctx* ctx, Batch& B, int precision) {
   }
   for (auto& e : ev) cudaEventDestroy(e);
   ctx->panel_variant = best;
+  // reported with the stage times: each variant's time and the choice
+  static const char* names[kPanelVariants] = {"tune_panel_s32_b4", "tune_panel_s64_b4",
+                                              "tune_panel_s32_b5"};
+  for (int v = 0; v < kPanelVariants; v++) {
+    lbl_ctx::Stage& st = ctx->stage(names[v]);
+    st.ms += ctx->tune_ms[v];
+    st.work = (v == best) ? 1. : 0.;
+  }
   return LBL_OK;
 }
 
@@ -844,10 +877,12 @@ int ensure_merge_buffers(lbl_ctx* ctx, size_t n) {
   return LBL_OK;
 }
 
-// Where the merged radiance and transmittance go (host or device memory).
+// Where the merged radiance and transmittance go (host or device memory);
+// dev < 0: ask the runtime which memory each pointer is.
 struct OutSink {
   double* rad;
   double* tr;  // may be null
+  int rad_dev = -1, tr_dev = -1;
 };
 
 // Merge every layer of the batch bottom-up; result in mbuf[res], mbuf[res+1].
@@ -903,10 +938,10 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
                           ctx->mbuf[cur + 1], ctx->mbuf[nxt], ctx->mbuf[nxt + 1], tbnd, R.bndemi,
                           R.iemit, ctx->stream, precision));
     } else {
-      const cudaMemcpyKind kr = is_device_ptr(sink->rad) ? cudaMemcpyDeviceToDevice
-                                                          : cudaMemcpyDeviceToHost;
-      const cudaMemcpyKind kt = (sink->tr && is_device_ptr(sink->tr)) ? cudaMemcpyDeviceToDevice
-                                                                      : cudaMemcpyDeviceToHost;
+      const bool rdev = sink->rad_dev >= 0 ? sink->rad_dev != 0 : is_device_ptr(sink->rad);
+      const bool tdev = sink->tr && (sink->tr_dev >= 0 ? sink->tr_dev != 0 : is_device_ptr(sink->tr));
+      const cudaMemcpyKind kr = rdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+      const cudaMemcpyKind kt = tdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
       const int64_t step = ((d.npts + nchunk - 1) / nchunk + 2399) / 2400 * 2400;
       // all pieces are queued before the first copy: a copy to pageable
       // host memory returns only when it is done
@@ -1007,9 +1042,16 @@ int forward_groups(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers,
       mx = std::max<size_t>(mx, (size_t)layer_npts(R, layers[l].dv));
   int rc = ensure_merge_buffers(ctx, mx + 8);
   if (rc) return rc;
+  rc = ensure_copy_stream(ctx);
+  if (rc) return rc;
   const size_t budget = group_budget(ctx, 0);
-  const bool rad_host = !is_device_ptr(rad) && !is_pinned(rad);
-  const bool tr_host = tr && !is_device_ptr(tr) && !is_pinned(tr);
+  const bool rad_dev = is_device_ptr(rad), tr_dev = tr && is_device_ptr(tr);
+  const bool rad_host = !rad_dev && !is_pinned(rad);
+  const bool tr_host = tr && !tr_dev && !is_pinned(tr);
+  // each group's device work is captured in a CUDA graph and launched as
+  // one unit (LBL_BATCH_GRAPHS=0 launches it directly)
+  const char* ge = std::getenv("LBL_BATCH_GRAPHS");
+  const bool graphs_on = !(ge && ge[0] == '0');
   Bounce bounce[2];
   int bi = 0;
   std::vector<LayerPlan> cur;      // plans of the open group
@@ -1024,9 +1066,19 @@ int forward_groups(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers,
     Batch B;
     B.plans = std::move(cur);
     cur.clear();
-    int rc2 = upload_batch(ctx, B);
-    if (rc2) return rc2;
-    rc2 = run_od(ctx, R, B, precision);
+    int64_t npan = 0;
+    for (const LayerPlan& P : B.plans) npan += P.d.npanel;
+    // a group is captured once the panel kernel's variant is settled (the
+    // autotuner synchronises), without stage timing, and with a free status
+    // slot (draining them synchronises)
+    const bool graph = graphs_on && !ctx->prof &&
+                       (ctx->panel_variant >= 0 || npan < kTuneMinPanels);
+    if (graph && ctx->nslot + 1 >= lbl_ctx::kStatSlots) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      const int rcs = finish_od(ctx);
+      if (rcs) return rcs;
+    }
+    int rc2 = upload_batch(ctx, B, graph);
     if (rc2) return rc2;
     // results of this group bound for pageable memory go to bounce[bi]
     Bounce& bb = bounce[bi];
@@ -1047,26 +1099,65 @@ int forward_groups(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers,
       }
       if (!bb.ev) CK(cudaEventCreateWithFlags(&bb.ev, cudaEventDisableTiming));
     }
+    if (graph) CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    // ends a capture that an error interrupted, so the stream is usable
+    auto abandon = [&](int code) {
+      if (graph) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(ctx->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+      }
+      return code;
+    };
+    if (graph && (rc2 = enqueue_upload(ctx, B))) return abandon(rc2);
+    if ((rc2 = run_od(ctx, R, B, precision))) return abandon(rc2);
     size_t boff = 0;
     int l0 = 0;
     for (int p : cur_prof) {
       const int n = (int)(lay0[p + 1] - lay0[p]);
       const size_t np = (size_t)(offsets[p + 1] - offsets[p]);
-      OutSink sink{rad + offsets[p], tr ? tr + offsets[p] : nullptr};
+      OutSink sink{rad + offsets[p], tr ? tr + offsets[p] : nullptr, rad_dev ? 1 : 0,
+                   tr_dev ? 1 : 0};
       if (rad_host) {
         bb.pend.push_back({rad + offsets[p], boff, np});
         sink.rad = bb.buf + boff;
+        sink.rad_dev = 0;
         boff += np;
       }
       if (tr_host) {
         bb.pend.push_back({tr + offsets[p], boff, np});
         sink.tr = bb.buf + boff;
+        sink.tr_dev = 0;
         boff += np;
       }
       int res = 0;
       rc2 = run_merge(ctx, R, layers + lay0[p], B, n, &res, precision, &sink, l0);
-      if (rc2) return rc2;
+      if (rc2) return abandon(rc2);
       l0 += n;
+    }
+    if (graph) {
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamEndCapture(ctx->stream, &g));
+      cudaGraphExecUpdateResultInfo info;
+      if (!ctx->gexec || cudaGraphExecUpdate(ctx->gexec, g, &info) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+        ctx->gexec = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&ctx->gexec, g, 0);
+        if (ie != cudaSuccess) {
+          cudaGraphDestroy(g);
+          ctx->gexec = nullptr;
+          return fail(ctx, LBL_E_CUDA, std::string("cudaGraphInstantiate: ") +
+                                           cudaGetErrorString(ie));
+        }
+      }
+      cudaGraphDestroy(g);
+      CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+      // the staging image may be rewritten once the graph has run
+      CK(cudaEventRecord(ctx->stage_ev[B.stage_k], ctx->stream));
+      ctx->stage_ev_set[B.stage_k] = true;
+      ctx->stage("graph_groups").launches += 1;
     }
     if (need) CK(cudaEventRecord(bb.ev, ctx->stream));
     bi ^= 1;
@@ -1413,7 +1504,8 @@ int lbl_ctx_create(int device, lbl_ctx** out) {
   }
   std::memset(hs, 0, slot_bytes);
   ctx->h_slots = static_cast<lbl_ctx::StatSlot*>(hs);
-  if (cudaEventCreateWithFlags(&ctx->stage_ev, cudaEventDisableTiming) != cudaSuccess) {
+  if (cudaEventCreateWithFlags(&ctx->stage_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->stage_ev[1], cudaEventDisableTiming) != cudaSuccess) {
     cudaFreeHost(hs);
     delete ctx;
     return LBL_E_CUDA;
@@ -1468,8 +1560,11 @@ int lbl_ctx_destroy(lbl_ctx* ctx) {
   if (!ctx) return LBL_E_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->h_slots) cudaFreeHost(ctx->h_slots);
-  if (ctx->stage_host) cudaFreeHost(ctx->stage_host);
-  if (ctx->stage_ev) cudaEventDestroy(ctx->stage_ev);
+  for (int k = 0; k < 2; k++) {
+    if (ctx->stage_host[k]) cudaFreeHost(ctx->stage_host[k]);
+    if (ctx->stage_ev[k]) cudaEventDestroy(ctx->stage_ev[k]);
+  }
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   for (int k = 0; k < lbl_ctx::kSmallRing; k++) {
     if (ctx->small_host[k]) cudaFreeHost(ctx->small_host[k]);
     if (ctx->small_evs[k]) cudaEventDestroy(ctx->small_evs[k]);

@@ -123,8 +123,13 @@ def test_adjoint_batch_channel_means(gpu_ctx, adj, lines3k):
         c = np.floor((v - run.v1) / dvc + 1e-12).astype(int)
         n = cjac.shape[2]
         assert n == int((run.v2 - run.v1) / dvc)
+        # channels with a grid point within 1e-9 cm-1 of an edge are skipped
+        # (the library places points by its panel origins, here by V1 + i DV)
+        edge = np.abs((v - run.v1) / dvc - np.round((v - run.v1) / dvc)) * dvc < 1e-9
         for i in range(0, n, 7):
             m = c == i
+            if np.any(edge[m]) or np.any(edge[c == i + 1]):
+                continue
             assert abs(crad[i] - rad[m].mean()) <= 1e-12 * abs(rad[m].mean())
             want = jac[:, :, m].mean(axis=2)
             assert np.allclose(cjac[:, :, i], want, rtol=1e-12, atol=1e-30)
@@ -177,3 +182,22 @@ def test_jacobian_recompute_per_parameter(gpu_ctx, lines3k):
         gpu_ctx.set_memory_limit(0)
     assert np.array_equal(part[0], full[0])
     assert np.array_equal(part[1], full[1])
+
+
+def test_forward_batch_graphs_and_direct_launches_agree(gpu_ctx, lines3k, monkeypatch):
+    """Each group's device work runs as one captured CUDA graph (default) or
+    as direct launches (LBL_BATCH_GRAPHS=0); the spectra are identical, and
+    a second call with the same topology reuses the executable graph."""
+    run = abi.make_run(v1=600.0, v2=700.0, iemit=1, ilblf4=1, tmpbnd=290.0, bndemi=0.98)
+    profs = profiles_small() * 2
+    gpu_ctx.upload_lines(lines3k)
+    gpu_ctx.profile_read()
+    g1 = gpu_ctx.forward_batch(run, profs)
+    g2 = gpu_ctx.forward_batch(run, profs, precision=abi.PREC_SPLIT)
+    stats = gpu_ctx.profile_read()
+    assert stats.get("graph_groups", (0, 0, 0))[1] >= 2
+    monkeypatch.setenv("LBL_BATCH_GRAPHS", "0")
+    d1 = gpu_ctx.forward_batch(run, profs)
+    d2 = gpu_ctx.forward_batch(run, profs, precision=abi.PREC_SPLIT)
+    for (a, b), (c, d) in zip(g1 + g2, d1 + d2):
+        assert np.array_equal(a, c) and np.array_equal(b, d)
