@@ -234,6 +234,7 @@ struct lbl_ctx {
   // the result's copy-out, overlapped with the last merge launch
   static constexpr int kOutChunks = 4;
   cudaStream_t cstream = nullptr;
+  cudaStream_t gstream = nullptr;  // the batched groups are captured here
   cudaEvent_t cev[kOutChunks + 1] = {};
   // merge buffers (ping-pong)
   double* mbuf[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -318,9 +319,11 @@ int fail(lbl_ctx* c, int code, const std::string& m) {
 #define CK(call)                                                                      \
   do {                                                                                \
     cudaError_t e_ = (call);                                                          \
-    if (e_ != cudaSuccess)                                                            \
+    if (e_ != cudaSuccess) {                                                          \
+      cudaGetLastError(); /* a later launch must not report this error again */       \
       return fail(ctx, e_ == cudaErrorMemoryAllocation ? LBL_E_NOMEM : LBL_E_CUDA,    \
                   std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    }                                                                                 \
   } while (0)
 
 // Device view of one batch of planned layers.
@@ -668,6 +671,7 @@ int enqueue_upload(lbl_ctx* ctx, Batch& B) {
 // copy-out) and its events, created on first use.
 int ensure_copy_stream(lbl_ctx* ctx) {
   if (ctx->cstream) return LBL_OK;
+  CK(cudaStreamCreateWithFlags(&ctx->gstream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
   for (auto& e : ctx->cev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return LBL_OK;
@@ -1099,14 +1103,22 @@ int forward_groups(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers,
       }
       if (!bb.ev) CK(cudaEventCreateWithFlags(&bb.ev, cudaEventDisableTiming));
     }
-    if (graph) CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    // ends a capture that an error interrupted, so the stream is usable
+    // The group is captured on the context's own capture stream (the
+    // caller's stream may be the legacy default stream, which cannot be
+    // captured); the graph is then launched on the caller's stream.
+    cudaStream_t user = ctx->stream;
+    if (graph) {
+      CK(cudaStreamBeginCapture(ctx->gstream, cudaStreamCaptureModeThreadLocal));
+      ctx->stream = ctx->gstream;
+    }
+    // ends a capture that an error interrupted, so the streams stay usable
     auto abandon = [&](int code) {
       if (graph) {
         cudaGraph_t g = nullptr;
-        cudaStreamEndCapture(ctx->stream, &g);
+        cudaStreamEndCapture(ctx->gstream, &g);
         if (g) cudaGraphDestroy(g);
         cudaGetLastError();
+        ctx->stream = user;
       }
       return code;
     };
@@ -1138,7 +1150,8 @@ int forward_groups(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers,
     }
     if (graph) {
       cudaGraph_t g = nullptr;
-      CK(cudaStreamEndCapture(ctx->stream, &g));
+      ctx->stream = user;
+      CK(cudaStreamEndCapture(ctx->gstream, &g));
       cudaGraphExecUpdateResultInfo info;
       if (!ctx->gexec || cudaGraphExecUpdate(ctx->gexec, g, &info) != cudaSuccess) {
         cudaGetLastError();
@@ -1423,7 +1436,7 @@ int jac_profile(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers, int nlay,
       const double tbnd = (l == 0) ? R.tmpbnd : 0.;
       CK(launch_jac_layer(B.d_ld + l, B.w.vft + d.off_panel, B.w.od + d.off_od, d.npts, l == 0,
                           dv_old, n_old, rt[cur], rt[cur + 1], rt[nxt], rt[nxt + 1], tbnd,
-                          R.bndemi, layers[l].tzu, dp, tp, nk, mode, s));
+                          R.bndemi, layers[l].tzu, dp, tp, nk, mode, k0, s));
       cur = nxt;
       dv_old = d.dv;
       n_old = d.npts;
@@ -1579,6 +1592,7 @@ int lbl_ctx_destroy(lbl_ctx* ctx) {
   for (auto e : ctx->cev)
     if (e) cudaEventDestroy(e);
   if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
+  if (ctx->gstream) cudaStreamDestroy(ctx->gstream);
   delete ctx;
   return LBL_OK;
 }

@@ -2356,6 +2356,7 @@ struct JacRows {
                                    // the perturbed run's optical depth (mode 1)
   int np;
   int mode;                     // 0: exact merge derivative; 1: TDERIVup/QDERIVup
+  int k0;                       // parameter of row 0 (0: temperature)
 };
 
 __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const double* od,
@@ -2437,7 +2438,7 @@ __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const d
     for (int k = 0; k < rows.np; k++) {
       const double x = rows.dtau[k][f];
       double d;
-      if (k == 0) {
+      if (k + rows.k0 == 0) {
         const double optdpt = tr > 1.e-06 ? -log(tr) : x;
         const double dtaudt = x - optdpt;
         d = a * dtaudt + bbd * (1. - tr) + (1. - tr) * ((bbdt - bbd) * fi + betai * dfi * dtaudt);
@@ -2451,7 +2452,7 @@ __global__ void k_jac_layer(const LayerDev* Lp, const double* vft_panel, const d
   const double dbt = dem_db * planck_dt(vi, L.tave);
   for (int k = 0; k < rows.np; k++) {
     double d = clamped ? 0. : dr_do * rows.dtau[k][f];
-    if (k == 0) d += dbt;
+    if (k + rows.k0 == 0) d += dbt;
     rows.d[k][f] = d;
   }
 }
@@ -2736,11 +2737,12 @@ cudaError_t launch_jac_layer(const LayerDev* Ld, const double* vft_panel, const 
                              const double* rad_in, const double* tr_in, double* rad_out,
                              double* tr_out, double tbnd, double emis, double tzu,
                              double* const* d, const double* const* dtau, int np,
-                             int mode, cudaStream_t s) {
+                             int mode, int k0, cudaStream_t s) {
   if (np < 1 || np > kJacMaxPar) return cudaErrorInvalidValue;
   JacRows rows;
   rows.np = np;
   rows.mode = mode;
+  rows.k0 = k0;
   for (int k = 0; k < kJacMaxPar; k++) {
     rows.d[k] = k < np ? d[k] : nullptr;
     rows.dtau[k] = k < np ? dtau[k] : nullptr;

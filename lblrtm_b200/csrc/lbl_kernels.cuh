@@ -193,7 +193,7 @@ cudaError_t launch_jac_layer(const LayerDev* Ld, const double* vft_panel, const 
                              const double* rad_in, const double* tr_in, double* rad_out,
                              double* tr_out, double tbnd, double emis, double tzu,
                              double* const* d, const double* const* dtau, int np,
-                             int mode, cudaStream_t s);
+                             int mode, int k0, cudaStream_t s);
 cudaError_t launch_jac_prop(const LayerDev* Ld, const double* od, int64_t npts, double dv_old,
                             int64_t n_old, const double* in, double* out, int64_t stride,
                             int nrows, cudaStream_t s);

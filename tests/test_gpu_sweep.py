@@ -142,7 +142,7 @@ def test_config2_slice_forward(gpu_ctx, c2slice, prec):
 
 # ---- RSYM -------------------------------------------------------------------
 
-def testmm_lines():
+def load_testmm_lines():
     return dict(np.load(os.path.join(HERE, "golden", "testmm_lines.npz")))
 
 
@@ -161,7 +161,7 @@ def test_rsym_first_panel_below_zero(gpu_ctx, src):
     """V1 < 32 DV: the first panel's origin lies below zero wavenumber and
     the grids are folded (RSYM) before PANEL."""
     if src == "testmm":
-        lines = testmm_lines()
+        lines = load_testmm_lines()
         run, lays, lh = lowband_case(lines, 0.1, 60.0)
     else:
         lines = configs.gen_lines(3000, 0.01, 70.0, seed=21, mols=configs.MOLS)
@@ -202,7 +202,7 @@ def test_rsym_changes_the_first_points(gpu_ctx):
 def test_testmm_layer_40_60(gpu_ctx):
     """The reference's TESTMM line list (0-80 cm-1, molecules 1, 3, 4, 7)
     through the GPU path against the oracle, one layer at 40-60 cm-1."""
-    lines = testmm_lines()
+    lines = load_testmm_lines()
     prof = {"pave": np.array([500.0]), "tave": np.array([250.0]), "pzl": np.array([550.0]),
             "pzu": np.array([450.0]), "tzl": np.array([250.0]), "tzu": np.array([250.0]),
             "wk": np.zeros((1, 60)), "wbroad": np.array([1e24]), "nmol": 7}
