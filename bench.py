@@ -434,9 +434,12 @@ def batch_leg(ctx, torch, dist, world, rank, nprof=256):
     for i in sample:
         p = profs[i]
         r64, _ = ctx.forward(run, abi.make_layers_like(p))
+        n64 = len(r64)
+        d64 = torch.empty(n64, dtype=torch.float64, device="cuda")
+        t64 = torch.empty_like(d64)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        ctx.forward(run, abi.make_layers_like(p))
+        ctx.forward(run, abi.make_layers_like(p), rad=d64, tr=t64)
         e1.record()
         e1.synchronize()
         f64_ms += e0.elapsed_time(e1)

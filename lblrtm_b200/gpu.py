@@ -200,9 +200,11 @@ class Context:
                                          _ptr(trb), n, precision), "forward")
         return rad, trb
 
-    def forward_batch(self, run, profiles, precision=abi.PREC_FP64):
+    def forward_batch(self, run, profiles, precision=abi.PREC_FP64, rad=None, tr=None):
         """Many profiles in one call: profiles is a list of lbl_layer arrays.
-        Returns a list of (rad, tr) per profile on each profile's top grid."""
+        Returns a list of (rad, tr) per profile on each profile's top grid.
+        rad/tr may be given as flat buffers (numpy arrays or CUDA tensors)
+        holding all profiles' points."""
         counts = [len(p) for p in profiles]
         allL = (abi.Layer * sum(counts))()
         k = 0
@@ -214,8 +216,8 @@ class Context:
             q = abi.make_layers_like(p)
             dv, _ = dv_rule(run, q)
             total += layer_npts(run, dv[-1])
-        rad = np.zeros(total)
-        tr = np.zeros(total)
+        rad = np.zeros(total) if rad is None else rad
+        tr = np.zeros(total) if tr is None else tr
         off = np.zeros(len(profiles) + 1, dtype=np.int64)
         nl = (C.c_int32 * len(profiles))(*counts)
         self._check(self.lib.lbl_forward_batch(self.h, C.byref(run), allL, nl, len(profiles),
