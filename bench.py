@@ -621,6 +621,8 @@ def gpu_arm(a):
     launches = sum(v[1] for v in stats.values()) // max(nstep, 1)
     stage_ms = {k: round(v[0] / nstep, 4) for k, v in stats.items()}
     stage_work = {k: v[2] / nstep for k, v in stats.items() if v[2]}
+    print("forward step ms", round(step_ms, 3), "stage ms", json.dumps(stage_ms),
+          "autotune", json.dumps(tuning), file=sys.stderr, flush=True)
 
     jleg = None
     if not a.no_jacobian:

@@ -1000,6 +1000,9 @@ size_t group_budget(lbl_ctx* ctx, size_t merge_bytes) {
     avail = fr + ctx->arena.cap;
     const size_t keep = (size_t)2 << 30;  // left to the caller and the runtime
     avail = avail > keep ? (avail - keep) / 10 * 9 : 0;
+    // a group larger than this gains nothing (a few profiles fill the
+    // device) and would leave the caller and the other work spaces no room
+    avail = std::min(avail, tot / 10 * 4);
   }
   return avail > merge_bytes ? avail - merge_bytes : 0;
 }
@@ -1326,12 +1329,19 @@ int jac_profile(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers, int nlay,
   for (int l = 0; l < nlay; l++) off[l + 1] = off[l] + layer_npts(R, layers[l].dv);
   const size_t need = z.bytes(nk, nlay, nchan);
   if (need > ctx->jac_cap) {
-    if (ctx->jac_mem) CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     ctx->mem.release(ctx->jac_mem, ctx->jac_cap);
     ctx->jac_mem = nullptr;
     ctx->jac_cap = 0;
     void* m = nullptr;
-    CK(ctx->mem.alloc(&m, need));
+    if (ctx->mem.alloc(&m, need) != cudaSuccess) {
+      // the arena of an earlier batch may hold the room: release it (the
+      // passes below reserve what they need) and try once more
+      ctx->mem.release(ctx->arena.base, ctx->arena.cap);
+      ctx->arena.base = nullptr;
+      ctx->arena.cap = 0;
+      CK(ctx->mem.alloc(&m, need));
+    }
     ctx->jac_mem = static_cast<char*>(m);
     ctx->jac_cap = need;
   }
