@@ -398,7 +398,7 @@ size_t layer_arena_bytes(const LayerDev& d) {
   const size_t nabs = (size_t)(d.icntnm ? d.nptabs : 0) + 8;
   return sizeof(LayerDev) + 64 + npanel * (8 + 4 + 4 + 16 + 8 * 3 * kPanelSegMax + 4) +
          nwin * (sizeof(WinDev) + 8 + 8 * kR4Stride) + nfar * 83 + 16 * (nfar / 1000 + 2) +
-         nnear * (117 + sizeof(NearRec) + 8) + 16 * nblk + 8 * nabs + 8 * (size_t)d.npts +
+         nnear * (96 + sizeof(NearRec) + 8) + 16 * nblk + 8 * nabs + 8 * (size_t)d.npts +
          (8 * kSegMaxBlk + 16) * nfblk;
 }
 
@@ -490,16 +490,12 @@ int upload_batch(lbl_ctx* ctx, Batch& B, bool defer) {
   lay.add<double>(o_b9 + 1);
   lay.add<int64_t>(n);
   lay.add<double>(o_near + 1);
-  lay.add<double>(o_near + 1);
   lay.add<double>(5 * (o_near + 1));
   lay.add<double>(o_near + 1);
-  for (int k = 0; k < 5; k++) lay.add<int32_t>(o_near + 1);
-  lay.add<int8_t>(o_near + 1);
   lay.add<NearPre>(o_near + 1);
   lay.add<int2>(o_nblk + 1);
   lay.add<NearRec>(o_near + 1);
   lay.add<double>(o_near + 1);
-  lay.add<int32_t>(o_nblk + 1);
   lay.add<int32_t>(o_nblk + 1);
   lay.add<int32_t>(n);
   lay.add<int32_t>(n);
@@ -549,21 +545,13 @@ int upload_batch(lbl_ctx* ctx, Batch& B, bool defer) {
   w.b9_start = A.take<int64_t>(o_b9 + 1);
   w.b9_vnuhi = A.take<double>(o_b9 + 1);
   w.b9_count = A.take<int64_t>(n);
-  w.n_zint = A.take<double>(o_near + 1);
   w.n_zslope = A.take<double>(o_near + 1);
   w.n_str = A.take<double>(5 * (o_near + 1));
   w.n_sppsp = A.take<double>(o_near + 1);
-  w.n_jmin1 = A.take<int32_t>(o_near + 1);
-  w.n_jmax1 = A.take<int32_t>(o_near + 1);
-  w.n_j2 = A.take<int32_t>(o_near + 1);
-  w.n_j3 = A.take<int32_t>(o_near + 1);
-  w.n_pconv = A.take<int32_t>(o_near + 1);
-  w.n_ok = A.take<int8_t>(o_near + 1);
   w.n_pre = A.take<NearPre>(o_near + 1);
   w.n_blk = A.take<int2>(o_nblk + 1);
   w.n_rec = A.take<NearRec>(o_near + 1);
   w.n_rvnu = A.take<double>(o_near + 1);
-  w.n_bcnt = A.take<int32_t>(o_nblk + 1);
   w.n_boff = A.take<int32_t>(o_nblk + 1);
   w.n_cnt = A.take<int32_t>(n);
   w.n_hw3 = A.take<int32_t>(n);
@@ -795,11 +783,11 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   CK(cudaStreamWaitEvent(s, ctx->cev[1], 0));
   {
     // the walk and the window limits; the per-line part ran on the second stream
-    StageTimer t(ctx, "near_scale", 3 + (R.icntnm ? 1 : 0) + 2 + 3);
+    StageTimer t(ctx, "near_scale", 3 + (R.icntnm ? 1 : 0) + 2 + 1);
+    // the walk, then the window limits and packed records of the accepted lines
     CK(launch_near_walk(w, ctx->dl, max_panel, max_win, max_nblk, s));
-    // accepted lines packed per layer, every panel's candidate records
-    CK(launch_near_pack(w, ctx->dl, max_nblk, B.npanel_total, B.d_panel_layer, B.d_panel_base,
-                        B.d_panel_rng, s));
+    // every panel's candidate records
+    CK(launch_panel_ranges(w, B.npanel_total, B.d_panel_layer, B.d_panel_base, B.d_panel_rng, s));
   }
   if (ctx->panel_variant < 0 && B.npanel_total >= kTuneMinPanels) {
     const int rc3 = tune_panels(ctx, B, precision);

@@ -1292,6 +1292,7 @@ __global__ void __launch_bounds__(32) k_near_walk(Work w, DevLines ln) {
   __syncwarp();
   for (int64_t bi = 0; bi < kWalkRing - 1; bi++) issue(bi);
   int pread = 0, rwin = -1;
+  int packed = 0;  // accepted lines of the panels walked so far
   bool stopped = false;
   for (int64_t bi = 0; bi < nblk; bi++) {
     issue(bi + kWalkRing - 1);
@@ -1335,15 +1336,31 @@ __global__ void __launch_bounds__(32) k_near_walk(Work w, DevLines ln) {
       for (int j = 0; j < 8; j++)
         if (lane + 32 * j < stop) pm = max(pm, pf[j]);
       const int pmax = __reduce_max_sync(full, pm);
-      if (lane == 0) w.n_blk[off_nblk + bi] = make_int2(pread, stop);
+      // accepted lines of this panel that CNVFNV reaches: their ranks in the
+      // layer's packed list start at `packed`
+      int cnt = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        if (pf[j] >= 0 && lane + 32 * j < stop) cnt++;
+      cnt = __reduce_add_sync(full, cnt);
+      if (lane == 0) {
+        w.n_blk[off_nblk + bi] = make_int2(pread, stop);
+        w.n_boff[off_nblk + bi] = packed;
+      }
+      packed += cnt;
       pread = pmax;
       if (stop != INT_MAX) stopped = true;
     } else if (lane == 0) {
       w.n_blk[off_nblk + bi] = make_int2(-1, 0);
+      w.n_boff[off_nblk + bi] = packed;
     }
     __syncwarp();  // the slot is refilled by the next issue
   }
   cp_async_wait<0>();
+  if (lane == 0) {
+    w.n_cnt[l] = packed;
+    w.n_hw3[l] = 0;
+  }
 }
 
 // Window limits of every near-wing line (one CTA per layer and TAPE3
@@ -1385,113 +1402,63 @@ __global__ void __launch_bounds__(256) k_near_out(Work w, DevLines ln) {
     if (ok) pfit = max(pread, r.pf_fl >> 2);
   }
   const int pconv = max(pread, block_max_scan(ok ? pfit : -1, s_scan));
+  // rank in the layer's packed list: the panel's start (from the walk) plus
+  // the accepted lines before this one in the panel
+  __shared__ int s_wc[8];
+  const int lane = tid & 31, warp = tid >> 5;
+  const unsigned m = __ballot_sync(0xffffffffu, ok);
+  if (lane == 0) s_wc[warp] = __popc(m);
+  __syncthreads();
   unsigned ntrip = 0;
+  int hw = 0;
   if (ok) {
+    int rank = w.n_boff[L.off_nblk + bi] + __popc(m & ((1u << lane) - 1u));
+    for (int k = 0; k < warp; k++) rank += s_wc[k];
     const double DV = L.dv;
-    const double bhw = kHWDXF / w.n_zslope[slot];
+    const double zslope = w.n_zslope[slot];
+    const double bhw = kHWDXF / zslope;
     const double zint = (r.vnu - w.vft[L.off_panel + pconv]) / DV;
     const long jmax1 = fint(zint + bhw + 1.5);
     const long jmin1 = fint(zint - bhw + 1.5);
     const double rs = zint < 0.0 ? -0.5 : 0.5;
     const long j2 = fint(zint * (1. - L.conf2) + rs);
     const long j3 = fint(zint * (1. - L.conf3) + rs);
-    w.n_zint[slot] = zint;
-    w.n_jmin1[slot] = (int32_t)jmin1;
-    w.n_jmax1[slot] = (int32_t)jmax1;
-    w.n_j2[slot] = (int32_t)j2;
-    w.n_j3[slot] = (int32_t)j3;
-    w.n_pconv[slot] = pconv;
     ntrip = (unsigned)(jmax1 - jmin1 + 1);
+    // the record: CNVFNV's constants and the windows on the three global
+    // grids (the convolution panel's windows shifted by 2400/600/150 points
+    // per panel)
+    const double* sv = w.n_str + 5 * slot;
+    NearRec q;
+    q.zint = zint;
+    q.zslope = zslope;
+    q.sppsp = w.n_sppsp[slot];
+    q.s0 = sv[0];
+    q.s2 = sv[1];
+    q.s3 = sv[2];
+    q.sg = sv[3];
+    q.sx = sv[4];
+    q.lo1 = (int32_t)jmin1 + 2400 * pconv;
+    q.hi1 = (int32_t)jmax1 + 2400 * pconv;
+    q.lo2 = (int32_t)(jmin1 - j2) + 600 * pconv;
+    q.hi2 = (int32_t)(jmax1 - j2) + 600 * pconv;
+    q.lo3 = (int32_t)(jmin1 - j3) + 150 * pconv;
+    q.hi3 = (int32_t)(jmax1 - j3) + 150 * pconv;
+    q.pc = pconv;
+    q.pad = 0;
+    w.n_rec[L.off_near + rank] = q;
+    const double v = ln.vnu[i];
+    w.n_rvnu[L.off_near + rank] = v;
+    // R3 half-window about the TAPE3 centre (g at VFT0 + (g-1) DVR3)
+    const double c3 = (v - L.vft0) / L.dvr3 + 1.;
+    hw = (int)ceil(fmax(c3 - double(q.lo3), double(q.hi3) - c3));
   }
-  if (in) w.n_ok[slot] = ok ? 1 : 0;
-  // one counter update per warp (a single address updated by every line
-  // would serialise the kernel)
+  // one update per warp of the near point-triple counter (a single address
+  // updated by every line would serialise the kernel) and of the layer's
+  // widest R3 half-window
   const unsigned wsum = __reduce_add_sync(0xffffffffu, ntrip);
-  if ((tid & 31) == 0 && wsum) atomicAdd(&w.counters[1], (unsigned long long)wsum);
-  // accepted lines of this TAPE3 panel, for the packing of the layer's list
-  const int nacc = __syncthreads_count(ok ? 1 : 0);
-  if (tid == 0) w.n_bcnt[L.off_nblk + bi] = nacc;
-}
-
-// Exclusive scan of the accepted-line counts over each layer's TAPE3 panels
-// (one warp per layer): where each panel's accepted lines start in the
-// layer's packed list, and the layer's total.
-__global__ void __launch_bounds__(32) k_near_scan(Work w) {
-  const int l = blockIdx.x;
-  const int lane = threadIdx.x;
-  const LayerDev& L = w.L[l];
-  const int nb = (int)(L.blk_hi - L.blk_lo);
-  int run = 0;
-  for (int b0 = 0; b0 < nb; b0 += 32) {
-    const int b = b0 + lane;
-    const int c = b < nb ? w.n_bcnt[L.off_nblk + b] : 0;
-    int x = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += t;
-    }
-    if (b < nb) w.n_boff[L.off_nblk + b] = run + x - c;
-    run += __shfl_sync(0xffffffffu, x, 31);
-  }
-  if (lane == 0) {
-    w.n_cnt[l] = run;
-    w.n_hw3[l] = 0;
-  }
-}
-
-// Pack the accepted near-wing lines of one TAPE3 panel of one layer into
-// NearRec records at their rank in the layer's list (file order), with the
-// windows on the three global grids (the convolution panel's windows shifted
-// by 2400/600/150 points per panel), and raise the layer's widest R3
-// half-window about the line centre.
-__global__ void __launch_bounds__(256) k_near_pack(Work w, DevLines ln) {
-  __shared__ int s_wc[8];
-  const int l = blockIdx.y;
-  const LayerDev& L = w.L[l];
-  const int64_t bi = blockIdx.x;
-  if (bi >= L.blk_hi - L.blk_lo) return;
-  const int64_t b = L.blk_lo + bi;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t a = ln.bs[b] > L.near_lo ? ln.bs[b] : L.near_lo;
-  const int64_t e = ln.bs[b + 1] < L.near_hi ? ln.bs[b + 1] : L.near_hi;
-  const int64_t i = a + tid;
-  const int64_t slot = (i - L.near_lo) + L.off_near;
-  const bool ok = i < e && w.n_ok[slot];
-  const unsigned m = __ballot_sync(0xffffffffu, ok);
-  if (lane == 0) s_wc[warp] = __popc(m);
-  __syncthreads();
-  if (!ok) return;
-  int rank = w.n_boff[L.off_nblk + bi] + __popc(m & ((1u << lane) - 1u));
-  for (int k = 0; k < warp; k++) rank += s_wc[k];
-  const int32_t pc = w.n_pconv[slot];
-  const int32_t j1a = w.n_jmin1[slot], j1b = w.n_jmax1[slot];
-  const int32_t j2 = w.n_j2[slot], j3 = w.n_j3[slot];
-  const double* sv = w.n_str + 5 * slot;
-  NearRec r;
-  r.zint = w.n_zint[slot];
-  r.zslope = w.n_zslope[slot];
-  r.sppsp = w.n_sppsp[slot];
-  r.s0 = sv[0];
-  r.s2 = sv[1];
-  r.s3 = sv[2];
-  r.sg = sv[3];
-  r.sx = sv[4];
-  r.lo1 = j1a + 2400 * pc;
-  r.hi1 = j1b + 2400 * pc;
-  r.lo2 = j1a - j2 + 600 * pc;
-  r.hi2 = j1b - j2 + 600 * pc;
-  r.lo3 = j1a - j3 + 150 * pc;
-  r.hi3 = j1b - j3 + 150 * pc;
-  r.pc = pc;
-  r.pad = 0;
-  w.n_rec[L.off_near + rank] = r;
-  const double v = ln.vnu[i];
-  w.n_rvnu[L.off_near + rank] = v;
-  // R3 point of the TAPE3 centre (global index g: VFT0 + (g-1) DVR3)
-  const double c3 = (v - L.vft0) / L.dvr3 + 1.;
-  const double hw = fmax(c3 - double(r.lo3), double(r.hi3) - c3);
-  atomicMax(&w.n_hw3[l], (int)ceil(hw));
+  if (lane == 0 && wsum) atomicAdd(&w.counters[1], (unsigned long long)wsum);
+  const int whw = __reduce_max_sync(0xffffffffu, hw);
+  if (lane == 0 && m) atomicMax(&w.n_hw3[l], whw);
 }
 
 __device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double x) {
@@ -1903,6 +1870,11 @@ __global__ void __launch_bounds__(kPanelThreads, MINB)
   const int tid = threadIdx.x, warp = tid >> 5;
   __shared__ __align__(128) NearRec st[2][STAGE];
   __shared__ __align__(8) uint64_t bar[2];
+  struct Meta {
+    uint32_t wm;
+    int32_t lo[3], hi[3];
+  };
+  __shared__ Meta smeta[STAGE];
   __shared__ __align__(16) double s1[kP1 * kPanelThreads];
   __shared__ __align__(16) double s2[kP2 * kPanelThreads];
   __shared__ __align__(16) double s3[kPanelThreads];
@@ -1947,29 +1919,40 @@ __global__ void __launch_bounds__(kPanelThreads, MINB)
     const int64_t c0 = clo + (int64_t)b * STAGE;
     const int n = (int)((chi - c0) < STAGE ? (chi - c0) : STAGE);
     const NearRec* batch = st[b & 1];
+    // one thread per record: its windows clipped to the panel's spans (local
+    // points) and the warps owning points of them, bits 0-7 R1, 8-15 R2,
+    // 16-23 R3
+    if (tid < n) {
+      const NearRec& q = batch[tid];
+      int lo1 = (q.lo1 > R.a1 ? q.lo1 : R.a1) - R.a1, hi1 = (q.hi1 < R.b1 ? q.hi1 : R.b1) - R.a1;
+      int lo2 = (q.lo2 > R.a2 ? q.lo2 : R.a2) - R.a2, hi2 = (q.hi2 < R.b2 ? q.hi2 : R.b2) - R.a2;
+      int lo3 = (q.lo3 > R.a3 ? q.lo3 : R.a3) - R.a3, hi3 = (q.hi3 < R.b3 ? q.hi3 : R.b3) - R.a3;
+      smeta[tid].wm = warps_of(lo1, hi1, n1p) | (warps_of(lo2, hi2, n2p) << 8) |
+                      (warps_of(lo3, hi3, n3p) << 16);
+      smeta[tid].lo[0] = lo1;
+      smeta[tid].hi[0] = hi1;
+      smeta[tid].lo[1] = lo2;
+      smeta[tid].hi[1] = hi2;
+      smeta[tid].lo[2] = lo3;
+      smeta[tid].hi[2] = hi3;
+    }
+    __syncthreads();
     for (int k = 0; k < n; k++) {
+      const uint32_t wm = smeta[k].wm >> warp;
+      if (!(wm & 0x10101u)) continue;  // none of the line's window points are this warp's
       const NearRec& q = batch[k];
       // R1 (DV grid): F1 + FG + VERFN terms
-      if (q.hi1 >= R.a1 && q.lo1 <= R.b1) {
-        const int lo = (q.lo1 > R.a1 ? q.lo1 : R.a1) - R.a1;
-        const int hi = (q.hi1 < R.b1 ? q.hi1 : R.b1) - R.a1;
-        if ((warps_of(lo, hi, n1p) >> warp) & 1u)
-          near_add<T, 1>(q, sh, tid, lo, hi, R.a1 - 2400 * q.pc - 1, q.zint, s1);
-      }
+      if (wm & 1u)
+        near_add<T, 1>(q, sh, tid, smeta[k].lo[0], smeta[k].hi[0], R.a1 - 2400 * q.pc - 1,
+                       q.zint, s1);
       // R2 (4 DV): F2
-      if (q.hi2 >= R.a2 && q.lo2 <= R.b2) {
-        const int lo = (q.lo2 > R.a2 ? q.lo2 : R.a2) - R.a2;
-        const int hi = (q.hi2 < R.b2 ? q.hi2 : R.b2) - R.a2;
-        if ((warps_of(lo, hi, n2p) >> warp) & 1u)
-          near_add<T, 2>(q, sh, tid, lo, hi, R.a2 - 600 * q.pc - 1, q.zint * L.conf2, s2);
-      }
+      if (wm & 0x100u)
+        near_add<T, 2>(q, sh, tid, smeta[k].lo[1], smeta[k].hi[1], R.a2 - 600 * q.pc - 1,
+                       q.zint * L.conf2, s2);
       // R3 (16 DV): F3
-      if (q.hi3 >= R.a3 && q.lo3 <= R.b3) {
-        const int lo = (q.lo3 > R.a3 ? q.lo3 : R.a3) - R.a3;
-        const int hi = (q.hi3 < R.b3 ? q.hi3 : R.b3) - R.a3;
-        if ((warps_of(lo, hi, n3p) >> warp) & 1u)
-          near_add<T, 3>(q, sh, tid, lo, hi, R.a3 - 150 * q.pc - 1, q.zint * L.conf3, s3);
-      }
+      if (wm & 0x10000u)
+        near_add<T, 3>(q, sh, tid, smeta[k].lo[2], smeta[k].hi[2], R.a3 - 150 * q.pc - 1,
+                       q.zint * L.conf3, s3);
     }
     __syncthreads();
   }
@@ -2086,17 +2069,13 @@ __global__ void __launch_bounds__(kPanelThreads, MINB)
     __syncthreads();
     const int ns = s_nseg;
     const int32_t ilo = (int32_t)seg[0], ihi = (int32_t)s_n2;
+    int lo = 0;  // this thread's segment: its points only increase
     for (int i = tid; i < n1p; i += kPanelThreads) {
       const int32_t g = R.a1 + i;
       const int32_t I = g - 2400 * p;
       if (I < ilo || I > ihi || g < 33) continue;
       double od = s1[i] + interp4(r2, (g - 1) / 4 + 1, (g - 1) % 4);
-      int lo = 0, hi = ns - 1;
-      while (lo < hi) {
-        const int m = (lo + hi + 1) >> 1;
-        if (seg[3 * m] <= double(I)) lo = m;
-        else hi = m - 1;
-      }
+      while (lo + 1 < ns && seg[3 * (lo + 1)] <= double(I)) lo++;
       od = od * (seg[3 * lo + 1] + double(I - (int32_t)seg[3 * lo]) * seg[3 * lo + 2]);
       od_out[g - 33] = od;
     }
@@ -2646,12 +2625,8 @@ cudaError_t launch_panel_segs(const Work& w, int64_t npanel_total, const int32_t
   return cudaGetLastError();
 }
 
-cudaError_t launch_near_pack(const Work& w, const DevLines& ln, int64_t max_nblk,
-                             int64_t npanel_total, const int32_t* panel_layer,
-                             const int64_t* panel_base, int64_t* rng, cudaStream_t s) {
-  if (w.nlay > 65535) return cudaErrorInvalidValue;
-  k_near_scan<<<w.nlay, 32, 0, s>>>(w);
-  if (max_nblk > 0) k_near_pack<<<dim3((unsigned)max_nblk, (unsigned)w.nlay), 256, 0, s>>>(w, ln);
+cudaError_t launch_panel_ranges(const Work& w, int64_t npanel_total, const int32_t* panel_layer,
+                                const int64_t* panel_base, int64_t* rng, cudaStream_t s) {
   if (npanel_total > 0)
     k_panel_ranges<<<(unsigned)((npanel_total + 127) / 128), 128, 0, s>>>(
         w, panel_layer, panel_base, npanel_total, rng);

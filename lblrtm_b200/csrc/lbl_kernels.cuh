@@ -49,7 +49,7 @@ struct NearPre {
 
 // One accepted near-wing line of one layer as the fused panel kernel reads
 // it: the constants of CNVFNV's three sums (src/oprop.f90:1283-1351) and the
-// line's windows on the three global grids.  Packed by k_near_pack in file
+// line's windows on the three global grids.  Packed by k_near_out in file
 // order, 96 bytes (a multiple of 16, so a run of records moves with one bulk
 // copy).
 struct NearRec {
@@ -88,17 +88,13 @@ struct Work {
   int64_t* seg_out;
   int64_t* seg_count;    // per layer
   // near-wing lines (slot = line index - near_lo)
-  double *n_zint, *n_zslope, *n_str;  // n_str: 5 per slot (F1,F2,F3,FG,VER)
+  double *n_zslope, *n_str;  // n_str: 5 per slot (F1,F2,F3,FG,VER)
   double* n_sppsp;
-  int32_t *n_jmin1, *n_jmax1, *n_j2, *n_j3;  // in the convolution panel's coordinates
-  int32_t* n_pconv;      // panel in which CNVFNV convolves the line
-  int8_t* n_ok;
   NearPre* n_pre;  // k_near_lines -> k_near_walk, k_near_out
   int2* n_blk;     // per near-range TAPE3 panel: read panel (-1 past the end), stop line
   // accepted near-wing lines packed in file order (slot = rank within the layer)
   NearRec* n_rec;
   double* n_rvnu;    // their TAPE3 centres (ascending), for the panels' candidate search
-  int32_t* n_bcnt;   // per near-range TAPE3 panel: accepted lines
   int32_t* n_boff;   // per near-range TAPE3 panel: accepted lines of the earlier panels
   int32_t* n_cnt;    // per layer: accepted lines
   int32_t* n_hw3;    // per layer: widest R3 half-window of an accepted line (R3 points)
@@ -138,11 +134,10 @@ cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, do
 cudaError_t launch_panel_segs(const Work& w, int64_t npanel_total, const int32_t* panel_layer,
                               const int64_t* panel_base, double* segs, int32_t* nseg,
                               cudaStream_t s);
-// Pack the accepted near-wing lines of every layer (after k_near_out) and
-// find every panel's candidate records.
-cudaError_t launch_near_pack(const Work& w, const DevLines& ln, int64_t max_nblk,
-                             int64_t npanel_total, const int32_t* panel_layer,
-                             const int64_t* panel_base, int64_t* rng, cudaStream_t s);
+// Every panel's candidate records (after k_near_out has packed the layers'
+// accepted near-wing lines).
+cudaError_t launch_panel_ranges(const Work& w, int64_t npanel_total, const int32_t* panel_layer,
+                                const int64_t* panel_base, int64_t* rng, cudaStream_t s);
 // Variants of the fused panel kernel the autotuner chooses among.
 constexpr int kPanelVariants = 3;
 int panel_stage_of(int variant);
