@@ -207,8 +207,9 @@ struct lbl_ctx {
   cudaGraphExec_t gexec = nullptr;
   bool have_lines = false;
   // fused panel kernel variant chosen by the autotuner (-1: not yet tuned)
-  int panel_variant = -1;
-  float tune_ms[kPanelVariants] = {};
+  // kernel variants chosen by the autotuner per precision (-1: not tuned)
+  int panel_variant[2] = {-1, -1};
+  int far_variant[2] = {-1, -1};
   // tables
   DevShapes sh{};
   void* shape_mem = nullptr;
@@ -668,53 +669,82 @@ int ensure_copy_stream(lbl_ctx* ctx) {
 int finish_od(lbl_ctx* ctx);
 
 // The autotuner: on the context's first batch of at least kTuneMinPanels
-// panels, every variant of the fused panel kernel (records staged per
-// batch) runs once on that batch, timed by CUDA events on the context's
-// stream, and the fastest is kept for the context's later calls.  Every
-// variant writes the same optical depths (each point sums its lines in file
-// order), so the batch's result does not depend on which ran last.  The
-// variant can be fixed by the environment variable LBL_PANEL_VARIANT (0-2).
+// panels (kTuneMinWindows far-wing windows) in a precision, every variant of
+// the fused panel kernel (records staged per batch, CTAs per SM) and of the
+// far-wing kernel (adders per window CTA) runs once on that batch, timed by
+// CUDA events on the context's stream, and the fastest is kept for the
+// context's later calls in that precision.  Every variant writes the same
+// results (the same sums in the same order), so the batch's result does not
+// depend on which ran last.  LBL_PANEL_VARIANT / LBL_FAR_VARIANT (0-2) fix a
+// variant.
 constexpr int64_t kTuneMinPanels = 4096;
-int tune_panels(lbl_ctx* ctx, Batch& B, int precision) {
-  cudaStream_t s = ctx->stream;
-  if (const char* e = std::getenv("LBL_PANEL_VARIANT")) {
+constexpr int64_t kTuneMinWindows = 128;
+
+template <typename Launch>
+int tune(lbl_ctx* ctx, int nvar, const char* env, const char* const* names, Launch launch,
+         int* chosen) {
+  if (const char* e = std::getenv(env)) {
     const int v = std::atoi(e);
-    if (v >= 0 && v < kPanelVariants) {
-      ctx->panel_variant = v;
+    if (v >= 0 && v < nvar) {
+      *chosen = v;
       return LBL_OK;
     }
   }
-  cudaEvent_t ev[kPanelVariants + 1];
+  cudaStream_t s = ctx->stream;
+  std::vector<cudaEvent_t> ev(nvar + 1);
   for (auto& e : ev) CK(cudaEventCreate(&e));
   CK(cudaEventRecord(ev[0], s));
-  for (int v = 0; v < kPanelVariants; v++) {
-    CK(launch_panels(B.w, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base,
-                     B.d_panel_rng, B.d_panel_segs, B.d_panel_nseg, precision, v, s));
+  for (int v = 0; v < nvar; v++) {
+    CK(launch(v));
     CK(cudaEventRecord(ev[v + 1], s));
   }
-  CK(cudaEventSynchronize(ev[kPanelVariants]));
-  int best = 1;
+  CK(cudaEventSynchronize(ev[nvar]));
+  int best = 0;
   float best_ms = 1e30f;
-  for (int v = 0; v < kPanelVariants; v++) {
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ev[v], ev[v + 1]));
-    ctx->tune_ms[v] = ms;
-    if (ms < best_ms) {
-      best_ms = ms;
+  std::vector<float> ms(nvar, 0.f);
+  for (int v = 0; v < nvar; v++) {
+    CK(cudaEventElapsedTime(&ms[v], ev[v], ev[v + 1]));
+    if (ms[v] < best_ms) {
+      best_ms = ms[v];
       best = v;
     }
   }
   for (auto& e : ev) cudaEventDestroy(e);
-  ctx->panel_variant = best;
+  *chosen = best;
   // reported with the stage times: each variant's time and the choice
-  static const char* names[kPanelVariants] = {"tune_panel_s32_b4", "tune_panel_s64_b4",
-                                              "tune_panel_s32_b5"};
-  for (int v = 0; v < kPanelVariants; v++) {
+  for (int v = 0; v < nvar; v++) {
     lbl_ctx::Stage& st = ctx->stage(names[v]);
-    st.ms += ctx->tune_ms[v];
+    st.ms += ms[v];
     st.work = (v == best) ? 1. : 0.;
   }
   return LBL_OK;
+}
+
+int tune_panels(lbl_ctx* ctx, Batch& B, int precision) {
+  static const char* names[2][kPanelVariants] = {
+      {"tune_panel_s32_b4", "tune_panel_s64_b4", "tune_panel_s32_b5"},
+      {"tune_panel32_s32_b4", "tune_panel32_s64_b4", "tune_panel32_s32_b5"}};
+  const int pk = precision == LBL_PREC_SPLIT ? 1 : 0;
+  return tune(ctx, kPanelVariants, "LBL_PANEL_VARIANT", names[pk],
+              [&](int v) {
+                return launch_panels(B.w, ctx->sh, B.npanel_total, B.d_panel_layer,
+                                     B.d_panel_base, B.d_panel_rng, B.d_panel_segs,
+                                     B.d_panel_nseg, precision, v, ctx->stream);
+              },
+              &ctx->panel_variant[pk]);
+}
+
+int tune_far(lbl_ctx* ctx, Batch& B, int precision) {
+  static const char* names[2][kFarVariants] = {
+      {"tune_far_a224", "tune_far_a352", "tune_far_a480"},
+      {"tune_far32_a224", "tune_far32_a352", "tune_far32_a480"}};
+  const int pk = precision == LBL_PREC_SPLIT ? 1 : 0;
+  return tune(ctx, kFarVariants, "LBL_FAR_VARIANT", names[pk],
+              [&](int v) {
+                return launch_far_wing(B.w, B.nwin_total, B.d_win_order, B.d_win_layer,
+                                       precision, v, ctx->stream);
+              },
+              &ctx->far_variant[pk]);
 }
 
 // A pinned host buffer of at least `bytes` for a table about to be copied
@@ -778,7 +808,14 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   }
   {
     StageTimer t(ctx, "far_wing", B.nwin_total > 0 ? 1 : 0);
-    CK(launch_far_wing(w, B.nwin_total, B.d_win_order, B.d_win_layer, precision, s));
+    const int fk = precision == LBL_PREC_SPLIT ? 1 : 0;
+    if (ctx->far_variant[fk] < 0 && B.nwin_total >= kTuneMinWindows) {
+      const int rc3 = tune_far(ctx, B, precision);
+      if (rc3) return rc3;
+    } else {
+      CK(launch_far_wing(w, B.nwin_total, B.d_win_order, B.d_win_layer, precision,
+                         ctx->far_variant[fk], s));
+    }
   }
   CK(cudaStreamWaitEvent(s, ctx->cev[1], 0));
   {
@@ -789,7 +826,8 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     // every panel's candidate records
     CK(launch_panel_ranges(w, B.npanel_total, B.d_panel_layer, B.d_panel_base, B.d_panel_rng, s));
   }
-  if (ctx->panel_variant < 0 && B.npanel_total >= kTuneMinPanels) {
+  const int pk = precision == LBL_PREC_SPLIT ? 1 : 0;
+  if (ctx->panel_variant[pk] < 0 && B.npanel_total >= kTuneMinPanels) {
     const int rc3 = tune_panels(ctx, B, precision);
     if (rc3) return rc3;
   }
@@ -797,7 +835,7 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
     // near-wing sums, PANEL combination and optical depth in one pass
     StageTimer t(ctx, "panels", 1);
     CK(launch_panels(w, ctx->sh, B.npanel_total, B.d_panel_layer, B.d_panel_base, B.d_panel_rng,
-                     B.d_panel_segs, B.d_panel_nseg, precision, ctx->panel_variant, s));
+                     B.d_panel_segs, B.d_panel_nseg, precision, ctx->panel_variant[pk], s));
   }
   if (ctx->nslot >= lbl_ctx::kStatSlots) {
     // every slot holds a pass not yet read: drain them
@@ -1061,13 +1099,19 @@ int forward_groups(lbl_ctx* ctx, const lbl_run& R, lbl_layer* layers,
     Batch B;
     B.plans = std::move(cur);
     cur.clear();
-    int64_t npan = 0;
-    for (const LayerPlan& P : B.plans) npan += P.d.npanel;
+    int64_t npan = 0, nwin = 0;
+    for (const LayerPlan& P : B.plans) {
+      npan += P.d.npanel;
+      nwin += P.d.nwin;
+    }
     // a group is captured once the panel kernel's variant is settled (the
     // autotuner synchronises), without stage timing, and with a free status
     // slot (draining them synchronises)
     const bool graph = graphs_on && !ctx->prof &&
-                       (ctx->panel_variant >= 0 || npan < kTuneMinPanels);
+                       (ctx->panel_variant[precision == LBL_PREC_SPLIT ? 1 : 0] >= 0 ||
+                        npan < kTuneMinPanels) &&
+                       (ctx->far_variant[precision == LBL_PREC_SPLIT ? 1 : 0] >= 0 ||
+                        nwin < kTuneMinWindows);
     if (graph && ctx->nslot + 1 >= lbl_ctx::kStatSlots) {
       CK(cudaStreamSynchronize(ctx->stream));
       const int rcs = finish_od(ctx);

@@ -683,14 +683,13 @@ __device__ __forceinline__ float f4_at(const F4Reg<float>& r, int, float kq, dou
   return f + xm * r.dptrat * f;
 }
 
-// A far-wing CTA is one deciding warp plus kFwAdders threads that own the
-// window's points (point j belongs to adder (j-1) % kFwAdders).
-constexpr int kFwAdders = 224;
-constexpr int kFwThreads = kFwAdders + 32;
-constexpr int kFwPts = (kLimOut + kFwAdders - 1) / kFwAdders;  // window points per adder
+// A far-wing CTA is one deciding warp plus ADDERS threads that own the
+// window's points (point j belongs to adder (j-1) % ADDERS).
 constexpr int kFwSmem = 2 * (int)kR4Stride * (int)sizeof(double);  // two R4 buffers
 // split precision adds one FP32 accumulator per adder point
-constexpr int kFwSmem32 = kFwSmem + kFwPts * kFwAdders * (int)sizeof(float);
+constexpr int fw_smem32(int adders) {
+  return kFwSmem + ((kLimOut + adders - 1) / adders) * adders * (int)sizeof(float);
+}
 constexpr int kFwBatch = 4;  // lines the deciding warp evaluates together
 
 // Sum, in list order, of both sides of lines cl[idx(0..n-1)] at point jj
@@ -739,9 +738,14 @@ __device__ __forceinline__ void f4_sum_lines(const F4Line* cl, int n, Idx idx, U
 // against the lines accepted on their own partial R4 alone; the lowest line
 // whose decision differs from that guess is exact, so the guess is corrected
 // there and the lines above it re-decided, until no line differs.
-template <typename T>
-__global__ void __launch_bounds__(kFwThreads, 3)
+//
+// ADDERS (224, 352 or 480) sets the CTA's width; the autotuner picks it.
+template <typename T, int ADDERS, int MINB>
+__global__ void __launch_bounds__(ADDERS + 32, MINB)
     k_far_wing(Work w, const int32_t* win_order, const int32_t* win_layer) {
+  constexpr int kFwAdders = ADDERS;
+  constexpr int kFwThreads = ADDERS + 32;
+  constexpr int kFwPts = (kLimOut + ADDERS - 1) / ADDERS;  // window points per adder
   extern __shared__ double fw_r4[];  // [2][kR4Stride]
   __shared__ F4Line cl[2][kChunk];
   __shared__ int s_idx[2][kChunk];
@@ -2527,10 +2531,24 @@ __global__ void k_jac_diff(double* plus, const double* minus, int64_t n, double 
 
 }  // namespace
 
+template <int ADDERS, int MINB>
+void far_wing_attributes() {
+  const cudaFuncAttribute c = cudaFuncAttributePreferredSharedMemoryCarveout;
+  cudaFuncSetAttribute(k_far_wing<double, ADDERS, MINB>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
+  cudaFuncSetAttribute(k_far_wing<float, ADDERS, MINB>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, fw_smem32(ADDERS));
+  cudaFuncSetAttribute(k_far_wing<double, ADDERS, MINB>, c, cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_far_wing<float, ADDERS, MINB>, c, cudaSharedmemCarveoutMaxShared);
+}
+
 void init_kernel_attributes() {
   // two R4 buffers per CTA; the largest carveout lets several CTAs share an SM
-  cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
-  cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem32);
+  // two R4 buffers per CTA (plus the FP32 accumulators of split precision);
+  // the largest carveout lets several CTAs share an SM
+  far_wing_attributes<224, 3>();
+  far_wing_attributes<352, 2>();
+  far_wing_attributes<480, 1>();
   cudaFuncSetAttribute(k_near_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kNearWalkSmemMax);
   {
@@ -2543,10 +2561,7 @@ void init_kernel_attributes() {
     cudaFuncSetAttribute(k_panel_od<float, 64, 4>, c, mx);
     cudaFuncSetAttribute(k_panel_od<float, 32, 5>, c, mx);
   }
-  cudaFuncSetAttribute(k_far_wing<double>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
-  cudaFuncSetAttribute(k_far_wing<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
+
 }
 
 void upload_voicon() {
@@ -2579,13 +2594,24 @@ cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_b
   return cudaGetLastError();
 }
 
-cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
-                            const int32_t* win_layer, int precision, cudaStream_t s) {
-  if (nwin_total <= 0) return cudaSuccess;
+template <int ADDERS, int MINB>
+void launch_far_wing_v(const Work& w, int32_t nwin_total, const int32_t* win_order,
+                       const int32_t* win_layer, int precision, cudaStream_t s) {
   if (precision == LBL_PREC_SPLIT)
-    k_far_wing<float><<<nwin_total, kFwThreads, kFwSmem32, s>>>(w, win_order, win_layer);
+    k_far_wing<float, ADDERS, MINB><<<nwin_total, ADDERS + 32, fw_smem32(ADDERS), s>>>(
+        w, win_order, win_layer);
   else
-    k_far_wing<double><<<nwin_total, kFwThreads, kFwSmem, s>>>(w, win_order, win_layer);
+    k_far_wing<double, ADDERS, MINB><<<nwin_total, ADDERS + 32, kFwSmem, s>>>(w, win_order,
+                                                                               win_layer);
+}
+
+cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
+                            const int32_t* win_layer, int precision, int variant,
+                            cudaStream_t s) {
+  if (nwin_total <= 0) return cudaSuccess;
+  if (variant == 1) launch_far_wing_v<352, 2>(w, nwin_total, win_order, win_layer, precision, s);
+  else if (variant == 2) launch_far_wing_v<480, 1>(w, nwin_total, win_order, win_layer, precision, s);
+  else launch_far_wing_v<224, 3>(w, nwin_total, win_order, win_layer, precision, s);
   return cudaGetLastError();
 }
 
