@@ -686,7 +686,10 @@ __device__ __forceinline__ float f4_at(const F4Reg<float>& r, int, float kq, dou
 // A far-wing CTA is one deciding warp plus ADDERS threads that own the
 // window's points (point j belongs to adder (j-1) % ADDERS).
 constexpr int kFwSmem = 2 * (int)kR4Stride * (int)sizeof(double);  // two R4 buffers
-
+// split precision adds one FP32 accumulator per adder point
+constexpr int fw_smem32(int adders) {
+  return kFwSmem + ((kLimOut + adders - 1) / adders) * adders * (int)sizeof(float);
+}
 constexpr int kFwBatch = 4;  // lines the deciding warp evaluates together
 
 // Sum, in list order, of both sides of lines cl[idx(0..n-1)] at point jj
@@ -736,9 +739,7 @@ __device__ __forceinline__ void f4_sum_lines(const F4Line* cl, int n, Idx idx, U
 // whose decision differs from that guess is exact, so the guess is corrected
 // there and the lines above it re-decided, until no line differs.
 //
-// ADDERS (224 or 352) sets the CTA's width and MINB the CTAs per SM the
-// registers are bounded for; the autotuner picks among (224, 3), (352, 2)
-// and (224, 2).
+// ADDERS (224, 352 or 480) sets the CTA's width; the autotuner picks it.
 template <typename T, int ADDERS, int MINB>
 __global__ void __launch_bounds__(ADDERS + 32, MINB)
     k_far_wing(Work w, const int32_t* win_order, const int32_t* win_layer) {
@@ -756,6 +757,10 @@ __global__ void __launch_bounds__(ADDERS + 32, MINB)
   const LayerDev& L = w.L[l];
   const WinDev& W = w.win[gw];
   for (int j = threadIdx.x; j < 2 * kR4Stride; j += kFwThreads) fw_r4[j] = 0.;
+  if constexpr (sizeof(T) == 4) {
+    float* acc32 = reinterpret_cast<float*>(fw_r4 + 2 * kR4Stride);
+    for (int j = threadIdx.x; j < kFwPts * kFwAdders; j += kFwThreads) acc32[j] = 0.f;
+  }
   const double dvr4 = L.dvr4, bnd = L.bound4, bndsq = bnd * bnd, rbndsq = 1. / bndsq;
   const int npt = W.nptr4;
   const int64_t S = L.off_shr;
@@ -944,14 +949,12 @@ __global__ void __launch_bounds__(ADDERS + 32, MINB)
       const int ad = (int)threadIdx.x - 32;
       const int na = s_nacc[prv];
       if constexpr (sizeof(T) == 8) {
-        // FP64: each point summed line by line, line before image, in
-        // CONVF4's order, in registers for the phase (the adder's points
-        // are fixed, so the unrolled point loop keeps them there)
-        double acc[kFwPts];
+        // FP64: each point summed in shared memory line by line, line
+        // before image, in CONVF4's order
 #pragma unroll
         for (int q = 0; q < kFwPts; q++) {
           const int j = 1 + ad + kFwAdders * q;
-          acc[q] = (j <= npt) ? R4r[j] : 0.;
+          if (j <= npt) R4w[j] = R4r[j];
         }
         for (int a = 0; a < na; a++) {
           const F4Line& pl = cl[prv][s_idx[prv][a]];
@@ -970,44 +973,33 @@ __global__ void __launch_bounds__(ADDERS + 32, MINB)
             const double step = double(kFwAdders) * dvr4;
             double xm = double(ad + kFwAdders * qlo) * dvr4 - rg.xnui;
             if (!rg.co2 && rg.dptrat == 0.) {
-#pragma unroll
-              for (int q = 0; q < kFwPts; q++) {
-                if (q < qlo || q > qhi) continue;
+#pragma unroll 2
+              for (int q = qlo; q <= qhi; q++, xm += step) {
                 const double xmsq = xm * xm;
                 const double zvsq = xmsq * rg.rvi2;
                 const double f = zvsq <= 4096. ? (rg.sa3 + zvsq * rg.sb3) - rg.f4bnd
                                                : rg.sil * recip_nr(rg.alfl2 + xmsq) - rg.f4bnd;
-                acc[q] += f;
-                xm += step;
+                R4w[1 + ad + kFwAdders * q] += f;
               }
             } else {
-#pragma unroll
-              for (int q = 0; q < kFwPts; q++) {
-                if (q < qlo || q > qhi) continue;
+#pragma unroll 2
+              for (int q = qlo; q <= qhi; q++, xm += step) {
                 const double xmsq = xm * xm;
                 const double zvsq = xmsq * rg.rvi2;
                 const double sub = rg.co2 ? (2. - xmsq * rbndsq) * rg.f4bnd : rg.f4bnd;
                 double f = zvsq <= 4096. ? (rg.sa3 + zvsq * rg.sb3) - sub
                                          : rg.sil * recip_nr(rg.alfl2 + xmsq) - sub;
                 f = f + xm * rg.dptrat * f;
-                acc[q] += f;
-                xm += step;
+                R4w[1 + ad + kFwAdders * q] += f;
               }
             }
             nevals += (unsigned)(qhi - qlo + 1);
           }
         }
-#pragma unroll
-        for (int q = 0; q < kFwPts; q++) {
-          const int j = 1 + ad + kFwAdders * q;
-          if (j <= npt) R4w[j] = acc[q];
-        }
       } else {
-        // split precision: the chunk's lines summed in FP32 in registers
+        // split precision: the chunk's lines summed in FP32 in shared memory
         // (each adder its own points), the chunk total added to the FP64 R4
-        float acc32[kFwPts];
-#pragma unroll
-        for (int q = 0; q < kFwPts; q++) acc32[q] = 0.f;
+        float* acc32 = reinterpret_cast<float*>(fw_r4 + 2 * kR4Stride) + ad;
         const float dvr4f = (float)dvr4, bndf = (float)bnd, rbndsqf = (float)rbndsq;
         for (int a = 0; a < na; a++) {
           const F4Line& pl = cl[prv][s_idx[prv][a]];
@@ -1019,19 +1011,18 @@ __global__ void __launch_bounds__(ADDERS + 32, MINB)
             if (qhi < qlo) continue;
             F4Reg<float> rg;
             f4_load(rg, pl, m, 1 + ad);
-#pragma unroll
-            for (int q = 0; q < kFwPts; q++) {
-              if (q < qlo || q > qhi) continue;
-              acc32[q] += f4_at(rg, 0, rg.k0 + (float)(kFwAdders * q), dvr4, rbndsq, dvr4f,
-                                bndf, rbndsqf);
-            }
+#pragma unroll 2
+            for (int q = qlo; q <= qhi; q++)
+              acc32[kFwAdders * q] += f4_at(rg, 0, rg.k0 + (float)(kFwAdders * q), dvr4, rbndsq,
+                                            dvr4f, bndf, rbndsqf);
             nevals += (unsigned)(qhi - qlo + 1);
           }
         }
 #pragma unroll
         for (int q = 0; q < kFwPts; q++) {
           const int j = 1 + ad + kFwAdders * q;
-          if (j <= npt) R4w[j] = R4r[j] + (double)acc32[q];
+          if (j <= npt) R4w[j] = R4r[j] + (double)acc32[kFwAdders * q];
+          acc32[kFwAdders * q] = 0.f;
         }
       }
     }
@@ -2546,7 +2537,7 @@ void far_wing_attributes() {
   cudaFuncSetAttribute(k_far_wing<double, ADDERS, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
   cudaFuncSetAttribute(k_far_wing<float, ADDERS, MINB>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, fw_smem32(ADDERS));
   cudaFuncSetAttribute(k_far_wing<double, ADDERS, MINB>, c, cudaSharedmemCarveoutMaxShared);
   cudaFuncSetAttribute(k_far_wing<float, ADDERS, MINB>, c, cudaSharedmemCarveoutMaxShared);
 }
@@ -2557,7 +2548,7 @@ void init_kernel_attributes() {
   // the largest carveout lets several CTAs share an SM
   far_wing_attributes<224, 3>();
   far_wing_attributes<352, 2>();
-  far_wing_attributes<224, 2>();
+  far_wing_attributes<480, 1>();
   cudaFuncSetAttribute(k_near_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kNearWalkSmemMax);
   {
@@ -2607,8 +2598,8 @@ template <int ADDERS, int MINB>
 void launch_far_wing_v(const Work& w, int32_t nwin_total, const int32_t* win_order,
                        const int32_t* win_layer, int precision, cudaStream_t s) {
   if (precision == LBL_PREC_SPLIT)
-    k_far_wing<float, ADDERS, MINB><<<nwin_total, ADDERS + 32, kFwSmem, s>>>(w, win_order,
-                                                                              win_layer);
+    k_far_wing<float, ADDERS, MINB><<<nwin_total, ADDERS + 32, fw_smem32(ADDERS), s>>>(
+        w, win_order, win_layer);
   else
     k_far_wing<double, ADDERS, MINB><<<nwin_total, ADDERS + 32, kFwSmem, s>>>(w, win_order,
                                                                                win_layer);
@@ -2619,7 +2610,7 @@ cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* wi
                             cudaStream_t s) {
   if (nwin_total <= 0) return cudaSuccess;
   if (variant == 1) launch_far_wing_v<352, 2>(w, nwin_total, win_order, win_layer, precision, s);
-  else if (variant == 2) launch_far_wing_v<224, 2>(w, nwin_total, win_order, win_layer, precision, s);
+  else if (variant == 2) launch_far_wing_v<480, 1>(w, nwin_total, win_order, win_layer, precision, s);
   else launch_far_wing_v<224, 3>(w, nwin_total, win_order, win_layer, precision, s);
   return cudaGetLastError();
 }

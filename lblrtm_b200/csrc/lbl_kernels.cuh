@@ -112,8 +112,8 @@ void upload_voicon();
 cudaError_t launch_far_scale(const Work& w, const DevLines& ln, int64_t max_far, cudaStream_t s);
 cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_base,
                           int64_t nblk_total, cudaStream_t s);
-// Far-wing variants the autotuner chooses among: 224 adders per window CTA at
-// 3 CTAs per SM, 352 at 2, 224 at 2 (more registers).
+// Far-wing variants the autotuner chooses among: 224, 352 or 480 adders per
+// window CTA (3, 2 or 1 CTAs per SM).
 constexpr int kFarVariants = 3;
 cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
                             const int32_t* win_layer, int precision, int variant,
