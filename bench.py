@@ -257,6 +257,22 @@ def jacobian_leg(ctx, prec, torch):
         torch.cuda.synchronize()
         jt.append(1e3 * (time.perf_counter() - t0))
     jac_ms = sum(jt) / len(jt)
+    # the reference's analytic-Jacobian definitions (one pass at T + 1 K and
+    # one per molecule alone) through the batched entry point, full grid
+    njr = (1 + len(mols)) * len(layers) * n
+    jref = torch.empty(njr, dtype=torch.float64, device="cuda")
+    ctx.adjoint_batch(run, [layers], mols, mode=abi.JAC_REFERENCE, precision=prec, rad=rad,
+                      jac=jref)
+    jr = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.adjoint_batch(run, [layers], mols, mode=abi.JAC_REFERENCE, precision=prec, rad=rad,
+                          jac=jref)
+        torch.cuda.synchronize()
+        jr.append(1e3 * (time.perf_counter() - t0))
+    del jref
+    jac_ref_ms = sum(jr) / len(jr)
     nfd = 2 * len(mols) * len(layers) + 2 * len(layers) + 1
     rows = (1 + len(mols)) * len(layers)
     del jac
@@ -265,6 +281,8 @@ def jacobian_leg(ctx, prec, torch):
             "ms_per_jacobian_set": jac_ms, "jacobian_sets_per_s": 1e3 / jac_ms,
             "forward_ms": fwd_ms, "fd_forwards": nfd, "fd_ms_estimate": fwd_ms * nfd,
             "speedup_vs_fd": fwd_ms * nfd / jac_ms,
+            "ms_per_jacobian_set_reference_mode": jac_ref_ms,
+            "speedup_vs_fd_reference_mode": fwd_ms * nfd / jac_ref_ms,
             "timing": "wall clock around the synchronous call (host planning included)"}
 
 
