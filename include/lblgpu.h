@@ -58,9 +58,12 @@ typedef enum lbl_status {
 /* Arithmetic of the line-shape, far-wing and merge kernels. */
 typedef enum lbl_precision {
   LBL_PREC_FP64 = 0,      /* plain FP64 throughout: the drop-in form */
-  LBL_PREC_SPLIT = 1      /* FP32 line shapes, far wing and merge; FP64 grid
-                             positions, line-centre offsets and compensated
-                             optical-depth sums */
+  LBL_PREC_SPLIT = 1      /* FP32 line shapes (near wing: FP32 values summed
+                             per grid point with Kahan compensation; far
+                             wing: FP32 per chunk of lines, added to an FP64
+                             total) and FP32 merge; FP64 grid positions,
+                             line-centre offsets, table indices and far-wing
+                             rejection decisions */
 } lbl_precision;
 
 /* Run-level control: TAPE5 records 1.2, 1.2a, 1.3, 1.4 (subset on the hot
