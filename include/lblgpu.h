@@ -149,11 +149,13 @@ int lbl_ctx_destroy(lbl_ctx* ctx);
 /* Last error message of this context (empty if none). */
 const char* lbl_last_error(const lbl_ctx* ctx);
 /* Set the CUDA stream (cudaStream_t) used by later calls; NULL = default.
- * The context also owns one internal non-blocking stream (created on first
- * use): the kernels that need only the layer plans run there beside the far
- * wing, and lbl_forward copies its result out there while the last merge
- * launch runs; both are joined to the caller's stream by events, and every
- * call that returns results synchronises before it returns. */
+ * The context also owns two internal non-blocking streams (created on first
+ * use): on one, the kernels that need only the layer plans run beside the
+ * far wing, and results are copied out while the last merge launch runs
+ * (joined to the caller's stream by events); on the other, each group of
+ * lbl_forward_batch is captured as a CUDA graph, which is then launched on
+ * the caller's stream.  Every call that returns results synchronises before
+ * it returns. */
 int lbl_set_stream(lbl_ctx* ctx, void* stream);
 
 /* Cap the device memory the context holds (lines, tables, work arenas,
