@@ -208,6 +208,28 @@ int64_t lbl_layer_npts(const lbl_run* run, double dv);
 int lbl_layer_od(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
                  int32_t* jrad, double* od, int64_t npts, int32_t precision);
 
+/* ---- optical depth on a DVOUT grid: PNLINT ---------------------------- */
+
+/* Points PNLINT writes (src/oprop.f90:1564-1806, called from PANEL
+ * :1524-1532 when /IODFLG/ DVOUT is nonzero) for a layer of spacing dv
+ * re-gridded to dvout: output panels of up to 2400 points from V1 in steps
+ * of dvout, ending at the first point >= V2.  |dvout-dv| < 1e-8 passes the
+ * layer grid through (lbl_layer_npts points).  Negative: minus a status
+ * (-LBL_E_ARG, also for dvout > dv: the reference prints "DVOUT MUST BE <
+ * DV", src/lblrtm.f90:5567-5568, and then reads past its panel buffer). */
+int64_t lbl_pnlint_npts(const lbl_run* run, double dv, double dvout);
+
+/* PNLINT: the layer optical depth od_in (n_in = lbl_layer_npts(run, dv)
+ * points on V1 + i*dv, as lbl_layer_od writes it) interpolated to the DVOUT
+ * grid with the reference's 4-point Lagrange weights tabulated at 1/100 of
+ * dv (n_out = lbl_pnlint_npts points).  Reproduces the reference's
+ * streaming order: each output point takes its interpolation coordinate
+ * from the PANEL panel that was current when the reference computed it.
+ * This is the layer output of IOD=1/4 (DVOUT from DVSET) and of the IOD=3
+ * common grid.  od_in, od_out: host or device. */
+int lbl_pnlint(lbl_ctx* ctx, const lbl_run* run, double dv, double dvout,
+               const double* od_in, int64_t n_in, double* od_out, int64_t n_out);
+
 /* ---- one merge step: XMERGE ------------------------------------------ */
 
 /* Merge one layer's optical depth into the accumulated radiance and

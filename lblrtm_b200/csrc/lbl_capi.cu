@@ -1890,6 +1890,61 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, in
   return LBL_OK;
 }
 
+int64_t lbl_pnlint_npts(const lbl_run* run, double dv, double dvout) {
+  if (!run || !(run->v2 > run->v1) || run->v2 - run->v1 > 2020. || !(run->v1 > 0.))
+    return -LBL_E_ARG;
+  PnlPlan P;
+  std::string e;
+  int rc = pnlint_plan(*run, dv, dvout, &P, &e);
+  if (rc) return -rc;
+  return P.n_out;
+}
+
+int lbl_pnlint(lbl_ctx* ctx, const lbl_run* run, double dv, double dvout, const double* od_in,
+               int64_t n_in, double* od_out, int64_t n_out) {
+  if (!ctx) return LBL_E_ARG;
+  if (!run || !od_in || !od_out) return fail(ctx, LBL_E_ARG, "NULL argument");
+  if (!(run->v2 > run->v1) || run->v2 - run->v1 > 2020. || !(run->v1 > 0.))
+    return fail(ctx, LBL_E_ARG, "V1/V2");
+  PnlPlan P;
+  std::string e;
+  int rc = pnlint_plan(*run, dv, dvout, &P, &e);
+  if (rc) return fail(ctx, rc, e);
+  if (layer_npts(*run, dv) != n_in) return fail(ctx, LBL_E_ARG, "n_in does not match the layer grid");
+  if (P.n_out != n_out) return fail(ctx, LBL_E_ARG, "n_out does not match the DVOUT grid");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if (P.copy) {
+    CK(cudaMemcpyAsync(od_out, od_in, n_in * 8, cudaMemcpyDefault, s));
+    CK(cudaStreamSynchronize(s));
+    return LBL_OK;
+  }
+  const bool in_dev = is_device_ptr(od_in), out_dev = is_device_ptr(od_out);
+  const size_t nseg = P.seg.size();
+  size_t bytes = nseg * sizeof(PnlSeg) + sizeof(P.a) + 3 * 256;
+  if (!in_dev) bytes += n_in * 8 + 256;
+  if (!out_dev) bytes += n_out * 8 + 256;
+  CK(ctx->arena.reserve(bytes, ctx->mem));
+  ctx->arena.reset();
+  PnlSeg* dseg = ctx->arena.take<PnlSeg>(nseg);
+  double* da = ctx->arena.take<double>(4 * 101);
+  const double* din = od_in;
+  double* dout = od_out;
+  if (!in_dev) {
+    double* t = ctx->arena.take<double>(n_in);
+    CK(cudaMemcpyAsync(t, od_in, n_in * 8, cudaMemcpyHostToDevice, s));
+    din = t;
+  }
+  if (!out_dev) dout = ctx->arena.take<double>(n_out);
+  CK(cudaMemcpyAsync(dseg, P.seg.data(), nseg * sizeof(PnlSeg), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(da, P.a, sizeof(P.a), cudaMemcpyHostToDevice, s));
+  const double ratdv = dvout / dv;
+  CK(launch_pnlint(dseg, (int64_t)nseg, da, din, n_in, ratdv, dout, n_out, s));
+  if (!out_dev) CK(cudaMemcpyAsync(od_out, dout, n_out * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return LBL_OK;
+}
+
 int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nlay, double* rad,
                 double* tr, int64_t npts, int32_t precision) {
   if (!ctx) return LBL_E_ARG;

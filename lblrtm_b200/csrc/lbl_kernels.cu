@@ -2784,4 +2784,53 @@ cudaError_t launch_jac_diff(double* plus, const double* minus, int64_t n, double
   return cudaGetLastError();
 }
 
+// ---- PNLINT (src/oprop.f90:1564-1806) ---------------------------------
+// Output point II of a segment: FJJ = FJ1DIF + RATDV*(II-1), JJ = INT(FJJ)-2,
+// JP = INT((FJJ-JJ)*100-199.5), value = A1(JP)*R1(JJ-1) + A2(JP)*R1(JJ) +
+// A3(JP)*R1(JJ+1) + A4(JP)*R1(JJ+2) (label 30), every product and sum
+// rounded separately and in that order.  R1(j) of input panel p is layer
+// point g0+j-1; the first panel repeats R1(1) below j=1 (R1(-1)=R1(0)=R1(1))
+// and the last repeats R1(NLIM) above NLIM (the two padded points).  Reads
+// are HBM-bound gathers: each input point is read by about DV/DVOUT
+// neighbouring threads of one CTA, so L1 serves the repeats.
+__global__ void __launch_bounds__(256) k_pnlint(const PnlSeg* __restrict__ seg,
+                                                const double* __restrict__ a,
+                                                const double* __restrict__ od, int64_t n_in,
+                                                double ratdv, double* __restrict__ out,
+                                                int64_t n_out) {
+  __shared__ double sa[4 * 101];
+  for (int i = threadIdx.x; i < 4 * 101; i += blockDim.x) sa[i] = a[i];
+  const PnlSeg S = seg[blockIdx.x];
+  __syncthreads();
+  const bool first = S.flags & 1, last = S.flags & 2;
+  auto r1 = [&](long j) -> double {
+    if (first && j < 1) j = 1;
+    if (last && j > S.nlim) j = S.nlim;
+    int64_t g = S.g0 + j - 1;
+    g = g < 0 ? 0 : (g >= n_in ? n_in - 1 : g);
+    return od[g];
+  };
+  for (int ii = S.ii_lo + (int)threadIdx.x; ii <= S.ii_hi; ii += blockDim.x) {
+    const double fjj = __dadd_rn(S.fj1dif, __dmul_rn(ratdv, (double)(ii - 1)));
+    const long jj = (long)fjj - 2;
+    int jp = (int)__dsub_rn(__dmul_rn(__dsub_rn(fjj, (double)jj), 100.), 199.5);
+    jp = jp < 0 ? 0 : (jp > 100 ? 100 : jp);
+    double v = __dmul_rn(sa[jp], r1(jj - 1));
+    v = __dadd_rn(v, __dmul_rn(sa[101 + jp], r1(jj)));
+    v = __dadd_rn(v, __dmul_rn(sa[202 + jp], r1(jj + 1)));
+    v = __dadd_rn(v, __dmul_rn(sa[303 + jp], r1(jj + 2)));
+    const int64_t k = S.k0 + ii - 1;
+    if (k < n_out) out[k] = v;
+  }
+}
+
+cudaError_t launch_pnlint(const PnlSeg* seg, int64_t nseg, const double* a, const double* od,
+                          int64_t n_in, double ratdv, double* out, int64_t n_out,
+                          cudaStream_t s) {
+  if (nseg <= 0) return cudaSuccess;
+  if (nseg >= (int64_t(1) << 31) || n_in < 1) return cudaErrorInvalidValue;
+  k_pnlint<<<(unsigned)nseg, 256, 0, s>>>(seg, a, od, n_in, ratdv, out, n_out);
+  return cudaGetLastError();
+}
+
 }  // namespace lbl

@@ -204,6 +204,11 @@ cudaError_t launch_jac_diff(double* plus, const double* minus, int64_t n, double
 cudaError_t launch_chan_mean(const double* x, int64_t n, int nrows, const int64_t* cb,
                              int64_t nchan, double* out, cudaStream_t s);
 constexpr int kJacMaxParams = 8;
+// PNLINT re-grid of one layer (one CTA per segment of the host plan);
+// a: the 4 x 101 Lagrange weights.
+cudaError_t launch_pnlint(const PnlSeg* seg, int64_t nseg, const double* a, const double* od,
+                          int64_t n_in, double ratdv, double* out, int64_t n_out,
+                          cudaStream_t s);
 
 void init_kernel_attributes();
 

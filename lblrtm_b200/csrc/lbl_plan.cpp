@@ -475,4 +475,135 @@ int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad_in, const HostLine
   return LBL_OK;
 }
 
+// PNLINT's panel loop (src/oprop.f90:1620-1800) replayed per PANEL output
+// panel (src/oprop.f90:1435-1451: V1P = VFT+(NLO-1)*DV, V2P by the
+// last-panel rule, VFT advanced by NLIM1-1 = 2400 points).  Segments are
+// recorded in place of the interpolation loop (label 30); every test,
+// truncation and accumulation follows the reference's order.
+int pnlint_plan(const lbl_run& R, double dv, double dvout, PnlPlan* P, std::string* err) {
+  P->seg.clear();
+  P->n_out = 0;
+  if (!(dv > 0.) || !(dvout > 0.)) {
+    *err = "DV and DVOUT must be positive";
+    return LBL_E_ARG;
+  }
+  for (int jp = 0; jp <= 100; jp++) {
+    double apg = jp, p = 0.01 * apg;
+    P->a[0][jp] = -p * (p - 1.0) * (p - 2.0) / 6.0;
+    P->a[1][jp] = (p * p - 1.0) * (p - 2.0) * 0.5;
+    P->a[2][jp] = -p * (p + 1.0) * (p - 2.0) * 0.5;
+    P->a[3][jp] = p * (p * p - 1.0) / 6.0;
+  }
+  P->copy = (dv == dvout) || std::fabs(dvout - dv) < 1.e-8;
+  if (P->copy) {
+    P->n_out = layer_npts(R, dv);
+    return LBL_OK;
+  }
+  if (dvout > dv) {
+    *err = "DVOUT MUST BE < DV";
+    return LBL_E_ARG;
+  }
+  const int limout = 2400;
+  double vft = R.v1 - double(kNShift) * dv;
+  double v1po = 0.;
+  long nlim1 = 1;
+  int64_t kq = 0;  // global output index of the open output panel's II=1
+  for (int64_t p = 0;; p++) {
+    long nhi = 2432;
+    double v2p;
+    bool istop = false;
+    if ((vft + double(nhi - 1) * dv) > R.v2) {
+      nhi = fint((R.v2 - vft) / dv + 1.);
+      v2p = vft + double(nhi - 1) * dv;
+      if (v2p < R.v2) {
+        v2p = v2p + dv;
+        nhi = nhi + 1;
+      }
+      istop = true;
+    } else {
+      v2p = vft + double(nhi - 1) * dv;
+    }
+    const long nlim = nhi - (kNShift + 1) + 1;
+    const double v1p = vft + double(kNShift) * dv;
+    // ---- PNLINT entry
+    int nppanl = 1;
+    int flags = istop ? 2 : 0;
+    if (v1po == 0.0) {
+      v1po = v1p;
+      nlim1 = 1;
+      flags |= 1;
+    }
+    if (istop) v2p = v2p + 2. * dv;
+    bool ilast = false;
+    for (;;) {
+      double v2po = v1po + double(limout) * dvout;
+      if (v2p <= v2po + dv && !ilast && nppanl <= 0) break;
+      long nlim2;
+      if ((v1po + double(limout - 1) * dvout) > R.v2) {
+        nlim2 = fint((R.v2 - v1po) / dvout + 1.);
+        v2po = v1po + double(nlim2 - 1) * dvout;
+        if (v2po < R.v2) {
+          v2po = v2po + dvout;
+          nlim2 = nlim2 + 1;
+        }
+        ilast = true;
+        if (!istop && v2po > v2p - dv) {
+          nlim2 = fint(((v2p - dv - v1po) / dvout) + 1.);
+          v2po = v1po + double(nlim2 - 1) * dvout;
+          if (v2po + dvout < v2p - dv) {
+            nlim2 = nlim2 + 1;
+            v2po = v2po + dvout;
+          }
+          ilast = false;
+        }
+      } else {
+        nlim2 = limout;
+        v2po = v1po + double(nlim2 - 1) * dvout;
+        if (v2po > v2p - dv) {
+          nlim2 = fint(((v2p - dv - v1po) / dvout) + 1.);
+          v2po = v1po + double(nlim2 - 1) * dvout;
+          if (v2po + dvout < v2p - dv) {
+            nlim2 = nlim2 + 1;
+            v2po = v2po + dvout;
+          }
+        }
+        ilast = false;
+      }
+      if (nlim2 >= nlim1 && nlim1 >= 1) {
+        PnlSeg s;
+        s.v1po = v1po;
+        s.v1p = v1p;
+        s.fj1dif = (v1po - v1p) / dv + 1. + 2.;
+        s.k0 = kq;
+        s.g0 = 2400 * p;
+        s.ii_lo = (int32_t)nlim1;
+        s.ii_hi = (int32_t)nlim2;
+        s.nlim = (int32_t)nlim;
+        s.flags = flags;
+        P->seg.push_back(s);
+      }
+      if (nlim2 == limout || ilast) {
+        kq += nlim2;
+        nlim1 = 1;
+        nppanl = 0;
+        v1po = v2po + dvout;
+        if ((v1po + double(limout) * dvout) > (v2p - dv)) nppanl = 1;
+      } else {
+        nlim1 = nlim2 + 1;
+        nppanl = -1;
+      }
+      if (ilast) break;
+    }
+    if (ilast) {
+      P->n_out = kq;
+      return LBL_OK;
+    }
+    vft = vft + double(kNlim1 - 1) * dv;
+    if (istop) {
+      *err = "internal: PNLINT did not reach V2";
+      return LBL_E_ARG;
+    }
+  }
+}
+
 }  // namespace lbl

@@ -122,4 +122,31 @@ int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad,
 // JRAD after OPDPTH for this layer (src/lblrtm.f90:6211).
 int next_jrad(const lbl_run& R, const lbl_layer& L, int jrad);
 
+// PNLINT (src/oprop.f90:1564-1806) re-grids each 2400-point PANEL output to
+// DVOUT as the panels stream past.  Which input panel computes an output
+// point decides the point's interpolation coordinate (V1PO and V1P are both
+// accumulated sums), so the host replays the reference's panel loop and
+// hands the kernel one segment per (output panel, input panel) pair: output
+// points ii_lo..ii_hi (1-based within the output panel that starts at
+// global output index k0) are interpolated from input panel p, whose R1(1)
+// is global layer point g0 = 2400*p.
+struct PnlSeg {
+  double v1po;                // V1PO of the output panel
+  double v1p;                 // V1P of the input panel
+  double fj1dif;              // FJ1DIF = (V1PO-V1P)/DVP+1+2
+  int64_t k0;                 // global output index of the output panel's II=1
+  int64_t g0;                 // global layer index of the input panel's R1(1)
+  int32_t ii_lo, ii_hi;       // II range computed during this input panel
+  int32_t nlim;               // NLIM of the input panel before the end pad
+  int32_t flags;              // 1: first input panel, 2: last input panel
+};
+struct PnlPlan {
+  std::vector<PnlSeg> seg;
+  int64_t n_out = 0;          // output points of the layer
+  bool copy = false;          // |DVOUT-DV| < 1e-8: panels pass through
+  double a[4][101];           // Lagrange weights A1..A4 at P = 0.01*JP
+};
+// Plan PNLINT for a layer of spacing dv; dvout must satisfy 0 < dvout <= dv.
+int pnlint_plan(const lbl_run& R, double dv, double dvout, PnlPlan* P, std::string* err);
+
 }  // namespace lbl

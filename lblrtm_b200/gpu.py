@@ -30,6 +30,9 @@ SIGNATURES = {
     "lbl_mtckd_upload": (C.c_int, [C.c_void_p, C.POINTER(abi.Mtckd)]),
     "lbl_dv_rule": (C.c_int, [C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32]),
     "lbl_layer_npts": (C.c_int64, [C.POINTER(abi.Run), C.c_double]),
+    "lbl_pnlint_npts": (C.c_int64, [C.POINTER(abi.Run), C.c_double, C.c_double]),
+    "lbl_pnlint": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.c_double, C.c_double, C.c_void_p,
+                             C.c_int64, C.c_void_p, C.c_int64]),
     "lbl_layer_od": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), P_I32,
                                C.c_void_p, C.c_int64, C.c_int32]),
     "lbl_merge_layer": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer),
@@ -102,6 +105,14 @@ def dv_rule(run, layers):
 
 def layer_npts(run, dv):
     return int(load().lbl_layer_npts(C.byref(run), C.c_double(dv)))
+
+
+def pnlint_npts(run, dv, dvout):
+    """Points of the DVOUT grid PNLINT writes for a layer of spacing dv."""
+    n = int(load().lbl_pnlint_npts(C.byref(run), C.c_double(dv), C.c_double(dvout)))
+    if n < 0:
+        raise LblError(-n, f"pnlint_npts: {abi.STATUS.get(-n, -n)}")
+    return n
 
 
 def brightness_temperature(rad, v1, dv):
@@ -180,6 +191,15 @@ class Context:
         self._check(self.lib.lbl_layer_od(self.h, C.byref(run), C.byref(layer), C.byref(j),
                                           _ptr(od), n, precision), "layer_od")
         return od, j.value
+
+    def pnlint(self, run, dv, dvout, od, out=None):
+        """PNLINT: a layer optical depth (numpy or CUDA tensor) on its own
+        grid re-gridded to DVOUT."""
+        n = pnlint_npts(run, dv, dvout)
+        res = np.zeros(n) if out is None else out
+        self._check(self.lib.lbl_pnlint(self.h, C.byref(run), C.c_double(dv), C.c_double(dvout),
+                                        _ptr(od), len(od), _ptr(res), n), "pnlint")
+        return res
 
     def merge_layer(self, run, layer, first, dv_old, rad_in, tr_in, od):
         n = len(od)

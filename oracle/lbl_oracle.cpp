@@ -1840,6 +1840,170 @@ int64_t npts_of(const lbl_run& R, double dv) {
   }
 }
 
+// ---- PNLINT (src/oprop.f90:1564-1806) -----------------------------------
+// The layer optical depth streamed through PANEL's 2400-point panels
+// (src/oprop.f90:1435-1451, 1524-1555) and re-gridded to DVOUT as PNLINT
+// does: the SAVEd V1PO/NLIM1, the 2400-point output panels (R1OUT), the
+// four cases at label 20, the A1..A4 weights at P=0.01*JP.  R1 here is the
+// panel passed as R1(NLO): R1(-2..0) hold the previous panel's last points
+// (PANEL's shift keeps NSHIFT=32 of them), R1(1..NLIM) the panel, and
+// R1(NLIM+1..NLIM+2) the next panel's first points -- which PNLINT reads
+// only with zero weight (JP=0) except in the last panel, where they are the
+// two padded copies of R1(NLIM).
+struct Pnlint {
+  double DVOUT;
+  double V1PO = 0., V1PO_SAVE = 0.;
+  long NLIM1 = 1;
+  double A1[101], A2[101], A3[101], A4[101];
+  std::vector<double> out;
+  explicit Pnlint(double dvout) : DVOUT(dvout) {
+    for (int JP = 0; JP <= 100; JP++) {
+      double APG = JP, P = 0.01 * APG;
+      A1[JP] = -P * (P - 1.0) * (P - 2.0) / 6.0;
+      A2[JP] = (P * P - 1.0) * (P - 2.0) * 0.5;
+      A3[JP] = -P * (P + 1.0) * (P - 2.0) * 0.5;
+      A4[JP] = P * (P * P - 1.0) / 6.0;
+    }
+  }
+  // One call: R1 points to R1(1) of a buffer valid from R1(-2) to R1(NLIM+2).
+  void call(double* R1, long NLIM, double V1P, double V2P, double DVP, double V2, int ISTOP) {
+    if (V1PO_SAVE != 0.0) V1PO = V1PO_SAVE;
+    int NPPANL = 1;
+    double ATYPE = 9.999E09;
+    if (DVP == DVOUT) ATYPE = 0.;
+    if (DVOUT > DVP) ATYPE = DVP / (DVOUT - DVP) + 0.5;
+    if (DVOUT < DVP) ATYPE = -DVOUT / (DVP - DVOUT) - 0.5;
+    if (std::fabs(DVOUT - DVP) < 1.E-8) ATYPE = 0.;
+    if (ATYPE == 0.) {
+      for (long i = 1; i <= NLIM; i++) out.push_back(R1[i - 1]);
+      V1PO_SAVE = V1PO;
+      return;
+    }
+    auto r1 = [&](long j) -> double& { return R1[j - 1]; };
+    if (V1PO == 0.0) {
+      r1(-1) = r1(1);
+      r1(0) = r1(1);
+      V1PO = V1P;
+      NLIM1 = 1;
+    }
+    if (ISTOP == 1) {
+      r1(NLIM + 1) = r1(NLIM);
+      r1(NLIM + 2) = r1(NLIM);
+      NLIM = NLIM + 2;
+      V2P = V2P + 2. * DVP;
+    }
+    const long LIMOUT = 2400;
+    double R1OUT[2401];
+    int ILAST = 0;
+    double V2PO;
+    long NLIM2;
+    for (;;) {  // label 20
+      V2PO = V1PO + double(LIMOUT) * DVOUT;
+      if (V2P <= V2PO + DVP && ILAST == 0 && NPPANL <= 0) break;
+      if ((V1PO + double(LIMOUT - 1) * DVOUT) > V2) {
+        NLIM2 = fint((V2 - V1PO) / DVOUT + 1.);
+        V2PO = V1PO + double(NLIM2 - 1) * DVOUT;
+        if (V2PO < V2) {
+          V2PO = V2PO + DVOUT;
+          NLIM2 = NLIM2 + 1;
+        }
+        ILAST = 1;
+        if (ISTOP != 1 && V2PO > V2P - DVP) {
+          NLIM2 = fint(((V2P - DVP - V1PO) / DVOUT) + 1.);
+          V2PO = V1PO + double(NLIM2 - 1) * DVOUT;
+          if (V2PO + DVOUT < V2P - DVP) {
+            NLIM2 = NLIM2 + 1;
+            V2PO = V2PO + DVOUT;
+          }
+          ILAST = 0;
+        }
+      } else {
+        NLIM2 = LIMOUT;
+        V2PO = V1PO + double(NLIM2 - 1) * DVOUT;
+        if (V2PO > V2P - DVP) {
+          NLIM2 = fint(((V2P - DVP - V1PO) / DVOUT) + 1.);
+          V2PO = V1PO + double(NLIM2 - 1) * DVOUT;
+          if (V2PO + DVOUT < V2P - DVP) {
+            NLIM2 = NLIM2 + 1;
+            V2PO = V2PO + DVOUT;
+          }
+        }
+        ILAST = 0;
+      }
+      const double RATDV = DVOUT / DVP;
+      const double FJ1DIF = (V1PO - V1P) / DVP + 1. + 2.;
+      for (long II = NLIM1; II <= NLIM2; II++) {  // label 30
+        double FJJ = FJ1DIF + RATDV * double(II - 1);
+        long JJ = fint(FJJ) - 2;
+        long JP = fint((FJJ - double(JJ)) * 100. - 199.5);
+        JP = JP < 0 ? 0 : (JP > 100 ? 100 : JP);
+        R1OUT[II] = A1[JP] * r1(JJ - 1) + A2[JP] * r1(JJ) + A3[JP] * r1(JJ + 1) +
+                    A4[JP] * r1(JJ + 2);
+      }
+      if (NLIM2 == LIMOUT || ILAST == 1) {
+        for (long i = 1; i <= NLIM2; i++) out.push_back(R1OUT[i]);
+        NLIM1 = 1;
+        NPPANL = 0;
+        V1PO = V2PO + DVOUT;
+        if ((V1PO + double(LIMOUT) * DVOUT) > (V2P - DVP)) NPPANL = 1;
+      } else {
+        NLIM1 = NLIM2 + 1;
+        NPPANL = -1;
+      }
+      if (ILAST == 1) break;
+    }
+    if (ILAST == 1) {
+      V1PO = 0.0;
+      NPPANL = 1;
+    }
+    V1PO_SAVE = V1PO;
+  }
+};
+
+// PANEL's panel geometry around PNLINT for a layer OD on V1 + i*DV.
+int pnlint_layer(const lbl_run& R, double DV, double DVOUT, const double* od, int64_t n,
+                 std::vector<double>* res) {
+  if (!(DVOUT > 0.) || !(DV > 0.)) return fail(LBL_E_ARG, "DV and DVOUT must be positive");
+  if (DVOUT > DV && !(std::fabs(DVOUT - DV) < 1.E-8))
+    return fail(LBL_E_ARG, "DVOUT MUST BE < DV");
+  if (npts_of(R, DV) != n) return fail(LBL_E_ARG, "n_in does not match the layer grid");
+  Pnlint S(DVOUT);
+  double VFT = R.v1 - 32. * DV;
+  const long NLO = 33;
+  std::vector<double> buf(2432 + 8);
+  int64_t g0 = 0;
+  for (;;) {
+    long NHI = 2432;
+    int ISTOP = 0;
+    double V2P;
+    if ((VFT + double(NHI - 1) * DV) > R.v2) {
+      NHI = fint((R.v2 - VFT) / DV + 1.);
+      V2P = VFT + double(NHI - 1) * DV;
+      if (V2P < R.v2) {
+        V2P = V2P + DV;
+        NHI = NHI + 1;
+      }
+      ISTOP = 1;
+    } else {
+      V2P = VFT + double(NHI - 1) * DV;
+    }
+    const long NLIM = NHI - NLO + 1;
+    const double V1P = VFT + double(NLO - 1) * DV;
+    // buf[3 + j - 1] = R1(j), j = -2 .. NLIM+2
+    double* R1 = buf.data() + 3;
+    for (long j = -2; j <= NLIM + 2; j++) {
+      int64_t g = g0 + j - 1;
+      R1[j - 1] = (g >= 0 && g < n) ? od[g] : 0.;
+    }
+    S.call(R1, NLIM, V1P, V2P, DV, R.v2, ISTOP);
+    if (ISTOP) break;
+    VFT = VFT + double(2401 - 1) * DV;
+    g0 += 2400;
+  }
+  *res = std::move(S.out);
+  return LBL_OK;
+}
+
 }  // namespace
 
 // =========================================================================
@@ -1913,6 +2077,22 @@ int orc_dv_rule(const lbl_run* R, lbl_layer* Ls, int nlay) {
 }
 
 int64_t orc_layer_npts(const lbl_run* R, double dv) { return npts_of(*R, dv); }
+
+// PNLINT re-grid of a layer optical depth to DVOUT.  *n_out receives the
+// point count; od_out may be NULL to ask for the count only.
+int orc_pnlint(const lbl_run* R, double dv, double dvout, const double* od, int64_t n,
+               double* od_out, int64_t cap, int64_t* n_out) {
+  g_err.clear();
+  std::vector<double> res;
+  int rc = pnlint_layer(*R, dv, dvout, od, n, &res);
+  if (rc) return rc;
+  *n_out = (int64_t)res.size();
+  if (od_out) {
+    if ((int64_t)res.size() > cap) return fail(LBL_E_ARG, "output capacity");
+    std::copy(res.begin(), res.end(), od_out);
+  }
+  return LBL_OK;
+}
 
 int orc_layer_od(const lbl_run* R, const lbl_layer* L, const lbl_lines* lines,
                  const lbl_mtckd* ck, int32_t* jrad, double* od, int64_t npts) {

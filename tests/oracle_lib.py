@@ -123,3 +123,17 @@ def jacobian(run, layers, lines_h, mols, mode, mtckd_h=None):
     check(L.orc_jacobian(C.byref(run), layers, nl, C.byref(lines_h.struct), ck, m, len(mols),
                          int(mode), rad.ctypes.data_as(P), jac.ctypes.data_as(P), C.c_int64(n)))
     return rad, jac
+
+
+def pnlint(run, dv, dvout, od):
+    """PNLINT re-grid of a layer optical depth (oracle restatement)."""
+    L = lib()
+    od = np.ascontiguousarray(od, dtype=np.float64)
+    n = C.c_int64(0)
+    args = [C.byref(run), C.c_double(dv), C.c_double(dvout), od.ctypes.data_as(C.POINTER(C.c_double)),
+            C.c_int64(len(od))]
+    check(L.orc_pnlint(*args, None, C.c_int64(0), C.byref(n)))
+    out = np.zeros(n.value)
+    check(L.orc_pnlint(*args, out.ctypes.data_as(C.POINTER(C.c_double)), C.c_int64(len(out)),
+                       C.byref(n)))
+    return out
