@@ -1859,8 +1859,7 @@ __global__ void k_panel_segs(Work w, const int32_t* panel_layer, const int64_t* 
 // The panel's candidate lines (packed 96-byte records of the layer's
 // accepted lines, in file order) arrive in batches of STAGE by bulk copies
 // into a two-buffer ring: batch b+1 is in flight while the warps add batch
-// b.  Each warp adds a record to the points it owns only where the
-// record's window reaches them.
+// b.  A warp visits only the records whose windows reach its points.
 template <typename T, int STAGE, int MINB>
 __global__ void __launch_bounds__(kPanelThreads, MINB)
     k_panel_od(Work w, DevShapes sh, const int32_t* panel_layer, const int64_t* panel_base,
@@ -1874,11 +1873,6 @@ __global__ void __launch_bounds__(kPanelThreads, MINB)
   const int tid = threadIdx.x, warp = tid >> 5;
   __shared__ __align__(128) NearRec st[2][STAGE];
   __shared__ __align__(8) uint64_t bar[2];
-  struct Meta {
-    uint32_t wm;
-    int32_t lo[3], hi[3];
-  };
-  __shared__ Meta smeta[STAGE];
   __shared__ __align__(16) double s1[kP1 * kPanelThreads];
   __shared__ __align__(16) double s2[kP2 * kPanelThreads];
   __shared__ __align__(16) double s3[kPanelThreads];
@@ -1887,6 +1881,7 @@ __global__ void __launch_bounds__(kPanelThreads, MINB)
   __shared__ long s_n2;
   const int n1p = (int)(R.b1 - R.a1 + 1), n2p = (int)(R.b2 - R.a2 + 1),
             n3p = (int)(R.b3 - R.a3 + 1);
+  const int lane = tid & 31;
   const int64_t clo = rng[2 * gp], chi = rng[2 * gp + 1];
   const NearRec* src = w.n_rec + L.off_near;
   const int nbatch = (int)((chi - clo + STAGE - 1) / STAGE);
@@ -1923,40 +1918,40 @@ __global__ void __launch_bounds__(kPanelThreads, MINB)
     const int64_t c0 = clo + (int64_t)b * STAGE;
     const int n = (int)((chi - c0) < STAGE ? (chi - c0) : STAGE);
     const NearRec* batch = st[b & 1];
-    // one thread per record: its windows clipped to the panel's spans (local
-    // points) and the warps owning points of them, bits 0-7 R1, 8-15 R2,
-    // 16-23 R3
-    if (tid < n) {
-      const NearRec& q = batch[tid];
-      int lo1 = (q.lo1 > R.a1 ? q.lo1 : R.a1) - R.a1, hi1 = (q.hi1 < R.b1 ? q.hi1 : R.b1) - R.a1;
-      int lo2 = (q.lo2 > R.a2 ? q.lo2 : R.a2) - R.a2, hi2 = (q.hi2 < R.b2 ? q.hi2 : R.b2) - R.a2;
-      int lo3 = (q.lo3 > R.a3 ? q.lo3 : R.a3) - R.a3, hi3 = (q.hi3 < R.b3 ? q.hi3 : R.b3) - R.a3;
-      smeta[tid].wm = warps_of(lo1, hi1, n1p) | (warps_of(lo2, hi2, n2p) << 8) |
-                      (warps_of(lo3, hi3, n3p) << 16);
-      smeta[tid].lo[0] = lo1;
-      smeta[tid].hi[0] = hi1;
-      smeta[tid].lo[1] = lo2;
-      smeta[tid].hi[1] = hi2;
-      smeta[tid].lo[2] = lo3;
-      smeta[tid].hi[2] = hi3;
-    }
-    __syncthreads();
-    for (int k = 0; k < n; k++) {
-      const uint32_t wm = smeta[k].wm >> warp;
-      if (!(wm & 0x10101u)) continue;  // none of the line's window points are this warp's
-      const NearRec& q = batch[k];
+    // Thread t owns local points t + 256 j of each grid.  Lane k of every
+    // warp tests record k0+k, one ballot per grid gives the records whose
+    // clipped window reaches the warp's points, and the warp adds those in
+    // file order.
+    for (int k0 = 0; k0 < n; k0 += 32) {
+      const int k = k0 + lane;
+      const NearRec& qk = batch[k < n ? k : 0];
       // R1 (DV grid): F1 + FG + VERFN terms
-      if (wm & 1u)
-        near_add<T, 1>(q, sh, tid, smeta[k].lo[0], smeta[k].hi[0], R.a1 - 2400 * q.pc - 1,
-                       q.zint, s1);
+      unsigned m = __ballot_sync(
+          0xffffffffu, k < n && ((warps_of(qk.lo1 - R.a1, qk.hi1 - R.a1, n1p) >> warp) & 1u));
+      while (m) {
+        const NearRec& q = batch[k0 + __ffs(m) - 1];
+        m &= m - 1;
+        near_add<T, 1>(q, sh, tid, max(q.lo1, R.a1) - R.a1, min(q.hi1, R.b1) - R.a1,
+                       R.a1 - 2400 * q.pc - 1, q.zint, s1);
+      }
       // R2 (4 DV): F2
-      if (wm & 0x100u)
-        near_add<T, 2>(q, sh, tid, smeta[k].lo[1], smeta[k].hi[1], R.a2 - 600 * q.pc - 1,
-                       q.zint * L.conf2, s2);
+      m = __ballot_sync(
+          0xffffffffu, k < n && ((warps_of(qk.lo2 - R.a2, qk.hi2 - R.a2, n2p) >> warp) & 1u));
+      while (m) {
+        const NearRec& q = batch[k0 + __ffs(m) - 1];
+        m &= m - 1;
+        near_add<T, 2>(q, sh, tid, max(q.lo2, R.a2) - R.a2, min(q.hi2, R.b2) - R.a2,
+                       R.a2 - 600 * q.pc - 1, q.zint * L.conf2, s2);
+      }
       // R3 (16 DV): F3
-      if (wm & 0x10000u)
-        near_add<T, 3>(q, sh, tid, smeta[k].lo[2], smeta[k].hi[2], R.a3 - 150 * q.pc - 1,
-                       q.zint * L.conf3, s3);
+      m = __ballot_sync(
+          0xffffffffu, k < n && ((warps_of(qk.lo3 - R.a3, qk.hi3 - R.a3, n3p) >> warp) & 1u));
+      while (m) {
+        const NearRec& q = batch[k0 + __ffs(m) - 1];
+        m &= m - 1;
+        near_add<T, 3>(q, sh, tid, max(q.lo3, R.a3) - R.a3, min(q.hi3, R.b3) - R.a3,
+                       R.a3 - 150 * q.pc - 1, q.zint * L.conf3, s3);
+      }
     }
     __syncthreads();
   }
