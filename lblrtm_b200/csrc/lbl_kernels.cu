@@ -690,61 +690,37 @@ constexpr int kFwSmem = 2 * (int)kR4Stride * (int)sizeof(double);  // two R4 buf
 constexpr int fw_smem32(int adders) {
   return kFwSmem + ((kLimOut + adders - 1) / adders) * adders * (int)sizeof(float);
 }
-constexpr int kFwBatch = 4;  // lines the deciding warp evaluates together
-
-// Sum, in list order, of both sides of lines cl[idx(0..n-1)] at point jj
-// into acc, where a line counts only if use(k) holds.
-template <typename Idx, typename Use>
-__device__ __forceinline__ void f4_sum_lines(const F4Line* cl, int n, Idx idx, Use use, int jj,
-                                             double dvr4, double rbndsq, double& acc) {
-  for (int a = 0; a < n; a += kFwBatch) {
-    double f[kFwBatch], g[kFwBatch];
-    int img = 0;
-#pragma unroll
-    for (int u = 0; u < kFwBatch; u++) {
-      const int k = idx(a + u < n ? a + u : n - 1);
-      const F4Line& q = cl[k];
-      const bool on = a + u < n && use(k);
-      f[u] = on ? f4_side(q, false, jj, dvr4, rbndsq) : 0.;
-      img |= on ? (q.has & 2) : 0;
-      g[u] = 0.;
-    }
-    if (__any_sync(__activemask(), img)) {
-#pragma unroll
-      for (int u = 0; u < kFwBatch; u++) {
-        const int k = idx(a + u < n ? a + u : n - 1);
-        const bool on = a + u < n && use(k);
-        g[u] = on ? f4_side(cl[k], true, jj, dvr4, rbndsq) : 0.;
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kFwBatch; u++) {
-      acc += f[u];
-      acc += g[u];
-    }
-  }
+// Barrier of the DEC deciding warps only (named barrier 1); the adders never
+// take part in it.
+template <int DEC>
+__device__ __forceinline__ void fw_dec_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"(DEC * 32) : "memory");
 }
 
 // The CTA works in phases separated by one barrier.  In phase t the deciding
-// warp takes chunk t (32 consecutive lines of the layer's shrunk list) and
-// decides every line exactly as CONVF4's in-order test against the partial
+// warps take chunk t (32 consecutive lines of the layer's shrunk list) and
+// decide every line exactly as CONVF4's in-order test against the partial
 // R4 at its point JJ, where that partial R4 is
 //     R4 through chunk t-2   (buffer written in phase t-1)
 //   + chunk t-1's accepted lines, evaluated at JJ directly
 //   + the earlier accepted lines of chunk t, evaluated at JJ directly;
 // meanwhile the adders evaluate chunk t-1's accepted lines over the whole
-// window and write R4 through chunk t-1 into the other buffer.  The in-chunk
-// order dependence is resolved speculatively: every line is first decided
-// against the lines accepted on their own partial R4 alone; the lowest line
-// whose decision differs from that guess is exact, so the guess is corrected
-// there and the lines above it re-decided, until no line differs.
+// window and write R4 through chunk t-1 into the other buffer.  The deciding
+// warps split the direct evaluations (up to 32 x 32 line-point pairs for each
+// of the two chunks) among themselves; warp 0 then sums each line's terms in
+// CONVF4's order.  The in-chunk order dependence is resolved speculatively:
+// every line is first decided against the lines accepted on their own
+// partial R4 alone; the lowest line whose decision differs from that guess is
+// exact, so the guess is corrected there and the lines above it re-decided,
+// until no line differs.
 //
-// ADDERS (224, 352 or 480) sets the CTA's width; the autotuner picks it.
-template <typename T, int ADDERS, int MINB>
-__global__ void __launch_bounds__(ADDERS + 32, MINB)
+// ADDERS and DEC (deciding warps) set the CTA's width; the autotuner picks
+// among the variants.
+template <typename T, int ADDERS, int DEC, int MINB>
+__global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
     k_far_wing(Work w, const int32_t* win_order, const int32_t* win_layer) {
   constexpr int kFwAdders = ADDERS;
-  constexpr int kFwThreads = ADDERS + 32;
+  constexpr int kFwThreads = ADDERS + 32 * DEC;
   constexpr int kFwPts = (kLimOut + ADDERS - 1) / ADDERS;  // window points per adder
   extern __shared__ double fw_r4[];  // [2][kR4Stride]
   __shared__ F4Line cl[2][kChunk];
@@ -752,6 +728,11 @@ __global__ void __launch_bounds__(ADDERS + 32, MINB)
   __shared__ int s_live[kChunk];
   __shared__ int s_nacc[2];
   __shared__ int s_state[2];  // by phase parity: a chunk was decided
+  __shared__ double s_x[kChunk][kChunk];  // chunk t-1's lines at chunk t's points
+  __shared__ double s_y[kChunk][kChunk];  // chunk t at its own points (line; image)
+  __shared__ int s_jj[kChunk];
+  __shared__ int s_go, s_nval;
+  __shared__ unsigned s_lm;
   const int gw = win_order[blockIdx.x];
   const int l = win_layer[gw];
   const LayerDev& L = w.L[l];
@@ -805,148 +786,205 @@ __global__ void __launch_bounds__(ADDERS + 32, MINB)
   for (int ph = 0;; ph++) {
     const double* R4r = fw_r4 + rb * kR4Stride;
     double* R4w = fw_r4 + (rb ^ 1) * kR4Stride;
-    if (warp == 0) {
-      int decided = 0;
-      if (dmore) {
-        const int nb = prv ^ 1;
-        const int64_t i = c0 + lane;
-        bool ok = false;
-        double speak = 0., r = 0., vnu = 0., spp = 0.;
-        int jj = 1, has = 0;
-        F4Line& p = cl[nb][lane];  // built in place in shared memory
-        p.has = 0;
-        if (i < b1) {
-          const double recpi = 1. / (2. * asin(1.));
-          const double zsq = 64. * 64.;
-          const double A3 = (1. + 2. * zsq) / ((1. + zsq) * (1. + zsq));
-          const double B3 = -1. / ((1. + zsq) * (1. + zsq));
-          const double sp = n_sp;
-          spp = n_spp;
-          ok = !(sp == 0. && spp == 0.);
-          const double ad = n_ad, al = n_al, v = n_v;
-          const double zeta = al / (al + ad);
-          long iz = fint(100. * zeta + kONEPL);
-          iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);  // zeta in [0,1]; guards bad input
-          const double zd = 100. * zeta - double(iz - 1);
-          const double alfav =
-              (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (al + ad);
-          const double ralfv = 1. / alfav;
-          const double sil = sp * recpi * al;
-          const double siv = (al * ralfv) * sp * recpi * ralfv;
-          speak = A3 * fabs(siv);
-          long jjl = fint((v - W.v1r4) / dvr4 + 1.);
-          jjl = jjl < 1 ? 1 : (jjl > npt ? npt : jjl);
-          jj = (int)jjl;
-          vnu = v;
-          const double dptrat = spp != 0. ? spp / (sp * alfav) : 0.;
-          p.xnui = v - W.v1r4;
-          p.sil = sil;
-          p.siv_a3 = siv * A3;
-          p.siv_b3 = siv * B3;
-          p.alfl2 = al * al;
-          p.rvi2 = 1. / (alfav * alfav);
-          p.f4bnd = sil / (al * al + bndsq);
-          p.dptrat = dptrat;
-          p.co2 = n_co2;
-          const long jmin = fint((p.xnui - bnd) / dvr4 + 2.);
-          const long jmax = fint((p.xnui + bnd) / dvr4 + 1.);
-          const bool beyond = jmin > npt;  // GO TO 60: no wing, no image
-          p.jmin = (int)(jmin < 1 ? 1 : jmin);
-          p.jmax = (int)(jmax > npt ? npt : jmax);
-          if (beyond || p.jmax < p.jmin) p.jmin = 1, p.jmax = 0;
-          else p.has |= 1;
-          p.mxnui = -v - W.v1r4;
-          p.mdptrat = -dptrat;
-          p.mjmin = 1;
-          p.mjmax = 0;
-          if (!beyond && v > 0. && v <= 25.) {  // Van Vleck-Weisskopf image (:4014-4024)
-            const long mjmin = fint((p.mxnui - bnd) / dvr4 + 2.);
-            const long mjmax = fint((p.mxnui + bnd) / dvr4 + 1.);
-            if (mjmin <= npt && (mjmax > npt ? npt : mjmax) >= (mjmin < 1 ? 1 : mjmin)) {
-              p.mjmin = (int)(mjmin < 1 ? 1 : mjmin);
-              p.mjmax = (int)(mjmax > npt ? npt : mjmax);
-              p.has |= 2;
+    if (warp < DEC) {
+      // Stage 1: warp 0 builds chunk t's lines (one per lane, shared memory
+      // cl[nb]) from the raw values prefetched in the previous phase.
+      const int nb = prv ^ 1;
+      bool ok = false;
+      double speak = 0., r = 0., vnu = 0., spp = 0.;
+      int jj = 1, has = 0;
+      if (warp == 0) {
+        if (dmore) {
+          const int64_t i = c0 + lane;
+          F4Line& p = cl[nb][lane];  // built in place in shared memory
+          p.has = 0;
+          if (i < b1) {
+            const double recpi = 1. / (2. * asin(1.));
+            const double zsq = 64. * 64.;
+            const double A3 = (1. + 2. * zsq) / ((1. + zsq) * (1. + zsq));
+            const double B3 = -1. / ((1. + zsq) * (1. + zsq));
+            const double sp = n_sp;
+            spp = n_spp;
+            ok = !(sp == 0. && spp == 0.);
+            const double ad = n_ad, al = n_al, v = n_v;
+            const double zeta = al / (al + ad);
+            long iz = fint(100. * zeta + kONEPL);
+            iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);  // zeta in [0,1]; guards bad input
+            const double zd = 100. * zeta - double(iz - 1);
+            const double alfav =
+                (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (al + ad);
+            const double ralfv = 1. / alfav;
+            const double sil = sp * recpi * al;
+            const double siv = (al * ralfv) * sp * recpi * ralfv;
+            speak = A3 * fabs(siv);
+            long jjl = fint((v - W.v1r4) / dvr4 + 1.);
+            jjl = jjl < 1 ? 1 : (jjl > npt ? npt : jjl);
+            jj = (int)jjl;
+            vnu = v;
+            const double dptrat = spp != 0. ? spp / (sp * alfav) : 0.;
+            p.xnui = v - W.v1r4;
+            p.sil = sil;
+            p.siv_a3 = siv * A3;
+            p.siv_b3 = siv * B3;
+            p.alfl2 = al * al;
+            p.rvi2 = 1. / (alfav * alfav);
+            p.f4bnd = sil / (al * al + bndsq);
+            p.dptrat = dptrat;
+            p.co2 = n_co2;
+            const long jmin = fint((p.xnui - bnd) / dvr4 + 2.);
+            const long jmax = fint((p.xnui + bnd) / dvr4 + 1.);
+            const bool beyond = jmin > npt;  // GO TO 60: no wing, no image
+            p.jmin = (int)(jmin < 1 ? 1 : jmin);
+            p.jmax = (int)(jmax > npt ? npt : jmax);
+            if (beyond || p.jmax < p.jmin) p.jmin = 1, p.jmax = 0;
+            else p.has |= 1;
+            p.mxnui = -v - W.v1r4;
+            p.mdptrat = -dptrat;
+            p.mjmin = 1;
+            p.mjmax = 0;
+            if (!beyond && v > 0. && v <= 25.) {  // Van Vleck-Weisskopf image (:4014-4024)
+              const long mjmin = fint((p.mxnui - bnd) / dvr4 + 2.);
+              const long mjmax = fint((p.mxnui + bnd) / dvr4 + 1.);
+              if (mjmin <= npt && (mjmax > npt ? npt : mjmax) >= (mjmin < 1 ? 1 : mjmin)) {
+                p.mjmin = (int)(mjmin < 1 ? 1 : mjmin);
+                p.mjmax = (int)(mjmax > npt ? npt : mjmax);
+                p.has |= 2;
+              }
             }
-          }
-          has = p.has;
-          if constexpr (sizeof(T) == 4) {
-            p.sil32 = (float)p.sil;
-            p.sa3_32 = (float)p.siv_a3;
-            p.sb3_32 = (float)p.siv_b3;
-            p.alfl2_32 = (float)p.alfl2;
-            p.rvi2_32 = (float)p.rvi2;
-            p.f4bnd32 = (float)p.f4bnd;
-            p.rdd32 = (float)(p.f4bnd * rbndsq);
-            const double rdv = 1. / dvr4;
-#pragma unroll
-            for (int m = 0; m < 2; m++) {
-              if (!(has & (1 << m))) continue;
-              F4Side32& sd = p.s32[m];
-              const double xn = m ? p.mxnui : p.xnui;
-              const double jc = floor(xn * rdv + 1.5);
-              const double dl = xn - (jc - 1.) * dvr4;
-              const double tp = (bnd + dl) * rdv, tm = (bnd - dl) * rdv;
-              const double mp = floor(tp), mm = floor(tm);
-              sd.jc = (int32_t)jc;
-              sd.dlt = (float)dl;
-              sd.php = (float)(tp - mp);
-              sd.phm = (float)(tm - mm);
-              sd.mpf = (float)mp;
-              sd.mmf = (float)mm;
-              sd.dptrat = (float)(m ? p.mdptrat : p.dptrat);
+            has = p.has;
+            if constexpr (sizeof(T) == 4) {
+              p.sil32 = (float)p.sil;
+              p.sa3_32 = (float)p.siv_a3;
+              p.sb3_32 = (float)p.siv_b3;
+              p.alfl2_32 = (float)p.alfl2;
+              p.rvi2_32 = (float)p.rvi2;
+              p.f4bnd32 = (float)p.f4bnd;
+              p.rdd32 = (float)(p.f4bnd * rbndsq);
+              const double rdv = 1. / dvr4;
+  #pragma unroll
+              for (int m = 0; m < 2; m++) {
+                if (!(has & (1 << m))) continue;
+                F4Side32& sd = p.s32[m];
+                const double xn = m ? p.mxnui : p.xnui;
+                const double jc = floor(xn * rdv + 1.5);
+                const double dl = xn - (jc - 1.) * dvr4;
+                const double tp = (bnd + dl) * rdv, tm = (bnd - dl) * rdv;
+                const double mp = floor(tp), mm = floor(tm);
+                sd.jc = (int32_t)jc;
+                sd.dlt = (float)dl;
+                sd.php = (float)(tp - mp);
+                sd.phm = (float)(tm - mm);
+                sd.mpf = (float)mp;
+                sd.mmf = (float)mm;
+                sd.dptrat = (float)(m ? p.mdptrat : p.dptrat);
+              }
             }
+            if (ok) r = R4r[jj];
           }
-          if (ok) r = R4r[jj];
+          s_jj[lane] = jj;
         }
-        __syncwarp();
-        // chunk t-1's accepted lines, not yet in the R4 buffer
-        const int np = have_prev ? s_nacc[prv] : 0;
-        f4_sum_lines(
-            cl[prv], np, [&](int a) { return s_idx[prv][a]; }, [&](int) { return ok; }, jj, dvr4,
-            rbndsq, r);
-        const double dptmn = W.dptmn, dptfc = L.dptfc;
-        bool live = ok && !(speak <= (dptmn + dptfc * r) && spp == 0.);
-        const unsigned lm = __ballot_sync(full, live);
-        // earlier lines of this chunk accepted on their own partial R4
-        if (live) s_live[__popc(lm & ((1u << lane) - 1u))] = lane;
-        __syncwarp();
-        double part = r;  // continues the running sum in CONVF4's order
-        f4_sum_lines(
-            cl[nb], __popc(lm), [&](int a) { return s_live[a]; },
-            [&](int k) { return ok && k < lane; }, jj, dvr4, rbndsq, part);
-        bool acc = ok && !(speak <= (dptmn + dptfc * part) && spp == 0.);
-        unsigned mis = __ballot_sync(full, acc != live);
-        while (mis) {
-          const int f = __ffs(mis) - 1;  // every line below f is decided exactly
-          const bool af = __shfl_sync(full, acc, f);
-          if (ok && lane > f) {
-            const double v = f4_side(cl[nb][f], false, jj, dvr4, rbndsq) +
-                             f4_side(cl[nb][f], true, jj, dvr4, rbndsq);
-            part += af ? v : -v;
-            acc = !(speak <= (dptmn + dptfc * part) && spp == 0.);
-          }
-          if (lane == f) live = acc;
-          mis = __ballot_sync(full, acc != live) & ~((2u << f) - 1u);
-        }
-        // the first accepted line at or beyond VNULST ends the window (:3928, IHI=-1)
-        const unsigned tm = __ballot_sync(full, acc && vnu >= W.vnulst);
-        const int lim = tm ? __ffs(tm) - 1 : kChunk;
-        const unsigned am = __ballot_sync(full, acc && has != 0 && lane < lim);
-        if ((am >> lane) & 1u) s_idx[nb][__popc(am & ((1u << lane) - 1u))] = lane;
-        if (lane == 0) s_nacc[nb] = __popc(am);
-        decided = 1;
-        if (tm) {
-          dmore = false;
-        } else {
-          c0 += kChunk;
-          if (c0 >= b1) dmore = next_block();
-          prefetch();
+        if (lane == 0) {
+          s_go = dmore ? 1 : 0;
+          s_nval = dmore ? (int)((b1 - c0) < kChunk ? (b1 - c0) : kChunk) : 0;
         }
       }
-      if (lane == 0) s_state[ph & 1] = decided;
+      fw_dec_sync<DEC>();
+      // Stage 2: the decider warps evaluate chunk t-1's accepted lines at
+      // every line's point JJ (s_x; their Van Vleck-Weisskopf images, rare,
+      // are evaluated in stage 3).
+      if (s_go) {
+        const int jjb = s_jj[lane];
+        const int np = have_prev ? s_nacc[prv] : 0;
+        for (int a = warp; a < np; a += DEC)
+          s_x[a][lane] = f4_side(cl[prv][s_idx[prv][a]], false, jjb, dvr4, rbndsq);
+      }
+      fw_dec_sync<DEC>();
+      // Stage 3: warp 0 completes each line's partial R4 through chunk t-1
+      // in CONVF4's order and guesses the lines accepted on it alone (live).
+      bool live = false;
+      const double dptmn = W.dptmn, dptfc = L.dptfc;
+      if (warp == 0 && dmore) {
+        const int np = have_prev ? s_nacc[prv] : 0;
+        if (ok) {
+          for (int a = 0; a < np; a++) {
+            const F4Line& q = cl[prv][s_idx[prv][a]];
+            r += s_x[a][lane];
+            r += (q.has & 2) ? f4_side(q, true, jj, dvr4, rbndsq) : 0.;
+          }
+        }
+        live = ok && !(speak <= (dptmn + dptfc * r) && spp == 0.);
+        const unsigned lm = __ballot_sync(full, live);
+        if (lane == 0) s_lm = lm;
+      }
+      fw_dec_sync<DEC>();
+      // Stage 4: the decider warps evaluate the live lines of chunk t at the
+      // points of the lines above them (s_y[a][b]: line a at b's point; its
+      // image at s_y[b][a]), the live lines shared out in turn.
+      if (s_go) {
+        const int jjb = s_jj[lane];
+        const int nv = s_nval;
+        int k = 0;
+        for (unsigned m = s_lm; m; m &= m - 1, k++) {
+          const int a = __ffs(m) - 1;
+          if (k % DEC != warp) continue;
+          if (lane > a && lane < nv) {
+            const F4Line& q = cl[nb][a];
+            s_y[a][lane] = f4_side(q, false, jjb, dvr4, rbndsq);
+            s_y[lane][a] = f4_side(q, true, jjb, dvr4, rbndsq);
+          }
+        }
+      }
+      fw_dec_sync<DEC>();
+      // Stage 5: warp 0 decides chunk t.
+      if (warp == 0) {
+        int decided = 0;
+        if (dmore) {
+          const unsigned lm = s_lm;
+          // earlier lines of this chunk accepted on their own partial R4
+          double part = r;  // continues the running sum in CONVF4's order
+          if (ok) {
+            for (unsigned m = lm & ((1u << lane) - 1u); m; m &= m - 1) {
+              const int a = __ffs(m) - 1;
+              part += s_y[a][lane];
+              part += s_y[lane][a];
+            }
+          }
+          bool acc = ok && !(speak <= (dptmn + dptfc * part) && spp == 0.);
+          unsigned mis = __ballot_sync(full, acc != live);
+          while (mis) {
+            const int f = __ffs(mis) - 1;  // every line below f is decided exactly
+            const bool af = __shfl_sync(full, acc, f);
+            if (ok && lane > f) {
+              const double v = ((lm >> f) & 1u)
+                                   ? s_y[f][lane] + s_y[lane][f]
+                                   : f4_side(cl[nb][f], false, jj, dvr4, rbndsq) +
+                                         f4_side(cl[nb][f], true, jj, dvr4, rbndsq);
+              part += af ? v : -v;
+              acc = !(speak <= (dptmn + dptfc * part) && spp == 0.);
+            }
+            if (lane == f) live = acc;
+            mis = __ballot_sync(full, acc != live) & ~((2u << f) - 1u);
+          }
+          // the first accepted line at or beyond VNULST ends the window (:3928, IHI=-1)
+          const unsigned tm = __ballot_sync(full, acc && vnu >= W.vnulst);
+          const int lim = tm ? __ffs(tm) - 1 : kChunk;
+          const unsigned am = __ballot_sync(full, acc && has != 0 && lane < lim);
+          if ((am >> lane) & 1u) s_idx[nb][__popc(am & ((1u << lane) - 1u))] = lane;
+          if (lane == 0) s_nacc[nb] = __popc(am);
+          decided = 1;
+          if (tm) {
+            dmore = false;
+          } else {
+            c0 += kChunk;
+            if (c0 >= b1) dmore = next_block();
+            prefetch();
+          }
+        }
+        if (lane == 0) s_state[ph & 1] = decided;
+      }
     } else if (have_prev) {
       // adders: chunk t-1's accepted lines over the whole window
-      const int ad = (int)threadIdx.x - 32;
+      const int ad = (int)threadIdx.x - 32 * DEC;
       const int na = s_nacc[prv];
       if constexpr (sizeof(T) == 8) {
         // FP64: each point summed in shared memory line by line, line
@@ -2526,24 +2564,23 @@ __global__ void k_jac_diff(double* plus, const double* minus, int64_t n, double 
 
 }  // namespace
 
-template <int ADDERS, int MINB>
+template <int ADDERS, int DEC, int MINB>
 void far_wing_attributes() {
   const cudaFuncAttribute c = cudaFuncAttributePreferredSharedMemoryCarveout;
-  cudaFuncSetAttribute(k_far_wing<double, ADDERS, MINB>,
+  cudaFuncSetAttribute(k_far_wing<double, ADDERS, DEC, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, kFwSmem);
-  cudaFuncSetAttribute(k_far_wing<float, ADDERS, MINB>,
+  cudaFuncSetAttribute(k_far_wing<float, ADDERS, DEC, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, fw_smem32(ADDERS));
-  cudaFuncSetAttribute(k_far_wing<double, ADDERS, MINB>, c, cudaSharedmemCarveoutMaxShared);
-  cudaFuncSetAttribute(k_far_wing<float, ADDERS, MINB>, c, cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_far_wing<double, ADDERS, DEC, MINB>, c, cudaSharedmemCarveoutMaxShared);
+  cudaFuncSetAttribute(k_far_wing<float, ADDERS, DEC, MINB>, c, cudaSharedmemCarveoutMaxShared);
 }
 
 void init_kernel_attributes() {
-  // two R4 buffers per CTA; the largest carveout lets several CTAs share an SM
   // two R4 buffers per CTA (plus the FP32 accumulators of split precision);
-  // the largest carveout lets several CTAs share an SM
-  far_wing_attributes<224, 3>();
-  far_wing_attributes<352, 2>();
-  far_wing_attributes<480, 1>();
+  // the largest carveout lets three CTAs share an SM
+  far_wing_attributes<192, 2, 3>();
+  far_wing_attributes<224, 1, 3>();
+  far_wing_attributes<160, 3, 3>();
   cudaFuncSetAttribute(k_near_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kNearWalkSmemMax);
   {
@@ -2589,24 +2626,30 @@ cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_b
   return cudaGetLastError();
 }
 
-template <int ADDERS, int MINB>
+template <int ADDERS, int DEC, int MINB>
 void launch_far_wing_v(const Work& w, int32_t nwin_total, const int32_t* win_order,
                        const int32_t* win_layer, int precision, cudaStream_t s) {
+  constexpr int threads = ADDERS + 32 * DEC;
   if (precision == LBL_PREC_SPLIT)
-    k_far_wing<float, ADDERS, MINB><<<nwin_total, ADDERS + 32, fw_smem32(ADDERS), s>>>(
+    k_far_wing<float, ADDERS, DEC, MINB><<<nwin_total, threads, fw_smem32(ADDERS), s>>>(
         w, win_order, win_layer);
   else
-    k_far_wing<double, ADDERS, MINB><<<nwin_total, ADDERS + 32, kFwSmem, s>>>(w, win_order,
-                                                                               win_layer);
+    k_far_wing<double, ADDERS, DEC, MINB><<<nwin_total, threads, kFwSmem, s>>>(w, win_order,
+                                                                                win_layer);
 }
 
+// Far-wing variants (adders, deciding warps, CTAs per SM): (192, 2, 3),
+// (224, 1, 3), (160, 3, 3).
 cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
                             const int32_t* win_layer, int precision, int variant,
                             cudaStream_t s) {
   if (nwin_total <= 0) return cudaSuccess;
-  if (variant == 1) launch_far_wing_v<352, 2>(w, nwin_total, win_order, win_layer, precision, s);
-  else if (variant == 2) launch_far_wing_v<480, 1>(w, nwin_total, win_order, win_layer, precision, s);
-  else launch_far_wing_v<224, 3>(w, nwin_total, win_order, win_layer, precision, s);
+  if (variant == 1)
+    launch_far_wing_v<224, 1, 3>(w, nwin_total, win_order, win_layer, precision, s);
+  else if (variant == 2)
+    launch_far_wing_v<160, 3, 3>(w, nwin_total, win_order, win_layer, precision, s);
+  else
+    launch_far_wing_v<192, 2, 3>(w, nwin_total, win_order, win_layer, precision, s);
   return cudaGetLastError();
 }
 
