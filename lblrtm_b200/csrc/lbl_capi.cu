@@ -736,8 +736,8 @@ int tune_panels(lbl_ctx* ctx, Batch& B, int precision) {
 
 int tune_far(lbl_ctx* ctx, Batch& B, int precision) {
   static const char* names[2][kFarVariants] = {
-      {"tune_far_a192_d2", "tune_far_a224_d1", "tune_far_a160_d3"},
-      {"tune_far32_a192_d2", "tune_far32_a224_d1", "tune_far32_a160_d3"}};
+      {"tune_far_a160_d3", "tune_far_a128_d4", "tune_far_a192_d2"},
+      {"tune_far32_a160_d3", "tune_far32_a128_d4", "tune_far32_a192_d2"}};
   const int pk = precision == LBL_PREC_SPLIT ? 1 : 0;
   return tune(ctx, kFarVariants, "LBL_FAR_VARIANT", names[pk],
               [&](int v) {

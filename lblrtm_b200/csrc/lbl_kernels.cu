@@ -2578,9 +2578,9 @@ void far_wing_attributes() {
 void init_kernel_attributes() {
   // two R4 buffers per CTA (plus the FP32 accumulators of split precision);
   // the largest carveout lets three CTAs share an SM
-  far_wing_attributes<192, 2, 3>();
-  far_wing_attributes<224, 1, 3>();
   far_wing_attributes<160, 3, 3>();
+  far_wing_attributes<128, 4, 3>();
+  far_wing_attributes<192, 2, 3>();
   cudaFuncSetAttribute(k_near_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kNearWalkSmemMax);
   {
@@ -2638,18 +2638,18 @@ void launch_far_wing_v(const Work& w, int32_t nwin_total, const int32_t* win_ord
                                                                                 win_layer);
 }
 
-// Far-wing variants (adders, deciding warps, CTAs per SM): (192, 2, 3),
-// (224, 1, 3), (160, 3, 3).
+// Far-wing variants (adders, deciding warps, CTAs per SM): (160, 3, 3),
+// (128, 4, 3), (192, 2, 3).
 cudaError_t launch_far_wing(const Work& w, int32_t nwin_total, const int32_t* win_order,
                             const int32_t* win_layer, int precision, int variant,
                             cudaStream_t s) {
   if (nwin_total <= 0) return cudaSuccess;
   if (variant == 1)
-    launch_far_wing_v<224, 1, 3>(w, nwin_total, win_order, win_layer, precision, s);
+    launch_far_wing_v<128, 4, 3>(w, nwin_total, win_order, win_layer, precision, s);
   else if (variant == 2)
-    launch_far_wing_v<160, 3, 3>(w, nwin_total, win_order, win_layer, precision, s);
-  else
     launch_far_wing_v<192, 2, 3>(w, nwin_total, win_order, win_layer, precision, s);
+  else
+    launch_far_wing_v<160, 3, 3>(w, nwin_total, win_order, win_layer, precision, s);
   return cudaGetLastError();
 }
 
