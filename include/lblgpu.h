@@ -74,7 +74,8 @@ typedef struct lbl_run {
                        2: as 1 but BOUND4=5 cm-1 when PAVE<=0.5 mb
                        (src/lblrtm.f90:6246-6247) */
   int32_t icntnm;   /* 0: no continuum; 1: MT_CKD-style H2O self+foreign
-                       (table from lbl_mtckd_upload) */
+                       (table from lbl_mtckd_upload) and Rayleigh
+                       extinction (see xrayl) */
   int32_t iemit;    /* 0: optical depth only (ABINIT/ABSMRG);
                        1: radiance and transmittance (EMINIT/RADMRG) */
   int32_t ipathl;   /* 1: upwelling (looking down, surface first); only 1 */
@@ -91,6 +92,9 @@ typedef struct lbl_run {
   double xfrgn;
   double tmpbnd;    /* boundary temperature TMPBND, K (record 1.4) */
   double bndemi;    /* boundary emissivity BNDEMI(1); BNDEMI(2:3)=0 */
+  double xrayl;     /* Rayleigh scale XRAYL, /CNTSCL/ (default 1, 0 = off):
+                       with ICNTNM=1 and V2 >= 820 cm-1 the continuum adds
+                       Rayleigh extinction (src/contnm.f90:955-976) */
 } lbl_run;
 
 /* One layer: the /FILHDR/ quantities OPDPTH and XMERGE read

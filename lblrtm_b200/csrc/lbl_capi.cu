@@ -798,7 +798,7 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   CK(cudaEventRecord(ctx->cev[0], s));
   CK(cudaStreamWaitEvent(s2, ctx->cev[0], 0));
   CK(launch_near_lines(w, ctx->dl, max_near, s2));
-  if (R.icntnm) CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, s2));
+  if (R.icntnm) CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, R.xrayl, s2));
   CK(launch_panel_segs(w, B.npanel_total, B.d_panel_layer, B.d_panel_base, B.d_panel_segs,
                        B.d_panel_nseg, s2));
   CK(cudaEventRecord(ctx->cev[1], s2));

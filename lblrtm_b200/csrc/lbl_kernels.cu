@@ -725,7 +725,6 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
   extern __shared__ double fw_r4[];  // [2][kR4Stride]
   __shared__ F4Line cl[2][kChunk];
   __shared__ int s_idx[2][kChunk];
-  __shared__ int s_live[kChunk];
   __shared__ int s_nacc[2];
   __shared__ int s_state[2];  // by phase parity: a chunk was decided
   __shared__ double s_x[kChunk][kChunk];  // chunk t-1's lines at chunk t's points
@@ -1516,15 +1515,10 @@ __device__ int64_t lower_bound_d(const double* v, int64_t lo, int64_t hi, double
 // Continuum: mt_ckd_h2o_absco + CONTNM (mt_ckd_h2o_module.f90:68-174,
 // contnm.f90:279-311), one CTA per layer onto the 1 cm-1 ABSRB grid.
 // =========================================================================
-__global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn) {
-  const int l = blockIdx.x;
-  const LayerDev& L = w.L[l];
-  double* absrb = w.absrb + L.off_abs;  // 1-based, nptabs+4
-  for (int64_t j = threadIdx.x; j < L.nptabs + 8; j += blockDim.x) absrb[j] = 0.;
-  if (!L.icntnm) return;
-  __syncthreads();
-  const double h2o_fac = L.h2o_fac;  // WK(1)/WTOT of CONTNM (contnm.f90:261)
-  if (!((L.v2 > -20.0) && (L.v1 < 20000.) && ((xself > 0.) || (xfrgn > 0)))) return;
+// The H2O self and foreign part of CONTNM (mt_ckd_h2o_absco onto the 1 cm-1
+// grid, src/contnm.f90:199-324), assigned to ABSRB.
+__device__ void h2o_part(const LayerDev& L, const DevMtckd& ck, double h2o_fac, double* absrb,
+                         double xself, double xfrgn) {
   const double wv1 = L.v1abs, wv2 = L.v2abs, dva = L.dvabs;
   auto wvn = [&](int64_t i) { return ck.v0 + ck.dv * double(i - 1); };
   __shared__ int64_t s_i1, s_i2;
@@ -1590,6 +1584,36 @@ __global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn) {
     double cf = -coef(J - 1, false) * b1 + coef(J, false) * (1. - C + b2) +
                 coef(J + 1, false) * (C + b1) - coef(J + 2, false) * b2;
     absrb[I] = L.wk[1] * cs * xself + L.wk[1] * cf * xfrgn;
+  }
+}
+
+__global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn, double xrayl) {
+  const int l = blockIdx.x;
+  const LayerDev& L = w.L[l];
+  double* absrb = w.absrb + L.off_abs;  // 1-based, nptabs+4
+  for (int64_t j = threadIdx.x; j < L.nptabs + 8; j += blockDim.x) absrb[j] = 0.;
+  if (!L.icntnm) return;
+  __syncthreads();
+  const double h2o_fac = L.h2o_fac;  // WK(1)/WTOT of CONTNM (contnm.f90:261)
+  if ((L.v2 > -20.0) && (L.v1 < 20000.) && ((xself > 0.) || (xfrgn > 0)))
+    h2o_part(L, ck, h2o_fac, absrb, xself, xfrgn);
+  // Rayleigh extinction (src/contnm.f90:955-976; no aerosols, IAERSL=0),
+  // added to every point of the 1 cm-1 grid after the H2O part
+  if (L.v2 >= 820. && xrayl > 0.) {
+    __syncthreads();
+    const double conv_cm2mol = xrayl * 1.E-20 / (2.68675e-1 * 1.e5);
+    const double xkt = L.tave / kRADCN2;
+    // NPTABS of OPDPTH (src/lblrtm.f90:6222)
+    for (int64_t i = 1 + threadIdx.x; i <= L.nptabs; i += blockDim.x) {
+      const double vr = L.v1abs + double(i - 1) * L.dvabs;
+      const double xv = vr / 1.e4;
+      double ray = __dmul_rn(__ddiv_rn(__dmul_rn(__dmul_rn(xv, xv), xv),
+                                       __dsub_rn(9.38076E2, __dmul_rn(10.8426, __dmul_rn(xv, xv)))),
+                             __dmul_rn(L.wtot, conv_cm2mol));
+      if (L.jrad == 1) ray = __dmul_rn(ray, xv);
+      else if (L.jrad == 0) ray = __ddiv_rn(__dmul_rn(ray, xv), radfn(vr, xkt));
+      absrb[i] += ray;
+    }
   }
 }
 
@@ -2674,8 +2698,8 @@ cudaError_t launch_near_walk(const Work& w, const DevLines& ln, int64_t max_pane
 }
 
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
-                             cudaStream_t s) {
-  k_continuum<<<w.nlay, 256, 0, s>>>(w, ck, xself, xfrgn);
+                             double xrayl, cudaStream_t s) {
+  k_continuum<<<w.nlay, 256, 0, s>>>(w, ck, xself, xfrgn, xrayl);
   return cudaGetLastError();
 }
 

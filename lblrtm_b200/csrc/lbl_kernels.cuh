@@ -133,7 +133,7 @@ cudaError_t launch_near_lines(const Work& w, const DevLines& ln, int64_t max_nea
 cudaError_t launch_near_walk(const Work& w, const DevLines& ln, int64_t max_panel,
                              int64_t max_win, int64_t max_nblk, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
-                             cudaStream_t s);
+                             double xrayl, cudaStream_t s);
 // RADFNI segments of every panel (needs only the plans).
 cudaError_t launch_panel_segs(const Work& w, int64_t npanel_total, const int32_t* panel_layer,
                               const int64_t* panel_base, double* segs, int32_t* nseg,

@@ -269,6 +269,7 @@ int plan_layer(const lbl_run& R, const lbl_layer& L, int jrad_in, const HostLine
   double wtot = L.wbroad;
   for (int m = 0; m < L.nmol; m++) wtot += L.wk[m];
   d.h2o_fac = L.wk[0] / wtot;
+  d.wtot = wtot;
   const double fad = std::log(2.) * 2. * AVOGAD * BOLTZ / (CLIGHT * CLIGHT);
   for (int m = 1; m <= L.nmol; m++) {
     d.wk[m] = L.wk[m - 1];

@@ -48,6 +48,7 @@ struct LayerDev {
   int32_t pad0;
   // continuum grid (OPDPTH)
   double v1abs, v2abs, dvabs, h2o_fac;
+  double wtot;                // WTOT of CONTNM: WBROAD + sum of WK
   int64_t nptabs;
   // molecular constants (MOLEC), 1-based molecule / isotopologue
   double wk[kNMolTab + 1];

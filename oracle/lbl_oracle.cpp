@@ -524,6 +524,22 @@ void contnm(Layer& S) {
       S.ABSRB[j] = S.ABSRB[j] + cself + cfor;
     }
   }
+  // Rayleigh extinction (src/contnm.f90:955-976), no aerosols (IAERSL=0)
+  if (S.V2 >= 820. && S.R->xrayl > 0.) {
+    const double conv_cm2mol = S.R->xrayl * 1.E-20 / (2.68675e-1 * 1.e5);
+    const double XKT = L.tave / RADCN2;
+    const long nptabs = S.NPTABS;  // OPDPTH (src/lblrtm.f90:6222)
+    for (long i = 1; i <= nptabs && i < (long)S.ABSRB.size(); i++) {
+      double vrayleigh = S.V1ABS + double(i - 1) * S.DVABS;
+      double xvrayleigh = vrayleigh / 1.e4;
+      double ray_ext = (xvrayleigh * xvrayleigh * xvrayleigh /
+                        (9.38076E2 - 10.8426 * (xvrayleigh * xvrayleigh))) *
+                       (WTOT * conv_cm2mol);
+      if (S.jrad == 1) ray_ext = ray_ext * xvrayleigh;
+      else if (S.jrad == 0) ray_ext = ray_ext * xvrayleigh / RADFN(vrayleigh, XKT);
+      S.ABSRB[i] = S.ABSRB[i] + ray_ext;
+    }
+  }
 }
 
 // ---- LINF4 + SHRINK (src/oprop.f90:2934-3640) ---------------------------

@@ -180,3 +180,30 @@ def test_coupling_record_without_line_is_rejected(gpu_ctx):
     bad["iflg"][10] = -1
     with pytest.raises(gpu.LblError):
         gpu_ctx.upload_lines(abi.LinesHandle(bad))
+
+
+def test_rayleigh_continuum_matches_oracle():
+    """CONTNM's Rayleigh extinction (contnm.f90:955-976) with the H2O table
+    zeroed, on both JRAD branches (850 cm-1: V1/XKT < 5, JRAD=0, the
+    radiation term applied by RADFNI; 3000 cm-1: JRAD=1), against the oracle."""
+    ctx = gpu.Context(0)
+    try:
+        lines = configs.gen_lines(500, 800.0, 3100.0, seed=11)
+        lh = abi.LinesHandle(lines)
+        zero = configs.mtckd_table(1)
+        zero["self_absco_ref"] = np.zeros_like(zero["self_absco_ref"])
+        zero["for_absco_ref"] = np.zeros_like(zero["for_absco_ref"])
+        ck = abi.MtckdHandle(zero)
+        ctx.upload_lines(lh)
+        ctx.upload_mtckd(ck)
+        for v1, v2 in ((850.0, 880.0), (3000.0, 3030.0)):
+            run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1)
+            lays = abi.make_layers(configs.atmosphere(20, ptop=300.0))
+            gpu.dv_rule(run, lays)
+            for l in (0, 10):
+                got, jg = ctx.layer_od(run, lays[l])
+                ref, jo = O.layer_od(run, lays[l], lh, ck)
+                assert jg == jo
+                assert np.max(floored_err(got, ref)) <= RTOL_FP64
+    finally:
+        ctx.close()

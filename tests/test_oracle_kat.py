@@ -187,3 +187,41 @@ def test_testmm_fixture_pins_tape3_format(tmp_path):
     O.dv_rule(run, lays)
     od, _ = O.layer_od(run, lays[0], abi.LinesHandle(R))
     assert np.all(np.isfinite(od)) and od.min() > 0
+
+
+def _rayleigh_only(v1, v2, xrayl):
+    """Oracle optical depth of one layer whose only absorber is the Rayleigh
+    term of CONTNM: a zero H2O continuum table and lines far outside the band."""
+    lines = configs.gen_lines(250, 6000.0, 6010.0, seed=3)
+    lh = abi.LinesHandle(lines)
+    zero = configs.mtckd_table(1)
+    zero["self_absco_ref"] = np.zeros_like(zero["self_absco_ref"])
+    zero["for_absco_ref"] = np.zeros_like(zero["for_absco_ref"])
+    ck = abi.MtckdHandle(zero)
+    run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1, xrayl=xrayl)
+    lay = abi.make_layers(configs.atmosphere(20, ptop=300.0))
+    O.dv_rule(run, lay)
+    od, _ = O.layer_od(run, lay[0], lh, ck)
+    wtot = lay[0].wbroad + sum(lay[0].wk[m] for m in range(lay[0].nmol))
+    v = v1 + lay[0].dv * np.arange(len(od))
+    return od, v, wtot
+
+
+def test_rayleigh_extinction_closed_form():
+    """contnm.f90:955-976: xv^4/(9.38076e2 - 10.8426 xv^2) * WTOT * XRAYL *
+    1e-20/(2.68675e-1 * 1e5), xv = v/1e4, with the radiation term (xv) put
+    back by PANEL's RADFNI, reproduced to the accuracy of the 1 cm-1 grid
+    interpolation and the piecewise-linear radiation term."""
+    od, v, wtot = _rayleigh_only(1500.0, 1520.0, 1.0)
+    xv = v / 1e4
+    expect = xv ** 4 / (9.38076e2 - 10.8426 * xv ** 2) * wtot * 1e-20 / (2.68675e-1 * 1e5)
+    np.testing.assert_allclose(od, expect, rtol=2e-4)
+    od2, _, _ = _rayleigh_only(1500.0, 1520.0, 2.0)
+    np.testing.assert_allclose(od2, 2.0 * od, rtol=1e-12)
+
+
+def test_rayleigh_only_above_820():
+    od, _, _ = _rayleigh_only(700.0, 719.0, 1.0)
+    assert np.all(od == 0.0)
+    od, _, _ = _rayleigh_only(1500.0, 1520.0, 0.0)
+    assert np.all(od == 0.0)
