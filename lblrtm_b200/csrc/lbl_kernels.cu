@@ -13,6 +13,7 @@
 #include <climits>
 #include <cstdint>
 #include <cstdio>
+#include <type_traits>
 
 #include "../data/ref_tables.h"
 #include "lbl_kernels.cuh"
@@ -567,11 +568,13 @@ struct F4Side32 {
   int32_t jc;
 };
 
-struct F4Line {
+struct F4Line64 {
   // FP64 constants (CONVF4 :3965-3986); dptrat is 0 for an uncoupled line
   double xnui, sil, siv_a3, siv_b3, alfl2, rvi2, f4bnd, dptrat, mxnui, mdptrat;
   int32_t jmin, jmax, mjmin, mjmax, co2, has;  // has: 1 line, 2 image; empty range if absent
-  // FP32 copies for split-precision evaluation
+};
+// with the FP32 copies for split-precision evaluation
+struct F4Line : F4Line64 {
   float sil32, sa3_32, sb3_32, alfl2_32, rvi2_32, f4bnd32, rdd32;  // rdd = F4BND/B^2
   F4Side32 s32[2];
 };
@@ -598,7 +601,7 @@ __device__ __forceinline__ float recip_nr(float x) {
 // F4 of one side of line q at window point j in FP64 (CONVF4 :3990-4009);
 // 0 outside the side's point range.  Branch-free apart from the range, so
 // that several lines evaluate together.
-__device__ __forceinline__ double f4_side(const F4Line& q, bool image, int j, double dvr4,
+__device__ __forceinline__ double f4_side(const F4Line64& q, bool image, int j, double dvr4,
                                           double rbndsq) {
   const double xnui = image ? q.mxnui : q.xnui;
   const int lo = image ? q.mjmin : q.jmin, hi = image ? q.mjmax : q.jmax;
@@ -628,7 +631,7 @@ struct F4Reg<float> {
   int co2;
 };
 
-__device__ __forceinline__ void f4_load(F4Reg<double>& r, const F4Line& p, int m, int) {
+__device__ __forceinline__ void f4_load(F4Reg<double>& r, const F4Line64& p, int m, int) {
   r.sil = p.sil;
   r.sa3 = p.siv_a3;
   r.sb3 = p.siv_b3;
@@ -721,16 +724,23 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
     k_far_wing(Work w, const int32_t* win_order, const int32_t* win_layer) {
   constexpr int kFwAdders = ADDERS;
   constexpr int kFwThreads = ADDERS + 32 * DEC;
+  static_assert(DEC >= 2, "warp 1 builds the line constants");
   constexpr int kFwPts = (kLimOut + ADDERS - 1) / ADDERS;  // window points per adder
   extern __shared__ double fw_r4[];  // [2][kR4Stride]
-  __shared__ F4Line cl[2][kChunk];
-  __shared__ int s_idx[2][kChunk];
-  __shared__ int s_nacc[2];
+  // FP64 line constants (and the FP32 copies in split precision) of chunks
+  // t-1, t and t+1, and what the decisions need of each line
+  using Line = typename std::conditional<sizeof(T) == 8, F4Line64, F4Line>::type;
+  __shared__ Line cl[3][kChunk];
+  __shared__ double s_speak[3][kChunk], s_vnu[3][kChunk], s_spp[3][kChunk];
+  __shared__ int s_jj[3][kChunk];
+  __shared__ unsigned s_okm[3];
+  __shared__ int s_nval[3];  // lines in the chunk (0: none)
+  __shared__ int s_idx[3][kChunk];
+  __shared__ int s_nacc[3];
   __shared__ int s_state[2];  // by phase parity: a chunk was decided
+  __shared__ int s_stop;      // a decided line ended the window
   __shared__ double s_x[kChunk][kChunk];  // chunk t-1's lines at chunk t's points
   __shared__ double s_y[kChunk][kChunk];  // chunk t at its own points (line; image)
-  __shared__ int s_jj[kChunk];
-  __shared__ int s_go, s_nval;
   __shared__ unsigned s_lm;
   const int gw = win_order[blockIdx.x];
   const int l = win_layer[gw];
@@ -748,7 +758,9 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
   const int64_t nb9 = w.b9_count[l];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned full = 0xffffffffu;
-  // deciding warp's position in the shrunk list (uniform over its lanes)
+  // The line stream: warp 1 walks the layer's shrunk list (TAPE9 blocks, 32
+  // lines a chunk), building each chunk's line constants one phase ahead of
+  // warp 0's decisions.
   int64_t b = -1, c0 = 0, b1 = 0;
   bool dmore = false;
   auto next_block = [&]() {
@@ -759,7 +771,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
     }
     return false;
   };
-  // raw values of the deciding warp's next line, loaded one phase ahead
+  // raw values of warp 1's next line, loaded one phase ahead
   double n_sp = 0., n_spp = 0., n_ad = 0., n_al = 0., n_v = 0.;
   int n_co2 = 0;
   auto prefetch = [&]() {
@@ -773,140 +785,160 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
       n_co2 = w.s_co2[S + i];
     }
   };
-  if (warp == 0) {
+  // Warp 1: the chunk at c0 into buffer k (one line per lane, CONVF4
+  // :3965-3986), then on to the next chunk, whose raw values it prefetches.
+  auto build = [&](int k) {
+    const int64_t i = c0 + lane;
+    Line& p = cl[k][lane];
+    p.has = 0;
+    bool ok = false;
+    double speak = 0., vnu = 0., spp = 0.;
+    int jj = 1, has = 0;
+    if (dmore && i < b1) {
+        const double recpi = 1. / (2. * asin(1.));
+        const double zsq = 64. * 64.;
+        const double A3 = (1. + 2. * zsq) / ((1. + zsq) * (1. + zsq));
+        const double B3 = -1. / ((1. + zsq) * (1. + zsq));
+        const double sp = n_sp;
+        spp = n_spp;
+        ok = !(sp == 0. && spp == 0.);
+        const double ad = n_ad, al = n_al, v = n_v;
+        const double zeta = al / (al + ad);
+        long iz = fint(100. * zeta + kONEPL);
+        iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);  // zeta in [0,1]; guards bad input
+        const double zd = 100. * zeta - double(iz - 1);
+        const double alfav =
+            (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (al + ad);
+        const double ralfv = 1. / alfav;
+        const double sil = sp * recpi * al;
+        const double siv = (al * ralfv) * sp * recpi * ralfv;
+        speak = A3 * fabs(siv);
+        long jjl = fint((v - W.v1r4) / dvr4 + 1.);
+        jjl = jjl < 1 ? 1 : (jjl > npt ? npt : jjl);
+        jj = (int)jjl;
+        vnu = v;
+        const double dptrat = spp != 0. ? spp / (sp * alfav) : 0.;
+        p.xnui = v - W.v1r4;
+        p.sil = sil;
+        p.siv_a3 = siv * A3;
+        p.siv_b3 = siv * B3;
+        p.alfl2 = al * al;
+        p.rvi2 = 1. / (alfav * alfav);
+        p.f4bnd = sil / (al * al + bndsq);
+        p.dptrat = dptrat;
+        p.co2 = n_co2;
+        const long jmin = fint((p.xnui - bnd) / dvr4 + 2.);
+        const long jmax = fint((p.xnui + bnd) / dvr4 + 1.);
+        const bool beyond = jmin > npt;  // GO TO 60: no wing, no image
+        p.jmin = (int)(jmin < 1 ? 1 : jmin);
+        p.jmax = (int)(jmax > npt ? npt : jmax);
+        if (beyond || p.jmax < p.jmin) p.jmin = 1, p.jmax = 0;
+        else p.has |= 1;
+        p.mxnui = -v - W.v1r4;
+        p.mdptrat = -dptrat;
+        p.mjmin = 1;
+        p.mjmax = 0;
+        if (!beyond && v > 0. && v <= 25.) {  // Van Vleck-Weisskopf image (:4014-4024)
+          const long mjmin = fint((p.mxnui - bnd) / dvr4 + 2.);
+          const long mjmax = fint((p.mxnui + bnd) / dvr4 + 1.);
+          if (mjmin <= npt && (mjmax > npt ? npt : mjmax) >= (mjmin < 1 ? 1 : mjmin)) {
+            p.mjmin = (int)(mjmin < 1 ? 1 : mjmin);
+            p.mjmax = (int)(mjmax > npt ? npt : mjmax);
+            p.has |= 2;
+          }
+        }
+        has = p.has;
+        if constexpr (sizeof(T) == 4) {
+          p.sil32 = (float)p.sil;
+          p.sa3_32 = (float)p.siv_a3;
+          p.sb3_32 = (float)p.siv_b3;
+          p.alfl2_32 = (float)p.alfl2;
+          p.rvi2_32 = (float)p.rvi2;
+          p.f4bnd32 = (float)p.f4bnd;
+          p.rdd32 = (float)(p.f4bnd * rbndsq);
+          const double rdv = 1. / dvr4;
+  #pragma unroll
+          for (int m = 0; m < 2; m++) {
+            if (!(has & (1 << m))) continue;
+            F4Side32& sd = p.s32[m];
+            const double xn = m ? p.mxnui : p.xnui;
+            const double jc = floor(xn * rdv + 1.5);
+            const double dl = xn - (jc - 1.) * dvr4;
+            const double tp = (bnd + dl) * rdv, tm = (bnd - dl) * rdv;
+            const double mp = floor(tp), mm = floor(tm);
+            sd.jc = (int32_t)jc;
+            sd.dlt = (float)dl;
+            sd.php = (float)(tp - mp);
+            sd.phm = (float)(tm - mm);
+            sd.mpf = (float)mp;
+            sd.mmf = (float)mm;
+            sd.dptrat = (float)(m ? p.mdptrat : p.dptrat);
+          }
+        }
+    }
+    (void)has;
+    s_speak[k][lane] = speak;
+    s_vnu[k][lane] = vnu;
+    s_spp[k][lane] = spp;
+    s_jj[k][lane] = jj;
+    const unsigned okm = __ballot_sync(0xffffffffu, ok);
+    if (lane == 0) {
+      s_okm[k] = okm;
+      s_nval[k] = dmore ? (int)((b1 - c0) < kChunk ? (b1 - c0) : kChunk) : 0;
+    }
+    if (dmore) {
+      c0 += kChunk;
+      if (c0 >= b1) dmore = next_block();
+      prefetch();
+    }
+  };
+  if (warp == 1) {
     dmore = next_block();
     prefetch();
+    build(0);
   }
+  if (threadIdx.x == 0) s_stop = 0;
   __syncthreads();
   int rb = 0;      // buffer holding R4 through chunk t-2 in phase t
-  int prv = 0;     // chunk buffer decided in the previous phase
+  int cur = 0;     // line buffer of chunk t (chunk t-1 and t+1 in the others)
   bool have_prev = false;
   unsigned long long nevals = 0;
   for (int ph = 0;; ph++) {
     const double* R4r = fw_r4 + rb * kR4Stride;
     double* R4w = fw_r4 + (rb ^ 1) * kR4Stride;
+    const int prv = cur == 0 ? 2 : cur - 1;  // chunk t-1
+    const int nxt = cur == 2 ? 0 : cur + 1;  // chunk t+1
     if (warp < DEC) {
-      // Stage 1: warp 0 builds chunk t's lines (one per lane, shared memory
-      // cl[nb]) from the raw values prefetched in the previous phase.
-      const int nb = prv ^ 1;
-      bool ok = false;
-      double speak = 0., r = 0., vnu = 0., spp = 0.;
-      int jj = 1, has = 0;
-      if (warp == 0) {
-        if (dmore) {
-          const int64_t i = c0 + lane;
-          F4Line& p = cl[nb][lane];  // built in place in shared memory
-          p.has = 0;
-          if (i < b1) {
-            const double recpi = 1. / (2. * asin(1.));
-            const double zsq = 64. * 64.;
-            const double A3 = (1. + 2. * zsq) / ((1. + zsq) * (1. + zsq));
-            const double B3 = -1. / ((1. + zsq) * (1. + zsq));
-            const double sp = n_sp;
-            spp = n_spp;
-            ok = !(sp == 0. && spp == 0.);
-            const double ad = n_ad, al = n_al, v = n_v;
-            const double zeta = al / (al + ad);
-            long iz = fint(100. * zeta + kONEPL);
-            iz = iz < 1 ? 1 : (iz > 101 ? 101 : iz);  // zeta in [0,1]; guards bad input
-            const double zd = 100. * zeta - double(iz - 1);
-            const double alfav =
-                (c_avrat[iz - 1] + zd * (c_avrat[iz] - c_avrat[iz - 1])) * (al + ad);
-            const double ralfv = 1. / alfav;
-            const double sil = sp * recpi * al;
-            const double siv = (al * ralfv) * sp * recpi * ralfv;
-            speak = A3 * fabs(siv);
-            long jjl = fint((v - W.v1r4) / dvr4 + 1.);
-            jjl = jjl < 1 ? 1 : (jjl > npt ? npt : jjl);
-            jj = (int)jjl;
-            vnu = v;
-            const double dptrat = spp != 0. ? spp / (sp * alfav) : 0.;
-            p.xnui = v - W.v1r4;
-            p.sil = sil;
-            p.siv_a3 = siv * A3;
-            p.siv_b3 = siv * B3;
-            p.alfl2 = al * al;
-            p.rvi2 = 1. / (alfav * alfav);
-            p.f4bnd = sil / (al * al + bndsq);
-            p.dptrat = dptrat;
-            p.co2 = n_co2;
-            const long jmin = fint((p.xnui - bnd) / dvr4 + 2.);
-            const long jmax = fint((p.xnui + bnd) / dvr4 + 1.);
-            const bool beyond = jmin > npt;  // GO TO 60: no wing, no image
-            p.jmin = (int)(jmin < 1 ? 1 : jmin);
-            p.jmax = (int)(jmax > npt ? npt : jmax);
-            if (beyond || p.jmax < p.jmin) p.jmin = 1, p.jmax = 0;
-            else p.has |= 1;
-            p.mxnui = -v - W.v1r4;
-            p.mdptrat = -dptrat;
-            p.mjmin = 1;
-            p.mjmax = 0;
-            if (!beyond && v > 0. && v <= 25.) {  // Van Vleck-Weisskopf image (:4014-4024)
-              const long mjmin = fint((p.mxnui - bnd) / dvr4 + 2.);
-              const long mjmax = fint((p.mxnui + bnd) / dvr4 + 1.);
-              if (mjmin <= npt && (mjmax > npt ? npt : mjmax) >= (mjmin < 1 ? 1 : mjmin)) {
-                p.mjmin = (int)(mjmin < 1 ? 1 : mjmin);
-                p.mjmax = (int)(mjmax > npt ? npt : mjmax);
-                p.has |= 2;
-              }
-            }
-            has = p.has;
-            if constexpr (sizeof(T) == 4) {
-              p.sil32 = (float)p.sil;
-              p.sa3_32 = (float)p.siv_a3;
-              p.sb3_32 = (float)p.siv_b3;
-              p.alfl2_32 = (float)p.alfl2;
-              p.rvi2_32 = (float)p.rvi2;
-              p.f4bnd32 = (float)p.f4bnd;
-              p.rdd32 = (float)(p.f4bnd * rbndsq);
-              const double rdv = 1. / dvr4;
-  #pragma unroll
-              for (int m = 0; m < 2; m++) {
-                if (!(has & (1 << m))) continue;
-                F4Side32& sd = p.s32[m];
-                const double xn = m ? p.mxnui : p.xnui;
-                const double jc = floor(xn * rdv + 1.5);
-                const double dl = xn - (jc - 1.) * dvr4;
-                const double tp = (bnd + dl) * rdv, tm = (bnd - dl) * rdv;
-                const double mp = floor(tp), mm = floor(tm);
-                sd.jc = (int32_t)jc;
-                sd.dlt = (float)dl;
-                sd.php = (float)(tp - mp);
-                sd.phm = (float)(tm - mm);
-                sd.mpf = (float)mp;
-                sd.mmf = (float)mm;
-                sd.dptrat = (float)(m ? p.mdptrat : p.dptrat);
-              }
-            }
-            if (ok) r = R4r[jj];
-          }
-          s_jj[lane] = jj;
-        }
-        if (lane == 0) {
-          s_go = dmore ? 1 : 0;
-          s_nval = dmore ? (int)((b1 - c0) < kChunk ? (b1 - c0) : kChunk) : 0;
-        }
-      }
-      fw_dec_sync<DEC>();
-      // Stage 2: the decider warps evaluate chunk t-1's accepted lines at
+      // chunk t exists and no earlier line ended the window
+      const bool go = s_nval[cur] > 0 && !s_stop;
+      // Stage 1: the deciding warps evaluate chunk t-1's accepted lines at
       // every line's point JJ (s_x; their Van Vleck-Weisskopf images, rare,
-      // are evaluated in stage 3).
-      if (s_go) {
-        const int jjb = s_jj[lane];
+      // are evaluated in stage 2).
+      if (go) {
+        const int jjb = s_jj[cur][lane];
         const int np = have_prev ? s_nacc[prv] : 0;
         for (int a = warp; a < np; a += DEC)
           s_x[a][lane] = f4_side(cl[prv][s_idx[prv][a]], false, jjb, dvr4, rbndsq);
       }
       fw_dec_sync<DEC>();
-      // Stage 3: warp 0 completes each line's partial R4 through chunk t-1
+      // Stage 2: warp 0 completes each line's partial R4 through chunk t-1
       // in CONVF4's order and guesses the lines accepted on it alone (live).
-      bool live = false;
+      bool ok = false, live = false;
+      double speak = 0., r = 0., vnu = 0., spp = 0.;
+      int jj = 1, has = 0;
       const double dptmn = W.dptmn, dptfc = L.dptfc;
-      if (warp == 0 && dmore) {
+      if (warp == 0 && go) {
+        ok = (s_okm[cur] >> lane) & 1u;
+        speak = s_speak[cur][lane];
+        vnu = s_vnu[cur][lane];
+        spp = s_spp[cur][lane];
+        jj = s_jj[cur][lane];
+        has = cl[cur][lane].has;
+        if (ok) r = R4r[jj];
         const int np = have_prev ? s_nacc[prv] : 0;
         if (ok) {
           for (int a = 0; a < np; a++) {
-            const F4Line& q = cl[prv][s_idx[prv][a]];
+            const Line& q = cl[prv][s_idx[prv][a]];
             r += s_x[a][lane];
             r += (q.has & 2) ? f4_side(q, true, jj, dvr4, rbndsq) : 0.;
           }
@@ -916,28 +948,29 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
         if (lane == 0) s_lm = lm;
       }
       fw_dec_sync<DEC>();
-      // Stage 4: the decider warps evaluate the live lines of chunk t at the
+      // Stage 3: the deciding warps evaluate the live lines of chunk t at the
       // points of the lines above them (s_y[a][b]: line a at b's point; its
       // image at s_y[b][a]), the live lines shared out in turn.
-      if (s_go) {
-        const int jjb = s_jj[lane];
-        const int nv = s_nval;
+      if (go) {
+        const int jjb = s_jj[cur][lane];
+        const int nv = s_nval[cur];
         int k = 0;
         for (unsigned m = s_lm; m; m &= m - 1, k++) {
           const int a = __ffs(m) - 1;
           if (k % DEC != warp) continue;
           if (lane > a && lane < nv) {
-            const F4Line& q = cl[nb][a];
+            const Line& q = cl[cur][a];
             s_y[a][lane] = f4_side(q, false, jjb, dvr4, rbndsq);
             s_y[lane][a] = f4_side(q, true, jjb, dvr4, rbndsq);
           }
         }
       }
       fw_dec_sync<DEC>();
-      // Stage 5: warp 0 decides chunk t.
+      // Stage 4: warp 0 decides chunk t while warp 1 builds chunk t+1 (used
+      // only if no line of chunk t ends the window).
       if (warp == 0) {
         int decided = 0;
-        if (dmore) {
+        if (go) {
           const unsigned lm = s_lm;
           // earlier lines of this chunk accepted on their own partial R4
           double part = r;  // continues the running sum in CONVF4's order
@@ -956,8 +989,8 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
             if (ok && lane > f) {
               const double v = ((lm >> f) & 1u)
                                    ? s_y[f][lane] + s_y[lane][f]
-                                   : f4_side(cl[nb][f], false, jj, dvr4, rbndsq) +
-                                         f4_side(cl[nb][f], true, jj, dvr4, rbndsq);
+                                   : f4_side(cl[cur][f], false, jj, dvr4, rbndsq) +
+                                         f4_side(cl[cur][f], true, jj, dvr4, rbndsq);
               part += af ? v : -v;
               acc = !(speak <= (dptmn + dptfc * part) && spp == 0.);
             }
@@ -968,18 +1001,17 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
           const unsigned tm = __ballot_sync(full, acc && vnu >= W.vnulst);
           const int lim = tm ? __ffs(tm) - 1 : kChunk;
           const unsigned am = __ballot_sync(full, acc && has != 0 && lane < lim);
-          if ((am >> lane) & 1u) s_idx[nb][__popc(am & ((1u << lane) - 1u))] = lane;
-          if (lane == 0) s_nacc[nb] = __popc(am);
-          decided = 1;
-          if (tm) {
-            dmore = false;
-          } else {
-            c0 += kChunk;
-            if (c0 >= b1) dmore = next_block();
-            prefetch();
+          if ((am >> lane) & 1u) s_idx[cur][__popc(am & ((1u << lane) - 1u))] = lane;
+          if (lane == 0) {
+            s_nacc[cur] = __popc(am);
+            if (tm) s_stop = 1;
           }
+          decided = 1;
         }
         if (lane == 0) s_state[ph & 1] = decided;
+      } else if (warp == 1) {
+        if (go) build(nxt);
+        else if (lane == 0) s_nval[nxt] = 0;
       }
     } else if (have_prev) {
       // adders: chunk t-1's accepted lines over the whole window
@@ -994,7 +1026,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
           if (j <= npt) R4w[j] = R4r[j];
         }
         for (int a = 0; a < na; a++) {
-          const F4Line& pl = cl[prv][s_idx[prv][a]];
+          const Line& pl = cl[prv][s_idx[prv][a]];
 #pragma unroll 1
           for (int m = 0; m < 2; m++) {
             const int lo = m ? pl.mjmin : pl.jmin, hi = m ? pl.mjmax : pl.jmax;
@@ -1039,7 +1071,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
         float* acc32 = reinterpret_cast<float*>(fw_r4 + 2 * kR4Stride) + ad;
         const float dvr4f = (float)dvr4, bndf = (float)bnd, rbndsqf = (float)rbndsq;
         for (int a = 0; a < na; a++) {
-          const F4Line& pl = cl[prv][s_idx[prv][a]];
+          const Line& pl = cl[prv][s_idx[prv][a]];
 #pragma unroll 1
           for (int m = 0; m < 2; m++) {
             const int lo = m ? pl.mjmin : pl.jmin, hi = m ? pl.mjmax : pl.jmax;
@@ -1066,7 +1098,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
     __syncthreads();
     const int decided = s_state[ph & 1];
     if (have_prev) rb ^= 1;
-    prv ^= 1;
+    cur = nxt;
     have_prev = decided != 0;
     if (!decided) break;
   }
