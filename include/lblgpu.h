@@ -78,7 +78,12 @@ typedef struct lbl_run {
                        extinction (see xrayl) */
   int32_t iemit;    /* 0: optical depth only (ABINIT/ABSMRG);
                        1: radiance and transmittance (EMINIT/RADMRG) */
-  int32_t ipathl;   /* 1: upwelling (looking down, surface first); only 1 */
+  int32_t ipathl;   /* 1: upwelling radiance, looking down (the first layer
+                          the surface's, TMPBND/BNDEMI its emission);
+                       3: downwelling radiance, looking up from the first
+                          layer (RADNN IPATH=3, src/xmerge.f90:3007-3013,
+                          3150-3166; TMPBND/BNDEMI a boundary beyond the
+                          last layer, EMBND :3652-3733); Jacobians: 1 only */
   int32_t jrad;     /* initial JRAD: 1 (IRAD=0) or -1 (no radiation term),
                        src/lblrtm.f90:828-833 */
   double v1, v2;    /* spectral range, cm-1 (V2-V1 <= 2020 as in TAPE5 1.3) */
@@ -239,9 +244,12 @@ int lbl_pnlint(lbl_ctx* ctx, const lbl_run* run, double dv, double dvout,
 /* Merge one layer's optical depth into the accumulated radiance and
  * transmittance (XMERGE IEMIT=1: EMINIT for the first layer, RADMRG/RADNN
  * after, src/xmerge.f90:25-167; IEMIT=0: ABINIT/ABSMRG).
+ *   first         bit 0: the first layer (EMINIT); bit 1: the last layer,
+ *                 which looking up (IPATHL=3) adds the boundary beyond it
+ *                 (XMERGE :136-141)
  *   od            layer optical depth, n_new points (host or device)
  *   rad_in/tr_in  accumulated radiance/transmittance on the previous
- *                 layer's grid, n_old points (ignored when first != 0)
+ *                 layer's grid, n_old points (ignored for the first layer)
  *   rad_out/tr_out results on the layer grid, n_new points
  * For IEMIT=0 rad_* carry accumulated optical depth and tr_* is unused. */
 int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
@@ -259,9 +267,10 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
  * be caller-owned memory of device `device` (host pointers or another
  * GPU's memory give LBL_E_ARG), and the call allocates nothing.  An output
  * must not share memory with rad_in, tr_in or the other output (LBL_E_ARG);
- * it may be od itself.  IEMIT must be 0 or 1; with IEMIT=0 tr_in and tr_out
- * are not used.  Its only scratch is a fixed device array inside the
- * library, about 72 KB on every device that loads it, kept until the
+ * it may be od itself.  IEMIT must be 0 or 1, IPATHL 1 and first 0 or 1;
+ * with IEMIT=0 tr_in and tr_out are not used.  Its only scratch is a
+ * fixed device array inside the library, about 72 KB on every device that
+ * loads it, kept until the
  * process exits; it bounds a layer to LBL_NOALLOC_MAX_PANELS panels of 2400
  * points (19,660,800 points); longer layers return LBL_E_RANGE.  The first
  * call on a device looks up that array's device address; make that first

@@ -886,7 +886,8 @@ int check_run(lbl_ctx* ctx, const lbl_run* R) {
   if (R->v1 - 32. * 1e-9 <= 0.) return fail(ctx, LBL_E_RANGE, "V1 must be positive");
   if (!(R->sample > 0.) || !(R->alfal0 > 0.)) return fail(ctx, LBL_E_ARG, "SAMPLE/ALFAL0");
   if (R->iemit != 0 && R->iemit != 1) return fail(ctx, LBL_E_ARG, "IEMIT must be 0 or 1");
-  if (R->iemit == 1 && R->ipathl != 1) return fail(ctx, LBL_E_ARG, "only IPATHL=1 is supported");
+  if (R->iemit == 1 && R->ipathl != 1 && R->ipathl != 3)
+    return fail(ctx, LBL_E_ARG, "IPATHL must be 1 (looking down) or 3 (looking up)");
   if (!ctx->have_lines) return fail(ctx, LBL_E_NOTREADY, "lines not uploaded");
   return LBL_OK;
 }
@@ -955,9 +956,16 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     m.first = (l == 0);
     m.itype = (l == 0 || dv_old == d.dv) ? 0 : (int32_t)(long)(d.dv / (dv_old - d.dv) + 0.5);
     m.n_old = (int32_t)n_old;
+    // looking up (IPATHL=3): EMIN's level temperature is the lower level's
+    // (XKTA, src/xmerge.f90:2405-2424), the merge adds the farther layer
+    // seen through the nearer ones, and the boundary TMPBND lies beyond
+    // the last layer (XMERGE :136-141)
+    const bool down = R.ipathl == 3;
+    m.down = down ? 1 : 0;
+    m.tbnd_last = (down && e == n && n > 1) ? R.tmpbnd : 0.;
     for (int k = l; k < e; k++) {
       m.od_off[k - l] = ld[k].off_od;
-      m.t[k - l] = emin_temps(ld[k].tave, layers[k].tzu);
+      m.t[k - l] = emin_temps(ld[k].tave, down ? layers[k].tzl : layers[k].tzu);
       ctx->stage("merge").work += (double)ld[k].npts;
     }
     const int nxt = cur ^ 2;
@@ -1850,6 +1858,10 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, in
                     double dv_old, const double* rad_in, const double* tr_in, int64_t n_old,
                     const double* od, double* rad_out, double* tr_out, int64_t n_new) {
   if (!ctx) return LBL_E_ARG;
+  // bit 0: the first layer (EMINIT); bit 1: the last layer (looking up, the
+  // boundary beyond it)
+  const bool last = (first & 2) != 0;
+  first &= 1;
   int rc = check_run(ctx, run);
   if (rc) return rc;
   if (!layer || !od || !rad_out || (run->iemit == 1 && !tr_out)) return fail(ctx, LBL_E_ARG, "NULL argument");
@@ -1882,8 +1894,11 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, in
     if (run->iemit == 1) CK(cudaMemcpyAsync(ctx->mbuf[1], tr_in, n_old * 8, cudaMemcpyDefault, s));
   }
   const double tbnd = (first && run->ipathl == 1) ? run->tmpbnd : 0.;
+  const bool down = run->ipathl == 3;
+  const double tbnd_last = (down && last && !first) ? run->tmpbnd : 0.;
   CK(launch_merge(dL, dv, dod, n_new, first, dv_old, n_old, ctx->mbuf[0], ctx->mbuf[1],
-                  ctx->mbuf[2], ctx->mbuf[3], tbnd, run->bndemi, run->iemit, layer->tzu, s));
+                  ctx->mbuf[2], ctx->mbuf[3], tbnd, run->bndemi, run->iemit,
+                  down ? layer->tzl : layer->tzu, s, LBL_PREC_FP64, down ? 1 : 0, tbnd_last));
   CK(cudaMemcpyAsync(rad_out, ctx->mbuf[2], n_new * 8, cudaMemcpyDefault, s));
   if (tr_out) CK(cudaMemcpyAsync(tr_out, ctx->mbuf[3], n_new * 8, cudaMemcpyDefault, s));
   CK(cudaStreamSynchronize(s));

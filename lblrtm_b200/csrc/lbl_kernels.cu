@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <type_traits>
@@ -937,10 +938,11 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
         if (ok) r = R4r[jj];
         const int np = have_prev ? s_nacc[prv] : 0;
         if (ok) {
+          // (adding an absent image's 0 would leave r unchanged: r is never -0)
           for (int a = 0; a < np; a++) {
             const Line& q = cl[prv][s_idx[prv][a]];
             r += s_x[a][lane];
-            r += (q.has & 2) ? f4_side(q, true, jj, dvr4, rbndsq) : 0.;
+            if (q.has & 2) r += f4_side(q, true, jj, dvr4, rbndsq);
           }
         }
         live = ok && !(speak <= (dptmn + dptfc * r) && spp == 0.);
@@ -978,7 +980,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
             for (unsigned m = lm & ((1u << lane) - 1u); m; m &= m - 1) {
               const int a = __ffs(m) - 1;
               part += s_y[a][lane];
-              part += s_y[lane][a];
+              if (cl[cur][a].has & 2) part += s_y[lane][a];
             }
           }
           bool acc = ok && !(speak <= (dptmn + dptfc * part) && spp == 0.);
@@ -1677,14 +1679,16 @@ constexpr double X00 = -7. / 128., X01 = 105. / 128., X02 = 35. / 128., X03 = -5
                  X10 = -1. / 16., X11 = 9. / 16.;
 
 __device__ __forceinline__ double interp4(const double* R, int64_t J, int r) {
-  // value added at fine point J*4-3+r from coarse points J-1..J+2; the four
-  // forms are all evaluated and one selected, so neighbouring lanes (with
-  // different r) do not diverge
+  // value added at fine point J*4-3+r from coarse points J-1..J+2; the forms
+  // are evaluated and one selected, so neighbouring lanes (with different r)
+  // do not diverge; r = 1 and r = 3 are the same weights on the four points
+  // taken in opposite order
   const double a = R[J - 1], b = R[J], c = R[J + 1], d = R[J + 2];
-  const double v1 = X00 * a + X01 * b + X02 * c + X03 * d;
+  const bool rev = r == 3;
+  const double p0 = rev ? d : a, p1 = rev ? c : b, p2 = rev ? b : c, p3 = rev ? a : d;
+  const double v13 = X00 * p0 + X01 * p1 + X02 * p2 + X03 * p3;
   const double v2 = X10 * (a + d) + X11 * (b + c);
-  const double v3 = X03 * a + X02 * b + X01 * c + X00 * d;
-  return r == 0 ? b : (r == 1 ? v1 : (r == 2 ? v2 : v3));
+  return r == 0 ? b : (r == 2 ? v2 : v13);
 }
 
 // Global grid index ranges of one panel (panel p of layer L):
@@ -1994,9 +1998,13 @@ __global__ void __launch_bounds__(kPanelThreads, MINB)
   };
   if (tid == 0 && nbatch > 0) issue(0);
   // the grids start at zero (FP32: sum and compensation pairs)
-  for (int i = tid; i < kP1 * kPanelThreads; i += kPanelThreads) s1[i] = 0.;
-  for (int i = tid; i < kP2 * kPanelThreads; i += kPanelThreads) s2[i] = 0.;
-  s3[tid] = 0.;
+  {
+    double2* z1 = reinterpret_cast<double2*>(s1);
+    double2* z2 = reinterpret_cast<double2*>(s2);
+    for (int i = tid; i < kP1 * kPanelThreads / 2; i += kPanelThreads) z1[i] = make_double2(0., 0.);
+    for (int i = tid; i < kP2 * kPanelThreads / 2; i += kPanelThreads) z2[i] = make_double2(0., 0.);
+    s3[tid] = 0.;
+  }
   int lost = -1;  // batch whose copy did not complete
   for (int b = 0; b < nbatch; b++) {
     // buffer (b+1)&1 was last read in batch b-1, which every thread has
@@ -2310,7 +2318,7 @@ template <typename T>
 __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const double* od,
                         int first, double dv_old, int64_t n_old64, const double* rad_in,
                         const double* tr_in, double* rad_out, double* tr_out, double tbnd,
-                        double emis, int iemit, double tzu) {
+                        double emis, int iemit, double tzu, int down, double tbnd_last) {
   const LayerDev& L = *Lp;
   const int32_t f = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
   if (f >= (int32_t)L.npts) return;
@@ -2336,17 +2344,23 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
     tr_out[f] = (double)tr;
     return;
   }
-  // RADNN (IPATH=1): R = T_layer R_old + E, T = T_layer T_old
+  // RADNN: IPATH=1, R = T_layer R_old + E; IPATH=3 (looking up), R = R_old +
+  // E T_old; T = T_layer T_old
   double ro, to;
   merge_regrid(rad_in, tr_in, n_old, f, itype, ro, to);
-  rad_out[f] = (double)tr * ro + (double)em;
-  tr_out[f] = (double)tr * to;
+  double rn = down ? ro + (double)em * to : (double)tr * ro + (double)em;
+  const double tn = (double)tr * to;
+  // EMBND (:3652-3733) beyond the last layer looking up
+  if (tbnd_last > 0.)
+    rn = rn + tn * emis * (double)planck_t<T>(vi, tbnd_last / kRADCN2, kRADCN2 / tbnd_last);
+  rad_out[f] = rn;
+  tr_out[f] = tn;
 }
 
 // k_merge over m.nl consecutive layers on one grid (in FP64 with EMIN's
 // quotients from one reciprocal, emin_point_1div); the next layer's optical
-// depth is fetched while this one merges.
-template <typename T>
+// depth is fetched while this one merges.  DOWN: looking up (m.down).
+template <typename T, bool DOWN>
 __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const double* vft_panel,
                                                    const double* od, int32_t f_lo, int32_t f_hi,
                                                    double DV, const double* rad_in,
@@ -2377,11 +2391,19 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
       if (tbnd > 0.) em = em + tr * planck_t<T>(vi, tbnd / kRADCN2, kRADCN2 / tbnd) * (T)emis;
       ro = (double)em;
       to = (double)tr;
+    } else if (DOWN) {
+      // RADNN IPATH=3 (:3007-3013, 3150-3166): the farther layer's emission
+      // seen through the nearer layers
+      ro = ro + (double)em * to;
+      to = (double)tr * to;
     } else {
       ro = (double)tr * ro + (double)em;
       to = (double)tr * to;
     }
   }
+  // EMBND (:3652-3733) beyond the last layer looking up (XMERGE :140, 157)
+  if (DOWN && iemit && m.tbnd_last > 0.)
+    ro = ro + to * emis * (double)planck_t<T>(vi, m.tbnd_last / kRADCN2, kRADCN2 / m.tbnd_last);
   rad_out[f] = ro;
   if (tr_out) tr_out[f] = iemit ? to : 0.;
 }
@@ -2631,6 +2653,25 @@ void far_wing_attributes() {
   cudaFuncSetAttribute(k_far_wing<float, ADDERS, DEC, MINB>, c, cudaSharedmemCarveoutMaxShared);
 }
 
+template <typename T, int STAGE, int MINB>
+void panel_carveout() {
+  cudaFuncAttributes fa;
+  int dev = 0, smem_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+          cudaSuccess ||
+      cudaFuncGetAttributes(&fa, k_panel_od<T, STAGE, MINB>) != cudaSuccess || smem_sm <= 0) {
+    cudaGetLastError();
+    return;
+  }
+  // MINB CTAs, each with its static shared memory and 1 KB the system keeps
+  const double need = double(MINB) * double(fa.sharedSizeBytes + 1024);
+  int pct = (int)std::ceil(100. * need / double(smem_sm));
+  pct = pct < 1 ? 1 : (pct > 100 ? 100 : pct);
+  cudaFuncSetAttribute(k_panel_od<T, STAGE, MINB>,
+                       cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
 void init_kernel_attributes() {
   // two R4 buffers per CTA (plus the FP32 accumulators of split precision);
   // the largest carveout lets three CTAs share an SM
@@ -2639,16 +2680,15 @@ void init_kernel_attributes() {
   far_wing_attributes<192, 2, 3>();
   cudaFuncSetAttribute(k_near_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kNearWalkSmemMax);
-  {
-    const cudaFuncAttribute c = cudaFuncAttributePreferredSharedMemoryCarveout;
-    const int mx = cudaSharedmemCarveoutMaxShared;
-    cudaFuncSetAttribute(k_panel_od<double, 32, 4>, c, mx);
-    cudaFuncSetAttribute(k_panel_od<double, 64, 4>, c, mx);
-    cudaFuncSetAttribute(k_panel_od<double, 32, 5>, c, mx);
-    cudaFuncSetAttribute(k_panel_od<float, 32, 4>, c, mx);
-    cudaFuncSetAttribute(k_panel_od<float, 64, 4>, c, mx);
-    cudaFuncSetAttribute(k_panel_od<float, 32, 5>, c, mx);
-  }
+  // the panel kernels read the shape tables (125 KB in FP64) through L1:
+  // their shared-memory carveout is only what their CTAs per SM need, so
+  // that the rest of the SM's 256 KB stays L1
+  panel_carveout<double, 32, 4>();
+  panel_carveout<double, 64, 4>();
+  panel_carveout<double, 32, 5>();
+  panel_carveout<float, 32, 4>();
+  panel_carveout<float, 64, 4>();
+  panel_carveout<float, 32, 5>();
 
 }
 
@@ -2792,15 +2832,15 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          int64_t npts, int first, double dv_old, int64_t n_old,
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
-                         cudaStream_t s, int precision) {
+                         cudaStream_t s, int precision, int down, double tbnd_last) {
   if (npts >= (int64_t(1) << 31) || n_old >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
   const unsigned nb = (unsigned)((npts + 255) / 256);
   if (precision == LBL_PREC_SPLIT)
     k_merge<float><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
-                                      rad_out, tr_out, tbnd, emis, iemit, tzu);
+                                      rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last);
   else
     k_merge<double><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
-                                       rad_out, tr_out, tbnd, emis, iemit, tzu);
+                                       rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last);
   return cudaGetLastError();
 }
 
@@ -2814,12 +2854,22 @@ cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const d
   if (f_lo < 0 || f_hi > npts || f_lo > f_hi) return cudaErrorInvalidValue;
   if (f_hi == f_lo) return cudaSuccess;
   const unsigned nb = (unsigned)((f_hi - f_lo + 255) / 256);
-  if (precision == LBL_PREC_SPLIT)
-    k_merge_run<float><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)f_lo, (int32_t)f_hi, dv,
-                                          rad_in, tr_in, rad_out, tr_out, tbnd, emis, iemit);
-  else
-    k_merge_run<double><<<nb, 256, 0, s>>>(m, vft_panel, od, (int32_t)f_lo, (int32_t)f_hi, dv,
-                                           rad_in, tr_in, rad_out, tr_out, tbnd, emis, iemit);
+  const int32_t a = (int32_t)f_lo, b = (int32_t)f_hi;
+  if (precision == LBL_PREC_SPLIT) {
+    if (m.down)
+      k_merge_run<float, true><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
+                                                  rad_out, tr_out, tbnd, emis, iemit);
+    else
+      k_merge_run<float, false><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
+                                                   rad_out, tr_out, tbnd, emis, iemit);
+  } else {
+    if (m.down)
+      k_merge_run<double, true><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
+                                                   rad_out, tr_out, tbnd, emis, iemit);
+    else
+      k_merge_run<double, false><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
+                                                    rad_out, tr_out, tbnd, emis, iemit);
+  }
   return cudaGetLastError();
 }
 

@@ -155,7 +155,8 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          int64_t npts, int first, double dv_old, int64_t n_old,
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
-                         cudaStream_t s, int precision = LBL_PREC_FP64);
+                         cudaStream_t s, int precision = LBL_PREC_FP64, int down = 0,
+                         double tbnd_last = 0.);
 constexpr double kRADCN1 = 1.191042722E-12;  // src/phys_consts.f90:73
 constexpr double kRADCN2 = 1.4387752;        // src/phys_consts.f90:74
 // Temperatures of one EMIN step: XKT = T/RADCN2 and RADCN2/T for the layer
@@ -176,6 +177,10 @@ struct MergeRun {
   int32_t first;                 // the launch starts at the bottom layer
   int32_t itype;                 // regrid of the incoming field (0: same grid)
   int32_t n_old;                 // points of the incoming field
+  int32_t down;                  // looking up (IPATHL=3): RADNN IPATH=3
+  int32_t pad;
+  double tbnd_last;              // > 0: the boundary beyond the run's last layer
+                                 // (EMBND, the profile's last layer looking up)
   int64_t od_off[kMergeRunMax];  // each layer's optical depths in Work::od
   EminT t[kMergeRunMax];
 };

@@ -1505,13 +1505,20 @@ struct MPanel {
   std::vector<double> rad, tr;
 };
 
-// EMINIT, IPATHL=1 with TBND>0 (src/xmerge.f90:2436-2484)
+// XKTA of EMINIT/RADMRG (src/xmerge.f90:2405-2424): the upper level's
+// temperature looking down (IPATHL=1), the lower level's looking up (3).
+double xkta_of(const lbl_run& R, const lbl_layer& L) {
+  return (R.ipathl == 3 ? L.tzl : L.tzu) / RADCN2;
+}
+
+// EMINIT (src/xmerge.f90:2436-2484): IPATHL=1 with the surface term when
+// TBND>0; IPATHL=3 with no boundary at the first layer (XMERGE :136-141).
 void eminit(const lbl_run& R, const lbl_layer& L, const std::vector<PanelOut>& od,
             std::vector<MPanel>& out) {
   double XKT = L.tave / RADCN2;
   double TBND = (R.ipathl == 1) ? R.tmpbnd : 0.;
   double XKTBND = TBND / RADCN2;
-  double XKTA = L.tzu / RADCN2;
+  double XKTA = xkta_of(R, L);
   out.clear();
   for (const PanelOut& p : od) {
     std::vector<double> EM, TR;
@@ -1553,7 +1560,8 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
   else ITYPE = -fint(DVL / (DVK - DVL) + 0.5);
   if (ITYPE < 0) return fail(LBL_E_ITYPE, " RADMRG; ITYPE LT 0 ");
   double XKT = L.tave / RADCN2;
-  double XKTA = L.tzu / RADCN2;
+  double XKTA = xkta_of(R, L);
+  const bool down = R.ipathl == 3;  // IPATH_FLG = 3
   double ATYPE = ITYPE;
   long LL = ITYPE + 1;
   double AP = 1.0 / (ATYPE + 1.0);
@@ -1603,7 +1611,8 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
       TRAO[NPE + 2] = TRAO[NPE];
     }
     long NPL = 1;
-    // RADNN, IPATH_FLG = 1
+    // RADNN, IPATH_FLG = 1 (upwelling) or 3 (downwelling,
+    // src/xmerge.f90:2989-2995, 3007-3013, 3117-3130, 3150-3166)
     long NLIM = p.nlim;
     long LLM1 = std::max(LL - 1, 1L);
     long IPL = 0;
@@ -1613,18 +1622,27 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
       if (NL == 1) {
         for (long I = NL; I <= NLIM; I += LL) {
           IPL = IPL + LLM1;
-          EM[I] = TR[I] * RADO[IPL] + EM[I];
+          if (down) EM[I] = RADO[IPL] + EM[I] * TRAO[IPL];
+          else EM[I] = TR[I] * RADO[IPL] + EM[I];
           TR[I] = TR[I] * TRAO[IPL];
         }
       } else {
         double A1N = A1[NL], A2N = A2[NL], A3N = A3[NL], A4N = A4[NL];
         for (long I = NL; I <= NLIM; I += LL) {
           IPL = IPL + LLM1;
-          EM[I] = TR[I] * (A1N * RADO[IPL - 1] + A2N * RADO[IPL] + A3N * RADO[IPL + 1] +
-                           A4N * RADO[IPL + 2]) +
-                  EM[I];
-          TR[I] = TR[I] * (A1N * TRAO[IPL - 1] + A2N * TRAO[IPL] + A3N * TRAO[IPL + 1] +
-                           A4N * TRAO[IPL + 2]);
+          if (down) {
+            double TRAOI = A1N * TRAO[IPL - 1] + A2N * TRAO[IPL] + A3N * TRAO[IPL + 1] +
+                           A4N * TRAO[IPL + 2];
+            EM[I] = A1N * RADO[IPL - 1] + A2N * RADO[IPL] + A3N * RADO[IPL + 1] +
+                    A4N * RADO[IPL + 2] + EM[I] * TRAOI;
+            TR[I] = TR[I] * TRAOI;
+          } else {
+            EM[I] = TR[I] * (A1N * RADO[IPL - 1] + A2N * RADO[IPL] + A3N * RADO[IPL + 1] +
+                             A4N * RADO[IPL + 2]) +
+                    EM[I];
+            TR[I] = TR[I] * (A1N * TRAO[IPL - 1] + A2N * TRAO[IPL] + A3N * TRAO[IPL + 1] +
+                             A4N * TRAO[IPL + 2]);
+          }
         }
       }
     }
@@ -1647,11 +1665,29 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
 int radmrg(const lbl_run& R, const lbl_layer& L, double DVL,
            const std::vector<MPanel>& old, const std::vector<PanelOut>& od,
            std::vector<MPanel>& out) {
-  const double XKT = L.tave / RADCN2, XKTA = L.tzu / RADCN2;
+  const double XKT = L.tave / RADCN2, XKTA = xkta_of(R, L);
   return radmrg_core(R, L, DVL, old, od,
                      [&](size_t, const PanelOut& p, std::vector<double>& EM,
                          std::vector<double>& TR) { emin(p, XKT, XKTA, EM, TR); },
                      out);
+}
+
+// EMBND (src/xmerge.f90:3652-3733) with a constant emissivity (BNDEMI(1);
+// BNDEMI(2:3) = 0): the boundary beyond the last layer seen through the
+// whole path, R += T * EMISIV * B(TBND); XMERGE applies it at the last layer
+// looking up (IPATHL=3, :140, 157).
+void embnd(const lbl_run& R, std::vector<MPanel>& acc) {
+  const double TBND = R.tmpbnd;
+  if (!(TBND > 0.)) return;
+  const double XKTBND = TBND / RADCN2;
+  for (MPanel& p : acc) {
+    double VI = p.v1p;
+    for (long J = 0; J < p.nlim; J++) {
+      double BB = PLANCK(VI, XKTBND);
+      p.rad[J] = p.rad[J] + p.tr[J] * R.bndemi * BB;
+      VI = VI + p.dvp;
+    }
+  }
 }
 
 // ABSMRG (src/xmerge.f90:437-682): optical-depth sum with 4-point regrid.
@@ -2140,6 +2176,9 @@ int orc_merge_layer(const lbl_run* R, const lbl_layer* L, int first,
   g_err.clear();
   std::vector<PanelOut> kp = panels_from_array(*R, L->dv, od, n_new);
   std::vector<MPanel> out;
+  // bit 0: the first layer; bit 1: the last layer (its boundary term, IPATHL=3)
+  const bool last = (first & 2) != 0;
+  first &= 1;
   if (first) {
     if (R->iemit == 0) {
       for (auto& p : kp) out.push_back(MPanel{p.v1p, p.v2p, p.dvp, p.nlim, p.r, std::vector<double>(p.nlim, 0.)});
@@ -2156,6 +2195,9 @@ int orc_merge_layer(const lbl_run* R, const lbl_layer* L, int first,
                              : radmrg(*R, *L, dv_old, old, kp, out);
     if (rc != LBL_OK) return rc;
   }
+  // (a layer that is both first and last goes through EMINIT, which has no
+  // boundary term looking up)
+  if (last && !first && R->iemit == 1 && R->ipathl == 3) embnd(*R, out);
   int64_t k = 0;
   for (auto& p : out)
     for (long i = 0; i < p.nlim; i++, k++) {
@@ -2197,6 +2239,7 @@ int orc_forward(const lbl_run* R, lbl_layer* Ls, int nlay, const lbl_lines* line
     acc.swap(out);
     dv_old = Ls[l].dv;
   }
+  if (R->iemit == 1 && R->ipathl == 3 && nlay > 1) embnd(*R, acc);
   int64_t k = 0;
   for (auto& p : acc)
     for (long i = 0; i < p.nlim; i++, k++)

@@ -207,3 +207,31 @@ def test_rayleigh_continuum_matches_oracle():
                 assert np.max(floored_err(got, ref)) <= RTOL_FP64
     finally:
         ctx.close()
+
+
+def test_downwelling_forward_matches_oracle_and_layer_steps(gpu_ctx):
+    """Looking up (IPATHL=3: RADNN IPATH=3, EMIN with the lower level's
+    temperature, TMPBND beyond the last layer) on a 40-layer profile: the
+    whole-profile forward (merge runs) against the oracle, and against
+    lbl_merge_layer applied layer by layer with the last-layer flag."""
+    cfg = configs.config1(nlines=4000)
+    lh = abi.LinesHandle(cfg["lines"])
+    gpu_ctx.upload_lines(lh)
+    run = abi.make_run(v1=600.0, v2=650.0, iemit=1, ipathl=3, ilblf4=1, tmpbnd=5800.0,
+                       bndemi=1e-5)
+    lays = abi.make_layers(configs.atmosphere(40))
+    rad_ref, tr_ref = O.forward(run, abi.make_layers_like(lays), lh)
+    frad, ftr = gpu_ctx.forward(run, lays)
+    assert len(frad) == len(rad_ref)
+    assert np.max(floored_err(frad, rad_ref)) <= 1e-7
+    assert np.max(np.abs(ftr - tr_ref)) <= 1e-9
+    rad = tr = None
+    dv_old = 0.0
+    j = run.jrad
+    for l in range(len(lays)):
+        od, j = gpu_ctx.layer_od(run, lays[l], jrad=j)
+        flag = (1 if l == 0 else 0) | (2 if l == len(lays) - 1 else 0)
+        rad, tr = gpu_ctx.merge_layer(run, lays[l], flag, dv_old, rad, tr, od)
+        dv_old = lays[l].dv
+    assert np.max(np.abs(frad - rad) / np.abs(rad)) < 1e-12
+    assert np.max(np.abs(ftr - tr)) < 1e-12

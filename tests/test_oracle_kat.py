@@ -225,3 +225,59 @@ def test_rayleigh_only_above_820():
     assert np.all(od == 0.0)
     od, _, _ = _rayleigh_only(1500.0, 1520.0, 0.0)
     assert np.all(od == 0.0)
+
+
+def _planck(v, t):
+    return RADCN1 * v ** 3 / np.expm1(RADCN2 * v / t)
+
+
+def _two_layers(t1, t2):
+    prof = {"pave": np.array([500.0, 400.0]), "tave": np.array([t1, t2]),
+            "pzl": np.array([550.0, 450.0]), "pzu": np.array([450.0, 350.0]),
+            "tzl": np.array([t1, t2]), "tzu": np.array([t1, t2]),
+            "wk": np.zeros((2, 60)), "wbroad": np.array([1e24, 1e24]), "nmol": 7}
+    prof["wk"][:, 0] = 1e20
+    return abi.make_layers(prof)
+
+
+def test_downwelling_order_of_layers():
+    """RADNN IPATH=3 (xmerge.f90:3007-3013) looking up from layer 1, against
+    IPATH=1 looking down onto it, for two isothermal layers of constant
+    optical depth on one grid (EMIN's linear-in-tau term vanishes):
+    down R = B1 (1-T1) + T1 B2 (1-T2), up R = B2 (1-T2) + T2 B1 (1-T1)."""
+    t1, t2, tau1, tau2 = 280.0, 230.0, 0.7, 1.3
+    lays = _two_layers(t1, t2)
+    for l in lays:
+        l.dv = 0.01
+    out = {}
+    for ipathl in (1, 3):
+        run = abi.make_run(v1=700.0, v2=710.0, iemit=1, ipathl=ipathl, tmpbnd=0.0)
+        n = O.npts(run, 0.01)
+        od1, od2 = np.full(n, tau1), np.full(n, tau2)
+        r1, x1 = O.merge_layer(run, lays[0], 1, 0.0, None, None, od1)
+        out[ipathl] = O.merge_layer(run, lays[1], 2, 0.01, r1, x1, od2)
+    v = 700.0 + 0.01 * np.arange(n)
+    b1, b2 = _planck(v, t1), _planck(v, t2)
+    e1, e2 = np.exp(-tau1), np.exp(-tau2)
+    np.testing.assert_allclose(out[3][0], b1 * (1 - e1) + e1 * b2 * (1 - e2), rtol=1e-12)
+    np.testing.assert_allclose(out[1][0], b2 * (1 - e2) + e2 * b1 * (1 - e1), rtol=1e-12)
+    np.testing.assert_allclose(out[3][1], e1 * e2, rtol=1e-14)
+
+
+def test_downwelling_boundary_beyond_last_layer():
+    """Looking up, TMPBND/BNDEMI lie beyond the last layer (EMBND,
+    xmerge.f90:3652-3733, applied by XMERGE at the last layer): through two
+    transparent layers the radiance is BNDEMI B(TMPBND); a single layer
+    (EMINIT) has no boundary term."""
+    lays = _two_layers(250.0, 250.0)
+    for l in lays:
+        l.dv = 0.01
+    run = abi.make_run(v1=700.0, v2=710.0, iemit=1, ipathl=3, tmpbnd=5800.0, bndemi=0.3)
+    n = O.npts(run, 0.01)
+    z = np.zeros(n)
+    r1, x1 = O.merge_layer(run, lays[0], 3, 0.0, None, None, z)
+    assert np.all(r1 == 0.0)
+    r1, x1 = O.merge_layer(run, lays[0], 1, 0.0, None, None, z)
+    r2, x2 = O.merge_layer(run, lays[1], 2, 0.01, r1, x1, z)
+    v = 700.0 + 0.01 * np.arange(n)
+    np.testing.assert_allclose(r2, 0.3 * _planck(v, 5800.0), rtol=1e-12)
