@@ -735,6 +735,8 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
   __shared__ double s_speak[3][kChunk], s_vnu[3][kChunk], s_spp[3][kChunk];
   __shared__ int s_jj[3][kChunk];
   __shared__ unsigned s_okm[3];
+  __shared__ unsigned s_imgc[3];  // lines of the chunk with a Van Vleck-Weisskopf image
+  __shared__ unsigned s_imgp[3];  // the same of the accepted lines, in s_idx order
   __shared__ int s_nval[3];  // lines in the chunk (0: none)
   __shared__ int s_idx[3][kChunk];
   __shared__ int s_nacc[3];
@@ -883,8 +885,10 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
     s_spp[k][lane] = spp;
     s_jj[k][lane] = jj;
     const unsigned okm = __ballot_sync(0xffffffffu, ok);
+    const unsigned imgc = __ballot_sync(0xffffffffu, (p.has & 2) != 0);
     if (lane == 0) {
       s_okm[k] = okm;
+      s_imgc[k] = imgc;
       s_nval[k] = dmore ? (int)((b1 - c0) < kChunk ? (b1 - c0) : kChunk) : 0;
     }
     if (dmore) {
@@ -918,6 +922,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
       if (go) {
         const int jjb = s_jj[cur][lane];
         const int np = have_prev ? s_nacc[prv] : 0;
+#pragma unroll 2
         for (int a = warp; a < np; a += DEC)
           s_x[a][lane] = f4_side(cl[prv][s_idx[prv][a]], false, jjb, dvr4, rbndsq);
       }
@@ -939,10 +944,10 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
         const int np = have_prev ? s_nacc[prv] : 0;
         if (ok) {
           // (adding an absent image's 0 would leave r unchanged: r is never -0)
+          const unsigned imgp = have_prev ? s_imgp[prv] : 0u;
           for (int a = 0; a < np; a++) {
-            const Line& q = cl[prv][s_idx[prv][a]];
             r += s_x[a][lane];
-            if (q.has & 2) r += f4_side(q, true, jj, dvr4, rbndsq);
+            if ((imgp >> a) & 1u) r += f4_side(cl[prv][s_idx[prv][a]], true, jj, dvr4, rbndsq);
           }
         }
         live = ok && !(speak <= (dptmn + dptfc * r) && spp == 0.);
@@ -956,6 +961,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
       if (go) {
         const int jjb = s_jj[cur][lane];
         const int nv = s_nval[cur];
+        const unsigned imgc = s_imgc[cur];
         int k = 0;
         for (unsigned m = s_lm; m; m &= m - 1, k++) {
           const int a = __ffs(m) - 1;
@@ -963,7 +969,7 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
           if (lane > a && lane < nv) {
             const Line& q = cl[cur][a];
             s_y[a][lane] = f4_side(q, false, jjb, dvr4, rbndsq);
-            s_y[lane][a] = f4_side(q, true, jjb, dvr4, rbndsq);
+            s_y[lane][a] = ((imgc >> a) & 1u) ? f4_side(q, true, jjb, dvr4, rbndsq) : 0.;
           }
         }
       }
@@ -976,11 +982,12 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
           const unsigned lm = s_lm;
           // earlier lines of this chunk accepted on their own partial R4
           double part = r;  // continues the running sum in CONVF4's order
+          const unsigned imgc = s_imgc[cur];
           if (ok) {
             for (unsigned m = lm & ((1u << lane) - 1u); m; m &= m - 1) {
               const int a = __ffs(m) - 1;
               part += s_y[a][lane];
-              if (cl[cur][a].has & 2) part += s_y[lane][a];
+              if ((imgc >> a) & 1u) part += s_y[lane][a];
             }
           }
           bool acc = ok && !(speak <= (dptmn + dptfc * part) && spp == 0.);
@@ -1003,9 +1010,13 @@ __global__ void __launch_bounds__(ADDERS + 32 * DEC, MINB)
           const unsigned tm = __ballot_sync(full, acc && vnu >= W.vnulst);
           const int lim = tm ? __ffs(tm) - 1 : kChunk;
           const unsigned am = __ballot_sync(full, acc && has != 0 && lane < lim);
-          if ((am >> lane) & 1u) s_idx[cur][__popc(am & ((1u << lane) - 1u))] = lane;
+          const int rank = __popc(am & ((1u << lane) - 1u));
+          if ((am >> lane) & 1u) s_idx[cur][rank] = lane;
+          const unsigned imgp =
+              __reduce_or_sync(full, (((am >> lane) & 1u) && (has & 2)) ? (1u << rank) : 0u);
           if (lane == 0) {
             s_nacc[cur] = __popc(am);
+            s_imgp[cur] = imgp;
             if (tm) s_stop = 1;
           }
           decided = 1;
