@@ -37,6 +37,21 @@ class Run(C.Structure):
     ]
 
 
+class Scan(C.Structure):
+    """lbl_scan: SCANFN controls (HWHM, V1, V2, SAMPL, JFN, JEMIT=-1)."""
+
+    _fields_ = [
+        ("hwhm", C.c_double), ("v1", C.c_double), ("v2", C.c_double), ("sampl", C.c_double),
+        ("jfn", C.c_int32), ("jabs", C.c_int32),
+    ]
+
+
+def make_scan(hwhm, v1, v2, jfn=2, sampl=0.0, jabs=0):
+    sc = Scan()
+    sc.hwhm, sc.v1, sc.v2, sc.sampl, sc.jfn, sc.jabs = hwhm, v1, v2, sampl, jfn, jabs
+    return sc
+
+
 class Layer(C.Structure):
     """lbl_layer: the /FILHDR/ quantities of one layer."""
 

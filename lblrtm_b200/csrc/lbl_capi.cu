@@ -1960,6 +1960,59 @@ int lbl_pnlint(lbl_ctx* ctx, const lbl_run* run, double dv, double dvout, const 
   return LBL_OK;
 }
 
+int64_t lbl_scan_npts(const lbl_scan* sc, double dv_in, double* dvout) {
+  if (!sc) return -LBL_E_ARG;
+  ScanPlan P;
+  std::string e;
+  const int rc = scan_plan(*sc, dv_in, &P, &e);
+  if (rc) return -rc;
+  if (dvout) *dvout = P.dvo;
+  return P.n_out;
+}
+
+int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int64_t n,
+                      double v1_in, double dv_in, double* out, int64_t n_out) {
+  if (!ctx) return LBL_E_ARG;
+  if (!sc || !spec || !out || n < 1) return fail(ctx, LBL_E_ARG, "NULL argument or empty spectrum");
+  ScanPlan P;
+  std::string e;
+  int rc = scan_plan(*sc, dv_in, &P, &e);
+  if (rc) return fail(ctx, rc, e);
+  if (P.n_out != n_out) return fail(ctx, LBL_E_ARG, "n_out does not match the output grid");
+  cudaSetDevice(ctx->device);
+  // SHRKSC: full groups of IRATSH points; the compressed input's first
+  // wavenumber and the CONVSC range from VBOT/VTOP (src/postsub.f90:1330-1355)
+  const int64_t nc = n / P.iratsh;
+  const double v1i = v1_in + P.v1shft;
+  int64_t ilo = (int64_t)(((P.vbot - v1i) / P.dvsc) + 1.5);
+  ilo = std::max<int64_t>(ilo, 1);
+  int64_t ihi = (int64_t)(((P.vtop - v1i) / P.dvsc) + 1.5);
+  ihi = std::min<int64_t>(ihi, nc);
+  const double zint = (v1i - P.vft0) / P.dvo;
+  const bool in_dev = is_device_ptr(spec), out_dev = is_device_ptr(out);
+  size_t bytes = (nc + 1) * 8 + P.xf.size() * 8 + 4 * 256;
+  if (!in_dev) bytes += n * 8 + 256;
+  if (!out_dev) bytes += n_out * 8 + 256;
+  CK(ctx->arena.reserve(bytes, ctx->mem));
+  ctx->arena.reset();
+  cudaStream_t s = ctx->stream;
+  double* dsc = ctx->arena.take<double>(nc + 1);
+  double* dxf = ctx->arena.take<double>(P.xf.size());
+  const double* din = spec;
+  if (!in_dev) {
+    double* t = ctx->arena.take<double>(n);
+    CK(cudaMemcpyAsync(t, spec, n * 8, cudaMemcpyHostToDevice, s));
+    din = t;
+  }
+  double* dout = out_dev ? out : ctx->arena.take<double>(n_out);
+  CK(cudaMemcpyAsync(dxf, P.xf.data(), P.xf.size() * 8, cudaMemcpyHostToDevice, s));
+  CK(launch_scan(din, n, (int)P.iratsh, sc->jabs ? 1 : 0, dsc, ilo, ihi, zint, P.ratio, P.zbound,
+                 P.zslope, P.xnorm, dxf, P.nfmax, dout, n_out, s));
+  if (!out_dev) CK(cudaMemcpyAsync(out, dout, n_out * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return LBL_OK;
+}
+
 int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nlay, double* rad,
                 double* tr, int64_t npts, int32_t precision) {
   if (!ctx) return LBL_E_ARG;

@@ -2988,4 +2988,81 @@ cudaError_t launch_pnlint(const PnlSeg* seg, int64_t nseg, const double* a, cons
   return cudaGetLastError();
 }
 
+// ---- SCANFN (src/postsub.f90:1276-1376 SHRKSC, :1516-1598 CONVSC) -------
+__global__ void k_scan_compress(const double* __restrict__ spec, int64_t nc, int ir, int jabs,
+                                double* __restrict__ sc) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  double sum = 0.;
+  for (int j = 0; j < ir; j++) {
+    double x = spec[k * ir + j];
+    if (jabs) x = __dsub_rn(1., x);
+    sum = __dadd_rn(sum, x);
+  }
+  sc[k] = __ddiv_rn(sum, (double)ir);
+}
+
+// Output point JF = 33 + j of the global grid: the inputs whose JMIN..JMAX
+// holds JF (both bounds rise with the input index, found by bisection),
+// summed in input order, each XNORM*S(I)*XF(|ZF|+1.5) with every product
+// and sum rounded separately.
+__device__ __forceinline__ double scan_zpeak(int64_t k, double ratio, double zint) {
+  return __dadd_rn(__dmul_rn((double)(k - 1), ratio), zint);
+}
+__global__ void k_scan_gather(const double* __restrict__ sc, int64_t ilo, int64_t ihi,
+                              double zint, double ratio, double zbound, double zslope,
+                              double xnorm, const double* __restrict__ xf, int64_t nfmax,
+                              double* __restrict__ out, int64_t n_out) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_out) return;
+  const int64_t jf = 33 + j;
+  auto jmax_of = [&](int64_t k) {
+    return (int64_t)__dadd_rn(__dadd_rn(scan_zpeak(k, ratio, zint), zbound), 1.5);
+  };
+  auto jmin_of = [&](int64_t k) {
+    return (int64_t)__dadd_rn(__dsub_rn(scan_zpeak(k, ratio, zint), zbound), 1.5);
+  };
+  // first k with JMAX >= JF
+  int64_t lo = ilo, hi = ihi + 1;
+  while (lo < hi) {
+    const int64_t m = lo + (hi - lo) / 2;
+    if (jmax_of(m) >= jf) hi = m;
+    else lo = m + 1;
+  }
+  const int64_t k0 = lo;
+  // last k with JMIN <= JF
+  lo = ilo;
+  hi = ihi + 1;
+  while (lo < hi) {
+    const int64_t m = lo + (hi - lo) / 2;
+    if (jmin_of(m) <= jf) lo = m + 1;
+    else hi = m;
+  }
+  const int64_t k1 = lo - 1;
+  double acc = 0.;
+  for (int64_t k = k0; k <= k1; k++) {
+    const double s = sc[k - 1];
+    if (s == 0.) continue;
+    const double zpeak = scan_zpeak(k, ratio, zint);
+    const double zf = __dmul_rn(__dsub_rn((double)(jf - 1), zpeak), zslope);
+    int64_t it = (int64_t)__dadd_rn(fabs(zf), 1.5);
+    it = it > nfmax ? nfmax : it;
+    acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(xnorm, s), xf[it]));
+  }
+  out[j] = acc;
+}
+
+cudaError_t launch_scan(const double* spec, int64_t n, int ir, int jabs, double* sc, int64_t ilo,
+                        int64_t ihi, double zint, double ratio, double zbound, double zslope,
+                        double xnorm, const double* xf, int64_t nfmax, double* out,
+                        int64_t n_out, cudaStream_t s) {
+  const int64_t nc = n / ir;
+  if (nc > 0)
+    k_scan_compress<<<(unsigned)((nc + 255) / 256), 256, 0, s>>>(spec, nc, ir, jabs, sc);
+  if (n_out > 0)
+    k_scan_gather<<<(unsigned)((n_out + 255) / 256), 256, 0, s>>>(
+        sc, ilo, ihi, zint, ratio, zbound, zslope, xnorm, xf, nfmax, out, n_out);
+  return cudaGetLastError();
+}
+
 }  // namespace lbl

@@ -209,6 +209,13 @@ cudaError_t launch_jac_diff(double* plus, const double* minus, int64_t n, double
 cudaError_t launch_chan_mean(const double* x, int64_t n, int nrows, const int64_t* cb,
                              int64_t nchan, double* out, cudaStream_t s);
 constexpr int kJacMaxParams = 8;
+// SCANFN: SHRKSC's compression of spec (n points, groups of ir, 1 - x when
+// jabs) into sc (n / ir points), then CONVSC's sums on the global output
+// grid, one thread per output point (the inputs ilo..ihi, 1-based).
+cudaError_t launch_scan(const double* spec, int64_t n, int ir, int jabs, double* sc, int64_t ilo,
+                        int64_t ihi, double zint, double ratio, double zbound, double zslope,
+                        double xnorm, const double* xf, int64_t nfmax, double* out,
+                        int64_t n_out, cudaStream_t s);
 // PNLINT re-grid of one layer (one CTA per segment of the host plan);
 // a: the 4 x 101 Lagrange weights.
 cudaError_t launch_pnlint(const PnlSeg* seg, int64_t nseg, const double* a, const double* od,

@@ -607,4 +607,114 @@ int pnlint_plan(const lbl_run& R, double dv, double dvout, PnlPlan* P, std::stri
   }
 }
 
+// SCANFN's set-up (src/postsub.f90:25-420): the function's extent, table
+// step and sampling (HWJ, DXJ, NJ, NJMX, SMPLJ, XSCAL :97-117), SAMPL, the
+// output spacing DVO = HWHM/SAMPLE and the bound, PANLSC's last point
+// (:1600-1660), the shapes (SHAPET :1377-1400, SHAPEG src/oprop.f90:
+// 1912-1942, SINCSQ :2445-2484, SINC :2486-2525), SHRKSC's ratio
+// (:1276-1320) and CONVSC's constants (:1516-1560).
+int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
+  static const double HWJ[5] = {1., 2., 4., 54.1826, 119.332818};
+  static const double DXJ[5] = {0., 0.02, 0.02, 0.02, 0.02};
+  static const int64_t NJ[5] = {0, 101, 201, 2710, 5968};
+  static const int64_t NJMX[5] = {0, 251, 251, 2760, 6018};
+  static const double SMPLJ[5] = {.5, 2., 4., 4., 4.};
+  static const double XSCAL[5] = {0., 0., 0., 1.391557377, 1.89549425};
+  static const long JRATIO[25] = {0, 1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20,
+                                  24, 25, 30, 32, 40, 48, 50, 60, 75, 80, 100, 120};
+  const double pi = 2. * std::asin(1.);
+  double hwhm = sc.hwhm;
+  int jfn = sc.jfn;
+  if (!(hwhm > 0.) || !(sc.v2 > sc.v1) || !(dv_in > 0.)) {
+    *err = "scan: HWHM, V1 < V2 and the input spacing must be positive";
+    return LBL_E_ARG;
+  }
+  if (jfn < 0) {
+    jfn = -jfn;
+    if (jfn != 3 && jfn != 4) {
+      *err = "SCANFN; INVALID JFN";
+      return LBL_E_ARG;
+    }
+  }
+  if (jfn < 1 || jfn > 4) {
+    *err = "scan: JFN must be 1-4 (triangle, Gaussian, sinc^2, sinc)";
+    return LBL_E_ARG;
+  }
+  const double xscale = XSCAL[jfn];
+  if (sc.jfn < 0) hwhm = hwhm / (pi / xscale);
+  P->jfn = jfn;
+  P->hwf = HWJ[jfn];
+  P->dxf = DXJ[jfn];
+  P->nf = NJ[jfn];
+  P->nfmax = NJMX[jfn];
+  double sample = SMPLJ[jfn];
+  if (sc.sampl < 0.) sample = hwhm / (-sc.sampl);
+  else if (sc.sampl > 0.) sample = sc.sampl;
+  if (dv_in > hwhm / 12.) {
+    *err = "scan: input spacing above HWHM/12 (the reference interpolates first, SCNINT)";
+    return LBL_E_RANGE;
+  }
+  P->hwhm = hwhm;
+  P->dvo = hwhm / sample;
+  const long nbound = fint((2. * P->hwf) * sample + 0.01);
+  P->bound = double(nbound) * P->dvo / 2.;
+  P->vft0 = sc.v1 - double(kNShift) * P->dvo;
+  P->vbot = sc.v1 - P->bound;
+  P->vtop = sc.v2 + P->bound;
+  P->nnhi = fint((sc.v2 - P->vft0) / P->dvo + 1.5);
+  P->n_out = P->nnhi - kNShift;
+  if (P->n_out < 1 || P->n_out > (int64_t(1) << 30)) {
+    *err = "scan: output grid size";
+    return LBL_E_RANGE;
+  }
+  P->xf.assign(P->nfmax + 2, 0.);
+  double* xf = P->xf.data();
+  if (jfn == 1) {
+    xf[1] = 0.5;
+    for (int64_t i = 2; i <= P->nf; i++) xf[i] = 0.5 * (1. - 0.5 * (double(i - 1) * P->dxf));
+  } else if (jfn == 2) {
+    const double fln2 = std::log(2.), recpi = 1. / (2. * std::asin(1.));
+    const double fgnorm = std::sqrt(fln2 * recpi);
+    xf[1] = fgnorm * std::exp(-fln2 * 0.);
+    for (int64_t j = 2; j <= P->nf; j++) {
+      const double x = double(j - 1) * P->dxf;
+      xf[j] = fgnorm * std::exp(-fln2 * (x * x));
+    }
+    xf[P->nf] = 0.;
+  } else {
+    const double xnorm = xscale / pi;
+    xf[1] = xnorm;
+    for (int64_t i = 2; i <= P->nf; i++) {
+      const double a = (double(i - 1) * P->dxf) * xscale;
+      const double sx = std::sin(a) / a;
+      xf[i] = (jfn == 3) ? xnorm * (sx * sx) : xnorm * sx;
+    }
+  }
+  // SHRKSC
+  double dvsc = hwhm / 12.;
+  long ir = fint(dvsc / dv_in + 0.5);
+  for (int i = 2; i <= 24; i++)
+    if (JRATIO[i] > ir) {
+      ir = JRATIO[i - 1];
+      break;
+    }
+  if (ir > JRATIO[24]) ir = JRATIO[24];
+  if (ir > 1) {
+    P->iratsh = ir;
+    P->dvsc = double(ir) * dv_in;
+    P->v1shft = double(ir - 1) * dv_in / 2.;
+  } else {
+    P->iratsh = 1;
+    P->dvsc = dv_in;
+    P->v1shft = 0.;
+  }
+  // CONVSC
+  P->ratio = P->dvsc / P->dvo;
+  const double dvodx = P->dvo / P->dxf, hwbnd = P->hwf / P->dvo;
+  P->zslope = dvodx / hwhm;
+  P->zbound = hwbnd * hwhm;
+  P->xnorm = P->dvsc / hwhm;
+  return LBL_OK;
+}
+
 }  // namespace lbl

@@ -150,4 +150,19 @@ struct PnlPlan {
 // Plan PNLINT for a layer of spacing dv; dvout must satisfy 0 < dvout <= dv.
 int pnlint_plan(const lbl_run& R, double dv, double dvout, PnlPlan* P, std::string* err);
 
+// SCANFN (src/postsub.f90:25-560) on the global output grid: the scanning
+// function table, SHRKSC's compression ratio and CONVSC's constants.
+struct ScanPlan {
+  int jfn = 0;
+  double hwhm = 0., dvo = 0., hwf = 0., dxf = 0., bound = 0., vft0 = 0., vbot = 0., vtop = 0.;
+  int64_t nf = 0, nfmax = 0, nnhi = 0;   // NNHI: last output point, R1 index
+  int64_t n_out = 0;                     // output points (R1 33..NNHI)
+  std::vector<double> xf;                // XF, 1-based
+  // compression and convolution for an input spacing
+  int64_t iratsh = 1;
+  double dvsc = 0., v1shft = 0., ratio = 0., zslope = 0., zbound = 0., xnorm = 0.;
+};
+// Grid, table and constants for input spacing dv_in.
+int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err);
+
 }  // namespace lbl

@@ -31,6 +31,9 @@ SIGNATURES = {
     "lbl_dv_rule": (C.c_int, [C.POINTER(abi.Run), C.POINTER(abi.Layer), C.c_int32]),
     "lbl_layer_npts": (C.c_int64, [C.POINTER(abi.Run), C.c_double]),
     "lbl_pnlint_npts": (C.c_int64, [C.POINTER(abi.Run), C.c_double, C.c_double]),
+    "lbl_scan_npts": (C.c_int64, [C.POINTER(abi.Scan), C.c_double, P_D]),
+    "lbl_scan_spectrum": (C.c_int, [C.c_void_p, C.POINTER(abi.Scan), C.c_void_p, C.c_int64,
+                                    C.c_double, C.c_double, C.c_void_p, C.c_int64]),
     "lbl_pnlint": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.c_double, C.c_double, C.c_void_p,
                              C.c_int64, C.c_void_p, C.c_int64]),
     "lbl_layer_od": (C.c_int, [C.c_void_p, C.POINTER(abi.Run), C.POINTER(abi.Layer), P_I32,
@@ -113,6 +116,15 @@ def pnlint_npts(run, dv, dvout):
     if n < 0:
         raise LblError(-n, f"pnlint_npts: {abi.STATUS.get(-n, -n)}")
     return n
+
+
+def scan_npts(sc, dv_in):
+    """Output points and spacing of a SCANFN convolution for input spacing dv_in."""
+    dvo = C.c_double(0.0)
+    n = int(load().lbl_scan_npts(C.byref(sc), C.c_double(dv_in), C.byref(dvo)))
+    if n < 0:
+        raise LblError(-n, f"scan_npts: {abi.STATUS.get(-n, -n)}")
+    return n, dvo.value
 
 
 def brightness_temperature(rad, v1, dv):
@@ -199,6 +211,16 @@ class Context:
         res = np.zeros(n) if out is None else out
         self._check(self.lib.lbl_pnlint(self.h, C.byref(run), C.c_double(dv), C.c_double(dvout),
                                         _ptr(od), len(od), _ptr(res), n), "pnlint")
+        return res
+
+    def scan_spectrum(self, sc, spec, v1_in, dv_in, out=None):
+        """SCANFN convolution of a spectrum (numpy or CUDA tensor) on
+        v1_in + i*dv_in; returns the output on sc.v1 + j*DVOUT."""
+        n, _ = scan_npts(sc, dv_in)
+        res = np.zeros(n) if out is None else out
+        self._check(self.lib.lbl_scan_spectrum(self.h, C.byref(sc), _ptr(spec), len(spec),
+                                               C.c_double(v1_in), C.c_double(dv_in), _ptr(res),
+                                               n), "scan_spectrum")
         return res
 
     def merge_layer(self, run, layer, first, dv_old, rad_in, tr_in, od):

@@ -2056,6 +2056,155 @@ int pnlint_layer(const lbl_run& R, double DV, double DVOUT, const double* od, in
   return LBL_OK;
 }
 
+// ---- SCANFN (src/postsub.f90:25-560) -------------------------------------
+// The scanning functions on the global output grid: the tabulated shapes
+// (SHAPET :1377-1400, SHAPEG src/oprop.f90:1912-1942, SINCSQ :2445-2484,
+// SINC :2486-2525), SHRKSC's compression (:1276-1376: the largest ratio of
+// JRATIO not above HWHM/12/DVI, group means), CONVSC's sums (:1516-1598: each
+// compressed input spread over its JMIN..JMAX with XF(|ZF|+1.5)), PANLSC's
+// last point (:1600-1660).  ZPEAK and ZF are taken from one global origin
+// (the reference's panel origins and incremental ZF round slightly
+// differently).
+struct ScanOracle {
+  int jfn = 0;
+  double hwhm = 0, sample = 0, dvo = 0, hwf = 0, dxf = 0, bound = 0, vft0 = 0, vbot = 0, vtop = 0;
+  long nf = 0, nfmax = 0, nnhi = 0;
+  std::vector<double> xf;  // 1-based
+};
+
+int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
+  static const double HWJ[5] = {1., 2., 4., 54.1826, 119.332818};
+  static const double DXJ[5] = {0., 0.02, 0.02, 0.02, 0.02};
+  static const long NJ[5] = {0, 101, 201, 2710, 5968};
+  static const long NJMX[5] = {0, 251, 251, 2760, 6018};
+  static const double SMPLJ[5] = {.5, 2., 4., 4., 4.};
+  static const double XSCAL[5] = {0., 0., 0., 1.391557377, 1.89549425};
+  const double PI = 2. * std::asin(1.);
+  double HWHM = sc.hwhm;
+  int JFN = sc.jfn;
+  if (!(HWHM > 0.) || !(sc.v2 > sc.v1) || !(dv_in > 0.)) return fail(LBL_E_ARG, "scan: HWHM, V1, V2, DV");
+  if (JFN < 0) {
+    JFN = -JFN;
+    if (JFN != 3 && JFN != 4) return fail(LBL_E_ARG, "SCANFN; INVALID JFN");
+  }
+  if (JFN < 1 || JFN > 4) return fail(LBL_E_ARG, "scan: JFN 1-4 (triangle, Gauss, sinc^2, sinc)");
+  const double XSCALE = XSCAL[JFN];
+  if (sc.jfn < 0) HWHM = HWHM / (PI / XSCALE);
+  S.jfn = JFN;
+  S.hwf = HWJ[JFN];
+  S.dxf = DXJ[JFN];
+  S.nf = NJ[JFN];
+  S.nfmax = NJMX[JFN];
+  double SAMPLE = SMPLJ[JFN];
+  if (sc.sampl < 0.) SAMPLE = HWHM / (-sc.sampl);
+  else if (sc.sampl > 0.) SAMPLE = sc.sampl;
+  const double DVINT = HWHM / 12.;
+  if (dv_in > DVINT) return fail(LBL_E_RANGE, "scan: input DV above HWHM/12 (SCNINT not built)");
+  S.hwhm = HWHM;
+  S.sample = SAMPLE;
+  S.dvo = HWHM / SAMPLE;
+  const long NBOUND = fint((2. * S.hwf) * SAMPLE + 0.01);
+  S.bound = double(NBOUND) * S.dvo / 2.;
+  S.vft0 = sc.v1 - 32. * S.dvo;
+  S.vbot = sc.v1 - S.bound;
+  S.vtop = sc.v2 + S.bound;
+  S.nnhi = fint((sc.v2 - S.vft0) / S.dvo + 1.5);
+  // the shape table
+  S.xf.assign(S.nfmax + 2, 0.);
+  std::vector<double>& XF = S.xf;
+  if (JFN == 1) {
+    XF[1] = 0.5;
+    for (long I = 2; I <= S.nf; I++) {
+      double X = double(I - 1) * S.dxf;
+      XF[I] = 0.5 * (1. - 0.5 * X);
+    }
+  } else if (JFN == 2) {
+    const double FLN2 = std::log(2.), RECPI = 1. / (2. * std::asin(1.));
+    const double FGNORM = std::sqrt(FLN2 * RECPI);
+    XF[1] = FGNORM * std::exp(-FLN2 * 0.);
+    for (long JJ = 2; JJ <= S.nf; JJ++) {
+      double X = double(JJ - 1) * S.dxf;
+      double XSQ = X * X;
+      XF[JJ] = FGNORM * std::exp(-FLN2 * XSQ);
+    }
+    XF[S.nf] = 0.;
+  } else {
+    const double XNORM = XSCALE / PI;
+    XF[1] = XNORM;
+    for (long I = 2; I <= S.nf; I++) {
+      double X = double(I - 1) * S.dxf;
+      double A = X * XSCALE;
+      double sx = std::sin(A) / A;
+      XF[I] = (JFN == 3) ? XNORM * (sx * sx) : XNORM * sx;
+    }
+  }
+  return LBL_OK;
+}
+
+int scan_spectrum(const lbl_scan& sc, const double* spec, int64_t n, double v1_in, double dv_in,
+                  std::vector<double>& out) {
+  ScanOracle S;
+  int rc = scan_setup(sc, dv_in, S);
+  if (rc) return rc;
+  // RDSCAN (:1411-1514): JEMIT=-1 convolves the absorption 1 - S
+  std::vector<double> s(spec, spec + n);
+  if (sc.jabs) for (auto& x : s) x = 1. - x;
+  // SHRKSC
+  static const long JRATIO[25] = {0, 1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20,
+                                  24, 25, 30, 32, 40, 48, 50, 60, 75, 80, 100, 120};
+  double DVI = dv_in;
+  double DVSC = S.hwhm / 12.;
+  long IRATSH = fint(DVSC / DVI + 0.5);
+  for (int I = 2; I <= 24; I++)
+    if (JRATIO[I] > IRATSH) {
+      IRATSH = JRATIO[I - 1];
+      break;
+    }
+  if (IRATSH > JRATIO[24]) IRATSH = JRATIO[24];
+  double V1SHFT = 0.;
+  if (IRATSH > 1) {
+    DVSC = double(IRATSH) * DVI;
+    V1SHFT = double(IRATSH - 1) * DVI / 2.;
+  } else {
+    IRATSH = 1;
+    DVSC = DVI;
+  }
+  const double SRATIO = IRATSH;
+  const int64_t nc = n / IRATSH;
+  std::vector<double> sc1(nc + 1, 0.);  // 1-based
+  for (int64_t k = 1; k <= nc; k++) {
+    double SUMK = 0.;
+    for (long j = 0; j < IRATSH; j++) SUMK = SUMK + s[(k - 1) * IRATSH + j];
+    sc1[k] = SUMK / SRATIO;
+  }
+  const double V1I = v1_in + V1SHFT;
+  // CONVSC on the global output grid (R1(1) at VFT0)
+  const double RATIO = DVSC / S.dvo, DVODX = S.dvo / S.dxf, HWBND = S.hwf / S.dvo;
+  const double ZINT = (V1I - S.vft0) / S.dvo;
+  const double ZSLOPE = DVODX / S.hwhm, ZBOUND = HWBND * S.hwhm, XNORM = DVSC / S.hwhm;
+  long ILO = fint(((S.vbot - V1I) / DVSC) + 1.5);
+  ILO = std::max(ILO, 1L);
+  long IHI = fint(((S.vtop - V1I) / DVSC) + 1.5);
+  IHI = std::min<long>(IHI, nc);
+  std::vector<double> R1(S.nnhi + 2, 0.);
+  for (long I = ILO; I <= IHI; I++) {
+    if (sc1[I] == 0.) continue;
+    const double ZPEAK = double(I - 1) * RATIO + ZINT;
+    long JMAX = fint(ZPEAK + ZBOUND + 1.5);
+    long JMIN = fint(ZPEAK - ZBOUND + 1.5);
+    JMIN = std::max(JMIN, 1L);
+    const double SI = XNORM * sc1[I];
+    for (long JF = JMIN; JF <= JMAX && JF <= S.nnhi; JF++) {
+      const double ZF = (double(JF - 1) - ZPEAK) * ZSLOPE;
+      long IT = fint(std::fabs(ZF) + 1.5);
+      if (IT > S.nfmax) IT = S.nfmax;
+      R1[JF] = R1[JF] + SI * S.xf[IT];
+    }
+  }
+  out.assign(R1.begin() + 33, R1.begin() + S.nnhi + 1);
+  return LBL_OK;
+}
+
 }  // namespace
 
 // =========================================================================
@@ -2129,6 +2278,25 @@ int orc_dv_rule(const lbl_run* R, lbl_layer* Ls, int nlay) {
 }
 
 int64_t orc_layer_npts(const lbl_run* R, double dv) { return npts_of(*R, dv); }
+
+// SCANFN convolution of a spectrum on v1_in + i*dv_in; *n_out receives the
+// output count, out may be NULL to ask for it only.
+int orc_scan(const lbl_scan* sc, const double* spec, int64_t n, double v1_in, double dv_in,
+             double* out, int64_t cap, int64_t* n_out, double* dvout) {
+  g_err.clear();
+  ScanOracle S;
+  int rc = scan_setup(*sc, dv_in, S);
+  if (rc) return rc;
+  *n_out = S.nnhi - 32;
+  if (dvout) *dvout = S.dvo;
+  if (!out) return LBL_OK;
+  std::vector<double> res;
+  rc = scan_spectrum(*sc, spec, n, v1_in, dv_in, res);
+  if (rc) return rc;
+  if ((int64_t)res.size() > cap) return fail(LBL_E_ARG, "output capacity");
+  std::copy(res.begin(), res.end(), out);
+  return LBL_OK;
+}
 
 // PNLINT re-grid of a layer optical depth to DVOUT.  *n_out receives the
 // point count; od_out may be NULL to ask for the count only.

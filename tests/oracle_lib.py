@@ -137,3 +137,18 @@ def pnlint(run, dv, dvout, od):
     check(L.orc_pnlint(*args, out.ctypes.data_as(C.POINTER(C.c_double)), C.c_int64(len(out)),
                        C.byref(n)))
     return out
+
+
+def scan(sc, spec, v1_in, dv_in):
+    """SCANFN convolution (oracle restatement)."""
+    L = lib()
+    spec = np.ascontiguousarray(spec, dtype=np.float64)
+    n = C.c_int64(0)
+    dvo = C.c_double(0.0)
+    P = C.POINTER(C.c_double)
+    args = [C.byref(sc), spec.ctypes.data_as(P), C.c_int64(len(spec)), C.c_double(v1_in),
+            C.c_double(dv_in)]
+    check(L.orc_scan(*args, None, C.c_int64(0), C.byref(n), C.byref(dvo)))
+    out = np.zeros(n.value)
+    check(L.orc_scan(*args, out.ctypes.data_as(P), C.c_int64(len(out)), C.byref(n), C.byref(dvo)))
+    return out, dvo.value
