@@ -1980,6 +1980,31 @@ int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int6
   if (rc) return fail(ctx, rc, e);
   if (P.n_out != n_out) return fail(ctx, LBL_E_ARG, "n_out does not match the output grid");
   cudaSetDevice(ctx->device);
+  if (P.jfn == 0) {
+    // CNVRCT: every box, with both of its end points, inside the input
+    const double vlast = sc->v1 + double(P.n_out - 1) * P.dvo + P.hwhm;
+    if (v1_in > sc->v1 - P.hwhm - dv_in || v1_in + double(n - 1) * dv_in < vlast + dv_in)
+      return fail(ctx, LBL_E_RANGE, "scan: the boxes must lie inside the spectrum");
+    const bool in_dev = is_device_ptr(spec), out_dev = is_device_ptr(out);
+    size_t bytes = 256;
+    if (!in_dev) bytes += n * 8 + 256;
+    if (!out_dev) bytes += n_out * 8 + 256;
+    CK(ctx->arena.reserve(bytes, ctx->mem));
+    ctx->arena.reset();
+    cudaStream_t s = ctx->stream;
+    const double* din = spec;
+    if (!in_dev) {
+      double* t = ctx->arena.take<double>(n);
+      CK(cudaMemcpyAsync(t, spec, n * 8, cudaMemcpyHostToDevice, s));
+      din = t;
+    }
+    double* dout = out_dev ? out : ctx->arena.take<double>(n_out);
+    CK(launch_scan_rect(din, n, sc->jabs ? 1 : 0, sc->v1, P.dvo, P.hwhm, v1_in, dv_in, dout, n_out,
+                        s));
+    if (!out_dev) CK(cudaMemcpyAsync(out, dout, n_out * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return LBL_OK;
+  }
   // SHRKSC: full groups of IRATSH points; the compressed input's first
   // wavenumber and the CONVSC range from VBOT/VTOP (src/postsub.f90:1330-1355)
   const int64_t nc = n / P.iratsh;

@@ -3065,4 +3065,46 @@ cudaError_t launch_scan(const double* spec, int64_t n, int ir, int jabs, double*
   return cudaGetLastError();
 }
 
+// CNVRCT (src/postsub.f90:1779-1985), one thread per box: the inner points
+// weighted 1, the end points by the fraction of their interval inside the
+// box, the weighted sum over the sum of the weights; the reference's order
+// of operations, each rounded separately.
+__global__ void k_scan_rect(const double* __restrict__ spec, int64_t n, int jabs, double v1,
+                            double dvo, double hwhm, double v1i, double dvi,
+                            double* __restrict__ out, int64_t n_out) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_out) return;
+  auto S = [&](int64_t i) {  // 1-based
+    const double x = spec[i - 1];
+    return jabs ? __dsub_rn(1., x) : x;
+  };
+  const double vcnt = __dadd_rn(v1, __dmul_rn((double)j, dvo));
+  const double vlft = __dsub_rn(vcnt, hwhm), vrgt = __dadd_rn(vcnt, hwhm);
+  const double rl = __dadd_rn(__ddiv_rn(__dsub_rn(vlft, v1i), dvi), 1.);
+  const double rr = __dadd_rn(__ddiv_rn(__dsub_rn(vrgt, v1i), dvi), 1.);
+  int64_t il = (int64_t)__dadd_rn(rl, 0.5), ih = (int64_t)__dadd_rn(rr, 0.5);
+  il = il < 1 ? 1 : il;
+  ih = ih > n ? n : ih;
+  const double half = __ddiv_rn(dvi, 2.);
+  const double wgtl = __ddiv_rn(
+      __dsub_rn(__dadd_rn(__dadd_rn(v1i, __dmul_rn((double)(il - 1), dvi)), half), vlft), dvi);
+  const double wgtr = __ddiv_rn(
+      __dsub_rn(vrgt, __dsub_rn(__dadd_rn(v1i, __dmul_rn((double)(ih - 1), dvi)), half)), dvi);
+  double sum = 0.;
+  for (int64_t i = il + 1; i <= ih - 1; i++) sum = __dadd_rn(sum, S(i));
+  sum = __dadd_rn(sum, __dmul_rn(S(il), wgtl));
+  sum = __dadd_rn(sum, __dmul_rn(S(ih), wgtr));
+  const double rnj = __dadd_rn(__dadd_rn((double)(ih - il + 1 - 2), wgtl), wgtr);
+  out[j] = __ddiv_rn(sum, rnj);
+}
+
+cudaError_t launch_scan_rect(const double* spec, int64_t n, int jabs, double v1, double dvo,
+                             double hwhm, double v1i, double dvi, double* out, int64_t n_out,
+                             cudaStream_t s) {
+  if (n_out > 0)
+    k_scan_rect<<<(unsigned)((n_out + 255) / 256), 256, 0, s>>>(spec, n, jabs, v1, dvo, hwhm,
+                                                                 v1i, dvi, out, n_out);
+  return cudaGetLastError();
+}
+
 }  // namespace lbl

@@ -212,6 +212,11 @@ constexpr int kJacMaxParams = 8;
 // SCANFN: SHRKSC's compression of spec (n points, groups of ir, 1 - x when
 // jabs) into sc (n / ir points), then CONVSC's sums on the global output
 // grid, one thread per output point (the inputs ilo..ihi, 1-based).
+// CNVRCT: weighted means of the input over boxes of half width hwhm centred
+// at v1 + j*dvo (j < n_out; every box inside the input).
+cudaError_t launch_scan_rect(const double* spec, int64_t n, int jabs, double v1, double dvo,
+                             double hwhm, double v1i, double dvi, double* out, int64_t n_out,
+                             cudaStream_t s);
 cudaError_t launch_scan(const double* spec, int64_t n, int ir, int jabs, double* sc, int64_t ilo,
                         int64_t ihi, double zint, double ratio, double zbound, double zslope,
                         double xnorm, const double* xf, int64_t nfmax, double* out,

@@ -636,8 +636,8 @@ int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
       return LBL_E_ARG;
     }
   }
-  if (jfn < 1 || jfn > 4) {
-    *err = "scan: JFN must be 1-4 (triangle, Gaussian, sinc^2, sinc)";
+  if (jfn < 0 || jfn > 4) {
+    *err = "scan: JFN must be 0-4 (rectangle, triangle, Gaussian, sinc^2, sinc)";
     return LBL_E_ARG;
   }
   const double xscale = XSCAL[jfn];
@@ -656,6 +656,22 @@ int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
   }
   P->hwhm = hwhm;
   P->dvo = hwhm / sample;
+  if (jfn == 0) {
+    // adjacent boxes of 2 HWHM (SCANFN :393-399, CNVRCT :1779-1985): DVO a
+    // whole number IRATIO of input steps; the boxes centred at V1 + (NB-1)
+    // DVO up to V2
+    const long iratio = fint(P->dvo / dv_in + 0.5);
+    P->dvo = double(iratio) * dv_in;
+    if (iratio < 2) {
+      *err = "scan: IRATIO LESS THAN 2, NO SCANFN";
+      return LBL_E_RANGE;
+    }
+    int64_t nb = 1;
+    while (sc.v1 + double(nb) * P->dvo <= sc.v2) nb++;
+    P->n_out = nb;
+    P->nnhi = nb + kNShift;
+    return LBL_OK;
+  }
   const long nbound = fint((2. * P->hwf) * sample + 0.01);
   P->bound = double(nbound) * P->dvo / 2.;
   P->vft0 = sc.v1 - double(kNShift) * P->dvo;

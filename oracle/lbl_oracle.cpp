@@ -2087,7 +2087,7 @@ int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
     JFN = -JFN;
     if (JFN != 3 && JFN != 4) return fail(LBL_E_ARG, "SCANFN; INVALID JFN");
   }
-  if (JFN < 1 || JFN > 4) return fail(LBL_E_ARG, "scan: JFN 1-4 (triangle, Gauss, sinc^2, sinc)");
+  if (JFN < 0 || JFN > 4) return fail(LBL_E_ARG, "scan: JFN 0-4 (rectangle, triangle, Gauss, sinc^2, sinc)");
   const double XSCALE = XSCAL[JFN];
   if (sc.jfn < 0) HWHM = HWHM / (PI / XSCALE);
   S.jfn = JFN;
@@ -2103,6 +2103,16 @@ int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
   S.hwhm = HWHM;
   S.sample = SAMPLE;
   S.dvo = HWHM / SAMPLE;
+  if (JFN == 0) {
+    // adjacent boxes of 2 HWHM (SCANFN :393-399): DVO a whole number of DVI
+    const long IRATIO = fint(S.dvo / dv_in + 0.5);
+    S.dvo = double(IRATIO) * dv_in;
+    if (IRATIO < 2) return fail(LBL_E_RANGE, "scan: IRATIO LESS THAN 2, NO SCANFN");
+    long NB = 1;
+    while (sc.v1 + double(NB) * S.dvo <= sc.v2) NB++;
+    S.nnhi = NB + 32;  // boxes NB = 1.. with VCNT <= V2
+    return LBL_OK;
+  }
   const long NBOUND = fint((2. * S.hwf) * SAMPLE + 0.01);
   S.bound = double(NBOUND) * S.dvo / 2.;
   S.vft0 = sc.v1 - 32. * S.dvo;
@@ -2149,6 +2159,51 @@ int scan_spectrum(const lbl_scan& sc, const double* spec, int64_t n, double v1_i
   // RDSCAN (:1411-1514): JEMIT=-1 convolves the absorption 1 - S
   std::vector<double> s(spec, spec + n);
   if (sc.jabs) for (auto& x : s) x = 1. - x;
+  if (S.jfn == 0) {
+    // CNVRCT (:1779-1985) on the whole input: box NB centred at V1 +
+    // (NB-1) DVO, half width HWHM; inner points weight 1, the end points
+    // the fraction of their interval inside the box; the weighted mean
+    const double DVI = dv_in, V1I = v1_in;
+    const long NNI = (long)n;
+    // the boxes must lie inside the spectrum (the reference outputs no box
+    // that runs past its data)
+    const double vlast = sc.v1 + double(S.nnhi - 33) * S.dvo + S.hwhm;
+    if (v1_in > sc.v1 - S.hwhm - DVI || v1_in + double(n - 1) * DVI < vlast + DVI)
+      return fail(LBL_E_RANGE, "scan: the boxes must lie inside the spectrum");
+    out.clear();
+    for (long NB = 1; NB <= S.nnhi - 32; NB++) {
+      const double VCNT = sc.v1 + double(NB - 1) * S.dvo;
+      const double VLFT = VCNT - S.hwhm, VRGT = VCNT + S.hwhm;
+      const double RL = (VLFT - V1I) / DVI + 1, RR = (VRGT - V1I) / DVI + 1;
+      long IL = fint(RL + 0.5), IH = fint(RR + 0.5);
+      double WGTL = ((V1I + double(IL - 1) * DVI) + DVI / 2. - VLFT) / DVI;
+      double WGTR = (VRGT - ((V1I + double(IH - 1) * DVI) - DVI / 2.)) / DVI;
+      long NEP = 2;
+      if (IH > NNI) {
+        IH = NNI;
+        WGTR = 1.;
+        if (IL == IH) {
+          WGTR = 0.;
+          NEP = 1;
+        }
+      }
+      if (IL <= 1) {
+        IL = 1;
+        WGTL = 1.;
+        if (IL >= IH) {
+          WGTL = 0.;
+          NEP = 1;
+        }
+      }
+      double SUMJ = 0.;
+      for (long I = IL + 1; I <= IH - 1; I++) SUMJ = SUMJ + s[I - 1];
+      SUMJ = SUMJ + s[IL - 1] * WGTL;
+      SUMJ = SUMJ + s[IH - 1] * WGTR;
+      const double RNJ = double(IH - IL + 1 - NEP) + WGTL + WGTR;
+      out.push_back(SUMJ / RNJ);
+    }
+    return LBL_OK;
+  }
   // SHRKSC
   static const long JRATIO[25] = {0, 1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20,
                                   24, 25, 30, 32, 40, 48, 50, 60, 75, 80, 100, 120};

@@ -3,7 +3,8 @@ restatement: the same compression, the same inputs summed in the same order
 for each output point, every product and sum rounded separately, so the
 results are compared exactly.  Inputs: a seeded synthetic radiance spectrum
 and the TOA radiance of a short forward, host and device buffers, all four
-functions, SAMPL given as points per HWHM and as an output spacing."""
+functions and the rectangle, SAMPL given as points per HWHM and as an
+output spacing."""
 import numpy as np
 import pytest
 
@@ -18,6 +19,8 @@ CASES = [
     (3, 0.3, -0.04, 1),
     (4, 0.8, 0.0, 0),
     (-3, 1.2, 0.0, 0),
+    (0, 0.3, 0.0, 0),
+    (0, 0.5, -0.07, 1),
 ]
 
 

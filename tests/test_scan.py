@@ -62,8 +62,53 @@ def test_output_grid_matches_oracle(jfn, sampl):
     assert abs(650.0 + (n - 1) * dvo - 751.3) <= 0.5 * dvo + 1e-9
 
 
+def _box_means(spec, v1, dv, centres, hwhm):
+    """Mean of the nearest-point (step) reconstruction of spec over each box
+    [c - hwhm, c + hwhm]: every point weighted by the length of its interval
+    [v_i - dv/2, v_i + dv/2] inside the box."""
+    v = v1 + dv * np.arange(len(spec))
+    out = []
+    for c in centres:
+        lo = np.maximum(v - dv / 2, c - hwhm)
+        hi = np.minimum(v + dv / 2, c + hwhm)
+        w = np.clip(hi - lo, 0.0, None)
+        out.append(np.dot(w, spec) / w.sum())
+    return np.array(out)
+
+
+@pytest.mark.parametrize("hwhm,sampl,jabs", [(0.5, 0.0, 0), (0.3, -0.07, 1), (1.25, 3.0, 0)])
+def test_rectangle_is_the_box_mean(hwhm, sampl, jabs):
+    """CNVRCT (JFN=0): each output point is the mean of the spectrum over a
+    box of half width HWHM, the end points weighted by the fraction of their
+    interval inside the box; DVOUT a whole number of input steps."""
+    v1, dv = 600.0, 0.0013
+    rng = np.random.default_rng(7)
+    spec = np.exp(-rng.exponential(1.0, 150000))
+    sc = abi.make_scan(hwhm=hwhm, v1=640.0, v2=760.0, jfn=0, sampl=sampl, jabs=jabs)
+    out, dvo = O.scan(sc, spec, v1, dv)
+    sample = sampl if sampl > 0 else (hwhm / -sampl if sampl < 0 else 0.5)
+    assert dvo == round(hwhm / sample / dv) * dv
+    n, dvo_lib = gpu.scan_npts(sc, dv)
+    assert (n, dvo_lib) == (len(out), dvo)
+    centres = 640.0 + dvo * np.arange(len(out))
+    assert centres[-1] <= 760.0 < centres[-1] + dvo
+    ref = _box_means(1.0 - spec if jabs else spec, v1, dv, centres, hwhm)
+    np.testing.assert_allclose(out, ref, rtol=1e-11)
+    const, _ = O.scan(sc, np.full(150000, 0.37), v1, dv)
+    np.testing.assert_allclose(const, 0.63 if jabs else 0.37, rtol=1e-13)
+
+
 def test_rejections():
     sc = abi.make_scan(hwhm=0.6, v1=650.0, v2=750.0, jfn=2)
     assert gpu.load().lbl_scan_npts(C.byref(sc), 0.06, None) == -7   # DV > HWHM/12
     bad = abi.make_scan(hwhm=0.6, v1=650.0, v2=750.0, jfn=-2)
     assert gpu.load().lbl_scan_npts(C.byref(bad), 0.001, None) == -1
+    # rectangle: DVOUT under two input steps (IRATIO < 2)
+    rect = abi.make_scan(hwhm=0.6, v1=650.0, v2=750.0, jfn=0, sampl=-0.004)
+    assert gpu.load().lbl_scan_npts(C.byref(rect), 0.004, None) == -7
+    with pytest.raises(RuntimeError, match="IRATIO"):
+        O.scan(rect, np.zeros(100000), 600.0, 0.004)
+    # the boxes must lie inside the spectrum
+    rect = abi.make_scan(hwhm=0.6, v1=650.0, v2=750.0, jfn=0)
+    with pytest.raises(RuntimeError, match="inside the spectrum"):
+        O.scan(rect, np.zeros(30000), 600.0, 0.004)
