@@ -80,6 +80,11 @@ typedef struct lbl_run {
                        1: radiance and transmittance (EMINIT/RADMRG) */
   int32_t ipathl;   /* 1: upwelling radiance, looking down (the first layer
                           the surface's, TMPBND/BNDEMI its emission);
+                       2: the symmetric tangent path (IANT=0): the first
+                          layer is the tangent layer, every layer is crossed
+                          twice, its far crossing radiating at TZL (EMINIT
+                          src/xmerge.f90:2442-2447, RADNN IPATH=2
+                          :2997-3005, 3132-3148; TZL > 0 required);
                        3: downwelling radiance, looking up from the first
                           layer (RADNN IPATH=3, src/xmerge.f90:3007-3013,
                           3150-3166; TMPBND/BNDEMI a boundary beyond the
@@ -100,6 +105,17 @@ typedef struct lbl_run {
   double xrayl;     /* Rayleigh scale XRAYL, /CNTSCL/ (default 1, 0 = off):
                        with ICNTNM=1 and V2 >= 820 cm-1 the continuum adds
                        Rayleigh extinction (src/contnm.f90:955-976) */
+  double xco2c;     /* CO2 continuum scale XCO2C, /CNTSCL/ (default 1, 0 =
+                       off): with ICNTNM=1 the continuum adds the CO2
+                       continuum (src/contnm.f90:326-378, FRNCO2 :1295-1349)
+                       between the H2O part and Rayleigh */
+  double xo2cn;     /* O2 continuum scale XO2CN (default 1, 0 = off): the
+                       collision-induced fundamental, 1340-1850 cm-1
+                       (src/contnm.f90:491-540, o2_ver_1 :7254-7318) */
+  double xn2cn;     /* N2 continuum scale XN2CN (default 1, 0 = off): the
+                       collision-induced rotational band below 350 cm-1
+                       (:745-792, xn2_r :2497-2566) and fundamental,
+                       2001.77-2897.59 cm-1 (:811-858, n2_ver_1 :2668-2754) */
 } lbl_run;
 
 /* One layer: the /FILHDR/ quantities OPDPTH and XMERGE read

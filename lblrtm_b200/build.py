@@ -16,7 +16,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_SRCS = ["lbl_kernels.cu", "lbl_capi.cu", "lbl_noalloc.cu"]
 CPP_SRCS = ["lbl_plan.cpp", "lbl_tape3.cpp"]
-HEADERS = ["lbl_kernels.cuh", "lbl_plan.h", "../../include/lblgpu.h", "../data/ref_tables.h"]
+HEADERS = ["lbl_kernels.cuh", "lbl_plan.h", "../../include/lblgpu.h", "../data/ref_tables.h",
+           "../data/cont_tables.h"]
 
 
 def _newer(target, deps):

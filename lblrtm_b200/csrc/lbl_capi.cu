@@ -798,7 +798,7 @@ int run_od(lbl_ctx* ctx, const lbl_run& R, Batch& B, int precision) {
   CK(cudaEventRecord(ctx->cev[0], s));
   CK(cudaStreamWaitEvent(s2, ctx->cev[0], 0));
   CK(launch_near_lines(w, ctx->dl, max_near, s2));
-  if (R.icntnm) CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, R.xrayl, s2));
+  if (R.icntnm) CK(launch_continuum(w, ctx->ck, R.xself, R.xfrgn, R.xrayl, R.xco2c, R.xo2cn, R.xn2cn, s2));
   CK(launch_panel_segs(w, B.npanel_total, B.d_panel_layer, B.d_panel_base, B.d_panel_segs,
                        B.d_panel_nseg, s2));
   CK(cudaEventRecord(ctx->cev[1], s2));
@@ -886,8 +886,9 @@ int check_run(lbl_ctx* ctx, const lbl_run* R) {
   if (R->v1 - 32. * 1e-9 <= 0.) return fail(ctx, LBL_E_RANGE, "V1 must be positive");
   if (!(R->sample > 0.) || !(R->alfal0 > 0.)) return fail(ctx, LBL_E_ARG, "SAMPLE/ALFAL0");
   if (R->iemit != 0 && R->iemit != 1) return fail(ctx, LBL_E_ARG, "IEMIT must be 0 or 1");
-  if (R->iemit == 1 && R->ipathl != 1 && R->ipathl != 3)
-    return fail(ctx, LBL_E_ARG, "IPATHL must be 1 (looking down) or 3 (looking up)");
+  if (R->iemit == 1 && R->ipathl != 1 && R->ipathl != 2 && R->ipathl != 3)
+    return fail(ctx, LBL_E_ARG,
+                "IPATHL must be 1 (looking down), 2 (tangent path) or 3 (looking up)");
   if (!ctx->have_lines) return fail(ctx, LBL_E_NOTREADY, "lines not uploaded");
   return LBL_OK;
 }
@@ -963,9 +964,16 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     const bool down = R.ipathl == 3;
     m.down = down ? 1 : 0;
     m.tbnd_last = (down && e == n && n > 1) ? R.tmpbnd : 0.;
+    // the symmetric tangent path (IPATHL=2, IANT=0): each layer's far
+    // crossing radiates at its lower level's temperature (XKTB,
+    // src/xmerge.f90:2417-2420, 2771-2773)
+    m.tangent = R.ipathl == 2 ? 1 : 0;
     for (int k = l; k < e; k++) {
       m.od_off[k - l] = ld[k].off_od;
       m.t[k - l] = emin_temps(ld[k].tave, down ? layers[k].tzl : layers[k].tzu);
+      const double tzl = layers[k].tzl;
+      m.tb_xkt[k - l] = (m.tangent && tzl > 0.) ? tzl / kRADCN2 : 0.;
+      m.tb_rk[k - l] = (m.tangent && tzl > 0.) ? kRADCN2 / tzl : 0.;
       ctx->stage("merge").work += (double)ld[k].npts;
     }
     const int nxt = cur ^ 2;
@@ -1893,12 +1901,15 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, in
     CK(cudaMemcpyAsync(ctx->mbuf[0], rad_in, n_old * 8, cudaMemcpyDefault, s));
     if (run->iemit == 1) CK(cudaMemcpyAsync(ctx->mbuf[1], tr_in, n_old * 8, cudaMemcpyDefault, s));
   }
+  if (run->iemit == 1 && run->ipathl == 2 && !(layer->tzl > 0.))
+    return fail(ctx, LBL_E_ARG, "the tangent path (IPATHL=2) needs TZL > 0");
   const double tbnd = (first && run->ipathl == 1) ? run->tmpbnd : 0.;
   const bool down = run->ipathl == 3;
   const double tbnd_last = (down && last && !first) ? run->tmpbnd : 0.;
   CK(launch_merge(dL, dv, dod, n_new, first, dv_old, n_old, ctx->mbuf[0], ctx->mbuf[1],
                   ctx->mbuf[2], ctx->mbuf[3], tbnd, run->bndemi, run->iemit,
-                  down ? layer->tzl : layer->tzu, s, LBL_PREC_FP64, down ? 1 : 0, tbnd_last));
+                  down ? layer->tzl : layer->tzu, s, LBL_PREC_FP64, down ? 1 : 0, tbnd_last,
+                  run->ipathl == 2 ? layer->tzl : 0.));
   CK(cudaMemcpyAsync(rad_out, ctx->mbuf[2], n_new * 8, cudaMemcpyDefault, s));
   if (tr_out) CK(cudaMemcpyAsync(tr_out, ctx->mbuf[3], n_new * 8, cudaMemcpyDefault, s));
   CK(cudaStreamSynchronize(s));

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <type_traits>
 
+#include "../data/cont_tables.h"
 #include "../data/ref_tables.h"
 #include "lbl_kernels.cuh"
 
@@ -1632,7 +1633,167 @@ __device__ void h2o_part(const LayerDev& L, const DevMtckd& ck, double h2o_fac, 
   }
 }
 
-__global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn, double xrayl) {
+// The continua of CONTNM after H2O (src/contnm.f90:326-994) each tabulate
+// coefficients on a coarse grid of their own (V1S, DVS, NPTS), set up alike
+// (FRNCO2 :1322-1337 and its siblings): from one point below V1ABS-DVS to
+// one above V2ABS+DVS.  The layer's coefficients C(J) on that grid are
+// added to ABSRB by XINT between pre_xint's IST and LAST (:994-1012); the
+// four C(J) a point's interpolation needs are formed where used.
+struct CoarseGrid {
+  int64_t i1, nptc;
+  double v1c, v2c, dvc;
+};
+__device__ CoarseGrid coarse_grid(double V1S, double DVS, int64_t NPTS, const LayerDev& L) {
+  CoarseGrid g;
+  g.dvc = DVS;
+  const double v1c = L.v1abs - DVS, v2c = L.v2abs + DVS;
+  g.i1 = (v1c < V1S) ? -1 : fint((v1c - V1S) / DVS + 0.01);
+  g.v1c = V1S + DVS * double(g.i1 - 1);
+  const int64_t i2 = fint((v2c - V1S) / DVS + 0.01);
+  g.nptc = i2 - g.i1 + 3;
+  if (g.nptc > NPTS) g.nptc = NPTS + 4;
+  g.v2c = g.v1c + DVS * double(g.nptc - 1);
+  return g;
+}
+
+// XINT (src/oprop.f90:2201-2234, AFACT = 1) of C(J) = coef(J, VJ) (0 for J
+// outside 1..NPTC) onto the layer's ABSRB points, the block's threads
+// taking points in turn.
+template <typename Coef>
+__device__ void xint_coarse(const LayerDev& L, const CoarseGrid& g, double V1SS, double V2SS,
+                            Coef coef, double* absrb) {
+  auto C = [&](int64_t j) -> double {
+    return (j < 1 || j > g.nptc) ? 0. : coef(j, g.v1c + g.dvc * double(j - 1));
+  };
+  int64_t ist = fint(2 + (V1SS - L.v1abs) / L.dvabs + 1.e-5);
+  if (ist < 1) ist = 1;
+  int64_t last = fint(1 + (V2SS - L.v1abs) / L.dvabs + 1.e-5);
+  if (last > L.nptabs) last = L.nptabs;
+  const double rec = 1. / g.dvc;
+  int64_t ilo = fint((g.v1c + g.dvc - L.v1abs) / L.dvabs + 1. + kONEMI);
+  if (ilo < ist) ilo = ist;
+  int64_t ihi = fint((g.v2c - g.dvc - L.v1abs) / L.dvabs + kONEMI);
+  if (ihi > last) ihi = last;
+  for (int64_t I = ilo + threadIdx.x; I <= ihi; I += blockDim.x) {
+    const double vi = L.v1abs + L.dvabs * double(I - 1);
+    const int64_t J = fint((vi - g.v1c) * rec + kONEPL);
+    const double vj = g.v1c + g.dvc * double(J - 1);
+    const double p = rec * (vi - vj);
+    const double Cq = (3. - 2. * p) * p * p;
+    const double B = 0.5 * p * (1. - p);
+    const double b1 = B * (1. - p), b2 = B * p;
+    const double conti =
+        -C(J - 1) * b1 + C(J) * (1. - Cq + b2) + C(J + 1) * (Cq + b1) - C(J + 2) * b2;
+    absrb[I] = absrb[I] + conti * 1.0;
+  }
+}
+
+__device__ const double d_fco2[LBL_FCO2_N] = {LBL_FCO2_VALUES};
+__device__ const double d_xfacco2[500] = {LBL_XFACCO2_VALUES};
+__device__ const double d_co2_tdep[25] = {LBL_CO2_TDEP_VALUES};
+__device__ const double d_o2f_x[LBL_O2F_N] = {LBL_O2F_XO2_VALUES};
+__device__ const double d_o2f_t[LBL_O2F_N] = {LBL_O2F_XO2T_VALUES};
+__device__ const double d_n2r_c296[LBL_N2R296_N] = {LBL_N2R296_C_VALUES};
+__device__ const double d_n2r_sf296[LBL_N2R296_N] = {LBL_N2R296_SF_VALUES};
+__device__ const double d_n2r_c220[LBL_N2R220_N] = {LBL_N2R220_C_VALUES};
+__device__ const double d_n2r_sf220[LBL_N2R220_N] = {LBL_N2R220_SF_VALUES};
+__device__ const double d_n2f_272[LBL_N2F_N] = {LBL_N2F_X272_VALUES};
+__device__ const double d_n2f_228[LBL_N2F_N] = {LBL_N2F_X228_VALUES};
+__device__ const double d_n2f_ah2o[LBL_N2F_N] = {LBL_N2F_AH2O_VALUES};
+
+struct ContScale {
+  double xco2c, xo2cn, xn2cn;
+};
+
+// CO2 (:326-378, FRNCO2 :1295-1349: the band-head temperature dependence
+// of points 1196-1220), the mt_ckd_2.5 factors XFACCO2 from 2000 to 2998
+// cm-1, WCO2; the O2 collision-induced fundamental (:491-540, o2_ver_1
+// :7254-7318); the N2 collision-induced rotational band (:745-792, xn2_r
+// :2497-2566) and fundamental (:811-858, n2_ver_1 :2668-2754); each times
+// the radiation term on its coarse grid when JRAD=1, and added in CONTNM's
+// order.
+__device__ void cia_parts(const LayerDev& L, const ContScale& xs, double* absrb) {
+  const double xkt = L.tave / kRADCN2;
+  const double rhoave = (L.pave / 1013.) * (296. / L.tave);
+  const double amagat = (L.pave / 1013.) * (273. / L.tave);
+  const double x_h2o = L.wk[1] / L.wtot, x_o2 = L.wk[7] / L.wtot;
+  const double x_n2 = 1. - x_h2o - x_o2;
+  const double wn2 = x_n2 * L.wtot;
+  const double xlosmt = 2.68675E+19;
+  auto rad = [&](double c, double vj) { return L.jrad == 1 ? c * radfn(vj, xkt) : c; };
+  if ((L.v2 > -20.0) && (L.v1 < 10000.) && xs.xco2c > 0.) {
+    __syncthreads();
+    const double wco2 = L.wk[2] * rhoave * 1.0E-20 * xs.xco2c;
+    const double trat = L.tave / LBL_CO2_TEFF;
+    const CoarseGrid g = coarse_grid(LBL_FCO2_V1, LBL_FCO2_DV, LBL_FCO2_N, L);
+    xint_coarse(L, g, LBL_FCO2_V1, LBL_FCO2_V2, [&](int64_t j, double vj) {
+      const int64_t I = g.i1 + (j - 1);
+      double c = 0.;
+      if (I >= 1 && I <= LBL_FCO2_N) {
+        double tcor = 1.;
+        if (I >= 1196 && I <= 1220) tcor = pow(trat, d_co2_tdep[I - 1196]);
+        c = tcor * d_fco2[I - 1];
+      }
+      double cfac = 1.;
+      if (vj >= 2000. && vj <= 2998.) cfac = d_xfacco2[fint((vj - 1998.) / 2. + 0.00001) - 1];
+      c = cfac * c;
+      return rad(c * wco2, vj);
+    }, absrb);
+  }
+  if ((L.v2 > 1340.0) && (L.v1 < 1850.) && xs.xo2cn > 0.) {
+    __syncthreads();
+    const double tau_fac = xs.xo2cn * L.wk[7] * 1.e-20 * amagat;
+    const double xktfac = (1. / 296.) - (1. / L.tave);
+    const double factor = (1.e+20 / xlosmt);
+    const CoarseGrid g = coarse_grid(LBL_O2F_V1, LBL_O2F_DV, LBL_O2F_N, L);
+    xint_coarse(L, g, LBL_O2F_V1, LBL_O2F_V2, [&](int64_t j, double vj) {
+      const int64_t I = g.i1 + (j - 1);
+      double c0 = 0.;
+      if (I >= 1 && I <= LBL_O2F_N) c0 = factor * d_o2f_x[I - 1] * exp(d_o2f_t[I - 1] * xktfac) / vj;
+      return rad(tau_fac * c0, vj);
+    }, absrb);
+  }
+  if ((L.v2 > -10.0) && (L.v1 < 350.) && xs.xn2cn > 0.) {
+    __syncthreads();
+    const double tau_fac = xs.xn2cn * (wn2 / xlosmt) * amagat;
+    const double tfac = (L.tave - 296.) / (220. - 296.);
+    const CoarseGrid g = coarse_grid(LBL_N2R296_V1, LBL_N2R296_DV, LBL_N2R296_N, L);
+    xint_coarse(L, g, LBL_N2R296_V1, LBL_N2R296_V2, [&](int64_t j, double vj) {
+      const int64_t I = g.i1 + (j - 1);
+      double c0 = 0., fo2 = 0.;
+      if (I >= 1 && I <= LBL_N2R296_N) {
+        c0 = d_n2r_c296[I - 1] * pow(d_n2r_c220[I - 1] / d_n2r_c296[I - 1], tfac);
+        const double sf_t = d_n2r_sf296[I - 1] * pow(d_n2r_sf220[I - 1] / d_n2r_sf296[I - 1], tfac);
+        fo2 = (sf_t - 1.) * (0.79) / (0.21);
+      }
+      return rad(tau_fac * c0 * (x_n2 + fo2 * x_o2 + 1. * x_h2o), vj);
+    }, absrb);
+  }
+  if ((L.v2 > 2001.77) && (L.v1 < 2897.59) && xs.xn2cn > 0.) {
+    __syncthreads();
+    const double tau_fac = xs.xn2cn * (wn2 / xlosmt) * amagat;
+    const double T = L.tave;
+    const double xtfac = ((1. / T) - (1. / 272.)) / ((1. / 228.) - (1. / 272.));
+    const double xt_lin = (T - 272.) / (228. - 272.);
+    const double a_o2 = 1.294 - 0.4545 * T / 296.;
+    const CoarseGrid g = coarse_grid(LBL_N2F_V1, LBL_N2F_DV, LBL_N2F_N, L);
+    xint_coarse(L, g, LBL_N2F_V1, LBL_N2F_V2, [&](int64_t j, double vj) {
+      const int64_t I = g.i1 + (j - 1);
+      double c0 = 0., c1 = 0., c2 = 0.;
+      if (I >= 1 && I <= LBL_N2F_N) {
+        const double a = d_n2f_272[I - 1], b = d_n2f_228[I - 1];
+        c0 = (a > 0. && b > 0.) ? a * pow(b / a, xtfac) : a + (b - a) * xt_lin;
+        c0 = c0 / vj;
+        c1 = a_o2 * c0;
+        c2 = (9. / 7.) * d_n2f_ah2o[I - 1] * c0;
+      }
+      return rad(tau_fac * (x_n2 * c0 + x_o2 * c1 + x_h2o * c2), vj);
+    }, absrb);
+  }
+}
+
+__global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn, double xrayl,
+                            ContScale xs) {
   const int l = blockIdx.x;
   const LayerDev& L = w.L[l];
   double* absrb = w.absrb + L.off_abs;  // 1-based, nptabs+4
@@ -1642,8 +1803,9 @@ __global__ void k_continuum(Work w, DevMtckd ck, double xself, double xfrgn, dou
   const double h2o_fac = L.h2o_fac;  // WK(1)/WTOT of CONTNM (contnm.f90:261)
   if ((L.v2 > -20.0) && (L.v1 < 20000.) && ((xself > 0.) || (xfrgn > 0)))
     h2o_part(L, ck, h2o_fac, absrb, xself, xfrgn);
+  cia_parts(L, xs, absrb);
   // Rayleigh extinction (src/contnm.f90:955-976; no aerosols, IAERSL=0),
-  // added to every point of the 1 cm-1 grid after the H2O part
+  // added to every point of the 1 cm-1 grid after the other parts
   if (L.v2 >= 820. && xrayl > 0.) {
     __syncthreads();
     const double conv_cm2mol = xrayl * 1.E-20 / (2.68675e-1 * 1.e5);
@@ -2231,6 +2393,25 @@ __device__ __forceinline__ void emin_point(double odv, double vi, const EminT& t
   em = ((T)1. - tr) * (bb + bbd * fi);
 }
 
+// EMIN at one point for the symmetric tangent path (XKTB > 0, specular,
+// src/xmerge.f90:1984-2019): the emission of the layer's near crossing (the
+// level term at XKTA) and of its far crossing (the level term at XKTB).
+template <typename T>
+__device__ __forceinline__ void emin_point_b(double odv, double vi, const EminT& t, double xktb,
+                                             double rkb, T& tr, T& em, T& emb) {
+  T o = (T)odv;
+  if (o < (T)-kODLO) o = (T)-kODLO;
+  tr = exp(-o);
+  const T d = tr - (T)1.;
+  const T fi = (o <= (T)kODLO) ? o * (T)(1. / 6.) : (T)1. - (T)2. * ((tr * o + d) / (d * o));
+  const T bb = planck_t<T>(vi, t.xkt, t.rk);
+  const T bba = (t.xkta > 0.) ? planck_t<T>(vi, t.xkta, t.rka) - bb : (T)0.;
+  const T bbb = (xktb > 0.) ? planck_t<T>(vi, xktb, rkb) - bb : (T)0.;
+  const T ab = (T)1. - tr;
+  em = ab * (bb + bba * fi);
+  emb = ab * (bb + bbb * fi);
+}
+
 // emin_point in FP64 with the three divisions (two Planck quotients
 // e/(1-e) and the source weight's common denominator) taken from one
 // reciprocal of their product; differs from emin_point by a few units in
@@ -2264,6 +2445,42 @@ __device__ __forceinline__ void emin_point_1div(double odv, double vi, const Emi
   const bool bnd = t.xkta > 0.;
   if (bnd) pre(t.xkta, t.rka, e2, s2, b2);
   else b2 = 0, e2 = 0., s2 = 0.;
+  const double D1 = b1 == 2 ? 1. - e1 : 1.;
+  const double D2 = b2 == 2 ? 1. - e2 : 1.;
+  const double D3 = lin ? 1. : d * o;
+  const double r = 1. / ((D1 * D2) * D3);
+  const double v3 = (vi * vi) * vi;
+  const double bb = kRADCN1 * (b1 == 2 ? v3 * e1 * ((D2 * D3) * r) : s1);
+  const double bt = kRADCN1 * (b2 == 2 ? v3 * e2 * ((D1 * D3) * r) : s2);
+  const double bbd = bnd ? bt - bb : 0.;
+  const double fi = lin ? o * (1. / 6.) : 1. - 2. * ((tr * o + d) * ((D1 * D2) * r));
+  em = (1. - tr) * (bb + bbd * fi);
+}
+
+// emin_point_1div with the two Planck exponentials e1 = exp(-vi*rk) and
+// e2 = exp(-vi*rka) supplied by the caller (used only where the main
+// Planck branch applies).
+__device__ __forceinline__ void emin_point_e(double odv, double vi, const EminT& t, double e1,
+                                             double e2, double& tr, double& em) {
+  double o = odv;
+  if (o < -kODLO) o = -kODLO;
+  tr = exp(-o);
+  const double d = tr - 1.;
+  const bool lin = o <= kODLO;
+  auto branch = [&](double xkt, double rk, double& small) {
+    small = 0.;
+    if (!(xkt > 0.0)) return 0;
+    const double x = vi * rk;
+    if (x < 1e-2) {
+      small = (vi * vi) * xkt / (1. + 0.5 * x);
+      return 1;
+    }
+    return x <= 80. ? 2 : 0;
+  };
+  double s1, s2 = 0.;
+  const int b1 = branch(t.xkt, t.rk, s1);
+  const bool bnd = t.xkta > 0.;
+  const int b2 = bnd ? branch(t.xkta, t.rka, s2) : 0;
   const double D1 = b1 == 2 ? 1. - e1 : 1.;
   const double D2 = b2 == 2 ? 1. - e2 : 1.;
   const double D3 = lin ? 1. : d * o;
@@ -2329,7 +2546,8 @@ template <typename T>
 __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const double* od,
                         int first, double dv_old, int64_t n_old64, const double* rad_in,
                         const double* tr_in, double* rad_out, double* tr_out, double tbnd,
-                        double emis, int iemit, double tzu, int down, double tbnd_last) {
+                        double emis, int iemit, double tzu, int down, double tbnd_last,
+                        double tzl_tangent) {
   const LayerDev& L = *Lp;
   const int32_t f = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
   if (f >= (int32_t)L.npts) return;
@@ -2347,6 +2565,24 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
     return;
   }
   T tr, em;
+  if (tzl_tangent > 0.) {
+    // the symmetric tangent path (IPATHL=2, IANT=0): EMINIT :2442-2447,
+    // RADNN IPATH=2 :2997-3005, 3132-3148
+    T emb;
+    emin_point_b<T>(odv, vi, emin_temps(L.tave, tzu), tzl_tangent / kRADCN2,
+                    kRADCN2 / tzl_tangent, tr, em, emb);
+    if (first) {
+      rad_out[f] = (double)em + (double)emb * (double)tr;
+      tr_out[f] = (double)tr * (double)tr;
+      return;
+    }
+    double ro, to;
+    merge_regrid(rad_in, tr_in, n_old, f, itype, ro, to);
+    const double tt = (double)tr * to;
+    rad_out[f] = (double)tr * ro + (double)em + (double)emb * tt;
+    tr_out[f] = (double)tr * tt;
+    return;
+  }
   emin_point<T>(odv, vi, emin_temps(L.tave, tzu), tr, em);
   if (first) {
     // EMINIT: boundary emission (:2436-2484)
@@ -2396,6 +2632,21 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
       continue;
     }
     T tr, em;
+    if (!DOWN && m.tangent) {
+      // the symmetric tangent path: EMINIT :2442-2447, RADNN IPATH=2
+      // :2997-3005, 3132-3148
+      T emb;
+      emin_point_b<T>(odv, vi, m.t[l], m.tb_xkt[l], m.tb_rk[l], tr, em, emb);
+      if (m.first && l == 0) {
+        ro = (double)em + (double)emb * (double)tr;
+        to = (double)tr * (double)tr;
+      } else {
+        const double tt = (double)tr * to;
+        ro = (double)tr * ro + (double)em + (double)emb * tt;
+        to = (double)tr * tt;
+      }
+      continue;
+    }
     if constexpr (sizeof(T) == 8) emin_point_1div(odv, vi, m.t[l], tr, em);
     else emin_point<T>(odv, vi, m.t[l], tr, em);
     if (m.first && l == 0) {
@@ -2417,6 +2668,99 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
     ro = ro + to * emis * (double)planck_t<T>(vi, m.tbnd_last / kRADCN2, kRADCN2 / m.tbnd_last);
   rad_out[f] = ro;
   if (tr_out) tr_out[f] = iemit ? to : 0.;
+}
+
+// k_merge_run in FP64 with MK points per thread, 256 apart (coalesced).
+// The Planck exponentials of a layer follow the points as a geometric
+// sequence: exp(-vi*rk) at the thread's first point, then one product by
+// exp(-256*DV*rk) per point (s_st1/s_st2, one per layer); the points'
+// wavenumbers differ from v + 256*j*DV only by the rounding of the panel
+// origins, a relative change of the exponential far below 1e-13.  Per point
+// and layer this leaves one exponential (the transmittance) and one
+// reciprocal.
+constexpr int kMergeThreads = 256;
+constexpr int kMergePointsPerThread = 2;
+template <bool DOWN, int MK>
+__global__ void __launch_bounds__(kMergeThreads) k_merge_run_f64(
+    const MergeRun m, const double* vft_panel, const double* od, int32_t f_lo, int32_t f_hi,
+    double DV, const double* rad_in, const double* tr_in, double* rad_out, double* tr_out,
+    double tbnd, double emis, int iemit) {
+  __shared__ double s_st1[kMergeRunMax], s_st2[kMergeRunMax];
+  const int tid = threadIdx.x;
+  if (tid < m.nl) {
+    const EminT& t = m.t[tid];
+    const double span = double(kMergeThreads) * DV;
+    s_st1[tid] = t.xkt > 0. ? exp(-span * t.rk) : 0.;
+    s_st2[tid] = t.xkta > 0. ? exp(-span * t.rka) : 0.;
+  }
+  __syncthreads();
+  const int32_t f0 = f_lo + (int32_t)blockIdx.x * (kMergeThreads * MK) + tid;
+  if (f0 >= f_hi) return;
+  double vi[MK], ro[MK], to[MK], odn[MK];
+#pragma unroll
+  for (int j = 0; j < MK; j++) {
+    const int32_t f = f0 + j * kMergeThreads;
+    const int32_t fc = f < f_hi ? f : f_hi - 1;  // clamped: loads stay in range
+    const int32_t p = fc / 2400;
+    vi[j] = (vft_panel[p] + double(33 - 1) * DV) + double(fc - 2400 * p) * DV;
+    ro[j] = 0.;
+    to[j] = 1.;
+    if (!m.first) {
+      if (iemit) merge_regrid(rad_in, tr_in, m.n_old, fc, m.itype, ro[j], to[j]);
+      else ro[j] = absmrg_regrid(rad_in, m.n_old, fc, m.itype);
+    }
+    odn[j] = od[m.od_off[0] + fc];
+  }
+  for (int l = 0; l < m.nl; l++) {
+    double odv[MK];
+#pragma unroll
+    for (int j = 0; j < MK; j++) {
+      odv[j] = odn[j];
+      if (l + 1 < m.nl) {
+        const int32_t f = f0 + j * kMergeThreads;
+        odn[j] = od[m.od_off[l + 1] + (f < f_hi ? f : f_hi - 1)];
+      }
+    }
+    if (iemit == 0) {
+#pragma unroll
+      for (int j = 0; j < MK; j++) ro[j] = (m.first && l == 0) ? odv[j] : odv[j] + ro[j];
+      continue;
+    }
+    const EminT t = m.t[l];
+    double e1 = t.xkt > 0. ? exp(-(vi[0] * t.rk)) : 0.;
+    double e2 = t.xkta > 0. ? exp(-(vi[0] * t.rka)) : 0.;
+    const double st1 = s_st1[l], st2 = s_st2[l];
+#pragma unroll
+    for (int j = 0; j < MK; j++) {
+      if (j > 0) {
+        e1 *= st1;
+        e2 *= st2;
+      }
+      double tr, em;
+      emin_point_e(odv[j], vi[j], t, e1, e2, tr, em);
+      if (m.first && l == 0) {
+        if (tbnd > 0.) em = em + tr * planck(vi[j], tbnd / kRADCN2, kRADCN2 / tbnd) * emis;
+        ro[j] = em;
+        to[j] = tr;
+      } else if (DOWN) {
+        ro[j] = ro[j] + em * to[j];
+        to[j] = tr * to[j];
+      } else {
+        ro[j] = tr * ro[j] + em;
+        to[j] = tr * to[j];
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < MK; j++) {
+    const int32_t f = f0 + j * kMergeThreads;
+    if (f >= f_hi) break;
+    double r = ro[j];
+    if (DOWN && iemit && m.tbnd_last > 0.)
+      r = r + to[j] * emis * planck(vi[j], m.tbnd_last / kRADCN2, kRADCN2 / m.tbnd_last);
+    rad_out[f] = r;
+    if (tr_out) tr_out[f] = iemit ? to[j] : 0.;
+  }
 }
 
 // =========================================================================
@@ -2781,8 +3125,9 @@ cudaError_t launch_near_walk(const Work& w, const DevLines& ln, int64_t max_pane
 }
 
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
-                             double xrayl, cudaStream_t s) {
-  k_continuum<<<w.nlay, 256, 0, s>>>(w, ck, xself, xfrgn, xrayl);
+                             double xrayl, double xco2c, double xo2cn, double xn2cn,
+                             cudaStream_t s) {
+  k_continuum<<<w.nlay, 256, 0, s>>>(w, ck, xself, xfrgn, xrayl, ContScale{xco2c, xo2cn, xn2cn});
   return cudaGetLastError();
 }
 
@@ -2843,15 +3188,18 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          int64_t npts, int first, double dv_old, int64_t n_old,
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
-                         cudaStream_t s, int precision, int down, double tbnd_last) {
+                         cudaStream_t s, int precision, int down, double tbnd_last,
+                         double tzl_tangent) {
   if (npts >= (int64_t(1) << 31) || n_old >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
   const unsigned nb = (unsigned)((npts + 255) / 256);
   if (precision == LBL_PREC_SPLIT)
     k_merge<float><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
-                                      rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last);
+                                      rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last,
+                                      tzl_tangent);
   else
     k_merge<double><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
-                                       rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last);
+                                       rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last,
+                                      tzl_tangent);
   return cudaGetLastError();
 }
 
@@ -2873,13 +3221,18 @@ cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const d
     else
       k_merge_run<float, false><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
                                                    rad_out, tr_out, tbnd, emis, iemit);
+  } else if (m.tangent) {
+    k_merge_run<double, false><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
+                                                  rad_out, tr_out, tbnd, emis, iemit);
   } else {
+    constexpr int MK = kMergePointsPerThread;
+    const unsigned nb64 = (unsigned)((f_hi - f_lo + kMergeThreads * MK - 1) / (kMergeThreads * MK));
     if (m.down)
-      k_merge_run<double, true><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
-                                                   rad_out, tr_out, tbnd, emis, iemit);
+      k_merge_run_f64<true, MK><<<nb64, kMergeThreads, 0, s>>>(
+          m, vft_panel, od, a, b, dv, rad_in, tr_in, rad_out, tr_out, tbnd, emis, iemit);
     else
-      k_merge_run<double, false><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
-                                                    rad_out, tr_out, tbnd, emis, iemit);
+      k_merge_run_f64<false, MK><<<nb64, kMergeThreads, 0, s>>>(
+          m, vft_panel, od, a, b, dv, rad_in, tr_in, rad_out, tr_out, tbnd, emis, iemit);
   }
   return cudaGetLastError();
 }

@@ -133,7 +133,8 @@ cudaError_t launch_near_lines(const Work& w, const DevLines& ln, int64_t max_nea
 cudaError_t launch_near_walk(const Work& w, const DevLines& ln, int64_t max_panel,
                              int64_t max_win, int64_t max_nblk, cudaStream_t s);
 cudaError_t launch_continuum(const Work& w, const DevMtckd& ck, double xself, double xfrgn,
-                             double xrayl, cudaStream_t s);
+                             double xrayl, double xco2c, double xo2cn, double xn2cn,
+                             cudaStream_t s);
 // RADFNI segments of every panel (needs only the plans).
 cudaError_t launch_panel_segs(const Work& w, int64_t npanel_total, const int32_t* panel_layer,
                               const int64_t* panel_base, double* segs, int32_t* nseg,
@@ -156,7 +157,7 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
                          cudaStream_t s, int precision = LBL_PREC_FP64, int down = 0,
-                         double tbnd_last = 0.);
+                         double tbnd_last = 0., double tzl_tangent = 0.);
 constexpr double kRADCN1 = 1.191042722E-12;  // src/phys_consts.f90:73
 constexpr double kRADCN2 = 1.4387752;        // src/phys_consts.f90:74
 // Temperatures of one EMIN step: XKT = T/RADCN2 and RADCN2/T for the layer
@@ -178,11 +179,15 @@ struct MergeRun {
   int32_t itype;                 // regrid of the incoming field (0: same grid)
   int32_t n_old;                 // points of the incoming field
   int32_t down;                  // looking up (IPATHL=3): RADNN IPATH=3
-  int32_t pad;
+  int32_t tangent;               // the symmetric tangent path (IPATHL=2):
+                                 // each layer crossed twice, RADNN IPATH=2
   double tbnd_last;              // > 0: the boundary beyond the run's last layer
                                  // (EMBND, the profile's last layer looking up)
   int64_t od_off[kMergeRunMax];  // each layer's optical depths in Work::od
   EminT t[kMergeRunMax];
+  // tangent path: XKTB (the lower level's temperature / RADCN2) and its
+  // reciprocal RADCN2 / TZL, per layer (0 when TZL <= 0)
+  double tb_xkt[kMergeRunMax], tb_rk[kMergeRunMax];
 };
 // Points [f_lo, f_hi) of the run's grid (f_hi < 0: to the end).
 cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const double* od,

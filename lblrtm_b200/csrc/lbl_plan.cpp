@@ -134,6 +134,11 @@ int dv_rule(const lbl_run& R, lbl_layer* Ls, int nlay, std::string* err) {
       *err = "layer " + std::to_string(l) + ": bad nmol/pave/tave";
       return LBL_E_ARG;
     }
+    if (R.iemit == 1 && R.ipathl == 2 && !(L.tzl > 0.)) {
+      // the tangent path's far crossing radiates at TZL (XKTB)
+      *err = "layer " + std::to_string(l) + ": the tangent path (IPATHL=2) needs TZL > 0";
+      return LBL_E_ARG;
+    }
     double sumwk = 0.;
     for (int m = 0; m < L.nmol; m++) sumwk = sumwk + L.wk[m];
     double wtotl = sumwk + L.wbroad;

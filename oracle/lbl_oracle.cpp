@@ -55,6 +55,7 @@
 
 #include "../include/lblgpu.h"
 #include "../lblrtm_b200/data/ref_tables.h"
+#include "../lblrtm_b200/data/cont_tables.h"
 
 namespace {
 
@@ -505,11 +506,40 @@ void mt_ckd_h2o(const lbl_mtckd* ck, double p_atm, double t_atm, double h2o_vmr,
   myxint(wvn(i1), wvn(i2), dvc, fh, 1.0, wv1abs, dvabs, for_absco, ist, lst);
 }
 
-// CONTNM H2O part (src/contnm.f90:199-324)
+// The coarse grid of a continuum table (V1S, DVS, NPTS) that FRNCO2,
+// o2_ver_1, xn2_r and n2_ver_1 set up alike (src/contnm.f90:1322-1337):
+// from one point below V1ABS-DVS to one above V2ABS+DVS.
+struct CoarseGrid {
+  long I1, NPTC;
+  double V1C, V2C, DVC;
+};
+CoarseGrid coarse_grid(double V1S, double DVS, long NPTS, const Layer& S) {
+  CoarseGrid g;
+  g.DVC = DVS;
+  double V1C = S.V1ABS - g.DVC, V2C = S.V2ABS + g.DVC;
+  g.I1 = (V1C < V1S) ? -1 : fint((V1C - V1S) / DVS + 0.01);
+  g.V1C = V1S + DVS * double(g.I1 - 1);
+  const long I2 = fint((V2C - V1S) / DVS + 0.01);
+  g.NPTC = I2 - g.I1 + 3;
+  if (g.NPTC > NPTS) g.NPTC = NPTS + 4;
+  g.V2C = g.V1C + DVS * double(g.NPTC - 1);
+  return g;
+}
+// pre_xint (:994-1012) and XINT of the coarse values C (1-based) onto ABSRB
+void xint_onto_absrb(Layer& S, const CoarseGrid& g, const std::vector<double>& C, double V1SS,
+                     double V2SS) {
+  const long nbnd_v1c = fint(2 + (V1SS - S.V1ABS) / S.DVABS + 1.e-5);
+  const long ist = std::max(1L, nbnd_v1c);
+  const long nbnd_v2c = fint(1 + (V2SS - S.V1ABS) / S.DVABS + 1.e-5);
+  const long last = std::min(S.NPTABS, nbnd_v2c);
+  myxint(g.V1C, g.V2C, g.DVC, C, 1.0, S.V1ABS, S.DVABS, S.ABSRB, ist, last);
+}
+
+// CONTNM (src/contnm.f90:199-994): H2O, CO2, the O2 and N2 collision-induced
+// bands of the infrared, Rayleigh
 void contnm(Layer& S) {
   const lbl_layer& L = *S.LY;
   double RHOAVE = (L.pave / 1013.) * (296. / L.tave);
-  (void)RHOAVE;
   double WTOT = L.wbroad;
   for (int m = 1; m <= L.nmol; m++) WTOT = WTOT + L.wk[m - 1];
   double h2o_fac = L.wk[0] / WTOT;
@@ -524,10 +554,120 @@ void contnm(Layer& S) {
       S.ABSRB[j] = S.ABSRB[j] + cself + cfor;
     }
   }
+  const double XKT = L.tave / RADCN2;
+  const double amagat = (L.pave / 1013.) * (273. / L.tave);
+  const double x_vmr_h2o = L.wk[0] / WTOT, x_vmr_o2 = L.wk[6] / WTOT;
+  const double x_vmr_n2 = 1. - x_vmr_h2o - x_vmr_o2;
+  const double wn2 = x_vmr_n2 * WTOT;
+  const double xlosmt = 2.68675E+19;
+  // CO2 (src/contnm.f90:326-378): FRNCO2's coefficients on its 2 cm-1 grid
+  // (:1295-1349, the band-head temperature dependence), the mt_ckd_2.5
+  // factors from 2000 to 2998 cm-1, times WCO2, the radiation term when
+  // JRAD=1, then XINT onto the ABSRB grid
+  if ((S.V2 > -20.0) && (S.V1 < 10000.) && S.R->xco2c > 0.) {
+    static const double FCO2T[LBL_FCO2_N] = {LBL_FCO2_VALUES};
+    static const double XFACCO2[500] = {LBL_XFACCO2_VALUES};
+    static const double TDEP[25] = {LBL_CO2_TDEP_VALUES};
+    const double WCO2 = L.wk[1] * RHOAVE * 1.0E-20 * S.R->xco2c;
+    const double trat = L.tave / LBL_CO2_TEFF;
+    const CoarseGrid g = coarse_grid(LBL_FCO2_V1, LBL_FCO2_DV, LBL_FCO2_N, S);
+    std::vector<double> C(g.NPTC + 3, 0.);  // 1-based, zero beyond NPTC
+    for (long J = 1; J <= g.NPTC; J++) {
+      const long I = g.I1 + (J - 1);
+      double fco2 = 0.;
+      if (I >= 1 && I <= LBL_FCO2_N) {
+        double tcor = 1.;
+        if (I >= 1196 && I <= 1220) tcor = std::pow(trat, TDEP[I - 1196]);
+        fco2 = tcor * FCO2T[I - 1];
+      }
+      const double VJ = g.V1C + g.DVC * double(J - 1);
+      double CFAC = 1.;
+      if (VJ >= 2000. && VJ <= 2998.) {
+        const long JFAC = fint((VJ - 1998.) / 2. + 0.00001);
+        CFAC = XFACCO2[JFAC - 1];
+      }
+      fco2 = CFAC * fco2;
+      C[J] = fco2 * WCO2;
+      if (S.jrad == 1) C[J] = C[J] * RADFN(VJ, XKT);
+    }
+    xint_onto_absrb(S, g, C, LBL_FCO2_V1, LBL_FCO2_V2);
+  }
+  // O2 collision-induced fundamental (:491-540, o2_ver_1 :7254-7318)
+  if ((S.V2 > 1340.0) && (S.V1 < 1850.) && S.R->xo2cn > 0.) {
+    static const double XO2[LBL_O2F_N] = {LBL_O2F_XO2_VALUES};
+    static const double XO2T[LBL_O2F_N] = {LBL_O2F_XO2T_VALUES};
+    const double tau_fac = S.R->xo2cn * L.wk[6] * 1.e-20 * amagat;
+    const double xktfac = (1. / 296.) - (1. / L.tave);
+    const double factor = (1.e+20 / xlosmt);
+    const CoarseGrid g = coarse_grid(LBL_O2F_V1, LBL_O2F_DV, LBL_O2F_N, S);
+    std::vector<double> C(g.NPTC + 3, 0.);
+    for (long J = 1; J <= g.NPTC; J++) {
+      const long I = g.I1 + (J - 1);
+      const double VJ = g.V1C + g.DVC * double(J - 1);
+      double c0 = 0.;
+      if (I >= 1 && I <= LBL_O2F_N) c0 = factor * XO2[I - 1] * std::exp(XO2T[I - 1] * xktfac) / VJ;
+      C[J] = tau_fac * c0;
+      if (S.jrad == 1) C[J] = C[J] * RADFN(VJ, XKT);
+    }
+    xint_onto_absrb(S, g, C, LBL_O2F_V1, LBL_O2F_V2);
+  }
+  // N2 collision-induced rotational band (:745-792, xn2_r :2497-2566)
+  if ((S.V2 > -10.0) && (S.V1 < 350.) && S.R->xn2cn > 0.) {
+    static const double C296[LBL_N2R296_N] = {LBL_N2R296_C_VALUES};
+    static const double SF296[LBL_N2R296_N] = {LBL_N2R296_SF_VALUES};
+    static const double C220[LBL_N2R220_N] = {LBL_N2R220_C_VALUES};
+    static const double SF220[LBL_N2R220_N] = {LBL_N2R220_SF_VALUES};
+    const double tau_fac = S.R->xn2cn * (wn2 / xlosmt) * amagat;
+    const double tfac = (L.tave - 296.) / (220. - 296.);
+    const CoarseGrid g = coarse_grid(LBL_N2R296_V1, LBL_N2R296_DV, LBL_N2R296_N, S);
+    std::vector<double> C(g.NPTC + 3, 0.);
+    for (long J = 1; J <= g.NPTC; J++) {
+      const long I = g.I1 + (J - 1);
+      const double VJ = g.V1C + g.DVC * double(J - 1);
+      double c0 = 0., fo2 = 0.;
+      if (I >= 1 && I <= LBL_N2R296_N) {
+        c0 = C296[I - 1] * std::pow(C220[I - 1] / C296[I - 1], tfac);
+        const double sf_T = SF296[I - 1] * std::pow(SF220[I - 1] / SF296[I - 1], tfac);
+        fo2 = (sf_T - 1.) * (0.79) / (0.21);
+      }
+      C[J] = tau_fac * c0 * (x_vmr_n2 + fo2 * x_vmr_o2 + 1. * x_vmr_h2o);
+      if (S.jrad == 1) C[J] = C[J] * RADFN(VJ, XKT);
+    }
+    xint_onto_absrb(S, g, C, LBL_N2R296_V1, LBL_N2R296_V2);
+  }
+  // N2 collision-induced fundamental (:811-858, n2_ver_1 :2668-2754)
+  if ((S.V2 > 2001.77) && (S.V1 < 2897.59) && S.R->xn2cn > 0.) {
+    static const double X272[LBL_N2F_N] = {LBL_N2F_X272_VALUES};
+    static const double X228[LBL_N2F_N] = {LBL_N2F_X228_VALUES};
+    static const double AH2O[LBL_N2F_N] = {LBL_N2F_AH2O_VALUES};
+    const double tau_fac = S.R->xn2cn * (wn2 / xlosmt) * amagat;
+    const double T = L.tave;
+    const double xtfac = ((1. / T) - (1. / 272.)) / ((1. / 228.) - (1. / 272.));
+    const double xt_lin = (T - 272.) / (228. - 272.);
+    const double a_o2 = 1.294 - 0.4545 * T / 296.;
+    const CoarseGrid g = coarse_grid(LBL_N2F_V1, LBL_N2F_DV, LBL_N2F_N, S);
+    std::vector<double> C(g.NPTC + 3, 0.);
+    for (long J = 1; J <= g.NPTC; J++) {
+      const long I = g.I1 + (J - 1);
+      const double VJ = g.V1C + g.DVC * double(J - 1);
+      double c0 = 0., c1 = 0., c2 = 0.;
+      if (I >= 1 && I <= LBL_N2F_N) {
+        if (X272[I - 1] > 0. && X228[I - 1] > 0.)
+          c0 = X272[I - 1] * std::pow(X228[I - 1] / X272[I - 1], xtfac);
+        else
+          c0 = X272[I - 1] + (X228[I - 1] - X272[I - 1]) * xt_lin;
+        c0 = c0 / VJ;
+        c1 = a_o2 * c0;
+        c2 = (9. / 7.) * AH2O[I - 1] * c0;
+      }
+      C[J] = tau_fac * (x_vmr_n2 * c0 + x_vmr_o2 * c1 + x_vmr_h2o * c2);
+      if (S.jrad == 1) C[J] = C[J] * RADFN(VJ, XKT);
+    }
+    xint_onto_absrb(S, g, C, LBL_N2F_V1, LBL_N2F_V2);
+  }
   // Rayleigh extinction (src/contnm.f90:955-976), no aerosols (IAERSL=0)
   if (S.V2 >= 820. && S.R->xrayl > 0.) {
     const double conv_cm2mol = S.R->xrayl * 1.E-20 / (2.68675e-1 * 1.e5);
-    const double XKT = L.tave / RADCN2;
     const long nptabs = S.NPTABS;  // OPDPTH (src/lblrtm.f90:6222)
     for (long i = 1; i <= nptabs && i < (long)S.ABSRB.size(); i++) {
       double vrayleigh = S.V1ABS + double(i - 1) * S.DVABS;
@@ -1476,17 +1616,22 @@ double PLANCK(double VI, double XKT) {
 }
 
 // EMIN, LTE branch with XKTB<=0 and IAERSL=0 (src/xmerge.f90:1795-1855)
+// With XKTB > 0 (the symmetric tangent path, IPATHL=2, and specular
+// reflection, src/xmerge.f90:1980-2019) also the emission EMB of the
+// layer's other crossing, with the other level's temperature.
 void emin(const PanelOut& p, double XKT, double XKTA, std::vector<double>& EM,
-          std::vector<double>& TR) {
+          std::vector<double>& TR, double XKTB = 0., std::vector<double>* EMB = nullptr) {
   long NLIM = p.nlim;
   EM.assign(NLIM + 1, 0.);
   TR.assign(NLIM + 1, 0.);
+  if (EMB) EMB->assign(NLIM + 1, 0.);
   double rec_6 = 1. / 6.;
   double VI = p.v1p;
-  double bb_dif = 0.;
+  double bb_dif = 0., bb_dif_b = 0.;
   for (long I = 1; I <= NLIM; I++) {
     double BB = PLANCK(VI, XKT);
     if (XKTA > 0.) bb_dif = PLANCK(VI, XKTA) - BB;
+    if (EMB && XKTB > 0.) bb_dif_b = PLANCK(VI, XKTB) - BB;
     double ODVI = p.r[I - 1];
     if (ODVI < -OD_LO) ODVI = -OD_LO;
     double tr_i = std::exp(-ODVI);
@@ -1494,7 +1639,9 @@ void emin(const PanelOut& p, double XKT, double XKTA, std::vector<double>& EM,
     if (ODVI <= OD_LO) f_i = rec_6 * ODVI;
     else f_i = 1. - 2. * (tr_i / (tr_i - 1.) + 1. / ODVI);
     TR[I] = tr_i;
-    EM[I] = (1. - tr_i) * (BB + bb_dif * f_i);
+    const double abs_i = 1. - tr_i;
+    EM[I] = abs_i * (BB + bb_dif * f_i);
+    if (EMB) (*EMB)[I] = abs_i * (BB + bb_dif_b * f_i);
     VI = VI + p.dvp;
   }
 }
@@ -1521,12 +1668,20 @@ void eminit(const lbl_run& R, const lbl_layer& L, const std::vector<PanelOut>& o
   double XKTA = xkta_of(R, L);
   out.clear();
   for (const PanelOut& p : od) {
-    std::vector<double> EM, TR;
-    emin(p, XKT, XKTA, EM, TR);
+    std::vector<double> EM, TR, EMB;
+    const bool tangent = R.ipathl == 2;
+    emin(p, XKT, XKTA, EM, TR, tangent ? L.tzl / RADCN2 : 0., tangent ? &EMB : nullptr);
     MPanel mp{p.v1p, p.v2p, p.dvp, p.nlim, {}, {}};
     mp.rad.resize(p.nlim);
     mp.tr.resize(p.nlim);
-    if (TBND > 0.) {
+    if (tangent) {
+      // IPATHL=2, IANT=0 (:2442-2447): the tangent layer crossed twice
+      for (long J = 1; J <= p.nlim; J++) {
+        const double TRJ = TR[J];
+        EM[J] = EM[J] + EMB[J] * TRJ;
+        TR[J] = TR[J] * TRJ;
+      }
+    } else if (TBND > 0.) {
       double EMISIV = R.bndemi;
       double VI = p.v1p;
       for (long J = 1; J <= p.nlim; J++) {
@@ -1552,7 +1707,7 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
                 const std::vector<MPanel>& old, const std::vector<PanelOut>& od,
                 const std::function<void(size_t, const PanelOut&, std::vector<double>&,
                                          std::vector<double>&)>& layer,
-                std::vector<MPanel>& out) {
+                std::vector<MPanel>& out, const std::vector<double>* EMBp = nullptr) {
   double DVK = L.dv;
   long ITYPE;
   if (DVL == DVK) ITYPE = 0;
@@ -1562,6 +1717,9 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
   double XKT = L.tave / RADCN2;
   double XKTA = xkta_of(R, L);
   const bool down = R.ipathl == 3;  // IPATH_FLG = 3
+  // IPATH_FLG = 2 (the symmetric tangent path): the layer's other crossing,
+  // EMB (filled by `layer` with EM and TR), seen through the old path
+  const bool tangent = R.ipathl == 2 && EMBp != nullptr;
   double ATYPE = ITYPE;
   long LL = ITYPE + 1;
   double AP = 1.0 / (ATYPE + 1.0);
@@ -1622,6 +1780,13 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
       if (NL == 1) {
         for (long I = NL; I <= NLIM; I += LL) {
           IPL = IPL + LLM1;
+          if (tangent) {
+            // :2997-3005
+            const double TRTEMP = TR[I] * TRAO[IPL];
+            EM[I] = TR[I] * RADO[IPL] + EM[I] + (*EMBp)[I] * TRTEMP;
+            TR[I] = TR[I] * TRTEMP;
+            continue;
+          }
           if (down) EM[I] = RADO[IPL] + EM[I] * TRAO[IPL];
           else EM[I] = TR[I] * RADO[IPL] + EM[I];
           TR[I] = TR[I] * TRAO[IPL];
@@ -1630,6 +1795,16 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
         double A1N = A1[NL], A2N = A2[NL], A3N = A3[NL], A4N = A4[NL];
         for (long I = NL; I <= NLIM; I += LL) {
           IPL = IPL + LLM1;
+          if (tangent) {
+            // :3132-3148
+            const double TRTEMP = TR[I] * (A1N * TRAO[IPL - 1] + A2N * TRAO[IPL] +
+                                           A3N * TRAO[IPL + 1] + A4N * TRAO[IPL + 2]);
+            EM[I] = TR[I] * (A1N * RADO[IPL - 1] + A2N * RADO[IPL] + A3N * RADO[IPL + 1] +
+                             A4N * RADO[IPL + 2]) +
+                    EM[I] + (*EMBp)[I] * TRTEMP;
+            TR[I] = TR[I] * TRTEMP;
+            continue;
+          }
           if (down) {
             double TRAOI = A1N * TRAO[IPL - 1] + A2N * TRAO[IPL] + A3N * TRAO[IPL + 1] +
                            A4N * TRAO[IPL + 2];
@@ -1666,10 +1841,16 @@ int radmrg(const lbl_run& R, const lbl_layer& L, double DVL,
            const std::vector<MPanel>& old, const std::vector<PanelOut>& od,
            std::vector<MPanel>& out) {
   const double XKT = L.tave / RADCN2, XKTA = xkta_of(R, L);
+  // IPATHL=2: XKTB the lower level's temperature (:2771-2773)
+  const bool tangent = R.ipathl == 2;
+  const double XKTB = tangent ? L.tzl / RADCN2 : 0.;
+  std::vector<double> EMB;
   return radmrg_core(R, L, DVL, old, od,
                      [&](size_t, const PanelOut& p, std::vector<double>& EM,
-                         std::vector<double>& TR) { emin(p, XKT, XKTA, EM, TR); },
-                     out);
+                         std::vector<double>& TR) {
+                       emin(p, XKT, XKTA, EM, TR, XKTB, tangent ? &EMB : nullptr);
+                     },
+                     out, tangent ? &EMB : nullptr);
 }
 
 // EMBND (src/xmerge.f90:3652-3733) with a constant emissivity (BNDEMI(1);

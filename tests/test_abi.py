@@ -88,3 +88,15 @@ def test_noalloc_rejects_bad_iemit_before_device_work():
     run = abi.make_run(v1=-5.0, v2=700.0, iemit=0)
     assert lib.lbl_merge_layer_noalloc(0, C.byref(run), C.byref(lay), 1, 0.0, None, None, 0,
                                        P[0], P[1], None, 8, None) == 1
+
+
+def test_tangent_path_needs_lower_level_temperature():
+    """IPATHL=2 radiates each layer's far crossing at TZL: the DV rule (run
+    by every forward before any device work) rejects a layer without it."""
+    run = abi.make_run(v1=600.0, v2=650.0, iemit=1, ipathl=2)
+    lays = abi.make_layers(configs.atmosphere(6, ptop=300.0))
+    gpu.dv_rule(run, lays)
+    lays[3].tzl = 0.0
+    with pytest.raises(gpu.LblError) as e:
+        gpu.dv_rule(run, lays)
+    assert e.value.code == 1  # LBL_E_ARG

@@ -235,3 +235,76 @@ def test_downwelling_forward_matches_oracle_and_layer_steps(gpu_ctx):
         dv_old = lays[l].dv
     assert np.max(np.abs(frad - rad) / np.abs(rad)) < 1e-12
     assert np.max(np.abs(ftr - tr)) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_SPLIT])
+def test_tangent_path_forward_matches_oracle_and_layer_steps(gpu_ctx, precision):
+    """The symmetric tangent path (IPATHL=2, IANT=0: EMINIT crosses the
+    tangent layer twice, RADNN IPATH=2 adds each outer layer's near crossing
+    and its far crossing at TZL seen through the inner path) on a 40-layer
+    profile: the whole-profile forward against the oracle (FP64: 1e-8
+    relative radiance; split: 0.01 K brightness temperature), and the FP64
+    forward against lbl_merge_layer applied layer by layer."""
+    cfg = configs.config1(nlines=4000)
+    lh = abi.LinesHandle(cfg["lines"])
+    gpu_ctx.upload_lines(lh)
+    run = abi.make_run(v1=600.0, v2=650.0, iemit=1, ipathl=2, ilblf4=1, tmpbnd=290.0,
+                       bndemi=0.98)
+    lays = abi.make_layers(configs.atmosphere(40))
+    rad_ref, tr_ref = O.forward(run, abi.make_layers_like(lays), lh)
+    frad, ftr = gpu_ctx.forward(run, lays, precision=precision)
+    assert len(frad) == len(rad_ref)
+    if precision == abi.PREC_FP64:
+        assert np.max(floored_err(frad, rad_ref)) <= 1e-8
+        assert np.max(np.abs(ftr - tr_ref)) <= 1e-12
+    else:
+        dv = lays[len(lays) - 1].dv
+        b = gpu.brightness_temperature(frad, run.v1, dv)
+        b_ref = gpu.brightness_temperature(rad_ref, run.v1, dv)
+        assert np.max(np.abs(b - b_ref)) < 0.01
+        return
+    rad = tr = None
+    dv_old = 0.0
+    j = run.jrad
+    for l in range(len(lays)):
+        od, j = gpu_ctx.layer_od(run, lays[l], jrad=j)
+        rad, tr = gpu_ctx.merge_layer(run, lays[l], 1 if l == 0 else 0, dv_old, rad, tr, od)
+        dv_old = lays[l].dv
+    assert np.max(np.abs(frad - rad) / np.abs(rad)) < 1e-12
+    assert np.max(np.abs(ftr - tr)) < 1e-12
+
+
+def test_co2_o2_n2_continua_match_oracle(gpu_ctx):
+    """CONTNM's CO2 continuum (contnm.f90:326-378, FRNCO2 :1295-1349) and
+    the O2 and N2 collision-induced bands (:491-540, :745-858) with the H2O
+    table zeroed and Rayleigh off: the 667 cm-1 CO2 band, the 2386-2434
+    cm-1 band head (temperature-dependent coefficients), the mt_ckd_2.5
+    factors above 2000 cm-1, the O2 fundamental, the N2 fundamental and the
+    N2 rotational band, in JRAD=0 and JRAD=1 layers, against the oracle;
+    and with the scales at 0."""
+    lines = configs.gen_lines(500, 80.0, 2600.0, seed=12)
+    lh = abi.LinesHandle(lines)
+    zero = configs.mtckd_table(1)
+    zero["self_absco_ref"] = np.zeros_like(zero["self_absco_ref"])
+    zero["for_absco_ref"] = np.zeros_like(zero["for_absco_ref"])
+    ck = abi.MtckdHandle(zero)
+    gpu_ctx.upload_lines(lh)
+    gpu_ctx.upload_mtckd(ck)
+    for v1, v2 in ((640.0, 700.0), (2370.0, 2450.0), (1990.0, 2030.0), (1480.0, 1560.0),
+                   (2280.0, 2360.0), (100.0, 160.0)):
+        run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1, xrayl=0.0)
+        lays = abi.make_layers(configs.atmosphere(20, ptop=300.0))
+        gpu.dv_rule(run, lays)
+        for l in (0, 12, 19):
+            for jrad in (0, 1):
+                got, jg = gpu_ctx.layer_od(run, lays[l], jrad=jrad)
+                ref, jo = O.layer_od(run, lays[l], lh, ck, jrad=jrad)
+                assert jg == jo
+                assert np.max(floored_err(got, ref)) <= RTOL_FP64, (v1, l, jrad)
+    run = abi.make_run(v1=1480.0, v2=1560.0, icntnm=1, ilblf4=0, xrayl=0.0, xco2c=0.0,
+                       xo2cn=0.5, xn2cn=0.0)
+    lays = abi.make_layers(configs.atmosphere(20, ptop=300.0))
+    gpu.dv_rule(run, lays)
+    got, _ = gpu_ctx.layer_od(run, lays[5])
+    ref, _ = O.layer_od(run, lays[5], lh, ck)
+    assert np.max(floored_err(got, ref)) <= RTOL_FP64

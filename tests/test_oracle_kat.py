@@ -198,7 +198,7 @@ def _rayleigh_only(v1, v2, xrayl):
     zero["self_absco_ref"] = np.zeros_like(zero["self_absco_ref"])
     zero["for_absco_ref"] = np.zeros_like(zero["for_absco_ref"])
     ck = abi.MtckdHandle(zero)
-    run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1, xrayl=xrayl)
+    run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1, xrayl=xrayl, xco2c=0.0)
     lay = abi.make_layers(configs.atmosphere(20, ptop=300.0))
     O.dv_rule(run, lay)
     od, _ = O.layer_od(run, lay[0], lh, ck)
@@ -281,3 +281,168 @@ def test_downwelling_boundary_beyond_last_layer():
     r2, x2 = O.merge_layer(run, lays[1], 2, 0.01, r1, x1, z)
     v = 700.0 + 0.01 * np.arange(n)
     np.testing.assert_allclose(r2, 0.3 * _planck(v, 5800.0), rtol=1e-12)
+
+
+def test_tangent_path_crosses_each_layer_twice():
+    """IPATHL=2, the symmetric tangent path (EMINIT :2442-2447, RADNN
+    IPATH=2 :2997-3005): the tangent layer is crossed twice, R1 = B1 (1 -
+    T1^2), and each outer layer adds its near crossing and its far crossing
+    seen through the inner path: R = T2 R1 + B2 (1-T2) + B2 (1-T2) T2 T1^2,
+    T = T2^2 T1^2 (isothermal layers of constant optical depth on one grid,
+    where EMIN's linear-in-tau term vanishes)."""
+    t1, t2, tau1, tau2 = 280.0, 230.0, 0.7, 1.3
+    lays = _two_layers(t1, t2)
+    for l in lays:
+        l.dv = 0.01
+    run = abi.make_run(v1=700.0, v2=710.0, iemit=1, ipathl=2, tmpbnd=290.0)
+    n = O.npts(run, 0.01)
+    r1, x1 = O.merge_layer(run, lays[0], 1, 0.0, None, None, np.full(n, tau1))
+    r2, x2 = O.merge_layer(run, lays[1], 2, 0.01, r1, x1, np.full(n, tau2))
+    v = 700.0 + 0.01 * np.arange(n)
+    b1, b2 = _planck(v, t1), _planck(v, t2)
+    e1, e2 = np.exp(-tau1), np.exp(-tau2)
+    np.testing.assert_allclose(r1, b1 * (1 - e1 * e1), rtol=1e-12)
+    np.testing.assert_allclose(x1, e1 * e1, rtol=1e-14)
+    np.testing.assert_allclose(r2, e2 * r1 + b2 * (1 - e2) * (1 + e2 * e1 * e1), rtol=1e-12)
+    np.testing.assert_allclose(x2, e2 * e2 * e1 * e1, rtol=1e-14)
+    # one temperature: the path's emission is B (1 - T_path)
+    lays = _two_layers(250.0, 250.0)
+    for l in lays:
+        l.dv = 0.01
+    r1, x1 = O.merge_layer(run, lays[0], 1, 0.0, None, None, np.full(n, tau1))
+    r2, x2 = O.merge_layer(run, lays[1], 2, 0.01, r1, x1, np.full(n, tau2))
+    np.testing.assert_allclose(r2, _planck(v, 250.0) * (1 - x2), rtol=1e-12)
+
+
+def _cont_macro(name):
+    """An initializer list of cont_tables.h (the continuum DATA of CONTNM)."""
+    import os
+    import re
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "lblrtm_b200", "data", "cont_tables.h")
+    txt = open(path).read()
+    m = re.search(r"#define LBL_%s \\\n(.*?)(\n#define|\n#endif)" % name, txt, re.S)
+    if m:
+        body = m.group(1)
+    else:
+        body = re.search(r"#define LBL_%s (\S+)" % name, txt).group(1)
+    return np.array([float(x) for x in body.replace("\\", " ").replace(",", " ").split()])
+
+
+def _fco2_table():
+    """The CO2 continuum table of cont_tables.h (BLOCK DATA BFCO2)."""
+    vals = _cont_macro("FCO2_VALUES")
+    assert len(vals) == 5003
+    return -4.0 + 2.0 * np.arange(5003), vals
+
+
+def _co2_continuum_only(v1, v2, xco2c, jrad=None, **scales):
+    """Oracle optical depth of one layer whose only absorbers are CONTNM's
+    CO2, O2 and N2 continua: zero H2O continuum table, no Rayleigh, lines
+    far away."""
+    lines = configs.gen_lines(250, 6000.0, 6010.0, seed=3)
+    lh = abi.LinesHandle(lines)
+    zero = configs.mtckd_table(1)
+    zero["self_absco_ref"] = np.zeros_like(zero["self_absco_ref"])
+    zero["for_absco_ref"] = np.zeros_like(zero["for_absco_ref"])
+    ck = abi.MtckdHandle(zero)
+    run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1, xrayl=0.0, xco2c=xco2c, **scales)
+    lay = abi.make_layers(configs.atmosphere(20, ptop=300.0))
+    O.dv_rule(run, lay)
+    od, j = O.layer_od(run, lay[0], lh, ck, jrad=jrad)
+    v = v1 + lay[0].dv * np.arange(len(od))
+    return od, v, lay[0], j
+
+
+def _radfn(v, t):
+    x = v * RADCN2 / t
+    e = np.exp(-np.minimum(x, 10.0))
+    return np.where(x <= 0.01, 0.5 * x * v, np.where(x <= 10.0, v * (1 - e) / (1 + e), v))
+
+
+def _xint_points(v1a, dva, a, vi):
+    """XINT's 4-point interpolation (src/oprop.f90:2201-2234) of the values
+    a (a[0] is point 1 at v1a, spacing dva) at the wavenumbers vi."""
+    ap = np.concatenate([[0.0], a, [0.0, 0.0]])          # 1-based with pads
+    j = ((vi - v1a) / dva + 1.0 + 1e-5).astype(int)     # J = (VI-V1A)/DVA + ONEPL
+    p = (vi - (v1a + dva * (j - 1))) / dva
+    c = (3 - 2 * p) * p * p
+    b = 0.5 * p * (1 - p)
+    b1, b2 = b * (1 - p), b * p
+    return -ap[j - 1] * b1 + ap[j] * (1 - c + b2) + ap[j + 1] * (c + b1) - ap[j + 2] * b2
+
+
+def test_co2_continuum_follows_its_table():
+    """contnm.f90:326-378 with FRNCO2: between 600 and 640 cm-1 the layer's
+    optical depth is WCO2 = WK(2) RHOAVE 1e-20 XCO2C times the 2 cm-1 table,
+    put on the 1 cm-1 continuum grid by XINT, carried to the layer grid by
+    the finer interpolations (XINT onto R3, PANEL onto R2 and R1) and
+    multiplied by the radiation term (PANEL's RADFNI for JRAD=0, on the
+    2 cm-1 grid for JRAD=1): within 1e-3 of XINT onto the 1 cm-1 grid
+    followed by a cubic spline (the later 4-point stages differ from the
+    spline by a few 1e-4).  Linear in XCO2C."""
+    from scipy.interpolate import CubicSpline
+    vt, st = _fco2_table()
+    for jrad in (0, 1):
+        od, v, lay, j = _co2_continuum_only(600.0, 640.0, 1.0, jrad=jrad)
+        wco2 = lay.wk[1] * (lay.pave / 1013.0) * (296.0 / lay.tave) * 1e-20
+        va = 597.0 + np.arange(47.0)                    # V1ABS = INT(V1)-3, DVABS = 1
+        c = st * wco2
+        if j == 1:
+            c = c * _radfn(vt, lay.tave)
+        cabs = _xint_points(vt[0], 2.0, c, va)
+        expect = CubicSpline(va, cabs)(v)
+        if j != 1:
+            expect = expect * _radfn(v, lay.tave)
+        np.testing.assert_allclose(od, expect, rtol=1e-3)
+    od2, _, _, _ = _co2_continuum_only(600.0, 640.0, 2.0, jrad=0)
+    od1, _, _, _ = _co2_continuum_only(600.0, 640.0, 1.0, jrad=0)
+    np.testing.assert_allclose(od2, 2.0 * od1, rtol=1e-12)
+    od0, _, _, _ = _co2_continuum_only(600.0, 640.0, 0.0, jrad=0)
+    assert np.all(od0 == 0.0)
+
+
+def test_o2_and_n2_collision_induced_bands_follow_their_tables():
+    """The O2 fundamental (contnm.f90:491-540, o2_ver_1 :7254-7318) at
+    1500-1540 cm-1 and the N2 fundamental (:811-858, n2_ver_1 :2668-2754) at
+    2300-2340 cm-1 as the layer's only absorbers: the coefficients formed on
+    their own grids from the two tables (O2: exp(XO2T (1/296 - 1/T)); N2:
+    log-interpolation in 1/T between 272 K and 228 K, the O2 and H2O
+    broadening efficiencies), XINT onto the 1 cm-1 grid restated here, then
+    a cubic spline and the radiation term: within 1e-3.  Linear in the
+    scale factors; no CO2 or N2/O2 term where the scale is 0."""
+    from scipy.interpolate import CubicSpline
+    lay0 = abi.make_layers(configs.atmosphere(20, ptop=300.0))[0]
+    wtot = lay0.wbroad + sum(lay0.wk[m] for m in range(lay0.nmol))
+    x_h2o, x_o2 = lay0.wk[0] / wtot, lay0.wk[6] / wtot
+    x_n2 = 1 - x_h2o - x_o2
+    t = lay0.tave
+    amagat = (lay0.pave / 1013.0) * (273.0 / t)
+    # O2: 5 cm-1 grid from 1340
+    vo = 1340.0 + 5.0 * np.arange(103)
+    co = (1e20 / 2.68675e19) * _cont_macro("O2F_XO2_VALUES") * np.exp(
+        _cont_macro("O2F_XO2T_VALUES") * (1 / 296.0 - 1 / t)) / vo
+    co = co * lay0.wk[6] * 1e-20 * amagat
+    # N2 fundamental: 228 points from 1997.784896 every 3.981461525
+    dvn = 3.981461525
+    vn = 1997.784896 + dvn * np.arange(228)
+    a, b = _cont_macro("N2F_X272_VALUES"), _cont_macro("N2F_X228_VALUES")
+    xtfac = (1 / t - 1 / 272.0) / (1 / 228.0 - 1 / 272.0)
+    pos = (a > 0) & (b > 0)
+    c0 = np.where(pos, a * (np.where(pos, b, 1) / np.where(pos, a, 1)) ** xtfac,
+                  a + (b - a) * (t - 272.0) / (228.0 - 272.0)) / vn
+    a_o2 = 1.294 - 0.4545 * t / 296.0
+    cn = (x_n2 * c0 + x_o2 * a_o2 * c0 + x_h2o * (9.0 / 7.0) * _cont_macro("N2F_AH2O_VALUES") * c0)
+    cn = cn * (x_n2 * wtot / 2.68675e19) * amagat
+    for (v1, v2), (vt, ct, dvt) in (((1500.0, 1540.0), (vo, co, 5.0)),
+                                    ((2300.0, 2340.0), (vn, cn, dvn))):
+        od, v, lay, j = _co2_continuum_only(v1, v2, 0.0, jrad=0)
+        assert j == 0
+        va = (int(v1) - 3.0) + np.arange(int(v2 + 3.5) - (int(v1) - 3.0) + 1)
+        cabs = _xint_points(vt[0], dvt, ct, va)
+        expect = CubicSpline(va, cabs)(v) * _radfn(v, t)
+        np.testing.assert_allclose(od, expect, rtol=1e-3)
+        od2, _, _, _ = _co2_continuum_only(v1, v2, 0.0, jrad=0, xo2cn=2.0, xn2cn=2.0)
+        np.testing.assert_allclose(od2, 2.0 * od, rtol=1e-12)
+        od0, _, _, _ = _co2_continuum_only(v1, v2, 0.0, jrad=0, xo2cn=0.0, xn2cn=0.0)
+        assert np.all(od0 == 0.0)
