@@ -116,6 +116,13 @@ typedef struct lbl_run {
                        collision-induced rotational band below 350 cm-1
                        (:745-792, xn2_r :2497-2566) and fundamental,
                        2001.77-2897.59 cm-1 (:811-858, n2_ver_1 :2668-2754) */
+  double bndrfl;    /* boundary reflectivity BNDRFL(1) (record 1.4; default
+                       0, BNDRFL(2:3)=0): with IPATHL=1 a value in (0, 1]
+                       makes the run the reflected atmosphere (IBPROP=1,
+                       IPATHL=-1, specular: EMINIT src/xmerge.f90:2486-2540,
+                       RADNN IPATH=-10 :3023-3066, 3168-3215): each layer's
+                       downward emission (at TZL) is reflected at the
+                       surface and seen back up through the layers below */
 } lbl_run;
 
 /* One layer: the /FILHDR/ quantities OPDPTH and XMERGE read
@@ -323,7 +330,7 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer,
  * be caller-owned memory of device `device` (host pointers or another
  * GPU's memory give LBL_E_ARG), and the call allocates nothing.  An output
  * must not share memory with rad_in, tr_in or the other output (LBL_E_ARG);
- * it may be od itself.  IEMIT must be 0 or 1, IPATHL 1 and first 0 or 1;
+ * it may be od itself.  IEMIT must be 0 or 1, IPATHL 1 (no reflectivity) and first 0 or 1;
  * with IEMIT=0 tr_in and tr_out are not used.  Its only scratch is a
  * fixed device array inside the library, about 72 KB on every device that
  * loads it, kept until the

@@ -34,7 +34,7 @@ class Run(C.Structure):
         ("dptmin", C.c_double), ("dptfac", C.c_double), ("xself", C.c_double),
         ("xfrgn", C.c_double), ("tmpbnd", C.c_double), ("bndemi", C.c_double),
         ("xrayl", C.c_double), ("xco2c", C.c_double), ("xo2cn", C.c_double),
-        ("xn2cn", C.c_double),
+        ("xn2cn", C.c_double), ("bndrfl", C.c_double),
     ]
 
 
@@ -99,7 +99,7 @@ def make_run(**kw):
     d = dict(ihirac=1, ilblf4=1, icntnm=0, iemit=0, ipathl=1, jrad=1,
              v1=0.0, v2=0.0, sample=4.0, dvset=0.0, alfal0=0.04, avmass=36.0,
              dptmin=2e-4, dptfac=1e-3, xself=1.0, xfrgn=1.0, tmpbnd=0.0,
-             bndemi=1.0, xrayl=1.0, xco2c=1.0, xo2cn=1.0, xn2cn=1.0)
+             bndemi=1.0, xrayl=1.0, xco2c=1.0, xo2cn=1.0, xn2cn=1.0, bndrfl=0.0)
     d.update(kw)
     r = Run()
     for k, v in d.items():

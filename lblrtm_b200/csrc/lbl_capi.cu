@@ -673,16 +673,15 @@ int finish_od(lbl_ctx* ctx);
 // the fused panel kernel (records staged per batch, CTAs per SM) and of the
 // far-wing kernel (adders per window CTA) runs once on that batch, timed by
 // CUDA events on the context's stream, and the fastest is kept for the
-// context's later calls in that precision.  Every variant writes the same
-// results (the same sums in the same order), so the batch's result does not
-// depend on which ran last.  LBL_PANEL_VARIANT / LBL_FAR_VARIANT (0-2) fix a
-// variant.
+// context's later calls in that precision (the far wing's tuning launches
+// are the batch's own: the chosen variant runs once more unless it ran
+// last).  LBL_PANEL_VARIANT / LBL_FAR_VARIANT (0-2) fix a variant.
 constexpr int64_t kTuneMinPanels = 4096;
 constexpr int64_t kTuneMinWindows = 128;
 
 template <typename Launch>
 int tune(lbl_ctx* ctx, int nvar, const char* env, const char* const* names, Launch launch,
-         int* chosen) {
+         int* chosen, bool keep_result) {
   if (const char* e = std::getenv(env)) {
     const int v = std::atoi(e);
     if (v >= 0 && v < nvar) {
@@ -711,6 +710,11 @@ int tune(lbl_ctx* ctx, int nvar, const char* env, const char* const* names, Laun
   }
   for (auto& e : ev) cudaEventDestroy(e);
   *chosen = best;
+  // keep_result: the tuning launches produce the batch's result, which
+  // must then be the chosen variant's (in the split form the far-wing
+  // variants' FP32 chunk sums are not bit-identical), so that a first call
+  // gives what every later call gives
+  if (keep_result && best != nvar - 1) CK(launch(best));
   // reported with the stage times: each variant's time and the choice
   for (int v = 0; v < nvar; v++) {
     lbl_ctx::Stage& st = ctx->stage(names[v]);
@@ -731,7 +735,7 @@ int tune_panels(lbl_ctx* ctx, Batch& B, int precision) {
                                      B.d_panel_base, B.d_panel_rng, B.d_panel_segs,
                                      B.d_panel_nseg, precision, v, ctx->stream);
               },
-              &ctx->panel_variant[pk]);
+              &ctx->panel_variant[pk], false);
 }
 
 int tune_far(lbl_ctx* ctx, Batch& B, int precision) {
@@ -744,7 +748,7 @@ int tune_far(lbl_ctx* ctx, Batch& B, int precision) {
                 return launch_far_wing(B.w, B.nwin_total, B.d_win_order, B.d_win_layer,
                                        precision, v, ctx->stream);
               },
-              &ctx->far_variant[pk]);
+              &ctx->far_variant[pk], true);
 }
 
 // A pinned host buffer of at least `bytes` for a table about to be copied
@@ -889,6 +893,8 @@ int check_run(lbl_ctx* ctx, const lbl_run* R) {
   if (R->iemit == 1 && R->ipathl != 1 && R->ipathl != 2 && R->ipathl != 3)
     return fail(ctx, LBL_E_ARG,
                 "IPATHL must be 1 (looking down), 2 (tangent path) or 3 (looking up)");
+  if (!(R->bndrfl >= 0. && R->bndrfl <= 1.))
+    return fail(ctx, LBL_E_ARG, "BNDRFL must lie in [0, 1] (no reflectivity file)");
   if (!ctx->have_lines) return fail(ctx, LBL_E_NOTREADY, "lines not uploaded");
   return LBL_OK;
 }
@@ -968,12 +974,16 @@ int run_merge(lbl_ctx* ctx, const lbl_run& R, const lbl_layer* layers, Batch& B,
     // crossing radiates at its lower level's temperature (XKTB,
     // src/xmerge.f90:2417-2420, 2771-2773)
     m.tangent = R.ipathl == 2 ? 1 : 0;
+    // the reflected atmosphere (IPATHL=1 with a boundary reflectivity: the
+    // reference's IPATHL=-1, src/xmerge.f90:2389, 2725)
+    m.refl = (R.iemit == 1 && R.ipathl == 1 && R.bndrfl > 0.) ? R.bndrfl : 0.;
+    const bool use_b = m.tangent || m.refl > 0.;
     for (int k = l; k < e; k++) {
       m.od_off[k - l] = ld[k].off_od;
       m.t[k - l] = emin_temps(ld[k].tave, down ? layers[k].tzl : layers[k].tzu);
       const double tzl = layers[k].tzl;
-      m.tb_xkt[k - l] = (m.tangent && tzl > 0.) ? tzl / kRADCN2 : 0.;
-      m.tb_rk[k - l] = (m.tangent && tzl > 0.) ? kRADCN2 / tzl : 0.;
+      m.tb_xkt[k - l] = (use_b && tzl > 0.) ? tzl / kRADCN2 : 0.;
+      m.tb_rk[k - l] = (use_b && tzl > 0.) ? kRADCN2 / tzl : 0.;
       ctx->stage("merge").work += (double)ld[k].npts;
     }
     const int nxt = cur ^ 2;
@@ -1277,8 +1287,9 @@ int check_jac_args(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layers,
     return fail(ctx, LBL_E_ARG, "Jacobians: bad argument");
   if (mode != LBL_JAC_CENTRAL && mode != LBL_JAC_REFERENCE)
     return fail(ctx, LBL_E_ARG, "Jacobians: mode must be LBL_JAC_CENTRAL or LBL_JAC_REFERENCE");
-  if (run->iemit != 1 || run->ipathl != 1)
-    return fail(ctx, LBL_E_ARG, "Jacobians: upwelling radiance only (IEMIT=1, IPATHL=1)");
+  if (run->iemit != 1 || run->ipathl != 1 || run->bndrfl != 0.)
+    return fail(ctx, LBL_E_ARG,
+                "Jacobians: upwelling radiance only (IEMIT=1, IPATHL=1, no reflectivity)");
   for (int p = 0; p < nprof; p++)
     if (nlay[p] < 1) return fail(ctx, LBL_E_ARG, "Jacobians: profile without layers");
   for (int k = 0; k < nq; k++)
@@ -1901,15 +1912,16 @@ int lbl_merge_layer(lbl_ctx* ctx, const lbl_run* run, const lbl_layer* layer, in
     CK(cudaMemcpyAsync(ctx->mbuf[0], rad_in, n_old * 8, cudaMemcpyDefault, s));
     if (run->iemit == 1) CK(cudaMemcpyAsync(ctx->mbuf[1], tr_in, n_old * 8, cudaMemcpyDefault, s));
   }
-  if (run->iemit == 1 && run->ipathl == 2 && !(layer->tzl > 0.))
-    return fail(ctx, LBL_E_ARG, "the tangent path (IPATHL=2) needs TZL > 0");
+  const double refl = (run->iemit == 1 && run->ipathl == 1 && run->bndrfl > 0.) ? run->bndrfl : 0.;
+  if (run->iemit == 1 && (run->ipathl == 2 || refl > 0.) && !(layer->tzl > 0.))
+    return fail(ctx, LBL_E_ARG, "the tangent path and the reflected atmosphere need TZL > 0");
   const double tbnd = (first && run->ipathl == 1) ? run->tmpbnd : 0.;
   const bool down = run->ipathl == 3;
   const double tbnd_last = (down && last && !first) ? run->tmpbnd : 0.;
   CK(launch_merge(dL, dv, dod, n_new, first, dv_old, n_old, ctx->mbuf[0], ctx->mbuf[1],
                   ctx->mbuf[2], ctx->mbuf[3], tbnd, run->bndemi, run->iemit,
                   down ? layer->tzl : layer->tzu, s, LBL_PREC_FP64, down ? 1 : 0, tbnd_last,
-                  run->ipathl == 2 ? layer->tzl : 0.));
+                  (run->ipathl == 2 || refl > 0.) ? layer->tzl : 0., refl));
   CK(cudaMemcpyAsync(rad_out, ctx->mbuf[2], n_new * 8, cudaMemcpyDefault, s));
   if (tr_out) CK(cudaMemcpyAsync(tr_out, ctx->mbuf[3], n_new * 8, cudaMemcpyDefault, s));
   CK(cudaStreamSynchronize(s));
@@ -1991,10 +2003,15 @@ int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int6
   if (rc) return fail(ctx, rc, e);
   if (P.n_out != n_out) return fail(ctx, LBL_E_ARG, "n_out does not match the output grid");
   cudaSetDevice(ctx->device);
-  if (P.jfn == 0) {
-    // CNVRCT: every box, with both of its end points, inside the input
-    const double vlast = sc->v1 + double(P.n_out - 1) * P.dvo + P.hwhm;
-    if (v1_in > sc->v1 - P.hwhm - dv_in || v1_in + double(n - 1) * dv_in < vlast + dv_in)
+  if (P.jfn == 0 || P.jfn == 5 || P.jfn == 6) {
+    // CNVRCT/CNVVRC/CNVVRL: every box, with both of its end points, inside
+    // the input (the first box's left edge, the last box's right edge)
+    const double b2 = P.bfov * P.bfov, vlast0 = sc->v1 + double(P.n_out - 1) * P.dvo;
+    const double vfirst = P.jfn == 0 ? sc->v1 - P.hwhm
+                          : P.jfn == 5 ? sc->v1 * (1. - b2 / 4.) : sc->v1;
+    const double vlast = P.jfn == 0 ? vlast0 + P.hwhm
+                         : P.jfn == 5 ? vlast0 * (1. + b2 / 4.) : vlast0 * (1. + b2 / 2.);
+    if (v1_in > vfirst - dv_in || v1_in + double(n - 1) * dv_in < vlast + dv_in)
       return fail(ctx, LBL_E_RANGE, "scan: the boxes must lie inside the spectrum");
     const bool in_dev = is_device_ptr(spec), out_dev = is_device_ptr(out);
     size_t bytes = 256;
@@ -2010,8 +2027,8 @@ int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int6
       din = t;
     }
     double* dout = out_dev ? out : ctx->arena.take<double>(n_out);
-    CK(launch_scan_rect(din, n, sc->jabs ? 1 : 0, sc->v1, P.dvo, P.hwhm, v1_in, dv_in, dout, n_out,
-                        s));
+    CK(launch_scan_rect(din, n, sc->jabs ? 1 : 0, P.jfn, sc->v1, P.dvo, P.hwhm, P.bfov, v1_in,
+                        dv_in, dout, n_out, s));
     if (!out_dev) CK(cudaMemcpyAsync(out, dout, n_out * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return LBL_OK;

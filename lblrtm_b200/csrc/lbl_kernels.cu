@@ -2028,58 +2028,64 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
 
 // Kahan-compensated FP32 accumulation of one grid point (sum, compensation).
 __device__ __forceinline__ void kahan_add(float2& a, float v) {
-  const float y = v - a.y;
-  const float t = a.x + y;
-  a.y = (t - a.x) - y;
+  const float y = __fsub_rn(v, a.y);
+  const float t = __fadd_rn(a.x, y);
+  a.y = __fsub_rn(__fsub_rn(t, a.x), y);
   a.x = t;
+}
+
+// Line q's contribution at panel coordinate gi (= off + local point) of one
+// grid, zc its centre on that grid: F1 + FG + VERFN terms on R1, F2 on R2,
+// F3 on R3, with the line-coupling factor (:1322-1351).  T = double: FP64;
+// T = float: the table index from the same FP64 position, the line shape in
+// FP32.  The fused multiply-adds are written out, so that every panel
+// variant rounds the shape alike wherever the compiler places this code.
+template <typename T, int GRID>
+__device__ __forceinline__ T near_val(const NearRec& q, const DevShapes& sh, int gi, double zc) {
+  const double cf = GRID == 1 ? 4. / 2000. : (GRID == 2 ? 16. / 2000. : 64. / 2000.);
+  const double zf = __dmul_rn(__dsub_rn(double(gi), zc), q.zslope);
+  int iz = (int)(fabs(zf) + 1.5);
+  iz = iz > kNfmx ? kNfmx : iz;
+  if constexpr (sizeof(T) == 8) {
+    double v;
+    if (GRID == 1) {
+      const double2 fab = *reinterpret_cast<const double2*>(sh.r1p + 4 * iz);
+      v = fma(q.sx, sh.r1p[4 * iz + 2], fma(q.sg, fab.y, __dmul_rn(q.s0, fab.x)));
+    } else {
+      v = __dmul_rn(GRID == 2 ? q.s2 : q.s3, GRID == 2 ? sh.f2[iz] : sh.f3[iz]);
+    }
+    if (q.sppsp != 0.) v = fma(v, __dmul_rn(__dmul_rn(cf, q.sppsp), zf), v);
+    return v;
+  } else {
+    float v;
+    if (GRID == 1) {
+      const float4 t = sh.r1p32[iz];
+      v = fmaf((float)q.sx, t.z, fmaf((float)q.sg, t.y, __fmul_rn((float)q.s0, t.x)));
+    } else {
+      v = __fmul_rn((float)(GRID == 2 ? q.s2 : q.s3), GRID == 2 ? sh.f2_32[iz] : sh.f3_32[iz]);
+    }
+    const float cs = (float)__dmul_rn(cf, q.sppsp);
+    if (cs != 0.f) v = fmaf(v, __fmul_rn(cs, (float)zf), v);
+    return v;
+  }
 }
 
 // Adds line q's contributions to the points this thread owns on one grid:
 // local points [lo, hi] of the panel's span (thread tid owns tid + 256 k);
 // `off` maps a local point to the line's panel coordinate.  T = double:
-// FP64 sums; T = float: the table index from the same FP64 position, the
-// line shape in FP32 and a Kahan-compensated FP32 sum.
+// FP64 sums; T = float: a Kahan-compensated FP32 sum.
 template <typename T, int GRID>
 __device__ __forceinline__ void near_add(const NearRec& q, const DevShapes& sh, int tid, int lo,
                                          int hi, int off, double zc, double* acc) {
   int i = tid + (lo > tid ? ((lo - tid + kPanelThreads - 1) / kPanelThreads) * kPanelThreads : 0);
-  const double cf = GRID == 1 ? 4. / 2000. : (GRID == 2 ? 16. / 2000. : 64. / 2000.);
   if constexpr (sizeof(T) == 8) {
 #pragma unroll 2
-    for (; i <= hi; i += kPanelThreads) {
-      const double zf = (double(off + i) - zc) * q.zslope;
-      int iz = (int)(fabs(zf) + 1.5);
-      iz = iz > kNfmx ? kNfmx : iz;
-      double v;
-      if (GRID == 1) {
-        const double2 fab = *reinterpret_cast<const double2*>(sh.r1p + 4 * iz);
-        v = q.s0 * fab.x + q.sg * fab.y + q.sx * sh.r1p[4 * iz + 2];
-      } else {
-        v = (GRID == 2 ? q.s2 * sh.f2[iz] : q.s3 * sh.f3[iz]);
-      }
-      if (q.sppsp != 0.) v = v + v * (cf * q.sppsp * zf);  // (:1322-1351)
-      acc[i] += v;
-    }
+    for (; i <= hi; i += kPanelThreads)
+      acc[i] = __dadd_rn(acc[i], near_val<double, GRID>(q, sh, off + i, zc));
   } else {
     float2* a2 = reinterpret_cast<float2*>(acc);
-    const float s0 = (float)q.s0, sg = (float)q.sg, sx = (float)q.sx;
-    const float s23 = (float)(GRID == 2 ? q.s2 : q.s3);
-    const float cs = (float)(cf * q.sppsp);
 #pragma unroll 2
-    for (; i <= hi; i += kPanelThreads) {
-      const double zf = (double(off + i) - zc) * q.zslope;
-      int iz = (int)(fabs(zf) + 1.5);
-      iz = iz > kNfmx ? kNfmx : iz;
-      float v;
-      if (GRID == 1) {
-        const float4 t = sh.r1p32[iz];
-        v = s0 * t.x + sg * t.y + sx * t.z;
-      } else {
-        v = s23 * (GRID == 2 ? sh.f2_32[iz] : sh.f3_32[iz]);
-      }
-      if (cs != 0.f) v = v + v * (cs * (float)zf);
-      kahan_add(a2[i], v);
-    }
+    for (; i <= hi; i += kPanelThreads) kahan_add(a2[i], near_val<float, GRID>(q, sh, off + i, zc));
   }
 }
 
@@ -2547,7 +2553,7 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
                         int first, double dv_old, int64_t n_old64, const double* rad_in,
                         const double* tr_in, double* rad_out, double* tr_out, double tbnd,
                         double emis, int iemit, double tzu, int down, double tbnd_last,
-                        double tzl_tangent) {
+                        double tzl_b, double refl) {
   const LayerDev& L = *Lp;
   const int32_t f = (int32_t)(blockIdx.x * blockDim.x + threadIdx.x);
   if (f >= (int32_t)L.npts) return;
@@ -2565,22 +2571,37 @@ __global__ void k_merge(const LayerDev* Lp, const double* vft_panel, const doubl
     return;
   }
   T tr, em;
-  if (tzl_tangent > 0.) {
-    // the symmetric tangent path (IPATHL=2, IANT=0): EMINIT :2442-2447,
-    // RADNN IPATH=2 :2997-3005, 3132-3148
+  if (tzl_b > 0.) {
+    // the symmetric tangent path (IPATHL=2, IANT=0: EMINIT :2442-2447,
+    // RADNN IPATH=2 :2997-3005, 3132-3148) or, with refl > 0, the reflected
+    // atmosphere (IPATHL=-1, specular: EMINIT :2486-2540, RADNN IPATH=-10
+    // :3051-3066, 3197-3215); EMB is the emission at the lower level's
+    // temperature
     T emb;
-    emin_point_b<T>(odv, vi, emin_temps(L.tave, tzu), tzl_tangent / kRADCN2,
-                    kRADCN2 / tzl_tangent, tr, em, emb);
+    emin_point_b<T>(odv, vi, emin_temps(L.tave, tzu), tzl_b / kRADCN2, kRADCN2 / tzl_b, tr, em,
+                    emb);
+    const double trd = (double)tr, emd = (double)em, embd = (double)emb;
     if (first) {
-      rad_out[f] = (double)em + (double)emb * (double)tr;
-      tr_out[f] = (double)tr * (double)tr;
+      if (refl > 0.) {
+        const double bb = tbnd > 0. ? planck(vi, tbnd / kRADCN2, kRADCN2 / tbnd) : 0.;
+        rad_out[f] = emd + embd * refl * trd + trd * bb * emis;
+        tr_out[f] = trd;
+      } else {
+        rad_out[f] = emd + embd * trd;
+        tr_out[f] = trd * trd;
+      }
       return;
     }
     double ro, to;
     merge_regrid(rad_in, tr_in, n_old, f, itype, ro, to);
-    const double tt = (double)tr * to;
-    rad_out[f] = (double)tr * ro + (double)em + (double)emb * tt;
-    tr_out[f] = (double)tr * tt;
+    const double tt = trd * to;
+    if (refl > 0.) {
+      rad_out[f] = trd * ro + emd + embd * to * tt * refl;
+      tr_out[f] = tt;
+    } else {
+      rad_out[f] = trd * ro + emd + embd * tt;
+      tr_out[f] = trd * tt;
+    }
     return;
   }
   emin_point<T>(odv, vi, emin_temps(L.tave, tzu), tr, em);
@@ -2632,18 +2653,31 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
       continue;
     }
     T tr, em;
-    if (!DOWN && m.tangent) {
-      // the symmetric tangent path: EMINIT :2442-2447, RADNN IPATH=2
-      // :2997-3005, 3132-3148
+    if (!DOWN && (m.tangent || m.refl > 0.)) {
+      // the symmetric tangent path (EMINIT :2442-2447, RADNN IPATH=2
+      // :2997-3005, 3132-3148) and the reflected atmosphere (EMINIT
+      // :2486-2540, RADNN IPATH=-10 :3051-3066, 3197-3215)
       T emb;
       emin_point_b<T>(odv, vi, m.t[l], m.tb_xkt[l], m.tb_rk[l], tr, em, emb);
+      const double trd = (double)tr, emd = (double)em, embd = (double)emb;
       if (m.first && l == 0) {
-        ro = (double)em + (double)emb * (double)tr;
-        to = (double)tr * (double)tr;
+        if (m.refl > 0.) {
+          const double bb = tbnd > 0. ? planck(vi, tbnd / kRADCN2, kRADCN2 / tbnd) : 0.;
+          ro = emd + embd * m.refl * trd + trd * bb * emis;
+          to = trd;
+        } else {
+          ro = emd + embd * trd;
+          to = trd * trd;
+        }
       } else {
-        const double tt = (double)tr * to;
-        ro = (double)tr * ro + (double)em + (double)emb * tt;
-        to = (double)tr * tt;
+        const double tt = trd * to;
+        if (m.refl > 0.) {
+          ro = trd * ro + emd + embd * to * tt * m.refl;
+          to = tt;
+        } else {
+          ro = trd * ro + emd + embd * tt;
+          to = trd * tt;
+        }
       }
       continue;
     }
@@ -2681,7 +2715,7 @@ __global__ void __launch_bounds__(256) k_merge_run(const MergeRun m, const doubl
 constexpr int kMergeThreads = 256;
 constexpr int kMergePointsPerThread = 2;
 template <bool DOWN, int MK>
-__global__ void __launch_bounds__(kMergeThreads) k_merge_run_f64(
+__global__ void __launch_bounds__(kMergeThreads, 3) k_merge_run_f64(
     const MergeRun m, const double* vft_panel, const double* od, int32_t f_lo, int32_t f_hi,
     double DV, const double* rad_in, const double* tr_in, double* rad_out, double* tr_out,
     double tbnd, double emis, int iemit) {
@@ -2694,15 +2728,21 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_run_f64(
     s_st2[tid] = t.xkta > 0. ? exp(-span * t.rka) : 0.;
   }
   __syncthreads();
-  const int32_t f0 = f_lo + (int32_t)blockIdx.x * (kMergeThreads * MK) + tid;
+  // groups of MK*256 points at absolute positions (a multiple of MK*256),
+  // so that a point's arithmetic does not depend on the launch's range
+  const int32_t g0 = (f_lo / (kMergeThreads * MK)) * (kMergeThreads * MK);
+  const int32_t f0 = g0 + (int32_t)blockIdx.x * (kMergeThreads * MK) + tid;
   if (f0 >= f_hi) return;
   double vi[MK], ro[MK], to[MK], odn[MK];
 #pragma unroll
   for (int j = 0; j < MK; j++) {
     const int32_t f = f0 + j * kMergeThreads;
-    const int32_t fc = f < f_hi ? f : f_hi - 1;  // clamped: loads stay in range
-    const int32_t p = fc / 2400;
-    vi[j] = (vft_panel[p] + double(33 - 1) * DV) + double(fc - 2400 * p) * DV;
+    // clamped into the range: loads stay in range (the group's first point
+    // is always a valid grid point, for its wavenumber)
+    const int32_t fc = f < f_lo ? f_lo : (f < f_hi ? f : f_hi - 1);
+    const int32_t fv = j == 0 ? f : fc;
+    const int32_t p = fv / 2400;
+    vi[j] = (vft_panel[p] + double(33 - 1) * DV) + double(fv - 2400 * p) * DV;
     ro[j] = 0.;
     to[j] = 1.;
     if (!m.first) {
@@ -2718,7 +2758,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_run_f64(
       odv[j] = odn[j];
       if (l + 1 < m.nl) {
         const int32_t f = f0 + j * kMergeThreads;
-        odn[j] = od[m.od_off[l + 1] + (f < f_hi ? f : f_hi - 1)];
+        odn[j] = od[m.od_off[l + 1] + (f < f_lo ? f_lo : (f < f_hi ? f : f_hi - 1))];
       }
     }
     if (iemit == 0) {
@@ -2755,6 +2795,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_run_f64(
   for (int j = 0; j < MK; j++) {
     const int32_t f = f0 + j * kMergeThreads;
     if (f >= f_hi) break;
+    if (f < f_lo) continue;
     double r = ro[j];
     if (DOWN && iemit && m.tbnd_last > 0.)
       r = r + to[j] * emis * planck(vi[j], m.tbnd_last / kRADCN2, kRADCN2 / m.tbnd_last);
@@ -3189,17 +3230,17 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
                          cudaStream_t s, int precision, int down, double tbnd_last,
-                         double tzl_tangent) {
+                         double tzl_b, double refl) {
   if (npts >= (int64_t(1) << 31) || n_old >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
   const unsigned nb = (unsigned)((npts + 255) / 256);
   if (precision == LBL_PREC_SPLIT)
     k_merge<float><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
                                       rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last,
-                                      tzl_tangent);
+                                      tzl_b, refl);
   else
     k_merge<double><<<nb, 256, 0, s>>>(Ld, vft_panel, od, first, dv_old, n_old, rad_in, tr_in,
                                        rad_out, tr_out, tbnd, emis, iemit, tzu, down, tbnd_last,
-                                      tzl_tangent);
+                                      tzl_b, refl);
   return cudaGetLastError();
 }
 
@@ -3221,12 +3262,13 @@ cudaError_t launch_merge_run(const MergeRun& m, const double* vft_panel, const d
     else
       k_merge_run<float, false><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
                                                    rad_out, tr_out, tbnd, emis, iemit);
-  } else if (m.tangent) {
+  } else if (m.tangent || m.refl > 0.) {
     k_merge_run<double, false><<<nb, 256, 0, s>>>(m, vft_panel, od, a, b, dv, rad_in, tr_in,
                                                   rad_out, tr_out, tbnd, emis, iemit);
   } else {
     constexpr int MK = kMergePointsPerThread;
-    const unsigned nb64 = (unsigned)((f_hi - f_lo + kMergeThreads * MK - 1) / (kMergeThreads * MK));
+    const int64_t g0 = (f_lo / (kMergeThreads * MK)) * (kMergeThreads * MK);
+    const unsigned nb64 = (unsigned)((f_hi - g0 + kMergeThreads * MK - 1) / (kMergeThreads * MK));
     if (m.down)
       k_merge_run_f64<true, MK><<<nb64, kMergeThreads, 0, s>>>(
           m, vft_panel, od, a, b, dv, rad_in, tr_in, rad_out, tr_out, tbnd, emis, iemit);
@@ -3418,21 +3460,42 @@ cudaError_t launch_scan(const double* spec, int64_t n, int ir, int jabs, double*
   return cudaGetLastError();
 }
 
-// CNVRCT (src/postsub.f90:1779-1985), one thread per box: the inner points
+// CNVRCT (src/postsub.f90:1779-1985; mode 0), CNVVRC (:1986-2214; mode 5)
+// and CNVVRL (:2216-2440; mode 6), one thread per box: the inner points
 // weighted 1, the end points by the fraction of their interval inside the
 // box, the weighted sum over the sum of the weights; the reference's order
-// of operations, each rounded separately.
-__global__ void k_scan_rect(const double* __restrict__ spec, int64_t n, int jabs, double v1,
-                            double dvo, double hwhm, double v1i, double dvi,
-                            double* __restrict__ out, int64_t n_out) {
+// of operations, each rounded separately.  Box j: mode 0 centred at
+// V1 + j DVO, half width HWHM; mode 5 centred there, from VCNT (1 - B^2/4)
+// to VCNT (1 + B^2/4); mode 6 from VLFT = V1 + j DVO to VLFT (1 + B^2/2),
+// B the field-of-view half angle in radians.
+__device__ __forceinline__ void scan_box(int mode, double v1, double dvo, double hwhm, double bfov,
+                                         int64_t j, double& vlft, double& vrgt) {
+  const double v0 = __dadd_rn(v1, __dmul_rn((double)j, dvo));
+  const double b2 = __dmul_rn(bfov, bfov);
+  if (mode == 5) {
+    const double q = __ddiv_rn(b2, 4.);
+    vlft = __dmul_rn(v0, __dsub_rn(1., q));
+    vrgt = __dmul_rn(v0, __dadd_rn(1., q));
+  } else if (mode == 6) {
+    vlft = v0;
+    vrgt = __dmul_rn(v0, __dadd_rn(1., __ddiv_rn(b2, 2.)));
+  } else {
+    vlft = __dsub_rn(v0, hwhm);
+    vrgt = __dadd_rn(v0, hwhm);
+  }
+}
+
+__global__ void k_scan_rect(const double* __restrict__ spec, int64_t n, int jabs, int mode,
+                            double v1, double dvo, double hwhm, double bfov, double v1i,
+                            double dvi, double* __restrict__ out, int64_t n_out) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n_out) return;
   auto S = [&](int64_t i) {  // 1-based
     const double x = spec[i - 1];
     return jabs ? __dsub_rn(1., x) : x;
   };
-  const double vcnt = __dadd_rn(v1, __dmul_rn((double)j, dvo));
-  const double vlft = __dsub_rn(vcnt, hwhm), vrgt = __dadd_rn(vcnt, hwhm);
+  double vlft, vrgt;
+  scan_box(mode, v1, dvo, hwhm, bfov, j, vlft, vrgt);
   const double rl = __dadd_rn(__ddiv_rn(__dsub_rn(vlft, v1i), dvi), 1.);
   const double rr = __dadd_rn(__ddiv_rn(__dsub_rn(vrgt, v1i), dvi), 1.);
   int64_t il = (int64_t)__dadd_rn(rl, 0.5), ih = (int64_t)__dadd_rn(rr, 0.5);
@@ -3451,12 +3514,12 @@ __global__ void k_scan_rect(const double* __restrict__ spec, int64_t n, int jabs
   out[j] = __ddiv_rn(sum, rnj);
 }
 
-cudaError_t launch_scan_rect(const double* spec, int64_t n, int jabs, double v1, double dvo,
-                             double hwhm, double v1i, double dvi, double* out, int64_t n_out,
-                             cudaStream_t s) {
+cudaError_t launch_scan_rect(const double* spec, int64_t n, int jabs, int mode, double v1,
+                             double dvo, double hwhm, double bfov, double v1i, double dvi,
+                             double* out, int64_t n_out, cudaStream_t s) {
   if (n_out > 0)
-    k_scan_rect<<<(unsigned)((n_out + 255) / 256), 256, 0, s>>>(spec, n, jabs, v1, dvo, hwhm,
-                                                                 v1i, dvi, out, n_out);
+    k_scan_rect<<<(unsigned)((n_out + 255) / 256), 256, 0, s>>>(spec, n, jabs, mode, v1, dvo,
+                                                                 hwhm, bfov, v1i, dvi, out, n_out);
   return cudaGetLastError();
 }
 

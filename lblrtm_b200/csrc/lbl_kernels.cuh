@@ -157,7 +157,7 @@ cudaError_t launch_merge(const LayerDev* Ld, const double* vft_panel, const doub
                          const double* rad_in, const double* tr_in, double* rad_out,
                          double* tr_out, double tbnd, double emis, int iemit, double tzu,
                          cudaStream_t s, int precision = LBL_PREC_FP64, int down = 0,
-                         double tbnd_last = 0., double tzl_tangent = 0.);
+                         double tbnd_last = 0., double tzl_tangent = 0., double refl = 0.);
 constexpr double kRADCN1 = 1.191042722E-12;  // src/phys_consts.f90:73
 constexpr double kRADCN2 = 1.4387752;        // src/phys_consts.f90:74
 // Temperatures of one EMIN step: XKT = T/RADCN2 and RADCN2/T for the layer
@@ -185,8 +185,12 @@ struct MergeRun {
                                  // (EMBND, the profile's last layer looking up)
   int64_t od_off[kMergeRunMax];  // each layer's optical depths in Work::od
   EminT t[kMergeRunMax];
-  // tangent path: XKTB (the lower level's temperature / RADCN2) and its
-  // reciprocal RADCN2 / TZL, per layer (0 when TZL <= 0)
+  // the reflected atmosphere (IPATHL=-1, specular): the boundary
+  // reflectivity BNDRFL(1); 0 otherwise
+  double refl;
+  // tangent path and reflected atmosphere: XKTB (the lower level's
+  // temperature / RADCN2) and its reciprocal RADCN2 / TZL, per layer (0 when
+  // TZL <= 0)
   double tb_xkt[kMergeRunMax], tb_rk[kMergeRunMax];
 };
 // Points [f_lo, f_hi) of the run's grid (f_hi < 0: to the end).
@@ -217,11 +221,12 @@ constexpr int kJacMaxParams = 8;
 // SCANFN: SHRKSC's compression of spec (n points, groups of ir, 1 - x when
 // jabs) into sc (n / ir points), then CONVSC's sums on the global output
 // grid, one thread per output point (the inputs ilo..ihi, 1-based).
-// CNVRCT: weighted means of the input over boxes of half width hwhm centred
-// at v1 + j*dvo (j < n_out; every box inside the input).
-cudaError_t launch_scan_rect(const double* spec, int64_t n, int jabs, double v1, double dvo,
-                             double hwhm, double v1i, double dvi, double* out, int64_t n_out,
-                             cudaStream_t s);
+// CNVRCT / CNVVRC / CNVVRL (mode 0 / 5 / 6): weighted means of the input
+// over boxes at v1 + j*dvo (j < n_out; every box inside the input): half
+// width hwhm (mode 0) or widths set by the field-of-view half angle bfov.
+cudaError_t launch_scan_rect(const double* spec, int64_t n, int jabs, int mode, double v1,
+                             double dvo, double hwhm, double bfov, double v1i, double dvi,
+                             double* out, int64_t n_out, cudaStream_t s);
 cudaError_t launch_scan(const double* spec, int64_t n, int ir, int jabs, double* sc, int64_t ilo,
                         int64_t ihi, double zint, double ratio, double zbound, double zslope,
                         double xnorm, const double* xf, int64_t nfmax, double* out,

@@ -77,7 +77,7 @@ extern "C" int lbl_merge_layer_noalloc(int device, const lbl_run* run, const lbl
   if (!run || !layer || !od || !rad_out || device < 0 || device >= kMaxDevices) return LBL_E_ARG;
   if (run->iemit != 0 && run->iemit != 1) return LBL_E_ARG;
   if (run->iemit == 1 && !tr_out) return LBL_E_ARG;
-  if (run->iemit == 1 && run->ipathl != 1) return LBL_E_ARG;
+  if (run->iemit == 1 && (run->ipathl != 1 || run->bndrfl != 0.)) return LBL_E_ARG;
   if (first != 0 && first != 1) return LBL_E_ARG;
   if (!first && (!rad_in || (run->iemit == 1 && !tr_in) || n_old < 1)) return LBL_E_ARG;
   if (!(layer->dv > 0.) || !(run->v2 > run->v1) || !(run->v1 > 0.) || n_new < 1)

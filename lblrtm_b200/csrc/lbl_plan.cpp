@@ -134,9 +134,11 @@ int dv_rule(const lbl_run& R, lbl_layer* Ls, int nlay, std::string* err) {
       *err = "layer " + std::to_string(l) + ": bad nmol/pave/tave";
       return LBL_E_ARG;
     }
-    if (R.iemit == 1 && R.ipathl == 2 && !(L.tzl > 0.)) {
-      // the tangent path's far crossing radiates at TZL (XKTB)
-      *err = "layer " + std::to_string(l) + ": the tangent path (IPATHL=2) needs TZL > 0";
+    if (R.iemit == 1 && (R.ipathl == 2 || (R.ipathl == 1 && R.bndrfl > 0.)) && !(L.tzl > 0.)) {
+      // the tangent path's far crossing and the reflected atmosphere's
+      // downward emission radiate at TZL (XKTB)
+      *err = "layer " + std::to_string(l) +
+             ": the tangent path and the reflected atmosphere need TZL > 0";
       return LBL_E_ARG;
     }
     double sumwk = 0.;
@@ -619,12 +621,12 @@ int pnlint_plan(const lbl_run& R, double dv, double dvout, PnlPlan* P, std::stri
 // 1912-1942, SINCSQ :2445-2484, SINC :2486-2525), SHRKSC's ratio
 // (:1276-1320) and CONVSC's constants (:1516-1560).
 int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
-  static const double HWJ[5] = {1., 2., 4., 54.1826, 119.332818};
-  static const double DXJ[5] = {0., 0.02, 0.02, 0.02, 0.02};
-  static const int64_t NJ[5] = {0, 101, 201, 2710, 5968};
-  static const int64_t NJMX[5] = {0, 251, 251, 2760, 6018};
-  static const double SMPLJ[5] = {.5, 2., 4., 4., 4.};
-  static const double XSCAL[5] = {0., 0., 0., 1.391557377, 1.89549425};
+  static const double HWJ[7] = {1., 2., 4., 54.1826, 119.332818, 1., 1.};
+  static const double DXJ[7] = {0., 0.02, 0.02, 0.02, 0.02, 0., 0.};
+  static const int64_t NJ[7] = {0, 101, 201, 2710, 5968, 0, 0};
+  static const int64_t NJMX[7] = {0, 251, 251, 2760, 6018, 0, 0};
+  static const double SMPLJ[7] = {.5, 2., 4., 4., 4., .5, .5};
+  static const double XSCAL[7] = {0., 0., 0., 1.391557377, 1.89549425, 0., 0.};
   static const long JRATIO[25] = {0, 1, 2, 3, 4, 5, 6, 8, 10, 12, 15, 16, 20,
                                   24, 25, 30, 32, 40, 48, 50, 60, 75, 80, 100, 120};
   const double pi = 2. * std::asin(1.);
@@ -641,8 +643,9 @@ int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
       return LBL_E_ARG;
     }
   }
-  if (jfn < 0 || jfn > 4) {
-    *err = "scan: JFN must be 0-4 (rectangle, triangle, Gaussian, sinc^2, sinc)";
+  if (jfn < 0 || jfn > 6) {
+    *err = "scan: JFN must be 0-6 (rectangle, triangle, Gaussian, sinc^2, sinc, field-of-view "
+           "boxes centred / left-aligned)";
     return LBL_E_ARG;
   }
   const double xscale = XSCAL[jfn];
@@ -655,12 +658,27 @@ int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
   double sample = SMPLJ[jfn];
   if (sc.sampl < 0.) sample = hwhm / (-sc.sampl);
   else if (sc.sampl > 0.) sample = sc.sampl;
-  if (dv_in > hwhm / 12.) {
-    *err = "scan: input spacing above HWHM/12 (the reference interpolates first, SCNINT)";
+  // DVINT (SCANFN :245-265): for JFN 5/6 a twelfth of the first box, whose
+  // width is V1 BFOV^2 / 2
+  const double dvint = (jfn == 5 || jfn == 6)
+                           ? sc.v1 * ((hwhm * 3.141592654 / 180.) * (hwhm * 3.141592654 / 180.)) / 24
+                           : hwhm / 12.;
+  if (dv_in > dvint) {
+    *err = "scan: input spacing above DVINT (the reference interpolates first, SCNINT)";
     return LBL_E_RANGE;
   }
   P->hwhm = hwhm;
   P->dvo = hwhm / sample;
+  if (jfn == 5 || jfn == 6) {
+    // boxes whose width grows with wavenumber (CNVVRC :1986-2214 centred at
+    // V1 + (NB-1) DVO, CNVVRL :2216-2440 starting there), up to V2
+    P->bfov = hwhm * 3.141592654 / 180.;
+    int64_t nb = 1;
+    while (sc.v1 + double(nb) * P->dvo <= sc.v2) nb++;
+    P->n_out = nb;
+    P->nnhi = nb + kNShift;
+    return LBL_OK;
+  }
   if (jfn == 0) {
     // adjacent boxes of 2 HWHM (SCANFN :393-399, CNVRCT :1779-1985): DVO a
     // whole number IRATIO of input steps; the boxes centred at V1 + (NB-1)

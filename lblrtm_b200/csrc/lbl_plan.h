@@ -157,6 +157,7 @@ struct ScanPlan {
   double hwhm = 0., dvo = 0., hwf = 0., dxf = 0., bound = 0., vft0 = 0., vbot = 0., vtop = 0.;
   int64_t nf = 0, nfmax = 0, nnhi = 0;   // NNHI: last output point, R1 index
   int64_t n_out = 0;                     // output points (R1 33..NNHI)
+  double bfov = 0.;                      // JFN 5/6: the field-of-view half angle, radians
   std::vector<double> xf;                // XF, 1-based
   // compression and convolution for an input spacing
   int64_t iratsh = 1;

@@ -1658,6 +1658,12 @@ double xkta_of(const lbl_run& R, const lbl_layer& L) {
   return (R.ipathl == 3 ? L.tzl : L.tzu) / RADCN2;
 }
 
+// The reflected atmosphere (IPATHL=-1): looking down with a boundary
+// reflectivity, EMINIT/RADMRG turn IPATHL=1 into -1 (src/xmerge.f90:2389,
+// 2725; IBPROP=1 when BNDRFL is non-zero, src/lblrtm.f90:979-980), specular
+// (SURF_REFL 's'), constant BNDRFL(1).
+bool reflected(const lbl_run& R) { return R.ipathl == 1 && R.bndrfl != 0.; }
+
 // EMINIT (src/xmerge.f90:2436-2484): IPATHL=1 with the surface term when
 // TBND>0; IPATHL=3 with no boundary at the first layer (XMERGE :136-141).
 void eminit(const lbl_run& R, const lbl_layer& L, const std::vector<PanelOut>& od,
@@ -1669,12 +1675,23 @@ void eminit(const lbl_run& R, const lbl_layer& L, const std::vector<PanelOut>& o
   out.clear();
   for (const PanelOut& p : od) {
     std::vector<double> EM, TR, EMB;
-    const bool tangent = R.ipathl == 2;
-    emin(p, XKT, XKTA, EM, TR, tangent ? L.tzl / RADCN2 : 0., tangent ? &EMB : nullptr);
+    const bool tangent = R.ipathl == 2, refl = reflected(R);
+    emin(p, XKT, XKTA, EM, TR, (tangent || refl) ? L.tzl / RADCN2 : 0.,
+         (tangent || refl) ? &EMB : nullptr);
     MPanel mp{p.v1p, p.v2p, p.dvp, p.nlim, {}, {}};
     mp.rad.resize(p.nlim);
     mp.tr.resize(p.nlim);
-    if (tangent) {
+    if (refl) {
+      // IPATHL=-1 (:2486-2540, constant EMISIV and REFLCT): the layer's
+      // downward emission reflected at the surface, and the surface's own
+      double EMISIV = R.bndemi, REFLCT = R.bndrfl;
+      double VI = p.v1p;
+      for (long J = 1; J <= p.nlim; J++) {
+        double BB = PLANCK(VI, XKTBND);
+        EM[J] = EM[J] + EMB[J] * REFLCT * TR[J] + TR[J] * BB * EMISIV;
+        VI = VI + p.dvp;
+      }
+    } else if (tangent) {
       // IPATHL=2, IANT=0 (:2442-2447): the tangent layer crossed twice
       for (long J = 1; J <= p.nlim; J++) {
         const double TRJ = TR[J];
@@ -1720,6 +1737,10 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
   // IPATH_FLG = 2 (the symmetric tangent path): the layer's other crossing,
   // EMB (filled by `layer` with EM and TR), seen through the old path
   const bool tangent = R.ipathl == 2 && EMBp != nullptr;
+  // IPATH_FLG = -10 (the reflected atmosphere, specular): EMB goes down
+  // through the old path, is reflected and comes back up through it
+  const bool refl = reflected(R) && EMBp != nullptr;
+  const double REFLCT = R.bndrfl;
   double ATYPE = ITYPE;
   long LL = ITYPE + 1;
   double AP = 1.0 / (ATYPE + 1.0);
@@ -1780,6 +1801,13 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
       if (NL == 1) {
         for (long I = NL; I <= NLIM; I += LL) {
           IPL = IPL + LLM1;
+          if (refl) {
+            // :3051-3066
+            const double TRTEMP = TR[I] * TRAO[IPL];
+            EM[I] = TR[I] * RADO[IPL] + EM[I] + (*EMBp)[I] * TRAO[IPL] * TRTEMP * REFLCT;
+            TR[I] = TRTEMP;
+            continue;
+          }
           if (tangent) {
             // :2997-3005
             const double TRTEMP = TR[I] * TRAO[IPL];
@@ -1795,6 +1823,17 @@ int radmrg_core(const lbl_run& R, const lbl_layer& L, double DVL,
         double A1N = A1[NL], A2N = A2[NL], A3N = A3[NL], A4N = A4[NL];
         for (long I = NL; I <= NLIM; I += LL) {
           IPL = IPL + LLM1;
+          if (refl) {
+            // :3197-3215
+            const double TRAOI = A1N * TRAO[IPL - 1] + A2N * TRAO[IPL] + A3N * TRAO[IPL + 1] +
+                                 A4N * TRAO[IPL + 2];
+            const double TRTEMP = TR[I] * TRAOI;
+            EM[I] = TR[I] * (A1N * RADO[IPL - 1] + A2N * RADO[IPL] + A3N * RADO[IPL + 1] +
+                             A4N * RADO[IPL + 2]) +
+                    EM[I] + (*EMBp)[I] * TRAOI * TRTEMP * REFLCT;
+            TR[I] = TRTEMP;
+            continue;
+          }
           if (tangent) {
             // :3132-3148
             const double TRTEMP = TR[I] * (A1N * TRAO[IPL - 1] + A2N * TRAO[IPL] +
@@ -1841,8 +1880,8 @@ int radmrg(const lbl_run& R, const lbl_layer& L, double DVL,
            const std::vector<MPanel>& old, const std::vector<PanelOut>& od,
            std::vector<MPanel>& out) {
   const double XKT = L.tave / RADCN2, XKTA = xkta_of(R, L);
-  // IPATHL=2: XKTB the lower level's temperature (:2771-2773)
-  const bool tangent = R.ipathl == 2;
+  // IPATHL=2 and -1: XKTB the lower level's temperature (:2765-2773)
+  const bool tangent = R.ipathl == 2 || reflected(R);
   const double XKTB = tangent ? L.tzl / RADCN2 : 0.;
   std::vector<double> EMB;
   return radmrg_core(R, L, DVL, old, od,
@@ -2250,16 +2289,17 @@ struct ScanOracle {
   int jfn = 0;
   double hwhm = 0, sample = 0, dvo = 0, hwf = 0, dxf = 0, bound = 0, vft0 = 0, vbot = 0, vtop = 0;
   long nf = 0, nfmax = 0, nnhi = 0;
+  double bfov = 0;         // JFN 5/6: the field-of-view half angle, radians
   std::vector<double> xf;  // 1-based
 };
 
 int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
-  static const double HWJ[5] = {1., 2., 4., 54.1826, 119.332818};
-  static const double DXJ[5] = {0., 0.02, 0.02, 0.02, 0.02};
-  static const long NJ[5] = {0, 101, 201, 2710, 5968};
-  static const long NJMX[5] = {0, 251, 251, 2760, 6018};
-  static const double SMPLJ[5] = {.5, 2., 4., 4., 4.};
-  static const double XSCAL[5] = {0., 0., 0., 1.391557377, 1.89549425};
+  static const double HWJ[7] = {1., 2., 4., 54.1826, 119.332818, 1., 1.};
+  static const double DXJ[7] = {0., 0.02, 0.02, 0.02, 0.02, 0., 0.};
+  static const long NJ[7] = {0, 101, 201, 2710, 5968, 0, 0};
+  static const long NJMX[7] = {0, 251, 251, 2760, 6018, 0, 0};
+  static const double SMPLJ[7] = {.5, 2., 4., 4., 4., .5, .5};
+  static const double XSCAL[7] = {0., 0., 0., 1.391557377, 1.89549425, 0., 0.};
   const double PI = 2. * std::asin(1.);
   double HWHM = sc.hwhm;
   int JFN = sc.jfn;
@@ -2268,7 +2308,8 @@ int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
     JFN = -JFN;
     if (JFN != 3 && JFN != 4) return fail(LBL_E_ARG, "SCANFN; INVALID JFN");
   }
-  if (JFN < 0 || JFN > 4) return fail(LBL_E_ARG, "scan: JFN 0-4 (rectangle, triangle, Gauss, sinc^2, sinc)");
+  if (JFN < 0 || JFN > 6)
+    return fail(LBL_E_ARG, "scan: JFN 0-6 (rectangle, triangle, Gauss, sinc^2, sinc, FOV boxes)");
   const double XSCALE = XSCAL[JFN];
   if (sc.jfn < 0) HWHM = HWHM / (PI / XSCALE);
   S.jfn = JFN;
@@ -2279,11 +2320,21 @@ int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
   double SAMPLE = SMPLJ[JFN];
   if (sc.sampl < 0.) SAMPLE = HWHM / (-sc.sampl);
   else if (sc.sampl > 0.) SAMPLE = sc.sampl;
-  const double DVINT = HWHM / 12.;
-  if (dv_in > DVINT) return fail(LBL_E_RANGE, "scan: input DV above HWHM/12 (SCNINT not built)");
+  // DVINT (:245-265)
+  double DVINT = HWHM / 12.;
+  if (JFN == 5 || JFN == 6) DVINT = sc.v1 * std::pow(HWHM * 3.141592654 / 180., 2) / 24;
+  if (dv_in > DVINT) return fail(LBL_E_RANGE, "scan: input DV above DVINT (SCNINT not built)");
   S.hwhm = HWHM;
   S.sample = SAMPLE;
   S.dvo = HWHM / SAMPLE;
+  if (JFN == 5 || JFN == 6) {
+    // CNVVRC / CNVVRL: boxes at V1 + (NB-1) DVO up to V2, no IRATIO
+    S.bfov = HWHM * 3.141592654 / 180.;
+    long NB = 1;
+    while (sc.v1 + double(NB) * S.dvo <= sc.v2) NB++;
+    S.nnhi = NB + 32;
+    return LBL_OK;
+  }
   if (JFN == 0) {
     // adjacent boxes of 2 HWHM (SCANFN :393-399): DVO a whole number of DVI
     const long IRATIO = fint(S.dvo / dv_in + 0.5);
@@ -2340,21 +2391,39 @@ int scan_spectrum(const lbl_scan& sc, const double* spec, int64_t n, double v1_i
   // RDSCAN (:1411-1514): JEMIT=-1 convolves the absorption 1 - S
   std::vector<double> s(spec, spec + n);
   if (sc.jabs) for (auto& x : s) x = 1. - x;
-  if (S.jfn == 0) {
-    // CNVRCT (:1779-1985) on the whole input: box NB centred at V1 +
-    // (NB-1) DVO, half width HWHM; inner points weight 1, the end points
-    // the fraction of their interval inside the box; the weighted mean
+  if (S.jfn == 0 || S.jfn == 5 || S.jfn == 6) {
+    // CNVRCT (:1779-1985), CNVVRC (:1986-2214), CNVVRL (:2216-2440) on the
+    // whole input: box NB at V1 + (NB-1) DVO, centred with half width HWHM
+    // (JFN 0), centred from VCNT (1 - BFOV^2/4) to VCNT (1 + BFOV^2/4) (5),
+    // from VLFT to VLFT (1 + BFOV^2/2) (6); inner points weight 1, the end
+    // points the fraction of their interval inside the box; the weighted mean
     const double DVI = dv_in, V1I = v1_in;
     const long NNI = (long)n;
+    const double BFOV = S.bfov;
+    auto edges = [&](long NB, double& VLFT, double& VRGT) {
+      const double V0 = sc.v1 + double(NB - 1) * S.dvo;
+      if (S.jfn == 5) {
+        VLFT = V0 * (1 - BFOV * BFOV / 4);
+        VRGT = V0 * (1 + BFOV * BFOV / 4);
+      } else if (S.jfn == 6) {
+        VLFT = V0;
+        VRGT = V0 * (1 + BFOV * BFOV / 2);
+      } else {
+        VLFT = V0 - S.hwhm;
+        VRGT = V0 + S.hwhm;
+      }
+    };
     // the boxes must lie inside the spectrum (the reference outputs no box
     // that runs past its data)
-    const double vlast = sc.v1 + double(S.nnhi - 33) * S.dvo + S.hwhm;
-    if (v1_in > sc.v1 - S.hwhm - DVI || v1_in + double(n - 1) * DVI < vlast + DVI)
+    double vfirst, vdum, vlast;
+    edges(1, vfirst, vdum);
+    edges(S.nnhi - 32, vdum, vlast);
+    if (v1_in > vfirst - DVI || v1_in + double(n - 1) * DVI < vlast + DVI)
       return fail(LBL_E_RANGE, "scan: the boxes must lie inside the spectrum");
     out.clear();
     for (long NB = 1; NB <= S.nnhi - 32; NB++) {
-      const double VCNT = sc.v1 + double(NB - 1) * S.dvo;
-      const double VLFT = VCNT - S.hwhm, VRGT = VCNT + S.hwhm;
+      double VLFT, VRGT;
+      edges(NB, VLFT, VRGT);
       const double RL = (VLFT - V1I) / DVI + 1, RR = (VRGT - V1I) / DVI + 1;
       long IL = fint(RL + 0.5), IH = fint(RR + 0.5);
       double WGTL = ((V1I + double(IL - 1) * DVI) + DVI / 2. - VLFT) / DVI;

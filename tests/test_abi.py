@@ -100,3 +100,17 @@ def test_tangent_path_needs_lower_level_temperature():
     with pytest.raises(gpu.LblError) as e:
         gpu.dv_rule(run, lays)
     assert e.value.code == 1  # LBL_E_ARG
+
+
+def test_reflected_atmosphere_needs_lower_level_temperature():
+    """IPATHL=1 with BNDRFL > 0 is the reflected atmosphere, whose layers
+    radiate downward at TZL: the DV rule (run by every forward before any
+    device work) rejects a layer without it, and accepts it without BNDRFL."""
+    run = abi.make_run(v1=600.0, v2=650.0, iemit=1, ipathl=1)
+    lays = abi.make_layers(configs.atmosphere(6, ptop=300.0))
+    lays[2].tzl = 0.0
+    gpu.dv_rule(run, lays)
+    run.bndrfl = 0.2
+    with pytest.raises(gpu.LblError) as e:
+        gpu.dv_rule(run, lays)
+    assert e.value.code == 1  # LBL_E_ARG

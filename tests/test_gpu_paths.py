@@ -238,18 +238,26 @@ def test_downwelling_forward_matches_oracle_and_layer_steps(gpu_ctx):
 
 
 @pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_SPLIT])
-def test_tangent_path_forward_matches_oracle_and_layer_steps(gpu_ctx, precision):
+@pytest.mark.parametrize("path", ["tangent", "reflected"])
+def test_tangent_and_reflected_forward_match_oracle_and_layer_steps(gpu_ctx, precision, path):
     """The symmetric tangent path (IPATHL=2, IANT=0: EMINIT crosses the
     tangent layer twice, RADNN IPATH=2 adds each outer layer's near crossing
-    and its far crossing at TZL seen through the inner path) on a 40-layer
-    profile: the whole-profile forward against the oracle (FP64: 1e-8
-    relative radiance; split: 0.01 K brightness temperature), and the FP64
-    forward against lbl_merge_layer applied layer by layer."""
+    and its far crossing at TZL seen through the inner path) and the
+    reflected atmosphere (IPATHL=1 with BNDRFL: the reference's IPATHL=-1,
+    RADNN IPATH=-10, each layer's downward emission reflected at the
+    surface) on a 40-layer profile: the whole-profile forward against the
+    oracle (FP64: 1e-8 relative radiance; split: 0.01 K brightness
+    temperature), and the FP64 forward against lbl_merge_layer applied
+    layer by layer."""
     cfg = configs.config1(nlines=4000)
     lh = abi.LinesHandle(cfg["lines"])
     gpu_ctx.upload_lines(lh)
-    run = abi.make_run(v1=600.0, v2=650.0, iemit=1, ipathl=2, ilblf4=1, tmpbnd=290.0,
-                       bndemi=0.98)
+    if path == "tangent":
+        run = abi.make_run(v1=600.0, v2=650.0, iemit=1, ipathl=2, ilblf4=1, tmpbnd=290.0,
+                           bndemi=0.98)
+    else:
+        run = abi.make_run(v1=600.0, v2=650.0, iemit=1, ipathl=1, ilblf4=1, tmpbnd=290.0,
+                           bndemi=0.9, bndrfl=0.1)
     lays = abi.make_layers(configs.atmosphere(40))
     rad_ref, tr_ref = O.forward(run, abi.make_layers_like(lays), lh)
     frad, ftr = gpu_ctx.forward(run, lays, precision=precision)

@@ -3,8 +3,9 @@ restatement: the same compression, the same inputs summed in the same order
 for each output point, every product and sum rounded separately, so the
 results are compared exactly.  Inputs: a seeded synthetic radiance spectrum
 and the TOA radiance of a short forward, host and device buffers, all four
-functions and the rectangle, SAMPL given as points per HWHM and as an
-output spacing."""
+functions, the rectangle and the field-of-view boxes (JFN 5, 6; HWHM the
+half angle in degrees), SAMPL given as points per HWHM and as an output
+spacing."""
 import numpy as np
 import pytest
 
@@ -21,6 +22,8 @@ CASES = [
     (-3, 1.2, 0.0, 0),
     (0, 0.3, 0.0, 0),
     (0, 0.5, -0.07, 1),
+    (5, 2.0, -0.1, 0),
+    (6, 1.5, 0.0, 1),
 ]
 
 

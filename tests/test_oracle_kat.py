@@ -446,3 +446,33 @@ def test_o2_and_n2_collision_induced_bands_follow_their_tables():
         np.testing.assert_allclose(od2, 2.0 * od, rtol=1e-12)
         od0, _, _, _ = _co2_continuum_only(v1, v2, 0.0, jrad=0, xo2cn=0.0, xn2cn=0.0)
         assert np.all(od0 == 0.0)
+
+
+def test_reflected_atmosphere_specular():
+    """IPATHL=1 with BNDRFL(1) > 0 is the reflected atmosphere (IPATHL=-1,
+    specular; EMINIT :2486-2540, RADNN IPATH=-10 :3051-3066): each layer's
+    downward emission reaches the surface through the layers below, is
+    reflected and comes back up: with surface temperature Ts, emissivity e
+    and reflectivity r, R1 = B1(1-T1)(1 + r T1) + T1 e B(Ts), and the next
+    layer adds B2(1-T2)(1 + r T1^2 T2) over T2 R1 (isothermal layers of
+    constant optical depth on one grid)."""
+    t1, t2, tau1, tau2, ts, emis, refl = 280.0, 230.0, 0.7, 1.3, 295.0, 0.9, 0.1
+    lays = _two_layers(t1, t2)
+    for l in lays:
+        l.dv = 0.01
+    run = abi.make_run(v1=700.0, v2=710.0, iemit=1, ipathl=1, tmpbnd=ts, bndemi=emis,
+                       bndrfl=refl)
+    n = O.npts(run, 0.01)
+    r1, x1 = O.merge_layer(run, lays[0], 1, 0.0, None, None, np.full(n, tau1))
+    r2, x2 = O.merge_layer(run, lays[1], 0, 0.01, r1, x1, np.full(n, tau2))
+    v = 700.0 + 0.01 * np.arange(n)
+    b1, b2, bs = _planck(v, t1), _planck(v, t2), _planck(v, ts)
+    e1, e2 = np.exp(-tau1), np.exp(-tau2)
+    np.testing.assert_allclose(r1, b1 * (1 - e1) * (1 + refl * e1) + e1 * emis * bs, rtol=1e-12)
+    np.testing.assert_allclose(x1, e1, rtol=1e-14)
+    np.testing.assert_allclose(r2, e2 * r1 + b2 * (1 - e2) * (1 + refl * e1 * e1 * e2), rtol=1e-12)
+    np.testing.assert_allclose(x2, e1 * e2, rtol=1e-14)
+    # no reflectivity: the plain upwelling merge
+    run0 = abi.make_run(v1=700.0, v2=710.0, iemit=1, ipathl=1, tmpbnd=ts, bndemi=emis)
+    q1, _ = O.merge_layer(run0, lays[0], 1, 0.0, None, None, np.full(n, tau1))
+    np.testing.assert_allclose(q1, b1 * (1 - e1) + e1 * emis * bs, rtol=1e-12)

@@ -112,3 +112,45 @@ def test_rejections():
     rect = abi.make_scan(hwhm=0.6, v1=650.0, v2=750.0, jfn=0)
     with pytest.raises(RuntimeError, match="inside the spectrum"):
         O.scan(rect, np.zeros(30000), 600.0, 0.004)
+
+
+@pytest.mark.parametrize("jfn,angle,sampl,jabs", [(5, 2.0, -0.1, 0), (6, 1.5, -0.25, 1),
+                                                  (5, 3.0, 0.0, 0)])
+def test_field_of_view_boxes_are_box_means(jfn, angle, sampl, jabs):
+    """CNVVRC (JFN 5) and CNVVRL (JFN 6): boxes whose width grows with
+    wavenumber, V B^2/2 for a field-of-view half angle B (HWHM in degrees):
+    centred at V1 + j DVOUT from VCNT (1 - B^2/4) to VCNT (1 + B^2/4), or
+    starting there and reaching VLFT (1 + B^2/2); each output the weighted
+    box mean of CNVRCT; DVOUT = HWHM/SAMPLE (SAMPLE 0.5 by default)."""
+    v1, dv = 600.0, 0.0013
+    rng = np.random.default_rng(8)
+    spec = np.exp(-rng.exponential(1.0, 300000))
+    sc = abi.make_scan(hwhm=angle, v1=640.0, v2=900.0, jfn=jfn, sampl=sampl, jabs=jabs)
+    out, dvo = O.scan(sc, spec, v1, dv)
+    sample = sampl if sampl > 0 else (angle / -sampl if sampl < 0 else 0.5)
+    assert dvo == angle / sample
+    n, dvo_lib = gpu.scan_npts(sc, dv)
+    assert (n, dvo_lib) == (len(out), dvo)
+    b = angle * 3.141592654 / 180.0
+    v0 = 640.0 + dvo * np.arange(len(out))
+    assert v0[-1] <= 900.0 < v0[-1] + dvo
+    lo = v0 * (1 - b * b / 4) if jfn == 5 else v0
+    hi = v0 * (1 + b * b / 4) if jfn == 5 else v0 * (1 + b * b / 2)
+    s = 1.0 - spec if jabs else spec
+    v = v1 + dv * np.arange(len(s))
+    ref = []
+    for a, c in zip(lo, hi):
+        w = np.clip(np.minimum(v + dv / 2, c) - np.maximum(v - dv / 2, a), 0.0, None)
+        ref.append(np.dot(w, s) / w.sum())
+    np.testing.assert_allclose(out, np.array(ref), rtol=1e-11)
+
+
+def test_field_of_view_needs_fine_input():
+    """DVINT for JFN 5/6 is a twelfth of the first box (V1 B^2/24); a coarser
+    input needs SCNINT, which is not built."""
+    sc = abi.make_scan(hwhm=1.0, v1=640.0, v2=700.0, jfn=5, sampl=-0.1)
+    dvint = 640.0 * (1.0 * 3.141592654 / 180.0) ** 2 / 24
+    assert gpu.load().lbl_scan_npts(C.byref(sc), dvint * 0.99, None) > 0
+    assert gpu.load().lbl_scan_npts(C.byref(sc), dvint * 1.01, None) == -7
+    bad = abi.make_scan(hwhm=1.0, v1=640.0, v2=700.0, jfn=-5)
+    assert gpu.load().lbl_scan_npts(C.byref(bad), 0.001, None) == -1
