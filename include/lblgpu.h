@@ -266,16 +266,20 @@ int lbl_pnlint(lbl_ctx* ctx, const lbl_run* run, double dv, double dvout,
 
 /* SCANFN's scanning functions (src/postsub.f90:25-560, CONVSC :1516-1598,
  * SHRKSC :1276-1376, shapes SHAPET :1377, SHAPEG src/oprop.f90:1912,
- * SINCSQ :2445, SINC :2486; the rectangle CNVRCT :1779-1985) convolved
+ * SINCSQ :2445, SINC :2486; the rectangle CNVRCT :1779-1985, the
+ * field-of-view boxes CNVVRC :1986-2214 and CNVVRL :2216-2440) convolved
  * with a spectrum on a uniform grid. */
 typedef struct lbl_scan {
   double hwhm;      /* HWHM of the function, cm-1 (JFN -3/-4: its first
-                       zero crossing, divided by pi/XSCALE as SCANFN does) */
+                       zero crossing, divided by pi/XSCALE as SCANFN does;
+                       JFN 5/6: the field of view's half angle, degrees) */
   double v1, v2;    /* output range, cm-1 */
   double sampl;     /* SAMPL: > 0 points per HWHM, < 0 minus the output
                        spacing, 0 the function's default (2 or 4) */
   int32_t jfn;      /* 0 rectangle, 1 triangle, 2 Gaussian, 3 sinc^2,
-                       4 sinc; -3, -4 */
+                       4 sinc, 5 boxes of width V*B^2/2 centred at the
+                       output points, 6 the same boxes starting there
+                       (B the half angle in radians); -3, -4 */
   int32_t jabs;     /* 1: convolve 1 - spectrum (JEMIT=-1, absorption) */
 } lbl_scan;
 
@@ -283,10 +287,11 @@ typedef struct lbl_scan {
  * dv_in: points V1 + j*DVOUT up to the one nearest V2 (PANLSC's last panel,
  * :1600-1660); for the rectangle, DVOUT = IRATIO*dv_in with IRATIO the
  * nearest whole number to HWHM/(SAMPLE*dv_in), and the boxes centred at
- * V1 + j*DVOUT <= V2.  Negative: minus a status (-LBL_E_ARG for a bad
- * argument, -LBL_E_RANGE when dv_in exceeds HWHM/12: the reference then
- * first interpolates the spectrum, SCNINT, which is not built; also when
- * the rectangle's IRATIO is below 2). */
+ * V1 + j*DVOUT <= V2.  An input spacing above SCANFN's DVINT (HWHM/12; for
+ * JFN 5/6 V1*B^2/24) is first interpolated onto DVINT as the reference does
+ * (SCNINT/INTERP, src/postsub.f90:824-1035, 2940-3215), and the grid is that
+ * of DVINT.  Negative: minus a status (-LBL_E_ARG for a bad argument,
+ * -LBL_E_RANGE when the rectangle's IRATIO is below 2). */
 int64_t lbl_scan_npts(const lbl_scan* sc, double dv_in, double* dvout);
 
 /* The scanned spectrum: spec on v1_in + i*dv_in (n points, host or device),
@@ -295,8 +300,9 @@ int64_t lbl_scan_npts(const lbl_scan* sc, double dv_in, double* dvout);
  * inputs whose function reaches it), on the global output grid (the
  * reference's panel origins and incremental table offsets round slightly
  * differently; see lbl_scan_npts for the grid).  The rectangle (JFN 0)
- * is CNVRCT's weighted box mean: the inner points weight 1, the two end
- * points the fraction of their interval inside the box; every box must
+ * (and JFN 5/6) is CNVRCT's weighted box mean: the inner points weight 1,
+ * the two end points the fraction of their interval inside the box; every
+ * box must
  * lie inside the input (LBL_E_RANGE otherwise).  out: n_out points, host
  * or device. */
 int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int64_t n,

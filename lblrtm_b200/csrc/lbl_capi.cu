@@ -1987,10 +1987,17 @@ int64_t lbl_scan_npts(const lbl_scan* sc, double dv_in, double* dvout) {
   if (!sc) return -LBL_E_ARG;
   ScanPlan P;
   std::string e;
-  const int rc = scan_plan(*sc, dv_in, &P, &e);
+  int rc = scan_plan(*sc, dv_in, &P, &e);
+  // a spectrum coarser than DVINT is scanned on DVINT after SCNINT
+  if (rc == LBL_E_RANGE && P.dvint > 0. && dv_in > P.dvint) rc = scan_plan(*sc, P.dvint, &P, &e);
   if (rc) return -rc;
   if (dvout) *dvout = P.dvo;
   return P.n_out;
+}
+
+namespace {
+int scan_core(lbl_ctx* ctx, const lbl_scan* sc, const ScanPlan& P, const double* spec, int64_t n,
+              double v1_in, double dv_in, double* out, int64_t n_out);
 }
 
 int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int64_t n,
@@ -2000,7 +2007,59 @@ int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int6
   ScanPlan P;
   std::string e;
   int rc = scan_plan(*sc, dv_in, &P, &e);
+  if (!(rc == LBL_E_RANGE && P.dvint > 0. && dv_in > P.dvint)) {
+    if (rc) return fail(ctx, rc, e);
+    return scan_core(ctx, sc, P, spec, n, v1_in, dv_in, out, n_out);
+  }
+  // SCANFN :322-345: the spectrum is first interpolated onto DVINT (SCNINT),
+  // then scanned there
+  const double dvint = P.dvint;
+  rc = scan_plan(*sc, dvint, &P, &e);
   if (rc) return fail(ctx, rc, e);
+  if (P.n_out != n_out) return fail(ctx, LBL_E_ARG, "n_out does not match the output grid");
+  std::vector<ScnChunk> chunks;
+  int64_t n_fine = 0;
+  rc = scnint_plan(n, v1_in, dv_in, dvint, &chunks, &n_fine, &e);
+  if (rc) return fail(ctx, rc, e);
+  static_assert(sizeof(ScnChunk) == sizeof(ScnChunkDev), "chunk layouts");
+  std::vector<double> coef(4 * 203);
+  scnint_coefs(coef.data());
+  cudaSetDevice(ctx->device);
+  const bool in_dev = is_device_ptr(spec);
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_fine = up((size_t)n_fine * 8), b_in = in_dev ? 0 : up((size_t)n * 8),
+               b_ch = up(chunks.size() * sizeof(ScnChunk)), b_co = up(coef.size() * 8);
+  const size_t bytes = b_fine + b_in + b_ch + b_co;
+  void* mem = nullptr;
+  CK(ctx->mem.alloc(&mem, bytes));
+  struct Release {
+    lbl_ctx* c;
+    void* m;
+    size_t b;
+    ~Release() { c->mem.release(m, b); }
+  } guard{ctx, mem, bytes};
+  char* base = static_cast<char*>(mem);
+  double* fine = reinterpret_cast<double*>(base);
+  double* din = in_dev ? const_cast<double*>(spec) : reinterpret_cast<double*>(base + b_fine);
+  ScnChunkDev* dch = reinterpret_cast<ScnChunkDev*>(base + b_fine + b_in);
+  double* dco = reinterpret_cast<double*>(base + b_fine + b_in + b_ch);
+  cudaStream_t s = ctx->stream;
+  if (!in_dev) CK(cudaMemcpyAsync(din, spec, (size_t)n * 8, cudaMemcpyHostToDevice, s));
+  if (!chunks.empty())
+    CK(cudaMemcpyAsync(dch, chunks.data(), chunks.size() * sizeof(ScnChunk),
+                       cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dco, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice, s));
+  CK(launch_scnint(dch, (int64_t)chunks.size(), din, n, dco, dvint / dv_in, fine, s));
+  rc = scan_core(ctx, sc, P, fine, n_fine, v1_in, dvint, out, n_out);
+  // the pageable copies above and the kernel finished before scan_core
+  // returned (it synchronises the stream)
+  CK(cudaStreamSynchronize(s));
+  return rc;
+}
+
+namespace {
+int scan_core(lbl_ctx* ctx, const lbl_scan* sc, const ScanPlan& P, const double* spec, int64_t n,
+              double v1_in, double dv_in, double* out, int64_t n_out) {
   if (P.n_out != n_out) return fail(ctx, LBL_E_ARG, "n_out does not match the output grid");
   cudaSetDevice(ctx->device);
   if (P.jfn == 0 || P.jfn == 5 || P.jfn == 6) {
@@ -2065,6 +2124,7 @@ int lbl_scan_spectrum(lbl_ctx* ctx, const lbl_scan* sc, const double* spec, int6
   CK(cudaStreamSynchronize(s));
   return LBL_OK;
 }
+}  // namespace
 
 int lbl_forward(lbl_ctx* ctx, const lbl_run* run, lbl_layer* layers, int32_t nlay, double* rad,
                 double* tr, int64_t npts, int32_t precision) {

@@ -3514,6 +3514,57 @@ __global__ void k_scan_rect(const double* __restrict__ spec, int64_t n, int jabs
   out[j] = __ddiv_rn(sum, rnj);
 }
 
+// SCNINT/INTERP (src/postsub.f90:2940-3215), one thread per chunk of output
+// points: the 4-point cubic with weights tabulated at P = (IP-1)/200, P
+// carried from point to point by adding DVO/DVI, as the reference does.
+// T(i) of input panel k is spectrum point 2400 k + i - 5; below the first
+// point T(4) = 2 T(5) - T(6) (and 0 further down), past the last point
+// 2 S(n) - S(n-1) (and 0 further up), as INTERP sets them.
+__global__ void k_scnint(const ScnChunkDev* __restrict__ chunks, int64_t nchunk,
+                         const double* __restrict__ spec, int64_t n,
+                         const double* __restrict__ coef, double vratio,
+                         double* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nchunk) return;
+  const ScnChunkDev c = chunks[t];
+  double* o = out + c.out0;
+  if (c.zero) {
+    for (int32_t j = 0; j < c.count; j++) o[j] = 0.;
+    return;
+  }
+  auto T = [&](int64_t i) -> double {
+    const int64_t g = 2400 * c.panel + i - 5;
+    if (g < 0) return g == -1 ? __dsub_rn(__dmul_rn(2.0, spec[0]), spec[1]) : 0.;
+    if (g >= n) return g == n ? __dsub_rn(__dmul_rn(2.0, spec[n - 1]), spec[n - 2]) : 0.;
+    return spec[g];
+  };
+  int64_t I = c.i0;
+  double P = c.p0;
+  for (int32_t j = 0; j < c.count; j++) {
+    int ip = (int)__dadd_rn(__dmul_rn(P, 201.), 1.00001);
+    ip = ip < 0 ? 0 : (ip > 202 ? 202 : ip);
+    double r = __dmul_rn(coef[ip], T(I - 1));
+    r = __dadd_rn(r, __dmul_rn(coef[203 + ip], T(I)));
+    r = __dadd_rn(r, __dmul_rn(coef[406 + ip], T(I + 1)));
+    r = __dadd_rn(r, __dmul_rn(coef[609 + ip], T(I + 2)));
+    o[j] = r;
+    P = __dadd_rn(P, vratio);
+    if (P >= 1.0) {
+      I = (int64_t)__dadd_rn((double)I, P);
+      P = __dsub_rn(P, (double)(int64_t)P);
+    }
+  }
+}
+
+cudaError_t launch_scnint(const ScnChunkDev* chunks, int64_t nchunk, const double* spec,
+                          int64_t n, const double* coef, double vratio, double* out,
+                          cudaStream_t s) {
+  if (nchunk > 0)
+    k_scnint<<<(unsigned)((nchunk + 127) / 128), 128, 0, s>>>(chunks, nchunk, spec, n, coef,
+                                                              vratio, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_scan_rect(const double* spec, int64_t n, int jabs, int mode, double v1,
                              double dvo, double hwhm, double bfov, double v1i, double dvi,
                              double* out, int64_t n_out, cudaStream_t s) {

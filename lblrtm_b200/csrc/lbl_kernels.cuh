@@ -221,6 +221,16 @@ constexpr int kJacMaxParams = 8;
 // SCANFN: SHRKSC's compression of spec (n points, groups of ir, 1 - x when
 // jabs) into sc (n / ir points), then CONVSC's sums on the global output
 // grid, one thread per output point (the inputs ilo..ihi, 1-based).
+// SCNINT/INTERP: the chunks of a host replay (lbl_plan.h ScnChunk, same
+// layout), the weights C1..C4 (4 x 203), out of the replay's size.
+struct ScnChunkDev {
+  int64_t out0, panel, i0;
+  double p0;
+  int32_t count, zero;
+};
+cudaError_t launch_scnint(const ScnChunkDev* chunks, int64_t nchunk, const double* spec,
+                          int64_t n, const double* coef, double vratio, double* out,
+                          cudaStream_t s);
 // CNVRCT / CNVVRC / CNVVRL (mode 0 / 5 / 6): weighted means of the input
 // over boxes at v1 + j*dvo (j < n_out; every box inside the input): half
 // width hwhm (mode 0) or widths set by the field-of-view half angle bfov.

@@ -663,8 +663,9 @@ int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
   const double dvint = (jfn == 5 || jfn == 6)
                            ? sc.v1 * ((hwhm * 3.141592654 / 180.) * (hwhm * 3.141592654 / 180.)) / 24
                            : hwhm / 12.;
+  P->dvint = dvint;
   if (dv_in > dvint) {
-    *err = "scan: input spacing above DVINT (the reference interpolates first, SCNINT)";
+    *err = "scan: input spacing above DVINT (interpolate first, SCNINT)";
     return LBL_E_RANGE;
   }
   P->hwhm = hwhm;
@@ -753,6 +754,128 @@ int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err) {
   P->zslope = dvodx / hwhm;
   P->zbound = hwbnd * hwhm;
   P->xnorm = P->dvsc / hwhm;
+  return LBL_OK;
+}
+
+}  // namespace lbl
+
+namespace lbl {
+
+void scnint_coefs(double* c) {
+  const long NUMCOF = 201;
+  const double XNUMCF = double(NUMCOF);
+  for (long IP = 0; IP <= NUMCOF + 1; IP++) {
+    const double P = (double(IP) - 1.0) / (XNUMCF - 1.0);
+    const double PP = P * P;
+    c[IP] = -P / 2.0 * ((1 - P) * (1 - P));
+    c[203 + IP] = 1.0 - PP * (3.0 - 2.0 * P) + PP / 2.0 * (1.0 - P);
+    c[406 + IP] = PP * (3.0 - 2.0 * P) + P / 2.0 * ((1.0 - P) * (1.0 - P));
+    c[609 + IP] = -PP / 2 * (1.0 - P);
+  }
+}
+
+// The host replay of INTERP's control flow (labels 20, 40, 80): the chunk
+// bounds, the panel reads and, to decide them, each chunk's I and P
+// carried point by point exactly as the kernel will carry them.
+int scnint_plan(int64_t n, double v1_in, double dv_in, double dvo, std::vector<ScnChunk>* chunks,
+                int64_t* n_fine, std::string* err) {
+  chunks->clear();
+  if (n < 2 || !(dv_in > 0.) || !(dvo > 0.)) {
+    *err = "SCNINT: at least two input points and positive spacings";
+    return LBL_E_ARG;
+  }
+  const double XNUMCF = 201.;
+  const double V1 = v1_in;
+  const long NUM = fint(((v1_in + double(n - 1) * dv_in - V1) / dvo) + 0.5);
+  const double V2 = V1 + double(NUM) * dvo;
+  const double DVI = dv_in, DVJ = dvo, VRATIO = DVJ / DVI;
+  int64_t k = 0, nout = 0;
+  double V1I = 0., V2I = 0.;
+  long NNI = 0;
+  bool eof = false;
+  auto rdpanl = [&]() {
+    const int64_t a = 2400 * k;
+    if (a >= n) {
+      eof = true;
+      return;
+    }
+    const int64_t m = std::min<int64_t>(2400, n - a);
+    V1I = (v1_in + double(a) * dv_in) - 4.0 * DVI;
+    V2I = v1_in + double(a + m - 1) * dv_in;
+    NNI = (long)m + 4;
+    k++;
+  };
+  rdpanl();
+  double V1J = V1, VJ = V1J;
+  long J1 = 0, J2 = 0;
+  auto emit = [&](long j1, long j2, int zero, long I, double P) {
+    if (j2 < j1) return;
+    ScnChunk c;
+    c.out0 = nout + (j1 - 1);
+    c.panel = k - 1;
+    c.i0 = I;
+    c.p0 = P;
+    c.count = (int32_t)(j2 - j1 + 1);
+    c.zero = zero;
+    chunks->push_back(c);
+  };
+  auto panel_out = [&](long NNJ) {
+    const double V2J = V1J + DVJ * double(NNJ - 1);
+    nout += NNJ;
+    V1J = V2J + DVJ;
+  };
+  while (V1J < V1I) {
+    J2 = std::min<long>(fint((V1I - V1J) / DVJ) + 1, 2400);
+    emit(1, J2, 1, 0, 0.);
+    panel_out(J2);
+    VJ = V1J;
+  }
+  for (long guard = 0;; guard++) {
+    if (guard > 100000000L || (int64_t)chunks->size() > (int64_t(1) << 28)) {
+      *err = "SCNINT: the interpolation makes no progress";
+      return LBL_E_RANGE;
+    }
+    long I = fint((VJ - V1I) / DVI + 1.00001);
+    const double VI = V1I + DVI * double(I - 1);
+    double P = (VJ - VI) / DVI;
+    J1 = fint((VJ - V1J) / DVJ + 1.001);
+    J2 = std::min(std::min(fint((V2 - V1J) / DVJ + 1.001), fint((V2I - DVI - V1J) / DVJ + 1.)),
+                  2400L);
+    emit(J1, J2, 0, I, P);
+    for (long J = J1; J <= J2; J++) {
+      (void)fint(P * XNUMCF + 1.00001);
+      P = P + VRATIO;
+      if (P >= 1.0) {
+        I = fint(double(I) + P);
+        P = P - double(fint(P));
+      }
+    }
+    VJ = V1J + DVJ * double(J2);
+    if (J2 >= 2400 || VJ >= V2) {
+      panel_out(J2);
+      J2 = 0;
+    }
+    if (VJ >= V2) break;
+    if (eof) {
+      for (;;) {
+        J1 = J2 + 1;
+        J2 = std::min<long>(fint((V2 - V1J) / DVJ + 1.0001), 2400);
+        emit(J1, J2, 1, 0, 0.);
+        VJ = V1J + DVJ * double(J2);
+        if (J2 >= 2400 || VJ >= V2) {
+          panel_out(J2);
+          J2 = 0;
+        }
+        if (!(VJ < V2)) break;
+      }
+      break;
+    }
+    if (I >= NNI - 2) {
+      rdpanl();
+      if (eof) V2I = V2I + DVI;
+    }
+  }
+  *n_fine = nout;
   return LBL_OK;
 }
 

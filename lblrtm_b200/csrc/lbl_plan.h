@@ -158,12 +158,31 @@ struct ScanPlan {
   int64_t nf = 0, nfmax = 0, nnhi = 0;   // NNHI: last output point, R1 index
   int64_t n_out = 0;                     // output points (R1 33..NNHI)
   double bfov = 0.;                      // JFN 5/6: the field-of-view half angle, radians
+  double dvint = 0.;                     // DVINT: coarser input is interpolated first
   std::vector<double> xf;                // XF, 1-based
   // compression and convolution for an input spacing
   int64_t iratsh = 1;
   double dvsc = 0., v1shft = 0., ratio = 0., zslope = 0., zbound = 0., xnorm = 0.;
 };
-// Grid, table and constants for input spacing dv_in.
+// Grid, table and constants for input spacing dv_in.  A spacing above
+// SCANFN's DVINT gives LBL_E_RANGE with P->dvint set: the spectrum is then
+// first interpolated onto DVINT (scnint_plan) and planned again.
 int scan_plan(const lbl_scan& sc, double dv_in, ScanPlan* P, std::string* err);
+
+// SCNINT/INTERP (src/postsub.f90:824-1035, 2940-3215): the output points in
+// chunks that carry the fraction P from point to point; each chunk starts
+// from the wavenumber at its first point.  panel: the input panel (2400
+// points) current in the chunk; i0, p0: INTERP's I (1-based in that
+// panel's T array, T(5) its first point) and P at the chunk's first point;
+// zero: points past the input, set to 0.
+struct ScnChunk {
+  int64_t out0, panel, i0;
+  double p0;
+  int32_t count, zero;
+};
+int scnint_plan(int64_t n, double v1_in, double dv_in, double dvo, std::vector<ScnChunk>* chunks,
+                int64_t* n_fine, std::string* err);
+// INTERP's weights C1..C4 at IP = 0..202 (P = (IP-1)/200), 4 x 203 values.
+void scnint_coefs(double* c);
 
 }  // namespace lbl

@@ -2290,6 +2290,7 @@ struct ScanOracle {
   double hwhm = 0, sample = 0, dvo = 0, hwf = 0, dxf = 0, bound = 0, vft0 = 0, vbot = 0, vtop = 0;
   long nf = 0, nfmax = 0, nnhi = 0;
   double bfov = 0;         // JFN 5/6: the field-of-view half angle, radians
+  double dvint = 0;        // SCANFN's DVINT: a coarser input is interpolated first
   std::vector<double> xf;  // 1-based
 };
 
@@ -2323,7 +2324,8 @@ int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
   // DVINT (:245-265)
   double DVINT = HWHM / 12.;
   if (JFN == 5 || JFN == 6) DVINT = sc.v1 * std::pow(HWHM * 3.141592654 / 180., 2) / 24;
-  if (dv_in > DVINT) return fail(LBL_E_RANGE, "scan: input DV above DVINT (SCNINT not built)");
+  S.dvint = DVINT;
+  if (dv_in > DVINT) return fail(LBL_E_RANGE, "scan: input DV above DVINT (interpolate first)");
   S.hwhm = HWHM;
   S.sample = SAMPLE;
   S.dvo = HWHM / SAMPLE;
@@ -2383,10 +2385,143 @@ int scan_setup(const lbl_scan& sc, double dv_in, ScanOracle& S) {
   return LBL_OK;
 }
 
+// SCNINT (src/postsub.f90:824-1035) with INTERP (:2940-3215, I4PT=1): the
+// spectrum, read in 2400-point panels (RDPANL :2768-2870, no conversion),
+// onto DVO = DVINT from V1 to V1 + NUM DVO, NUM = (V2-V1)/DVO + 0.5, by the
+// 4-point cubic whose weights are tabulated at 201 values of the fraction P
+// (C1..C4 :2990-3001); P is carried from point to point by adding
+// DVO/DVI and restarted from the wavenumber at each output panel (2400
+// points) and whenever the input panel runs out.
+int scnint(const double* spec, long n, double v1_in, double dv_in, double DVO,
+           std::vector<double>& out) {
+  const long NUMCOF = 201;
+  const double XNUMCF = double(NUMCOF);
+  double C1[203], C2[203], C3[203], C4[203];
+  for (long IP = 0; IP <= NUMCOF + 1; IP++) {
+    const double P = (double(IP) - 1.0) / (XNUMCF - 1.0);
+    const double PP = P * P;
+    C1[IP] = -P / 2.0 * ((1 - P) * (1 - P));
+    C2[IP] = 1.0 - PP * (3.0 - 2.0 * P) + PP / 2.0 * (1.0 - P);
+    C3[IP] = PP * (3.0 - 2.0 * P) + P / 2.0 * ((1.0 - P) * (1.0 - P));
+    C4[IP] = -PP / 2 * (1.0 - P);
+  }
+  const double V1 = v1_in;
+  long NUM = fint(((v1_in + double(n - 1) * dv_in - V1) / DVO) + 0.5);
+  const double V2 = V1 + double(NUM) * DVO;
+  out.clear();
+  std::vector<double> T(2410 + 8, 0.), R(2401 + 8, 0.);
+  // RDPANL: panel k, its points into T(5..), VMIN = V1P - 4 DVI, NNI = NLIMP + 4
+  long k = 0;
+  double V1I = 0., V2I = 0.;
+  const double DVI = dv_in;
+  long NNI = 0;
+  bool eof = false;
+  auto rdpanl = [&]() {
+    const long a = 2400 * k;
+    if (a >= n) {
+      eof = true;
+      return;
+    }
+    const long m = std::min(2400L, n - a);
+    const double V1P = v1_in + double(a) * dv_in, V2P = v1_in + double(a + m - 1) * dv_in;
+    for (long i = 0; i < m; i++) T[5 + i] = spec[a + i];
+    V1I = V1P - 4.0 * DVI;
+    V2I = V2P;
+    NNI = m + 4;
+    k++;
+  };
+  for (long II = 1; II <= 4; II++) T[II] = 0.0;
+  rdpanl();
+  if (eof) return fail(LBL_E_ARG, "SCNINT: empty spectrum");
+  double V1J = V1;
+  const double DVJ = DVO;
+  const double VRATIO = DVJ / DVI;
+  double VJ = V1J;
+  T[4] = 2.0 * T[5] - T[6];
+  long J1 = 0, J2 = 0;
+  auto otpanl = [&](long NNJ) {
+    for (long J = 1; J <= NNJ; J++) out.push_back(R[J]);
+  };
+  while (V1J < V1I) {  // label 20: output points below the input
+    J1 = 1;
+    J2 = std::min(fint((V1I - V1J) / DVJ) + 1, 2400L);
+    for (long J = J1; J <= J2; J++) R[J] = 0.0;
+    const double V2J = V1J + DVJ * double(J2 - 1);
+    otpanl(J2);
+    V1J = V2J + DVJ;
+    VJ = V1J;
+  }
+  long guard = 0;
+  for (;;) {  // label 40
+    if (++guard > 100000000L) return fail(LBL_E_ARG, "SCNINT: no progress");
+    long I = fint((VJ - V1I) / DVI + 1.00001);
+    const double VI = V1I + DVI * double(I - 1);
+    double P = (VJ - VI) / DVI;
+    J1 = fint((VJ - V1J) / DVJ + 1.001);
+    J2 = std::min(std::min(fint((V2 - V1J) / DVJ + 1.001), fint((V2I - DVI - V1J) / DVJ + 1.)),
+                  2400L);
+    for (long J = J1; J <= J2; J++) {
+      const long IP = fint(P * XNUMCF + 1.00001);
+      R[J] = C1[IP] * T[I - 1] + C2[IP] * T[I] + C3[IP] * T[I + 1] + C4[IP] * T[I + 2];
+      P = P + VRATIO;
+      if (P >= 1.0) {
+        I = fint(double(I) + P);
+        P = P - double(fint(P));
+      }
+    }
+    VJ = V1J + DVJ * double(J2);
+    if (J2 >= 2400 || VJ >= V2) {
+      const double V2J = V1J + DVJ * double(J2 - 1);
+      otpanl(J2);
+      V1J = V2J + DVJ;
+      J2 = 0;
+    }
+    if (VJ >= V2) break;
+    if (eof) {  // label 80: zeros to V2
+      for (;;) {
+        J1 = J2 + 1;
+        J2 = std::min(fint((V2 - V1J) / DVJ + 1.0001), 2400L);
+        for (long J = J1; J <= J2; J++) R[J] = 0.0;
+        VJ = V1J + DVJ * double(J2);
+        if (J2 >= 2400 || VJ >= V2) {
+          const double V2J = V1J + DVJ * double(J2 - 1);
+          otpanl(J2);
+          V1J = V2J + DVJ;
+          J2 = 0;
+        }
+        if (!(VJ < V2)) break;
+      }
+      break;
+    }
+    if (I >= NNI - 2) {
+      for (long II = 1; II <= 4; II++) T[II] = T[II + NNI - 4];
+      rdpanl();
+      if (eof) {
+        T[NNI + 1] = 2.0 * T[NNI] - T[NNI - 1];
+        T[NNI + 2] = 0.0;
+        V2I = V2I + DVI;
+      }
+    }
+  }
+  return LBL_OK;
+}
+
+int orc_scnint_impl(const double* spec, long n, double v1_in, double dv_in, double dvo,
+                    std::vector<double>& out) {
+  return scnint(spec, n, v1_in, dv_in, dvo, out);
+}
+
 int scan_spectrum(const lbl_scan& sc, const double* spec, int64_t n, double v1_in, double dv_in,
                   std::vector<double>& out) {
   ScanOracle S;
   int rc = scan_setup(sc, dv_in, S);
+  if (rc == LBL_E_RANGE && dv_in > S.dvint && S.dvint > 0.) {
+    // SCANFN :322-345: a spectrum coarser than DVINT is first interpolated
+    std::vector<double> fine;
+    rc = scnint(spec, (long)n, v1_in, dv_in, S.dvint, fine);
+    if (rc) return rc;
+    return scan_spectrum(sc, fine.data(), (int64_t)fine.size(), v1_in, S.dvint, out);
+  }
   if (rc) return rc;
   // RDSCAN (:1411-1514): JEMIT=-1 convolves the absorption 1 - S
   std::vector<double> s(spec, spec + n);
@@ -2586,11 +2721,25 @@ int64_t orc_layer_npts(const lbl_run* R, double dv) { return npts_of(*R, dv); }
 
 // SCANFN convolution of a spectrum on v1_in + i*dv_in; *n_out receives the
 // output count, out may be NULL to ask for it only.
+// SCNINT/INTERP alone: spec (n points from v1_in, spacing dv_in) onto dvo.
+int orc_scnint(const double* spec, int64_t n, double v1_in, double dv_in, double dvo, double* out,
+               int64_t cap, int64_t* n_out) {
+  g_err.clear();
+  std::vector<double> res;
+  const int rc = orc_scnint_impl(spec, (long)n, v1_in, dv_in, dvo, res);
+  if (rc) return rc;
+  *n_out = (int64_t)res.size();
+  if ((int64_t)res.size() > cap) return fail(LBL_E_ARG, "output capacity");
+  for (size_t i = 0; i < res.size(); i++) out[i] = res[i];
+  return LBL_OK;
+}
+
 int orc_scan(const lbl_scan* sc, const double* spec, int64_t n, double v1_in, double dv_in,
              double* out, int64_t cap, int64_t* n_out, double* dvout) {
   g_err.clear();
   ScanOracle S;
   int rc = scan_setup(*sc, dv_in, S);
+  if (rc == LBL_E_RANGE && dv_in > S.dvint && S.dvint > 0.) rc = scan_setup(*sc, S.dvint, S);
   if (rc) return rc;
   *n_out = S.nnhi - 32;
   if (dvout) *dvout = S.dvo;

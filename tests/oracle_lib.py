@@ -152,3 +152,17 @@ def scan(sc, spec, v1_in, dv_in):
     out = np.zeros(n.value)
     check(L.orc_scan(*args, out.ctypes.data_as(P), C.c_int64(len(out)), C.byref(n), C.byref(dvo)))
     return out, dvo.value
+
+
+def scnint(spec, v1_in, dv_in, dvo):
+    """SCNINT/INTERP (oracle restatement): spec onto the spacing dvo."""
+    L = lib()
+    spec = np.ascontiguousarray(spec, dtype=np.float64)
+    P = C.POINTER(C.c_double)
+    num = int((len(spec) - 1) * dv_in / dvo + 0.5) + 1
+    out = np.zeros(num + 2400)
+    n = C.c_int64(0)
+    check(L.orc_scnint(spec.ctypes.data_as(P), C.c_int64(len(spec)), C.c_double(v1_in),
+                       C.c_double(dv_in), C.c_double(dvo), out.ctypes.data_as(P),
+                       C.c_int64(len(out)), C.byref(n)))
+    return out[:n.value]

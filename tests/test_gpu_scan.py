@@ -54,3 +54,20 @@ def test_scan_device_buffers_and_forward(gpu_ctx):
     d_out = torch.zeros(n, dtype=torch.float64, device="cuda")
     gpu_ctx.scan_spectrum(sc, d_in, 600.0, dv, out=d_out)
     assert np.array_equal(d_out.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("jfn,hwhm,sampl,dv", [(2, 0.5, 0.0, 0.07), (0, 0.6, -0.2, 0.09),
+                                              (5, 2.0, -0.1, 0.05), (4, 0.8, 0.0, 0.1)])
+def test_scan_coarse_input_bit_exact(gpu_ctx, jfn, hwhm, sampl, dv):
+    """A spectrum coarser than DVINT: SCNINT/INTERP onto DVINT (host replay of
+    the chunk structure, one GPU thread per chunk carrying P from point to
+    point), then the scan, against the oracle's restatement of both."""
+    v1 = 600.0
+    rng = np.random.default_rng(jfn + 10)
+    n = int(400.0 / dv)
+    spec = np.exp(-rng.exponential(1.0, n))
+    sc = abi.make_scan(hwhm=hwhm, v1=640.0, v2=900.0, jfn=jfn, sampl=sampl)
+    ref, _ = O.scan(sc, spec, v1, dv)
+    got = gpu_ctx.scan_spectrum(sc, spec, v1, dv)
+    assert len(got) == len(ref)
+    assert np.array_equal(got, ref), np.flatnonzero(got != ref)[:10]

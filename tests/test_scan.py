@@ -100,7 +100,9 @@ def test_rectangle_is_the_box_mean(hwhm, sampl, jabs):
 
 def test_rejections():
     sc = abi.make_scan(hwhm=0.6, v1=650.0, v2=750.0, jfn=2)
-    assert gpu.load().lbl_scan_npts(C.byref(sc), 0.06, None) == -7   # DV > HWHM/12
+    # DV > HWHM/12: scanned on HWHM/12 after SCNINT, the same output grid
+    assert gpu.load().lbl_scan_npts(C.byref(sc), 0.06, None) == \
+        gpu.load().lbl_scan_npts(C.byref(sc), 0.05, None) > 0
     bad = abi.make_scan(hwhm=0.6, v1=650.0, v2=750.0, jfn=-2)
     assert gpu.load().lbl_scan_npts(C.byref(bad), 0.001, None) == -1
     # rectangle: DVOUT under two input steps (IRATIO < 2)
@@ -145,12 +147,52 @@ def test_field_of_view_boxes_are_box_means(jfn, angle, sampl, jabs):
     np.testing.assert_allclose(out, np.array(ref), rtol=1e-11)
 
 
-def test_field_of_view_needs_fine_input():
+def test_field_of_view_dvint():
     """DVINT for JFN 5/6 is a twelfth of the first box (V1 B^2/24); a coarser
-    input needs SCNINT, which is not built."""
+    input is interpolated onto it (SCNINT) and gives the same output grid."""
     sc = abi.make_scan(hwhm=1.0, v1=640.0, v2=700.0, jfn=5, sampl=-0.1)
     dvint = 640.0 * (1.0 * 3.141592654 / 180.0) ** 2 / 24
-    assert gpu.load().lbl_scan_npts(C.byref(sc), dvint * 0.99, None) > 0
-    assert gpu.load().lbl_scan_npts(C.byref(sc), dvint * 1.01, None) == -7
+    n = gpu.load().lbl_scan_npts(C.byref(sc), dvint * 0.99, None)
+    assert n > 0
+    assert gpu.load().lbl_scan_npts(C.byref(sc), dvint * 1.5, None) == n
     bad = abi.make_scan(hwhm=1.0, v1=640.0, v2=700.0, jfn=-5)
     assert gpu.load().lbl_scan_npts(C.byref(bad), 0.001, None) == -1
+
+
+def test_scnint_reproduces_constants_and_lines():
+    """SCNINT/INTERP (postsub.f90:824-1035, 2940-3215): the 4-point cubic
+    (weights summing to one, tabulated at P = (IP-1)/200) keeps a constant
+    to rounding and a straight line to within its slope times DVI/200 (the
+    tabulation step of P); the output runs from V1 in steps of DVO up to the
+    input's last point."""
+    v1, dv, n = 600.0, 0.05, 6000
+    v = v1 + dv * np.arange(n)
+    dvo = 0.0117
+    const = O.scnint(np.full(n, 0.37), v1, dv, dvo)
+    assert abs(len(const) - ((n - 1) * dv / dvo + 1)) <= 1.5
+    np.testing.assert_allclose(const, 0.37, rtol=1e-15)
+    line = O.scnint(1.0 + 0.01 * (v - 600.0), v1, dv, dvo)
+    vo = v1 + dvo * np.arange(len(line))
+    assert np.max(np.abs(line - (1.0 + 0.01 * (vo - 600.0)))) <= 0.01 * dv / 200 * (1 + 1e-6)
+
+
+def test_coarse_spectrum_scanned_after_interpolation():
+    """A spectrum coarser than DVINT is scanned as the reference does: SCNINT
+    onto DVINT, then the scan of the interpolated spectrum (SCANFN
+    :322-345); for a smooth spectrum the result is within 1e-5 of the scan
+    of the same function sampled exactly on DVINT (the interpolation's own
+    error, 6e-5 at most here, smoothed by the scanning function)."""
+    v1, dv = 600.0, 0.07
+    v = v1 + dv * np.arange(5000)
+    f = lambda x: 1.0 + 0.3 * np.sin(x / 3.0) + 0.1 * np.cos(x / 1.7)  # noqa: E731
+    sc = abi.make_scan(hwhm=0.5, v1=640.0, v2=900.0, jfn=2)
+    dvint = 0.5 / 12
+    got, dvo = O.scan(sc, f(v), v1, dv)
+    fine = O.scnint(f(v), v1, dv, dvint)
+    ref, dvo2 = O.scan(sc, fine, v1, dvint)
+    assert dvo == dvo2 and np.array_equal(got, ref)
+    vf = v1 + dvint * np.arange(len(fine))
+    assert np.max(np.abs(fine - f(vf))) < 6e-5
+    direct, _ = O.scan(sc, f(vf), v1, dvint)
+    assert len(direct) == len(got)
+    np.testing.assert_allclose(got, direct, atol=1e-5)
