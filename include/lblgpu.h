@@ -111,11 +111,15 @@ typedef struct lbl_run {
                        between the H2O part and Rayleigh */
   double xo2cn;     /* O2 continuum scale XO2CN (default 1, 0 = off): the
                        collision-induced fundamental, 1340-1850 cm-1
-                       (src/contnm.f90:491-540, o2_ver_1 :7254-7318) */
+                       (src/contnm.f90:491-540, o2_ver_1 :7254-7318), and
+                       the 1.27 um band, 7536-8500 cm-1 (:543-584, O2INF1
+                       :7384-7440) */
   double xn2cn;     /* N2 continuum scale XN2CN (default 1, 0 = off): the
                        collision-induced rotational band below 350 cm-1
-                       (:745-792, xn2_r :2497-2566) and fundamental,
-                       2001.77-2897.59 cm-1 (:811-858, n2_ver_1 :2668-2754) */
+                       (:745-792, xn2_r :2497-2566), fundamental,
+                       2001.77-2897.59 cm-1 (:811-858, n2_ver_1 :2668-2754),
+                       and first overtone, 4340-4910 cm-1 (:860-906,
+                       n2_overtone1 :2916-2968) */
   double bndrfl;    /* boundary reflectivity BNDRFL(1) (record 1.4; default
                        0, BNDRFL(2:3)=0): with IPATHL=1 a value in (0, 1]
                        makes the run the reflected atmosphere (IBPROP=1,

@@ -1700,6 +1700,8 @@ __device__ const double d_n2r_sf220[LBL_N2R220_N] = {LBL_N2R220_SF_VALUES};
 __device__ const double d_n2f_272[LBL_N2F_N] = {LBL_N2F_X272_VALUES};
 __device__ const double d_n2f_228[LBL_N2F_N] = {LBL_N2F_X228_VALUES};
 __device__ const double d_n2f_ah2o[LBL_N2F_N] = {LBL_N2F_AH2O_VALUES};
+__device__ const double d_n2o1[LBL_N2O1_N] = {LBL_N2O1_X_VALUES};
+__device__ const double d_o2i1[LBL_O2I1_N] = {LBL_O2I1_X_VALUES};
 
 struct ContScale {
   double xco2c, xo2cn, xn2cn;
@@ -1753,6 +1755,18 @@ __device__ void cia_parts(const LayerDev& L, const ContScale& xs, double* absrb)
       return rad(tau_fac * c0, vj);
     }, absrb);
   }
+  if ((L.v2 > 7536.0) && (L.v1 < 8500.) && xs.xo2cn > 0.) {
+    // the O2 1.27 um band (:543-584, O2INF1 :7384-7440)
+    __syncthreads();
+    const double tau_fac = xs.xo2cn * (L.wk[7] / xlosmt) * amagat *
+                           ((1. / 0.446) * x_o2 + (0.3 / 0.446) * x_n2 + 1. * x_h2o);
+    const CoarseGrid g = coarse_grid(LBL_O2I1_V1, LBL_O2I1_DV, LBL_O2I1_N, L);
+    xint_coarse(L, g, LBL_O2I1_V1, LBL_O2I1_V2, [&](int64_t j, double vj) {
+      const int64_t I = g.i1 + (j - 1);
+      const double c0 = (I >= 1 && I <= LBL_O2I1_N) ? d_o2i1[I - 1] / vj : 0.;
+      return rad(tau_fac * c0, vj);
+    }, absrb);
+  }
   if ((L.v2 > -10.0) && (L.v1 < 350.) && xs.xn2cn > 0.) {
     __syncthreads();
     const double tau_fac = xs.xn2cn * (wn2 / xlosmt) * amagat;
@@ -1788,6 +1802,17 @@ __device__ void cia_parts(const LayerDev& L, const ContScale& xs, double* absrb)
         c2 = (9. / 7.) * d_n2f_ah2o[I - 1] * c0;
       }
       return rad(tau_fac * (x_n2 * c0 + x_o2 * c1 + x_h2o * c2), vj);
+    }, absrb);
+  }
+  if ((L.v2 > 4340.0) && (L.v1 < 4910.) && xs.xn2cn > 0.) {
+    // the N2 first overtone (:860-906, n2_overtone1 :2916-2968)
+    __syncthreads();
+    const double tau_fac = xs.xn2cn * (wn2 / xlosmt) * amagat * (x_n2 + 1. * x_o2 + 1. * x_h2o);
+    const CoarseGrid g = coarse_grid(LBL_N2O1_V1, LBL_N2O1_DV, LBL_N2O1_N, L);
+    xint_coarse(L, g, LBL_N2O1_V1, LBL_N2O1_V2, [&](int64_t j, double vj) {
+      const int64_t I = g.i1 + (j - 1);
+      const double c0 = (I >= 1 && I <= LBL_N2O1_N) ? d_n2o1[I - 1] / vj : 0.;
+      return rad(tau_fac * c0, vj);
     }, absrb);
   }
 }

@@ -21,6 +21,10 @@ mechanically:
 * ``BLOCK DATA bn2f`` (src/contnm.f90:2756-2912): the N2 collision-induced
   fundamental at 272 K and 228 K and the H2O broadening efficiency, 228
   points from 1997.78 cm-1.
+* ``BLOCK DATA bn2f1`` (src/contnm.f90:2970-3020): the N2 collision-induced
+  first overtone, 4340-4910 cm-1 every 3 cm-1 (191 values).
+* ``BLOCK DATA bo2inf1`` (src/contnm.f90:7441-7562): the O2 1.27 um
+  collision-induced band (Mate et al.), 7536-8500 cm-1 every 2 cm-1 (483).
 
 Usage:  python gen_cont_tables.py <lblrtm-src-dir> <out.h>
 """
@@ -75,6 +79,8 @@ def extract(src):
     t["N2R220"] = block("BN2T220", {"C": ["CT220"], "SF": ["sf_220"]}, r"V1N2CR\s*,")
     t["N2F"] = block("bn2f", {"X272": ["xn2_272"], "X228": ["xn2_228"], "AH2O": ["a_h2o"]},
                      r"V1n2f\s*,")
+    t["N2O1"] = block("bn2f1", {"X": ["xn2"]}, r"V1n2f\s*,")
+    t["O2I1"] = block("bo2inf1", {"X": ["o%04d" % k for k in range(1, 482, 50)]}, r"V1\s*,")
     return t
 
 
@@ -107,7 +113,7 @@ def write_header(t, out):
     lines.append("#define LBL_CO2_TDEP_VALUES \\")
     lines.append("  " + ", ".join(map(_fmt, t["TDEP"])))
     for key, tag in (("O2F", "O2F"), ("N2R296", "N2R296"), ("N2R220", "N2R220"),
-                     ("N2F", "N2F")):
+                     ("N2F", "N2F"), ("N2O1", "N2O1"), ("O2I1", "O2I1")):
         (a, b, d, n), arrays = t[key]
         lines.append("#define LBL_%s_V1 %s" % (tag, _fmt(a)))
         lines.append("#define LBL_%s_V2 %s" % (tag, _fmt(b)))

@@ -611,6 +611,24 @@ void contnm(Layer& S) {
     }
     xint_onto_absrb(S, g, C, LBL_O2F_V1, LBL_O2F_V2);
   }
+  // O2 1.27 um collision-induced band (:543-584, O2INF1 :7384-7440)
+  if ((S.V2 > 7536.0) && (S.V1 < 8500.) && S.R->xo2cn > 0.) {
+    static const double XO2I1[LBL_O2I1_N] = {LBL_O2I1_X_VALUES};
+    const double a_o2 = 1. / 0.446, a_n2 = 0.3 / 0.446, a_h2o = 1.;
+    const double tau_fac = S.R->xo2cn * (L.wk[6] / xlosmt) * amagat *
+                           (a_o2 * x_vmr_o2 + a_n2 * x_vmr_n2 + a_h2o * x_vmr_h2o);
+    const CoarseGrid g = coarse_grid(LBL_O2I1_V1, LBL_O2I1_DV, LBL_O2I1_N, S);
+    std::vector<double> C(g.NPTC + 3, 0.);
+    for (long J = 1; J <= g.NPTC; J++) {
+      const long I = g.I1 + (J - 1);
+      const double VJ = g.V1C + g.DVC * double(J - 1);
+      double c0 = 0.;
+      if (I >= 1 && I <= LBL_O2I1_N) c0 = XO2I1[I - 1] / VJ;
+      C[J] = tau_fac * c0;
+      if (S.jrad == 1) C[J] = C[J] * RADFN(VJ, XKT);
+    }
+    xint_onto_absrb(S, g, C, LBL_O2I1_V1, LBL_O2I1_V2);
+  }
   // N2 collision-induced rotational band (:745-792, xn2_r :2497-2566)
   if ((S.V2 > -10.0) && (S.V1 < 350.) && S.R->xn2cn > 0.) {
     static const double C296[LBL_N2R296_N] = {LBL_N2R296_C_VALUES};
@@ -664,6 +682,23 @@ void contnm(Layer& S) {
       if (S.jrad == 1) C[J] = C[J] * RADFN(VJ, XKT);
     }
     xint_onto_absrb(S, g, C, LBL_N2F_V1, LBL_N2F_V2);
+  }
+  // N2 collision-induced first overtone (:860-906, n2_overtone1 :2916-2968)
+  if ((S.V2 > 4340.0) && (S.V1 < 4910.) && S.R->xn2cn > 0.) {
+    static const double XN2O[LBL_N2O1_N] = {LBL_N2O1_X_VALUES};
+    const double tau_fac = S.R->xn2cn * (wn2 / xlosmt) * amagat *
+                           (x_vmr_n2 + 1. * x_vmr_o2 + 1. * x_vmr_h2o);
+    const CoarseGrid g = coarse_grid(LBL_N2O1_V1, LBL_N2O1_DV, LBL_N2O1_N, S);
+    std::vector<double> C(g.NPTC + 3, 0.);
+    for (long J = 1; J <= g.NPTC; J++) {
+      const long I = g.I1 + (J - 1);
+      const double VJ = g.V1C + g.DVC * double(J - 1);
+      double c0 = 0.;
+      if (I >= 1 && I <= LBL_N2O1_N) c0 = XN2O[I - 1] / VJ;
+      C[J] = tau_fac * c0;
+      if (S.jrad == 1) C[J] = C[J] * RADFN(VJ, XKT);
+    }
+    xint_onto_absrb(S, g, C, LBL_N2O1_V1, LBL_N2O1_V2);
   }
   // Rayleigh extinction (src/contnm.f90:955-976), no aerosols (IAERSL=0)
   if (S.V2 >= 820. && S.R->xrayl > 0.) {

@@ -284,11 +284,11 @@ def test_tangent_and_reflected_forward_match_oracle_and_layer_steps(gpu_ctx, pre
 
 def test_co2_o2_n2_continua_match_oracle(gpu_ctx):
     """CONTNM's CO2 continuum (contnm.f90:326-378, FRNCO2 :1295-1349) and
-    the O2 and N2 collision-induced bands (:491-540, :745-858) with the H2O
+    the O2 and N2 collision-induced bands (:491-584, :745-906) with the H2O
     table zeroed and Rayleigh off: the 667 cm-1 CO2 band, the 2386-2434
     cm-1 band head (temperature-dependent coefficients), the mt_ckd_2.5
-    factors above 2000 cm-1, the O2 fundamental, the N2 fundamental and the
-    N2 rotational band, in JRAD=0 and JRAD=1 layers, against the oracle;
+    factors above 2000 cm-1, the O2 fundamental, the N2 fundamental and
+    rotational band, in JRAD=0 and JRAD=1 layers, against the oracle;
     and with the scales at 0."""
     lines = configs.gen_lines(500, 80.0, 2600.0, seed=12)
     lh = abi.LinesHandle(lines)

@@ -405,7 +405,8 @@ def test_co2_continuum_follows_its_table():
 def test_o2_and_n2_collision_induced_bands_follow_their_tables():
     """The O2 fundamental (contnm.f90:491-540, o2_ver_1 :7254-7318) at
     1500-1540 cm-1 and the N2 fundamental (:811-858, n2_ver_1 :2668-2754) at
-    2300-2340 cm-1 as the layer's only absorbers: the coefficients formed on
+    2300-2340 cm-1, the N2 first overtone (:860-906) and the O2 1.27 um band
+    (:543-584) as the layer's only absorbers: the coefficients formed on
     their own grids from the two tables (O2: exp(XO2T (1/296 - 1/T)); N2:
     log-interpolation in 1/T between 272 K and 228 K, the O2 and H2O
     broadening efficiencies), XINT onto the 1 cm-1 grid restated here, then
@@ -434,8 +435,17 @@ def test_o2_and_n2_collision_induced_bands_follow_their_tables():
     a_o2 = 1.294 - 0.4545 * t / 296.0
     cn = (x_n2 * c0 + x_o2 * a_o2 * c0 + x_h2o * (9.0 / 7.0) * _cont_macro("N2F_AH2O_VALUES") * c0)
     cn = cn * (x_n2 * wtot / 2.68675e19) * amagat
+    # N2 first overtone: 4340-4910 every 3 cm-1; O2 1.27 um: 7536-8500 every 2
+    vo1 = 4340.0 + 3.0 * np.arange(191)
+    co1 = _cont_macro("N2O1_X_VALUES") / vo1 * (x_n2 * wtot / 2.68675e19) * amagat * (
+        x_n2 + x_o2 + x_h2o)
+    vo2 = 7536.0 + 2.0 * np.arange(483)
+    co2 = _cont_macro("O2I1_X_VALUES") / vo2 * (lay0.wk[6] / 2.68675e19) * amagat * (
+        x_o2 / 0.446 + 0.3 / 0.446 * x_n2 + x_h2o)
     for (v1, v2), (vt, ct, dvt) in (((1500.0, 1540.0), (vo, co, 5.0)),
-                                    ((2300.0, 2340.0), (vn, cn, dvn))):
+                                    ((2300.0, 2340.0), (vn, cn, dvn)),
+                                    ((4500.0, 4540.0), (vo1, co1, 3.0)),
+                                    ((7800.0, 7840.0), (vo2, co2, 2.0))):
         od, v, lay, j = _co2_continuum_only(v1, v2, 0.0, jrad=0)
         assert j == 0
         va = (int(v1) - 3.0) + np.arange(int(v2 + 3.5) - (int(v1) - 3.0) + 1)
