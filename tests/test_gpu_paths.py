@@ -316,3 +316,28 @@ def test_co2_o2_n2_continua_match_oracle(gpu_ctx):
     got, _ = gpu_ctx.layer_od(run, lays[5])
     ref, _ = O.layer_od(run, lays[5], lh, ck)
     assert np.max(floored_err(got, ref)) <= RTOL_FP64
+
+
+def test_near_infrared_continua_match_oracle(gpu_ctx):
+    """The N2 collision-induced first overtone (contnm.f90:860-906) and the
+    O2 1.27 um band (:543-584) with the H2O table zeroed and Rayleigh off,
+    lines present around both ranges, JRAD=0 and JRAD=1 layers, against the
+    oracle."""
+    lines = configs.gen_lines(800, 4200.0, 8000.0, seed=13)
+    lh = abi.LinesHandle(lines)
+    zero = configs.mtckd_table(1)
+    zero["self_absco_ref"] = np.zeros_like(zero["self_absco_ref"])
+    zero["for_absco_ref"] = np.zeros_like(zero["for_absco_ref"])
+    ck = abi.MtckdHandle(zero)
+    gpu_ctx.upload_lines(lh)
+    gpu_ctx.upload_mtckd(ck)
+    for v1, v2 in ((4400.0, 4480.0), (7800.0, 7880.0)):
+        run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1, xrayl=0.0)
+        lays = abi.make_layers(configs.atmosphere(20, ptop=300.0))
+        gpu.dv_rule(run, lays)
+        for l in (0, 19):
+            for jrad in (0, 1):
+                got, jg = gpu_ctx.layer_od(run, lays[l], jrad=jrad)
+                ref, jo = O.layer_od(run, lays[l], lh, ck, jrad=jrad)
+                assert jg == jo
+                assert np.max(floored_err(got, ref)) <= RTOL_FP64, (v1, l, jrad)
