@@ -3134,12 +3134,15 @@ cudaError_t launch_far_scale(const Work& w, const DevLines& ln, int64_t max_far,
 
 cudaError_t launch_shrink(const Work& w, const int64_t* bs, const int64_t* blk_base,
                           int64_t nblk_total, cudaStream_t s) {
-  if (nblk_total > 0) {
-    // one warp per start block, then one warp per segment
+  // one warp per start block, then one warp per layer, then one warp per
+  // segment; the plan runs also when no layer of the batch has far-wing
+  // lines, since it sets every layer's shrunk-line, block and segment
+  // counts (then 0) that the far-wing kernel reads
+  if (nblk_total > 0)
     k_shr_count<<<(unsigned)((nblk_total + 3) / 4), 128, 0, s>>>(w, bs, blk_base, w.nlay);
-    k_shr_plan<<<w.nlay, 32, 0, s>>>(w, blk_base);
+  k_shr_plan<<<w.nlay, 32, 0, s>>>(w, blk_base);
+  if (nblk_total > 0)
     k_shr_write<<<(unsigned)((nblk_total + 3) / 4), 128, 0, s>>>(w, bs, blk_base, w.nlay);
-  }
   return cudaGetLastError();
 }
 

@@ -298,8 +298,10 @@ def test_co2_o2_n2_continua_match_oracle(gpu_ctx):
     ck = abi.MtckdHandle(zero)
     gpu_ctx.upload_lines(lh)
     gpu_ctx.upload_mtckd(ck)
+    # 4300-4400 and 7800-7880: no line within reach (every layer's near and
+    # far line ranges empty), the continuum alone
     for v1, v2 in ((640.0, 700.0), (2370.0, 2450.0), (1990.0, 2030.0), (1480.0, 1560.0),
-                   (2280.0, 2360.0), (100.0, 160.0)):
+                   (2280.0, 2360.0), (100.0, 160.0), (4300.0, 4400.0), (7800.0, 7880.0)):
         run = abi.make_run(v1=v1, v2=v2, icntnm=1, ilblf4=1, xrayl=0.0)
         lays = abi.make_layers(configs.atmosphere(20, ptop=300.0))
         gpu.dv_rule(run, lays)
